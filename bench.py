@@ -1,0 +1,536 @@
+#!/usr/bin/env python
+"""Benchmark: Q(f) cell-evals/s of the collision contraction on B200.
+
+Workload (default): hard spheres (gamma = 1), L = 10, K = 8 radial functions (M = 968 coefficients
+per cell), a batch of B = 4096 cells per GPU, FP64.  Each cell is a seeded Maxwellian plus a
+perturbation N(0,1) exp(-0.6 (k+l)) at amplitude 1e-2 (synthetic data).  One step = Q(f) for the
+whole batch through the library's public device API (zero Q, layout pass, contraction, layout
+pass back).  The batch (f, Q and their tiled copies, ~127 MB) is about the size of L2, so L2 is
+flushed with a 256 MB write before every timed step (outside the timed interval).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank takes its own 4096 cells (weak scaling, no collective on the data path);
+the reported time is the max over ranks.  ``--impl reference`` times the reference's own
+angular_first_collision_kernel_mex, compiled unmodified from its sources (oracle/_ref), once per
+cell on all host cores, on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "collision-factorization_b200"
+for _p in (str(PKG), str(ROOT)):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "Q(f) cell-evals/s at <=1e-10 rel err vs FP64: plain vs chosen form; % roofline"
+WORKLOADS = {
+    # name: (L, K, B, gamma)
+    "hs_l10_k8_b4096": (10, 8, 4096, 1.0),
+    "hs_l8_k8_b2048": (8, 8, 2048, 1.0),
+    "hs_l16_k12_b1024": (16, 12, 1024, 1.0),
+}
+R_FILES = {(10, 8): "R_hs_k7_l10_pad20.npy", (8, 8): "R_hs_k7_l8_pad20.npy"}
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="hs_l10_k8_b4096")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=20260)
+    ap.add_argument("--profile", action="store_true",
+                    help="only build the workload and launch the contraction (steps+1 times); for ncu captures")
+    return ap.parse_args(argv)
+
+
+# --------------------------------------------------------------------------------------------
+# workload
+# --------------------------------------------------------------------------------------------
+def make_operator(L: int, K: int, gamma: float, seed: int):
+    from cf_b200 import geometry, workloads
+
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    rfile = ROOT / "tests" / "golden" / R_FILES.get((L, K), "__none__")
+    if rfile.exists() and gamma == 1.0:
+        R = np.asfortranarray(np.load(rfile))
+        r_source = f"reference quadrature (compute_rtensor_sumfac_mex, pad 20): {rfile.name}"
+    else:
+        from cf_b200.geometry import Geometry  # noqa: F401
+
+        lt = np.floor(np.sqrt(geo.labels - 1.0)).astype(np.int64)
+        trip = np.zeros((geo.n_l, 3), dtype=np.int64)
+        trip[geo.ic_map.astype(np.int64) - 1] = lt
+        R = workloads.synthetic_R(trip, K, seed=seed)
+        r_source = "seeded synthetic R with the conservation rows zeroed"
+    return geo, R, r_source
+
+
+def make_cells(L: int, K: int, B: int, seed: int):
+    from cf_b200 import workloads
+
+    return workloads.maxwellian_cells(K, L, B, seed=seed, amplitude=1e-2, decay=0.6)
+
+
+# --------------------------------------------------------------------------------------------
+# clocks
+# --------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.idx = device_index
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+                power.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+            "power_w_max": max(power) if power else None,
+        }
+
+
+# --------------------------------------------------------------------------------------------
+# distributed plumbing (timing only; the data path has no collective)
+# --------------------------------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# --------------------------------------------------------------------------------------------
+# CPU baseline: the reference's own kernel, compiled unmodified, once per cell on host cores
+# --------------------------------------------------------------------------------------------
+def cpu_reference_rate(geo, R, cells, K, target_seconds: float, nthreads: int = 0):
+    from oracle.reference import Reference
+
+    ref = Reference("fast")
+    nthreads = nthreads or ref.num_threads()
+    NQ = geo.n_q
+    # calibrate with one cell per thread
+    n0 = max(nthreads, 1)
+    f0 = np.asfortranarray(cells[:n0].transpose(2, 1, 0))
+    Q0 = np.zeros_like(f0, order="F")
+    t = time.perf_counter()
+    ref.batch("af", Q0, f0, geo.labels, geo.vals, geo.ic_map, R, NQ, K, nthreads=nthreads)
+    dt = time.perf_counter() - t
+    per_round = max(dt, 1e-6)
+    rounds = max(1, int(target_seconds / per_round))
+    n = min(cells.shape[0], n0 * rounds)
+    f = np.asfortranarray(cells[:n].transpose(2, 1, 0))
+    Q = np.zeros_like(f, order="F")
+    t = time.perf_counter()
+    ref.batch("af", Q, f, geo.labels, geo.vals, geo.ic_map, R, NQ, K, nthreads=nthreads)
+    dt = time.perf_counter() - t
+    return n / dt, n, dt, nthreads
+
+
+# --------------------------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+
+    import cf_b200
+    from cf_b200 import _lib
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L, K, B, gamma = WORKLOADS[args.workload]
+    geo, R, r_source = make_operator(L, K, gamma, args.seed)
+    NQ = geo.n_q
+    M = NQ * K
+    cells = make_cells(L, K, B, seed=args.seed + rank)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, NQ, K, device=local)
+    lib = _lib.load()
+
+    f = torch.from_numpy(cells).to(dev)
+    Q = torch.zeros_like(f)
+    ws = torch.empty(op.workspace_bytes(B) // 8 + 64, dtype=torch.float64, device=dev)
+    n_tiles = (B + 31) // 32
+    fT = torch.zeros(n_tiles * 32 * M, dtype=torch.float64, device=dev)
+    QT = torch.zeros_like(fT)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sh = int(stream.cuda_stream)
+
+    def step(form="af"):
+        Q.zero_()
+        op.q(f, out=Q, form=form, workspace=ws)
+
+    def kernel_only(form="af"):
+        _lib.check(lib.cf_q_tiled(op._h, int(QT.data_ptr()), int(fT.data_ptr()), B, _lib.FORMS[form], sh))
+
+    _lib.check(lib.cf_pack_cells(op._h, int(fT.data_ptr()), int(f.data_ptr()), B, sh))
+
+    # accuracy of the fast form against the reference's exact operation order (bitwise = reference MEX)
+    step("af_exact")
+    Q_exact = Q.clone()
+    step("af")
+    num = (Q - Q_exact).abs().reshape(B, -1).amax(dim=1)
+    den = Q_exact.abs().reshape(B, -1).amax(dim=1).clamp_min(1e-300)
+    err_af = float((num / den).max())
+    inv = Q.reshape(B, -1)[:, [0, 1, 2, 3, NQ]].abs().max().item()
+
+    # FP64 peak of this GPU (DFMA probe, cuBLAS DGEMM)
+    probe = ctypes_double()
+    _lib.check(lib.cf_fp64_fma_peak(local, probe))
+    dfma_tf = probe.value
+    dgemm_tf = dgemm_peak(dev)
+    peak_tf = max(dfma_tf, dgemm_tf)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+        kernel_only()
+    torch.cuda.synchronize(dev)
+
+    def timed(fn, steps):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.fill_(float(i))
+            evs[i][0].record(stream)
+            fn()
+            evs[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        return [a.elapsed_time(b) for a, b in evs]
+
+    clocks = ClockSampler(local)
+    dist_barrier(world)
+    torch.cuda.synchronize(dev)
+    launches0 = _lib.launch_count()
+    clocks.start()
+    t_wall = time.perf_counter()
+    step_ms = timed(step, args.steps)
+    t_wall = time.perf_counter() - t_wall
+    launches = _lib.launch_count() - launches0
+    kern_ms = timed(kernel_only, args.steps)
+    rf_ms = timed(lambda: step("rf"), max(2, args.steps // 4))
+    exact_ms = timed(lambda: step("af_exact"), max(2, args.steps // 4))
+    clk = clocks.stop()
+    torch.cuda.synchronize(dev)
+    dist_barrier(world)
+
+    total_s = dist_max(sum(step_ms) / 1e3, world)
+    value = world * B * args.steps / total_s
+    ms_per_step = 1e3 * total_s / args.steps
+    kern_s = sum(kern_ms) / len(kern_ms) / 1e3
+    flops_launch = op.flops_q * B
+    achieved_tf = flops_launch / kern_s / 1e12
+
+    # end to end through the host C-ABI entry point, pinned host buffers
+    e2e = run_e2e(op, geo, R, cells, K, args, world)
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                rate, n, dt, thr = cpu_reference_rate(geo, R, cells, K, args.cpu_seconds)
+                cpu = {"value": rate, "unit": "cell-evals/s", "cores": thr, "kind": "reference",
+                       "sample": f"{n} cells of this workload through angular_first_collision_kernel_mex compiled "
+                                 f"unmodified (-O3 -mavx2 -mfma), one call per cell under an OpenMP loop over "
+                                 f"cells, {dt:.1f} s"}
+            except Exception as e:  # the baseline is reported, not required
+                cpu = {"value": None, "unit": "cell-evals/s", "cores": None, "kind": "reference",
+                       "sample": f"unavailable: {e}"}
+        rf_rate = B / (sum(rf_ms) / len(rf_ms) / 1e3)
+        exact_rate = B / (sum(exact_ms) / len(exact_ms) / 1e3)
+        out = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "cell-evals/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": max(args.warmup, 3),
+            "ms_per_step": ms_per_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic (seeded Maxwellians + N(0,1) exp(-0.6(k+l)) perturbation, amplitude 1e-2)",
+            "config": {
+                "workload": args.workload, "L": L, "K": K, "M": M, "cells_per_gpu": B, "gamma": gamma,
+                "n_g": op.n_g, "n_l": op.n_l, "n_slices": op.n_slices, "form": "af (plain FP64)",
+                "R": r_source, "l2": "flushed (256 MB write) before every timed step",
+                "parallelism": f"cells sharded, {B} per GPU, no collective",
+            },
+            "forms": {
+                "af": {"cells_per_s": B * args.steps / (sum(step_ms) / 1e3), "max_rel_err_vs_fp64": err_af},
+                "af_exact": {"cells_per_s": exact_rate, "max_rel_err_vs_fp64": 0.0},
+                "rf": {"cells_per_s": rf_rate},
+                "chosen": "af",
+            },
+            "invariants_abs_max": inv,
+            "roofline": {
+                "bound": "fp64", "kernel": f"af_kernel<K={K}>", "achieved": achieved_tf, "peak": peak_tf,
+                "unit": "TFLOP/s", "frac": achieved_tf / peak_tf, "traffic": None,
+                "algorithmic_flop_per_launch": flops_launch, "kernel_ms": kern_s * 1e3,
+                "peak_source": f"measured on this GPU in this run: DFMA probe {dfma_tf:.2f}, cuBLAS DGEMM "
+                               f"{dgemm_tf:.2f} TFLOP/s (max); MEASURED_PEAKS.json has no FP64 entry",
+                "hbm_gbs_algorithmic": 16.0 * M * B / kern_s / 1e9,
+            },
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "wall_s_timed_loop": t_wall,
+        }
+        print(json.dumps(out), flush=True)
+    op.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return out
+
+
+def ctypes_double():
+    import ctypes
+
+    return ctypes.c_double()
+
+
+def dgemm_peak(dev, n: int = 8192, reps: int = 3) -> float:
+    import torch
+
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = 1e30
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 2.0 * n**3 / (best * 1e-3) / 1e12
+
+
+def run_e2e(op, geo, R, cells, K, args, world):
+    """Same metric through the host-pointer C-ABI call (cf_contract_host): H2D f and Q, contract, D2H Q."""
+    import ctypes
+
+    import torch
+
+    from cf_b200 import _lib
+
+    lib = _lib.load()
+    B = cells.shape[0]
+    NQ = geo.n_q
+    f_h = torch.from_numpy(cells).pin_memory()
+    Q_h = torch.zeros_like(f_h).pin_memory()
+    D = ctypes.POINTER(ctypes.c_double)
+    lab, vals, ic = geo.labels, geo.vals, geo.ic_map
+    Rr = np.asfortranarray(R)
+    n_l = Rr.size // K**3
+
+    def call():
+        _lib.check(lib.cf_contract_host(ctypes.cast(Q_h.data_ptr(), D), ctypes.cast(f_h.data_ptr(), D), B,
+                                        lab.ctypes.data_as(D), vals.ctypes.data_as(D), ic.ctypes.data_as(D),
+                                        Rr.ctypes.data_as(D), geo.n_g, n_l, NQ, K, _lib.FORM_AF))
+
+    for _ in range(2):
+        Q_h.zero_()
+        call()
+    times = []
+    steps = max(3, args.steps // 2)
+    for _ in range(steps):
+        Q_h.zero_()
+        t = time.perf_counter()
+        call()
+        times.append(time.perf_counter() - t)
+    tot = dist_max(sum(times), world)
+    nbytes = B * NQ * K * 8
+    return {"value": world * B * steps / tot, "unit": "cell-evals/s", "h2d_bytes_per_step": 2 * nbytes,
+            "d2h_bytes_per_step": nbytes,
+            "path": "cf_contract_host (the MEX-compatible host entry point), pinned host buffers, synchronous"}
+
+
+# --------------------------------------------------------------------------------------------
+# reference arm
+# --------------------------------------------------------------------------------------------
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    from oracle.reference import Reference, reference_available
+
+    L, K, B, gamma = WORKLOADS[args.workload]
+    if not reference_available("fast"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_fast.so not built"}), flush=True)
+        return None
+    geo, R, r_source = make_operator(L, K, gamma, args.seed)
+    ref = Reference("fast")
+    nthreads = ref.num_threads()
+    # size one step so that warmup + steps fit in about two minutes
+    budget = 120.0 / max(args.steps + args.warmup, 1)
+    cells_all = make_cells(L, K, min(B, 8 * nthreads), seed=args.seed)
+    f0 = np.asfortranarray(cells_all[:nthreads].transpose(2, 1, 0))
+    Q0 = np.zeros_like(f0, order="F")
+    t = time.perf_counter()
+    ref.batch("af", Q0, f0, geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K, nthreads=nthreads)
+    per_round = time.perf_counter() - t
+    rounds = max(1, min(8, int(budget / max(per_round, 1e-6))))
+    n = min(cells_all.shape[0], nthreads * rounds)
+    f = np.asfortranarray(cells_all[:n].transpose(2, 1, 0))
+
+    def one():
+        Q = np.zeros_like(f, order="F")
+        ref.batch("af", Q, f, geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K, nthreads=nthreads)
+
+    for _ in range(args.warmup):
+        one()
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t)
+    value = n * args.steps / sum(times)
+    sample = (f"{n} cells per step of the {args.workload} workload through angular_first_collision_kernel_mex "
+              f"compiled unmodified (-O3 -mavx2 -mfma), one call per cell, OpenMP over cells")
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-evals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (same seeded cells as the GPU arm)",
+        "config": {"workload": args.workload, "L": L, "K": K, "M": geo.n_q * K, "gamma": gamma, "R": r_source,
+                   "cells_per_step": n},
+        "cpu_baseline": {"value": value, "unit": "cell-evals/s", "cores": nthreads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "cell-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_profile(args):
+    """Minimal launch sequence for ncu: pack once, then steps+1 launches of the plain contraction."""
+    import torch
+
+    import cf_b200
+    from cf_b200 import _lib
+
+    L, K, B, gamma = WORKLOADS[args.workload]
+    geo, R, _ = make_operator(L, K, gamma, args.seed)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K, device=0)
+    lib = _lib.load()
+    f = torch.from_numpy(make_cells(L, K, B, seed=args.seed)).cuda()
+    M = geo.n_q * K
+    fT = torch.zeros(((B + 31) // 32) * 32 * M, dtype=torch.float64, device="cuda")
+    QT = torch.zeros_like(fT)
+    sh = int(torch.cuda.current_stream().cuda_stream)
+    _lib.check(lib.cf_pack_cells(op._h, int(fT.data_ptr()), int(f.data_ptr()), B, sh))
+    for _ in range(args.steps + 1):
+        _lib.check(lib.cf_q_tiled(op._h, int(QT.data_ptr()), int(fT.data_ptr()), B, _lib.FORM_AF, sh))
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": args.workload, "launches": args.steps + 1, "B": B}))
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.profile:
+        run_profile(args)
+    elif args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

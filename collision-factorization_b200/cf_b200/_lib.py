@@ -1,0 +1,98 @@
+"""ctypes binding of libcf_b200.so (the C ABI declared in include/cf_b200.h).
+
+The library is built in-tree by ``collision-factorization_b200/build.py``.  There is no CPU
+fallback: if the library is missing, or a call is made without a CUDA device, the call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libcf_b200.so"
+
+_D = C.POINTER(C.c_double)
+_I64 = C.c_int64
+_I32 = C.c_int32
+
+CF_OK = 0
+STATUS_NAMES = {
+    0: "CF_OK", 1: "CF_EINVAL", 2: "CF_ESHAPE", 3: "CF_EBADIDX", 4: "CF_ENONFINITE", 5: "CF_ECUDA",
+    6: "CF_ENOMEM", 7: "CF_ENODEVICE", 8: "CF_EUNSUPPORTED", 9: "CF_ETIMEOUT",
+}
+
+FORM_AF, FORM_RF, FORM_AF_EXACT, FORM_RF_EXACT = 0, 1, 2, 3
+FORMS = {"af": FORM_AF, "rf": FORM_RF, "af_exact": FORM_AF_EXACT, "rf_exact": FORM_RF_EXACT}
+
+# Every symbol the header declares; the tests check that the library exports all of them.
+EXPORTS = [
+    "cf_angular_first", "cf_radial_first", "cf_contract_host", "cf_jacobian_apply_host",
+    "cf_plan_create", "cf_plan_destroy", "cf_plan_get_info", "cf_plan_workspace_size",
+    "cf_q_device", "cf_q_device_ws", "cf_jv_device",
+    "cf_pack_cells", "cf_unpack_cells", "cf_q_tiled", "cf_jv_tiled", "cf_fp64_fma_peak",
+    "cf_status_string", "cf_last_error", "cf_launch_count", "cf_version",
+]
+
+
+class CFError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+
+
+class PlanInfo(C.Structure):
+    _fields_ = [
+        ("n_g", C.c_int64), ("n_slices", C.c_int64), ("n_l", C.c_int32), ("n_q", C.c_int32),
+        ("k", C.c_int32), ("device", C.c_int32), ("flops_q", C.c_double), ("flops_jv", C.c_double),
+        ("device_bytes", C.c_int64),
+    ]
+
+
+_lib = None
+
+
+def load(path: str | Path | None = None) -> C.CDLL:
+    """Load libcf_b200.so (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise CFError(7, f"{p} is missing: build it with `python collision-factorization_b200/build.py`")
+    lib = C.CDLL(str(p))
+    op = [_D, _D, _D, _D, _D, _I64, _I32, _I32, _I32]
+    lib.cf_angular_first.argtypes = [_D] + op
+    lib.cf_radial_first.argtypes = [_D] + op
+    lib.cf_contract_host.argtypes = [_D, _D, _I64, _D, _D, _D, _D, _I64, _I32, _I32, _I32, _I32]
+    lib.cf_jacobian_apply_host.argtypes = [_D, _D, _D, _I64, _D, _D, _D, _D, _I64, _I32, _I32, _I32, _I32]
+    lib.cf_plan_create.argtypes = [C.POINTER(C.c_void_p), _D, _D, _D, _D, _I64, _I32, _I32, _I32, _I32]
+    lib.cf_plan_destroy.argtypes = [C.c_void_p]
+    lib.cf_plan_get_info.argtypes = [C.c_void_p, C.POINTER(PlanInfo)]
+    lib.cf_plan_workspace_size.argtypes = [C.c_void_p, _I64, _I32, C.POINTER(C.c_size_t)]
+    lib.cf_q_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]
+    lib.cf_q_device_ws.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p, C.c_size_t,
+                                   C.c_void_p]
+    lib.cf_jv_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]
+    lib.cf_pack_cells.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, C.c_void_p]
+    lib.cf_unpack_cells.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, C.c_void_p]
+    lib.cf_q_tiled.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]
+    lib.cf_jv_tiled.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]
+    lib.cf_fp64_fma_peak.argtypes = [_I32, C.POINTER(C.c_double)]
+    lib.cf_status_string.restype = C.c_char_p
+    lib.cf_status_string.argtypes = [C.c_int]
+    lib.cf_last_error.restype = C.c_char_p
+    lib.cf_launch_count.restype = C.c_int64
+    lib.cf_version.restype = C.c_char_p
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(status: int) -> None:
+    if status != CF_OK:
+        lib = load()
+        raise CFError(status, lib.cf_last_error().decode(errors="replace"))
+
+
+def launch_count() -> int:
+    return int(load().cf_launch_count())

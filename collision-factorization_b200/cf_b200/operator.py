@@ -1,0 +1,127 @@
+"""Device-resident collision operator for batched cells on one GPU.
+
+``CollisionOperator`` uploads the COO lists and R once (``cf_plan_create``) and then applies
+Q(f) or J(f).v to batches of cells held in device memory.  Cell data is a torch CUDA tensor of
+shape ``[B, K, N_Q]`` (C-contiguous), which is the same memory as the reference's column-major
+``[N_Q x K x B]``.  torch only provides device memory and streams here; the contraction is the
+library's own sm_100a kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+
+def _np_operator(labels, vals, ic_map, R, K):
+    labels = np.asfortranarray(np.asarray(labels, dtype=np.float64))
+    vals = np.ascontiguousarray(np.asarray(vals, dtype=np.float64).ravel())
+    ic_map = np.ascontiguousarray(np.asarray(ic_map, dtype=np.float64).ravel())
+    R = np.asfortranarray(np.asarray(R, dtype=np.float64))
+    n_l = R.size // (K * K * K)
+    return labels, vals, ic_map, R, n_l
+
+
+def _dptr(t) -> int:
+    return int(t.data_ptr())
+
+
+def _stream_handle(stream) -> int | None:
+    if stream is None:
+        import torch
+
+        return int(torch.cuda.current_stream().cuda_stream)
+    return int(getattr(stream, "cuda_stream", stream))
+
+
+class CollisionOperator:
+    """Q(f) and J(f).v for batches of cells, on the GPU.
+
+    Parameters mirror what the reference's ``GeneralCollisionTensor`` holds
+    (src/GeneralCollisionTensor.m:9-12): ``labels [N_G x 3]`` (1-based), ``vals [N_G]``,
+    ``ic_map [N_G]`` (1-based), ``R [K x K x K x N_L]``, plus ``N_Q`` and ``K``.
+    """
+
+    def __init__(self, labels, vals, ic_map, R, N_Q: int, K: int, device: int = 0):
+        self.N_Q, self.K = int(N_Q), int(K)
+        lab, v, ic, Rr, n_l = _np_operator(labels, vals, ic_map, R, self.K)
+        self.n_g = lab.shape[0]
+        self.n_l = n_l
+        lib = _lib.load()
+        h = C.c_void_p()
+        D = C.POINTER(C.c_double)
+        _lib.check(lib.cf_plan_create(C.byref(h), lab.ctypes.data_as(D), v.ctypes.data_as(D), ic.ctypes.data_as(D),
+                                      Rr.ctypes.data_as(D), self.n_g, n_l, self.N_Q, self.K, int(device)))
+        self._h = h
+        self.device = int(device)
+        info = _lib.PlanInfo()
+        _lib.check(lib.cf_plan_get_info(h, C.byref(info)))
+        self.n_slices = int(info.n_slices)
+        self.flops_q = float(info.flops_q)
+        self.flops_jv = float(info.flops_jv)
+
+    # ------------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().cf_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        inf = _lib.PlanInfo()
+        _lib.check(_lib.load().cf_plan_get_info(self._h, C.byref(inf)))
+        return {f: getattr(inf, f) for f, _ in inf._fields_}
+
+    def workspace_bytes(self, B: int, jacobian: bool = False) -> int:
+        n = C.c_size_t()
+        _lib.check(_lib.load().cf_plan_workspace_size(self._h, int(B), int(jacobian), C.byref(n)))
+        return int(n.value)
+
+    def _check_cells(self, *ts):
+        import torch
+
+        B = None
+        for t in ts:
+            if not isinstance(t, torch.Tensor) or t.dtype != torch.float64 or not t.is_cuda:
+                raise _lib.CFError(1, "cell arrays must be float64 CUDA tensors")
+            if not t.is_contiguous() or t.dim() != 3 or t.shape[1] != self.K or t.shape[2] != self.N_Q:
+                raise _lib.CFError(2, f"cell arrays must be contiguous [B, K={self.K}, N_Q={self.N_Q}]")
+            if B is None:
+                B = t.shape[0]
+            elif t.shape[0] != B:
+                raise _lib.CFError(2, "batch sizes differ")
+        return B
+
+    def q(self, f, out=None, form: str = "af", stream=None, workspace=None):
+        """out += Q(f) for every cell; returns out (zeros if not given)."""
+        import torch
+
+        if out is None:
+            out = torch.zeros_like(f)
+        B = self._check_cells(f, out)
+        lib = _lib.load()
+        if workspace is None:
+            st = lib.cf_q_device(self._h, _dptr(out), _dptr(f), B, _lib.FORMS[form], _stream_handle(stream))
+        else:
+            st = lib.cf_q_device_ws(self._h, _dptr(out), _dptr(f), B, _lib.FORMS[form], _dptr(workspace),
+                                    workspace.numel() * workspace.element_size(), _stream_handle(stream))
+        _lib.check(st)
+        return out
+
+    def jv(self, f, v, out=None, exact: bool = False, stream=None):
+        """out += J(f).v = Q(v,f) + Q(f,v) for every cell; returns out."""
+        import torch
+
+        if out is None:
+            out = torch.zeros_like(f)
+        B = self._check_cells(f, v, out)
+        _lib.check(_lib.load().cf_jv_device(self._h, _dptr(out), _dptr(f), _dptr(v), B, int(bool(exact)),
+                                            _stream_handle(stream)))
+        return out

@@ -1,0 +1,42 @@
+// common.cuh -- device-side operator layout shared by the contraction kernels.
+//
+// HBM layout of one uploaded operator (built on the host by plan.cu):
+//
+//   slices     runs of equal (t, q1) of the caller's COO list, grouped by q1 (each q1's runs
+//              keep the caller's order, so Q[q1] receives its contributions in the same
+//              order as in the reference's angular-first loop).
+//   q1_begin   [N_Q+1]  slice range of each q1
+//   slice_t    [S]      l-triplet of each slice (0-based)
+//   slice_e    [S+1]    entry range of each slice
+//   e_q23      [N_G]    packed 0-based (q2 | q3 << 16) of each entry, in slice order
+//   e_g        [N_G]    Gaunt value of each entry, in slice order
+//   R          [K^3 N_L] reduced radial tensor, R[k1 + K k2 + K^2 k3 + K^3 t]
+//   item_q1    [n_items] the q1 values that have slices, heaviest first
+//
+// Cell data is kept in a tiled "cell-fastest" layout: 32 cells per tile, one per lane,
+//   X_tiled[tile][q][k][lane]   (row r = q*K + k, 32 doubles = 256 B per row)
+// so a warp that handles 32 cells reads one contiguous 256-byte line per (q, k) and every
+// COO entry is uniform across the warp.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define CF_TILE 32
+
+struct DevOp {
+    const int* q1_begin;
+    const int* slice_t;
+    const int* slice_e;
+    const uint32_t* e_q23;
+    const double* e_g;
+    const double* R;
+    const int* item_q1;
+    int n_items;  // number of q1 with at least one slice
+    int n_q;
+    int k;
+    int n_l;
+};
+
+// Lanes per cell used by the angular-first kernels: the K x K Phi accumulator of one cell
+// is split over P lanes (by k3 column) once it no longer fits one lane's registers.
+__host__ __device__ constexpr int af_lanes_per_cell(int K) { return K <= 8 ? 1 : (K <= 12 ? 2 : 4); }

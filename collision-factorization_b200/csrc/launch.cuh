@@ -1,0 +1,42 @@
+// launch.cuh -- per-K launch entry points.  Each K is instantiated in its own translation unit
+// (inst_k<K>.cu) so the kernels compile in parallel; plan.cu calls them through cf_launch().
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace cf {
+
+enum Op { OP_AF = 0, OP_RF = 1, OP_JV = 2 };
+
+struct LaunchArgs {
+    DevOp op;
+    const double* fT;
+    const double* vT;
+    double* QT;
+    int64_t n_tiles;
+    cudaStream_t stream;
+    int what;    // Op
+    bool exact;  // reference operation order, no FMA
+};
+
+// Status codes mirror cf_status: 0 ok, 5 CUDA error, 8 unsupported, 2 shape.
+struct LaunchResult {
+    int status;
+    int launches;
+    cudaError_t cuda;
+};
+
+#define CF_DECLARE_K(KK) LaunchResult launch_k##KK(const LaunchArgs& a);
+CF_DECLARE_K(1) CF_DECLARE_K(2) CF_DECLARE_K(3) CF_DECLARE_K(4) CF_DECLARE_K(5) CF_DECLARE_K(6)
+CF_DECLARE_K(7) CF_DECLARE_K(8) CF_DECLARE_K(9) CF_DECLARE_K(10) CF_DECLARE_K(11) CF_DECLARE_K(12)
+CF_DECLARE_K(13) CF_DECLARE_K(14) CF_DECLARE_K(15) CF_DECLARE_K(16)
+#undef CF_DECLARE_K
+
+// Lanes per cell (P) of the fast kernels: the K x K Phi accumulator is split over P lanes by
+// k3 column once it no longer fits one lane's registers.
+constexpr int af_P(int K) { return K <= 8 ? 1 : (K <= 12 ? 2 : 4); }
+constexpr int jv_P(int K) { return K <= 6 ? 1 : (K <= 8 ? 2 : 4); }
+
+}  // namespace cf

@@ -1,0 +1,676 @@
+// plan.cu -- host side of libcf_b200: validation, COO re-bucketing, device plans, C ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <list>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/cf_b200.h"
+#include "common.cuh"
+#include "launch.cuh"
+#include "layout.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+std::atomic<int64_t> g_launches{0};
+
+int fail(int status, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return status;
+}
+
+#define CF_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(e_ == cudaErrorMemoryAllocation ? CF_ENOMEM : CF_ECUDA, "%s: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e_), __FILE__, __LINE__);                    \
+    } while (0)
+
+#define CF_TRY(expr)              \
+    do {                          \
+        int s_ = (expr);          \
+        if (s_ != CF_OK) return s_; \
+    } while (0)
+
+constexpr int kMaxK = 16;
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// The plan: one operator resident on one device
+// ------------------------------------------------------------------------------------------
+struct cf_plan {
+    int device = 0;
+    int n_q = 0, k = 0, n_l = 0;
+    int64_t n_g = 0, n_slices = 0;
+    int n_items = 0;
+    double flops_q = 0, flops_jv = 0;
+    int64_t dev_bytes = 0;
+    // device operator
+    int* d_q1_begin = nullptr;
+    int* d_slice_t = nullptr;
+    int* d_slice_e = nullptr;
+    uint32_t* d_e_q23 = nullptr;
+    double* d_e_g = nullptr;
+    double* d_R = nullptr;
+    int* d_item_q1 = nullptr;
+    // scratch owned by the plan (tiled copies; device copies of host inputs)
+    void* d_ws = nullptr;
+    size_t ws_bytes = 0;
+    double* d_io = nullptr;
+    size_t io_bytes = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+
+    DevOp op() const {
+        DevOp o;
+        o.q1_begin = d_q1_begin;
+        o.slice_t = d_slice_t;
+        o.slice_e = d_slice_e;
+        o.e_q23 = d_e_q23;
+        o.e_g = d_e_g;
+        o.R = d_R;
+        o.item_q1 = d_item_q1;
+        o.n_items = n_items;
+        o.n_q = n_q;
+        o.k = k;
+        o.n_l = n_l;
+        return o;
+    }
+};
+
+namespace {
+
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = true;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) ok = (cudaSetDevice(dev) == cudaSuccess);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int check_device_available() {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return fail(CF_ENODEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
+    return CF_OK;
+}
+
+bool is_index(double x, int hi) {
+    if (!(x >= 1.0 && x <= (double)hi)) return false;
+    return std::floor(x) == x;
+}
+
+int validate(const double* labels, const double* vals, const double* ic_map, const double* R,
+             int64_t n_g, int32_t n_l, int32_t n_q, int32_t k) {
+    if (n_g < 0) return fail(CF_ESHAPE, "N_G = %lld is negative", (long long)n_g);
+    if (n_q < 1 || n_q > 65535) return fail(CF_ESHAPE, "N_Q = %d outside [1, 65535]", n_q);
+    if (k < 1 || k > kMaxK) return fail(CF_EUNSUPPORTED, "K = %d outside [1, %d]", k, kMaxK);
+    if (n_g > INT32_MAX - 64) return fail(CF_ESHAPE, "N_G = %lld too large", (long long)n_g);
+    if (n_g == 0) return CF_OK;
+    if (!labels || !vals || !ic_map || !R) return fail(CF_EINVAL, "null operator array");
+    if (n_l < 1) return fail(CF_ESHAPE, "N_L = %d must be >= 1", n_l);
+    for (int64_t z = 0; z < n_g; ++z) {
+        for (int c = 0; c < 3; ++c) {
+            const double q = labels[z + c * n_g];
+            if (!is_index(q, n_q))
+                return fail(CF_EBADIDX, "labels(%lld,%d) = %g is not an integer in [1, %d]", (long long)z + 1,
+                            c + 1, q, n_q);
+        }
+        if (!is_index(ic_map[z], n_l))
+            return fail(CF_EBADIDX, "ic_map(%lld) = %g is not an integer in [1, %d]", (long long)z + 1, ic_map[z],
+                        n_l);
+        if (!std::isfinite(vals[z])) return fail(CF_ENONFINITE, "vals(%lld) is not finite", (long long)z + 1);
+    }
+    const int64_t nr = (int64_t)k * k * k * n_l;
+    for (int64_t i = 0; i < nr; ++i)
+        if (!std::isfinite(R[i])) return fail(CF_ENONFINITE, "R(%lld) is not finite", (long long)i + 1);
+    return CF_OK;
+}
+
+template <typename T>
+int upload(T** dst, const std::vector<T>& src, int64_t& bytes) {
+    const size_t nb = std::max<size_t>(src.size(), 1) * sizeof(T);
+    CF_CUDA(cudaMalloc((void**)dst, nb));
+    if (!src.empty()) CF_CUDA(cudaMemcpy(*dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice));
+    bytes += (int64_t)nb;
+    return CF_OK;
+}
+
+void free_plan_memory(cf_plan* p) {
+    cudaFree(p->d_q1_begin);
+    cudaFree(p->d_slice_t);
+    cudaFree(p->d_slice_e);
+    cudaFree(p->d_e_q23);
+    cudaFree(p->d_e_g);
+    cudaFree(p->d_R);
+    cudaFree(p->d_item_q1);
+    cudaFree(p->d_ws);
+    cudaFree(p->d_io);
+    if (p->stream) cudaStreamDestroy(p->stream);
+}
+
+// Build the q1-grouped run structure (host) and upload it.
+int build_plan(cf_plan* p, const double* labels, const double* vals, const double* ic_map, const double* R) {
+    const int64_t NG = p->n_g;
+    const int NQ = p->n_q, K = p->k;
+    struct Run {
+        int q1, t;
+        int64_t z0, z1;
+    };
+    std::vector<Run> runs;
+    for (int64_t z = 0; z < NG;) {
+        const int t = (int)ic_map[z] - 1, q1 = (int)labels[z] - 1;
+        int64_t e = z + 1;
+        while (e < NG && (int)ic_map[e] - 1 == t && (int)labels[e] - 1 == q1) ++e;
+        runs.push_back({q1, t, z, e});
+        z = e;
+    }
+    // group runs by q1, keeping the caller's order inside each q1
+    std::vector<int> count(NQ + 1, 0);
+    for (const Run& r : runs) count[r.q1 + 1]++;
+    std::vector<int> q1_begin(NQ + 1, 0);
+    for (int q = 0; q < NQ; ++q) q1_begin[q + 1] = q1_begin[q] + count[q + 1];
+    std::vector<int> fill(q1_begin.begin(), q1_begin.end() - 1);
+    std::vector<int> order(runs.size());
+    for (size_t i = 0; i < runs.size(); ++i) order[fill[runs[i].q1]++] = (int)i;
+
+    const int64_t S = (int64_t)runs.size();
+    std::vector<int> slice_t(S), slice_e(S + 1);
+    std::vector<uint32_t> e_q23(NG);
+    std::vector<double> e_g(NG);
+    std::vector<double> cost(NQ, 0.0);
+    int64_t pos = 0;
+    for (int64_t s = 0; s < S; ++s) {
+        const Run& r = runs[order[s]];
+        slice_t[s] = r.t;
+        slice_e[s] = (int)pos;
+        for (int64_t z = r.z0; z < r.z1; ++z, ++pos) {
+            const uint32_t q2 = (uint32_t)labels[z + NG] - 1, q3 = (uint32_t)labels[z + 2 * NG] - 1;
+            e_q23[pos] = q2 | (q3 << 16);
+            e_g[pos] = vals[z];
+        }
+        cost[r.q1] += (double)(r.z1 - r.z0) * K * K + (double)K * K * K;
+    }
+    slice_e[S] = (int)pos;
+
+    std::vector<int> items;
+    for (int q = 0; q < NQ; ++q)
+        if (q1_begin[q + 1] > q1_begin[q]) items.push_back(q);
+    std::stable_sort(items.begin(), items.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+
+    p->n_slices = S;
+    p->n_items = (int)items.size();
+    p->flops_q = (double)NG * (2.0 * K * K + K) + (double)S * 2.0 * K * K * K;
+    p->flops_jv = (double)NG * (4.0 * K * K + 2.0 * K) + (double)S * 2.0 * K * K * K;
+
+    std::vector<double> Rv((size_t)K * K * K * p->n_l);
+    if (NG > 0) std::memcpy(Rv.data(), R, Rv.size() * sizeof(double));
+    int64_t bytes = 0;
+    CF_TRY(upload(&p->d_q1_begin, q1_begin, bytes));
+    CF_TRY(upload(&p->d_slice_t, slice_t, bytes));
+    CF_TRY(upload(&p->d_slice_e, slice_e, bytes));
+    CF_TRY(upload(&p->d_e_q23, e_q23, bytes));
+    CF_TRY(upload(&p->d_e_g, e_g, bytes));
+    CF_TRY(upload(&p->d_R, Rv, bytes));
+    CF_TRY(upload(&p->d_item_q1, items, bytes));
+    p->dev_bytes = bytes;
+    return CF_OK;
+}
+
+int64_t n_tiles_for(int64_t B) { return (B + CF_TILE - 1) / CF_TILE; }
+
+size_t tiled_bytes(const cf_plan* p, int64_t B) {
+    return (size_t)n_tiles_for(B) * CF_TILE * (size_t)p->n_q * p->k * sizeof(double);
+}
+
+// ------------------------------------------------------------------------------------------
+// Kernel dispatch over K (each K lives in its own translation unit, inst.cu)
+// ------------------------------------------------------------------------------------------
+int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const double* vT, double* QT, int64_t nt,
+             cudaStream_t st) {
+    cf::LaunchArgs a{p->op(), fT, vT, QT, nt, st, what, exact};
+    cf::LaunchResult r{8, 0, cudaSuccess};
+    switch (p->k) {
+#define CF_K(KK) \
+    case KK: r = cf::launch_k##KK(a); break;
+        CF_K(1) CF_K(2) CF_K(3) CF_K(4) CF_K(5) CF_K(6) CF_K(7) CF_K(8)
+        CF_K(9) CF_K(10) CF_K(11) CF_K(12) CF_K(13) CF_K(14) CF_K(15) CF_K(16)
+#undef CF_K
+        default: return fail(CF_EUNSUPPORTED, "K = %d not built", p->k);
+    }
+    g_launches += r.launches;
+    if (r.status == CF_ECUDA) return fail(CF_ECUDA, "kernel launch: %s", cudaGetErrorString(r.cuda));
+    if (r.status == CF_EUNSUPPORTED)
+        return fail(CF_EUNSUPPORTED, "form not built for K = %d (the exact angular-first order needs K <= 8)", p->k);
+    if (r.status != CF_OK) return fail(r.status, "launch failed for K = %d", p->k);
+    return CF_OK;
+}
+
+int launch_pack(const cf_plan* p, const double* src, double* dst, int64_t B, cudaStream_t st) {
+    const int M = p->n_q * p->k;
+    const int64_t nt = n_tiles_for(B);
+    if (nt == 0) return CF_OK;
+    if (nt > 65535) return fail(CF_ESHAPE, "B = %lld exceeds %d cells per call", (long long)B, 65535 * CF_TILE);
+    dim3 grid((M + 31) / 32, (unsigned)nt), block(32, 8);
+    cf::pack_tiles_kernel<<<grid, block, 0, st>>>(src, dst, B, p->n_q, p->k);
+    g_launches++;
+    CF_CUDA(cudaGetLastError());
+    return CF_OK;
+}
+
+int launch_unpack(const cf_plan* p, const double* src, double* dst, int64_t B, cudaStream_t st) {
+    const int M = p->n_q * p->k;
+    const int64_t nt = n_tiles_for(B);
+    if (nt == 0) return CF_OK;
+    dim3 grid((M + 31) / 32, (unsigned)nt), block(32, 8);
+    cf::unpack_tiles_kernel<<<grid, block, 0, st>>>(src, dst, B, p->n_q, p->k);
+    g_launches++;
+    CF_CUDA(cudaGetLastError());
+    return CF_OK;
+}
+
+// Q_dev (cell-major) += op(f_dev[, v_dev]) using the tiled workspace ws (>= 2 or 3 tiled buffers).
+int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_dev, const double* v_dev,
+               int64_t B, void* ws, size_t ws_bytes, cudaStream_t st) {
+    if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
+    if (B == 0 || p->n_g == 0) return CF_OK;
+    if (!q_dev || !f_dev || (what == 2 && !v_dev)) return fail(CF_EINVAL, "null device buffer");
+    const size_t tb = tiled_bytes(p, B);
+    const size_t need = tb * (what == 2 ? 3 : 2);
+    if (ws_bytes < need) return fail(CF_EINVAL, "workspace of %zu bytes is smaller than %zu", ws_bytes, need);
+    double* fT = (double*)ws;
+    double* QT = (double*)((char*)ws + tb);
+    double* vT = what == 2 ? (double*)((char*)ws + 2 * tb) : nullptr;
+    const int64_t nt = n_tiles_for(B);
+    CF_TRY(launch_pack(p, f_dev, fT, B, st));
+    if (what == 2) CF_TRY(launch_pack(p, v_dev, vT, B, st));
+    CF_TRY(launch_pack(p, q_dev, QT, B, st));
+    CF_TRY(dispatch(p, what, exact, fT, vT, QT, nt, st));
+    CF_TRY(launch_unpack(p, QT, q_dev, B, st));
+    return CF_OK;
+}
+
+int ensure_ws(cf_plan* p, size_t need) {
+    if (p->ws_bytes >= need) return CF_OK;
+    if (p->d_ws) {
+        CF_CUDA(cudaStreamSynchronize(p->stream));
+        cudaFree(p->d_ws);
+        p->d_ws = nullptr;
+        p->ws_bytes = 0;
+    }
+    CF_CUDA(cudaMalloc(&p->d_ws, need));
+    p->ws_bytes = need;
+    return CF_OK;
+}
+
+int ensure_io(cf_plan* p, size_t need) {
+    if (p->io_bytes >= need) return CF_OK;
+    if (p->d_io) {
+        CF_CUDA(cudaStreamSynchronize(p->stream));
+        cudaFree(p->d_io);
+        p->d_io = nullptr;
+        p->io_bytes = 0;
+    }
+    CF_CUDA(cudaMalloc((void**)&p->d_io, need));
+    p->io_bytes = need;
+    return CF_OK;
+}
+
+int plan_create(cf_plan** out, const double* labels, const double* vals, const double* ic_map, const double* R,
+                int64_t n_g, int32_t n_l, int32_t n_q, int32_t k, int32_t device) {
+    if (!out) return fail(CF_EINVAL, "null plan pointer");
+    *out = nullptr;
+    CF_TRY(check_device_available());
+    CF_TRY(validate(labels, vals, ic_map, R, n_g, n_l, n_q, k));
+    if (device < 0) CF_CUDA(cudaGetDevice(&device));
+    DeviceGuard guard(device);
+    if (!guard.ok) return fail(CF_ENODEVICE, "cannot select device %d", device);
+    cf_plan* p = new cf_plan();
+    p->device = device;
+    p->n_q = n_q;
+    p->k = k;
+    p->n_l = n_g > 0 ? n_l : std::max(n_l, 0);
+    p->n_g = n_g;
+    int s = build_plan(p, labels, vals, ic_map, R);
+    if (s == CF_OK) {
+        cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) s = fail(CF_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    if (s != CF_OK) {
+        free_plan_memory(p);
+        delete p;
+        return s;
+    }
+    *out = p;
+    return CF_OK;
+}
+
+// ------------------------------------------------------------------------------------------
+// Content-keyed cache of plans for the MEX-style host entry points
+// ------------------------------------------------------------------------------------------
+uint64_t hash_words(const double* a, int64_t n, uint64_t h) {
+    const uint64_t* w = reinterpret_cast<const uint64_t*>(a);
+    for (int64_t i = 0; i < n; ++i) {
+        h ^= w[i];
+        h *= 0x100000001b3ULL;
+        h ^= h >> 29;
+    }
+    return h;
+}
+
+struct CacheEntry {
+    uint64_t key;
+    int64_t n_g;
+    int n_l, n_q, k, device;
+    cf_plan* plan;
+};
+
+std::mutex g_cache_mu;
+std::list<CacheEntry> g_cache;  // most recent first
+constexpr size_t kCacheMax = 8;
+
+int cached_plan(cf_plan** out, const double* labels, const double* vals, const double* ic_map, const double* R,
+                int64_t n_g, int32_t n_l, int32_t n_q, int32_t k) {
+    CF_TRY(check_device_available());
+    int device = 0;
+    CF_CUDA(cudaGetDevice(&device));
+    if (n_g < 0 || k < 1 || k > kMaxK || n_l < 0) return validate(labels, vals, ic_map, R, n_g, n_l, n_q, k);
+    uint64_t h = 0xcbf29ce484222325ULL;
+    if (n_g > 0 && labels && vals && ic_map && R) {
+        h = hash_words(labels, 3 * n_g, h);
+        h = hash_words(vals, n_g, h);
+        h = hash_words(ic_map, n_g, h);
+        h = hash_words(R, (int64_t)k * k * k * n_l, h);
+    }
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (auto it = g_cache.begin(); it != g_cache.end(); ++it) {
+        if (it->key == h && it->n_g == n_g && it->n_l == n_l && it->n_q == n_q && it->k == k && it->device == device) {
+            g_cache.splice(g_cache.begin(), g_cache, it);
+            *out = g_cache.front().plan;
+            return CF_OK;
+        }
+    }
+    cf_plan* p = nullptr;
+    CF_TRY(plan_create(&p, labels, vals, ic_map, R, n_g, n_l, n_q, k, device));
+    g_cache.push_front({h, n_g, n_l, n_q, k, device, p});
+    while (g_cache.size() > kCacheMax) {
+        cf_plan* old = g_cache.back().plan;
+        g_cache.pop_back();
+        {
+            std::lock_guard<std::mutex> pl(old->mu);
+            DeviceGuard g(old->device);
+            cudaStreamSynchronize(old->stream);
+            free_plan_memory(old);
+        }
+        delete old;
+    }
+    *out = p;
+    return CF_OK;
+}
+
+// Host-pointer contraction: upload, run, download.  what: 0 AF, 1 RF, 2 JV.
+int run_host(int what, bool exact, double* Q, const double* f, const double* v, int64_t B, const double* labels,
+             const double* vals, const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
+             int32_t k) {
+    if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
+    if (!Q || !f || (what == 2 && !v)) return fail(CF_EINVAL, "null host buffer");
+    cf_plan* p = nullptr;
+    CF_TRY(cached_plan(&p, labels, vals, ic_map, R, n_g, n_l, n_q, k));
+    if (B == 0 || n_g == 0) return CF_OK;
+    std::lock_guard<std::mutex> lk(p->mu);
+    DeviceGuard guard(p->device);
+    const size_t cell_bytes = (size_t)B * n_q * k * sizeof(double);
+    const int nbuf = what == 2 ? 3 : 2;
+    CF_TRY(ensure_io(p, cell_bytes * nbuf));
+    const size_t tb = tiled_bytes(p, B);
+    CF_TRY(ensure_ws(p, tb * nbuf));
+    double* dQ = p->d_io;
+    double* df = (double*)((char*)p->d_io + cell_bytes);
+    double* dv = what == 2 ? (double*)((char*)p->d_io + 2 * cell_bytes) : nullptr;
+    CF_CUDA(cudaMemcpyAsync(dQ, Q, cell_bytes, cudaMemcpyHostToDevice, p->stream));
+    CF_CUDA(cudaMemcpyAsync(df, f, cell_bytes, cudaMemcpyHostToDevice, p->stream));
+    if (dv) CF_CUDA(cudaMemcpyAsync(dv, v, cell_bytes, cudaMemcpyHostToDevice, p->stream));
+    CF_TRY(run_device(p, what, exact, dQ, df, dv, B, p->d_ws, p->ws_bytes, p->stream));
+    CF_CUDA(cudaMemcpyAsync(Q, dQ, cell_bytes, cudaMemcpyDeviceToHost, p->stream));
+    CF_CUDA(cudaStreamSynchronize(p->stream));
+    return CF_OK;
+}
+
+int form_what(int form, bool& exact) {
+    switch (form) {
+        case CF_FORM_AF: exact = false; return 0;
+        case CF_FORM_RF: exact = false; return 1;
+        case CF_FORM_AF_EXACT: exact = true; return 0;
+        case CF_FORM_RF_EXACT: exact = true; return 1;
+        default: return -1;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------
+extern "C" {
+
+int cf_angular_first(double* Q, const double* f, const double* labels, const double* vals, const double* ic_map,
+                     const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k) {
+    g_last_error.clear();
+    return run_host(0, false, Q, f, nullptr, 1, labels, vals, ic_map, R, n_g, n_l, n_q, k);
+}
+
+int cf_radial_first(double* Q, const double* f, const double* labels, const double* vals, const double* ic_map,
+                    const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k) {
+    g_last_error.clear();
+    return run_host(1, false, Q, f, nullptr, 1, labels, vals, ic_map, R, n_g, n_l, n_q, k);
+}
+
+int cf_contract_host(double* Q, const double* f, int64_t b, const double* labels, const double* vals,
+                     const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k,
+                     int32_t form) {
+    g_last_error.clear();
+    bool exact = false;
+    const int what = form_what(form, exact);
+    if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
+    return run_host(what, exact, Q, f, nullptr, b, labels, vals, ic_map, R, n_g, n_l, n_q, k);
+}
+
+int cf_jacobian_apply_host(double* out, const double* f, const double* v, int64_t b, const double* labels,
+                           const double* vals, const double* ic_map, const double* R, int64_t n_g, int32_t n_l,
+                           int32_t n_q, int32_t k, int32_t exact) {
+    g_last_error.clear();
+    return run_host(2, exact != 0, out, f, v, b, labels, vals, ic_map, R, n_g, n_l, n_q, k);
+}
+
+int cf_plan_create(cf_plan** plan, const double* labels, const double* vals, const double* ic_map, const double* R,
+                   int64_t n_g, int32_t n_l, int32_t n_q, int32_t k, int32_t device) {
+    g_last_error.clear();
+    return plan_create(plan, labels, vals, ic_map, R, n_g, n_l, n_q, k, device);
+}
+
+int cf_plan_destroy(cf_plan* plan) {
+    if (!plan) return CF_OK;
+    {
+        std::lock_guard<std::mutex> lk(plan->mu);
+        DeviceGuard g(plan->device);
+        if (plan->stream) cudaStreamSynchronize(plan->stream);
+        free_plan_memory(plan);
+    }
+    delete plan;
+    return CF_OK;
+}
+
+int cf_plan_get_info(const cf_plan* plan, cf_plan_info* info) {
+    if (!plan || !info) return fail(CF_EINVAL, "null argument");
+    info->n_g = plan->n_g;
+    info->n_slices = plan->n_slices;
+    info->n_l = plan->n_l;
+    info->n_q = plan->n_q;
+    info->k = plan->k;
+    info->device = plan->device;
+    info->flops_q = plan->flops_q;
+    info->flops_jv = plan->flops_jv;
+    info->device_bytes = plan->dev_bytes + (int64_t)plan->ws_bytes + (int64_t)plan->io_bytes;
+    return CF_OK;
+}
+
+int cf_plan_workspace_size(const cf_plan* plan, int64_t b, int32_t jacobian, size_t* bytes) {
+    if (!plan || !bytes) return fail(CF_EINVAL, "null argument");
+    if (b < 0) return fail(CF_ESHAPE, "B is negative");
+    *bytes = tiled_bytes(plan, b) * (jacobian ? 3 : 2);
+    return CF_OK;
+}
+
+int cf_q_device_ws(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form, void* workspace,
+                   size_t workspace_bytes, void* stream) {
+    g_last_error.clear();
+    if (!plan) return fail(CF_EINVAL, "null plan");
+    bool exact = false;
+    const int what = form_what(form, exact);
+    if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
+    DeviceGuard guard(plan->device);
+    return run_device(plan, what, exact, q_dev, f_dev, nullptr, b, workspace, workspace_bytes, (cudaStream_t)stream);
+}
+
+int cf_q_device(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form, void* stream) {
+    g_last_error.clear();
+    if (!plan) return fail(CF_EINVAL, "null plan");
+    bool exact = false;
+    const int what = form_what(form, exact);
+    if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard guard(plan->device);
+    CF_TRY(ensure_ws(plan, tiled_bytes(plan, b) * 2));
+    return run_device(plan, what, exact, q_dev, f_dev, nullptr, b, plan->d_ws, plan->ws_bytes, (cudaStream_t)stream);
+}
+
+int cf_jv_device(cf_plan* plan, double* out_dev, const double* f_dev, const double* v_dev, int64_t b, int32_t exact,
+                 void* stream) {
+    g_last_error.clear();
+    if (!plan) return fail(CF_EINVAL, "null plan");
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard guard(plan->device);
+    CF_TRY(ensure_ws(plan, tiled_bytes(plan, b) * 3));
+    return run_device(plan, 2, exact != 0, out_dev, f_dev, v_dev, b, plan->d_ws, plan->ws_bytes,
+                      (cudaStream_t)stream);
+}
+
+int cf_pack_cells(const cf_plan* plan, double* dst_tiled, const double* src_cells, int64_t b, void* stream) {
+    g_last_error.clear();
+    if (!plan) return fail(CF_EINVAL, "null plan");
+    if (b < 0) return fail(CF_ESHAPE, "B is negative");
+    if (b > 0 && (!dst_tiled || !src_cells)) return fail(CF_EINVAL, "null device buffer");
+    DeviceGuard guard(plan->device);
+    return launch_pack(plan, src_cells, dst_tiled, b, (cudaStream_t)stream);
+}
+
+int cf_unpack_cells(const cf_plan* plan, double* dst_cells, const double* src_tiled, int64_t b, void* stream) {
+    g_last_error.clear();
+    if (!plan) return fail(CF_EINVAL, "null plan");
+    if (b < 0) return fail(CF_ESHAPE, "B is negative");
+    if (b > 0 && (!dst_cells || !src_tiled)) return fail(CF_EINVAL, "null device buffer");
+    DeviceGuard guard(plan->device);
+    return launch_unpack(plan, src_tiled, dst_cells, b, (cudaStream_t)stream);
+}
+
+int cf_q_tiled(cf_plan* plan, double* q_tiled, const double* f_tiled, int64_t b, int32_t form, void* stream) {
+    g_last_error.clear();
+    if (!plan) return fail(CF_EINVAL, "null plan");
+    bool exact = false;
+    const int what = form_what(form, exact);
+    if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
+    if (b < 0) return fail(CF_ESHAPE, "B is negative");
+    if (b == 0 || plan->n_g == 0) return CF_OK;
+    if (!q_tiled || !f_tiled) return fail(CF_EINVAL, "null device buffer");
+    DeviceGuard guard(plan->device);
+    return dispatch(plan, what, exact, f_tiled, nullptr, q_tiled, n_tiles_for(b), (cudaStream_t)stream);
+}
+
+int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const double* v_tiled, int64_t b,
+                int32_t exact, void* stream) {
+    g_last_error.clear();
+    if (!plan) return fail(CF_EINVAL, "null plan");
+    if (b < 0) return fail(CF_ESHAPE, "B is negative");
+    if (b == 0 || plan->n_g == 0) return CF_OK;
+    if (!out_tiled || !f_tiled || !v_tiled) return fail(CF_EINVAL, "null device buffer");
+    DeviceGuard guard(plan->device);
+    return dispatch(plan, cf::OP_JV, exact != 0, f_tiled, v_tiled, out_tiled, n_tiles_for(b), (cudaStream_t)stream);
+}
+
+int cf_fp64_fma_peak(int32_t device, double* tflops) {
+    g_last_error.clear();
+    if (!tflops) return fail(CF_EINVAL, "null output");
+    CF_TRY(check_device_available());
+    DeviceGuard guard(device);
+    if (!guard.ok) return fail(CF_ENODEVICE, "cannot select device %d", device);
+    int sms = 0;
+    CF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    double* sink = nullptr;
+    CF_CUDA(cudaMalloc(&sink, sizeof(double) * blocks * threads));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 6; ++rep) {
+        cudaEventRecord(e0);
+        cf::fp64_fma_probe_kernel<<<blocks, threads>>>(sink, iters, 1.0 + 1e-12 * rep);
+        g_launches++;
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) best = std::min(best, ms);
+    }
+    const cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (e != cudaSuccess) return fail(CF_ECUDA, "probe: %s", cudaGetErrorString(e));
+    const double flops = 2.0 * cf::kProbeChains * (double)iters * blocks * threads;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return CF_OK;
+}
+
+const char* cf_status_string(int status) {
+    switch (status) {
+        case CF_OK: return "ok";
+        case CF_EINVAL: return "invalid argument";
+        case CF_ESHAPE: return "inconsistent sizes";
+        case CF_EBADIDX: return "index out of range";
+        case CF_ENONFINITE: return "non-finite operator value";
+        case CF_ECUDA: return "CUDA error";
+        case CF_ENOMEM: return "out of memory";
+        case CF_ENODEVICE: return "no usable CUDA device";
+        case CF_EUNSUPPORTED: return "unsupported form or size";
+        case CF_ETIMEOUT: return "device wait timed out";
+        default: return "unknown status";
+    }
+}
+
+const char* cf_last_error(void) { return g_last_error.c_str(); }
+int64_t cf_launch_count(void) { return g_launches.load(); }
+const char* cf_version(void) { return "cf_b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

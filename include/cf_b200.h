@@ -1,0 +1,161 @@
+/*
+ * cf_b200.h -- C ABI of the B200 collision-contraction library (libcf_b200.so).
+ *
+ * The operator is the Wigner-Eckart-factorised spectral Boltzmann contraction
+ *
+ *   Q(f)[q1,k1] = sum_{z : q1(z) = q1} G_z sum_{k2,k3} R_{t(z)}[k1,k2,k3] f[q2(z),k2] f[q3(z),k3]
+ *
+ * routed through the COO Gaunt lists of the reference (labels, vals, ic_map) and
+ * its reduced radial tensor R.  All arrays use the reference's MEX conventions:
+ *
+ *   f, Q    column-major double [N_Q x K] per cell; batched [N_Q x K x B]
+ *           (element (q,k) of cell b at q + k*N_Q + b*N_Q*K)
+ *   labels  column-major double [N_G x 3], 1-based (q1, q2, q3)
+ *   vals    double [N_G]       real Gaunt values
+ *   ic_map  double [N_G]       1-based l-triplet index t
+ *   R       column-major double [K x K x K x N_L]: R[k1 + K*k2 + K^2*k3 + K^3*t]
+ *
+ * Every contraction ACCUMULATES into its output (out += ...), exactly as the
+ * reference kernels write into their first argument.  The entries may be in any
+ * order; Q is summed run by run of equal (ic_map, q1), as the reference does.
+ *
+ * Every function returns a cf_status.  Nothing here falls back to the CPU: without
+ * a usable CUDA device the calls return CF_ENODEVICE.
+ */
+#ifndef CF_B200_H
+#define CF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cf_status {
+    CF_OK = 0,
+    CF_EINVAL = 1,        /* a null pointer or an out-of-range scalar argument      */
+    CF_ESHAPE = 2,        /* sizes that do not fit together (N_G, K, N_L, B ...)     */
+    CF_EBADIDX = 3,       /* a label outside [1, N_Q] or an ic_map outside [1, N_L] */
+    CF_ENONFINITE = 4,    /* NaN or Inf in vals or R                                  */
+    CF_ECUDA = 5,         /* a CUDA runtime error (message in cf_last_error())       */
+    CF_ENOMEM = 6,        /* device or host allocation failed                         */
+    CF_ENODEVICE = 7,     /* no CUDA device, or the library was not built for it      */
+    CF_EUNSUPPORTED = 8,  /* a form / K combination this build does not provide       */
+    CF_ETIMEOUT = 9       /* a bounded device-side wait gave up                       */
+} cf_status;
+
+/* Contraction forms.  All compute in FP64 unless stated otherwise. */
+typedef enum cf_form {
+    CF_FORM_AF = 0,        /* angular first: Phi = sum G f2 (x) f3 per (t,q1) run, then R_t . Phi      */
+    CF_FORM_RF = 1,        /* radial first: Psi_z = R_t . (f2 (x) f3) per entry, then Q += G Psi       */
+    CF_FORM_AF_EXACT = 2,  /* angular first in the reference's exact operation order (no FMA):
+                              reproduces angular_first_collision_kernel_mex bit for bit (K <= 8)        */
+    CF_FORM_RF_EXACT = 3   /* radial first in the reference's exact operation order (no FMA)           */
+} cf_form;
+
+typedef struct cf_plan cf_plan;
+
+typedef struct cf_plan_info {
+    int64_t n_g;          /* COO entries                                        */
+    int64_t n_slices;     /* runs of equal (ic_map, q1): the S of the K^3 step  */
+    int32_t n_l;          /* l-triplets (R channels)                            */
+    int32_t n_q;          /* angular modes (L+1)^2                              */
+    int32_t k;            /* radial functions per l                             */
+    int32_t device;       /* CUDA device the plan lives on                      */
+    double  flops_q;      /* algorithmic FLOP per cell for Q:  N_G(2K^2+K) + S 2K^3 */
+    double  flops_jv;     /* algorithmic FLOP per cell for J.v: N_G(4K^2+2K) + S 2K^3 */
+    int64_t device_bytes; /* device memory held by the plan (COO, R, buffers)   */
+} cf_plan_info;
+
+/* ------------------------------------------------------------------------------------------
+ * MEX-compatible entry points: host pointers, one call = one contraction, synchronous.
+ * The COO/R upload and re-bucketing is cached per content, so repeated calls with the same
+ * operator pay only for f and Q.
+ * ------------------------------------------------------------------------------------------ */
+
+/* Replaces angular_first_collision_kernel_mex (src/mex/angular_first_collision_kernel_mex.cpp:6-75):
+ * Q(N_Q x K) += AF contraction of f(N_Q x K).  N_L is what the MEX implies by numel(R)/K^3. */
+int cf_angular_first(double* Q, const double* f, const double* labels, const double* vals,
+                     const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
+                     int32_t k);
+
+/* Replaces radial_first_collision_kernel_mex (src/mex/radial_first_collision_kernel_mex.cpp:5-76). */
+int cf_radial_first(double* Q, const double* f, const double* labels, const double* vals,
+                    const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
+                    int32_t k);
+
+/* Batched host-pointer form of both (Q, f: [N_Q x K x B]); form is a cf_form.  The host-side
+ * counterpart of calling the reference MEX once per cell (benchmark_collision_contraction_scaling.m:96-108). */
+int cf_contract_host(double* Q, const double* f, int64_t b, const double* labels, const double* vals,
+                     const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
+                     int32_t k, int32_t form);
+
+/* J(f).v = Q(v,f) + Q(f,v), accumulated into out; no counterpart in the reference (the reference
+ * linearises only densely at equilibrium, tutorial_collisions_spectral_properties.m:43).  Host pointers,
+ * [N_Q x K x B]. */
+int cf_jacobian_apply_host(double* out, const double* f, const double* v, int64_t b,
+                           const double* labels, const double* vals, const double* ic_map,
+                           const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k,
+                           int32_t exact);
+
+/* ------------------------------------------------------------------------------------------
+ * Plan API: a device-resident operator and batched contractions on device buffers.
+ * Device arrays are in the MEX-native layout [N_Q x K x B].  stream is a cudaStream_t
+ * (NULL = the legacy default stream).  Calls are asynchronous on that stream.
+ * ------------------------------------------------------------------------------------------ */
+
+/* Validate and upload an operator (host arrays, same conventions as above) to device `device`
+ * (-1 = the current device).  The same inputs the reference's GeneralCollisionTensor holds
+ * (src/GeneralCollisionTensor.m:9-12). */
+int cf_plan_create(cf_plan** plan, const double* labels, const double* vals, const double* ic_map,
+                   const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k,
+                   int32_t device);
+int cf_plan_destroy(cf_plan* plan);
+int cf_plan_get_info(const cf_plan* plan, cf_plan_info* info);
+
+/* Bytes of device scratch the batched calls need for B cells (the tiled copies of the inputs
+ * and of the output).  Passing a workspace of at least this size to the *_ws calls makes
+ * them allocation-free; the other calls allocate it inside the plan on first use. */
+int cf_plan_workspace_size(const cf_plan* plan, int64_t b, int32_t jacobian, size_t* bytes);
+
+/* Q_dev += Q(f_dev) for B cells. */
+int cf_q_device(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form,
+                void* stream);
+int cf_q_device_ws(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* out_dev += J(f_dev).v_dev for B cells. */
+int cf_jv_device(cf_plan* plan, double* out_dev, const double* f_dev, const double* v_dev,
+                 int64_t b, int32_t exact, void* stream);
+
+/* Tiled cell layout: [ceil(B/32)][N_Q][K][32] (32 cells per tile, cell index fastest).  Callers
+ * that keep their cells resident (time steppers, Krylov solvers) use it directly and skip the
+ * two layout passes.  cf_pack_cells / cf_unpack_cells convert from / to [N_Q x K x B]; pack fills
+ * the padding cells of the last tile with zeros, unpack overwrites the B cells of dst. */
+int cf_pack_cells(const cf_plan* plan, double* dst_tiled, const double* src_cells, int64_t b, void* stream);
+int cf_unpack_cells(const cf_plan* plan, double* dst_cells, const double* src_tiled, int64_t b, void* stream);
+int cf_q_tiled(cf_plan* plan, double* q_tiled, const double* f_tiled, int64_t b, int32_t form, void* stream);
+int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const double* v_tiled, int64_t b,
+                int32_t exact, void* stream);
+
+/* Measured FP64 FMA throughput of `device` in TFLOP/s (independent DFMA chains on every SM, timed
+ * with CUDA events): the peak the FP64 forms are compared against. */
+int cf_fp64_fma_peak(int32_t device, double* tflops);
+
+/* ------------------------------------------------------------------------------------------
+ * Status and introspection
+ * ------------------------------------------------------------------------------------------ */
+const char* cf_status_string(int status);
+/* Detail of the last failing call on this host thread ("" if none). */
+const char* cf_last_error(void);
+/* Number of CUDA kernel launches this library has issued in this process. */
+int64_t cf_launch_count(void);
+/* Library version string. */
+const char* cf_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CF_B200_H */

@@ -1,0 +1,239 @@
+"""GPU parity: the sm_100a kernels, called through the C ABI, against the oracle and the reference.
+
+Tolerances: FP64 forms <= 1e-12 normwise per cell; the EXACT forms are
+bit-for-bit equal to the reference's own compiled kernels.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_op, normwise_err, per_cell_err
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-12
+OPS = ["wcu_k2_l2_g0", "cfg1_k3_l4_g0", "hs_k4_l4_g1", "bkw_k5_l1_g0"]
+
+
+def _cells_cm(cells):
+    """[B, K, NQ] C-order -> column-major [NQ, K, B] (same bytes)."""
+    return np.asfortranarray(cells.transpose(2, 1, 0))
+
+
+@pytest.mark.parametrize("name", OPS)
+def test_mex_angular_first_matches_reference(name, cuda_available):
+    import cf_b200
+
+    d = load_op(name)
+    NQ, K = d["NQ"], d["K"]
+    Q = np.zeros((NQ, K), order="F")
+    cf_b200.angular_first_collision_kernel_mex(Q, d["f"], d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"],
+                                               d["R"], NQ, K)
+    assert normwise_err(Q, d["Q_af"]) <= TOL_FP64
+    Q2 = np.zeros((NQ, K), order="F")
+    cf_b200.radial_first_collision_kernel_mex(Q2, d["f"], d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"],
+                                              d["R"], NQ, K)
+    assert normwise_err(Q2, d["Q_rf"]) <= TOL_FP64
+
+
+@pytest.mark.parametrize("name", OPS)
+def test_exact_forms_bitwise_equal_reference(name, cuda_available):
+    """The EXACT forms reproduce the compiled reference kernels bit for bit (golden outputs)."""
+    import cf_b200
+
+    d = load_op(name)
+    NQ, K = d["NQ"], d["K"]
+    for form, key in (("af_exact", "Q_af"), ("rf_exact", "Q_rf")):
+        Q = np.zeros((NQ, K), order="F")
+        cf_b200.contract_batched(Q, d["f"], d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"], d["R"], NQ, K,
+                                 form=form)
+        assert np.array_equal(Q, d[key]), f"{form}: max |diff| = {np.abs(Q - d[key]).max()}"
+
+
+def test_exact_form_bitwise_on_batch_and_nonzero_q(cuda_available, oracle_lib, reference_lib):
+    """Bitwise parity with the reference's MEX called cell by cell, Q_out nonzero on entry (+= semantics)."""
+    import cf_b200
+    from cf_b200 import workloads
+
+    d = load_op("hs_k4_l4_g1")
+    NQ, K = d["NQ"], d["K"]
+    cells = workloads.maxwellian_cells(K, d["L"], 45, seed=21)
+    f = _cells_cm(cells)
+    rng = np.random.default_rng(5)
+    Q0 = np.asfortranarray(rng.standard_normal(f.shape))
+    args = (d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"], d["R"], NQ, K)
+    Qr = Q0.copy(order="F")
+    reference_lib.batch("af", Qr, f, *args, nthreads=4)
+    Qg = Q0.copy(order="F")
+    cf_b200.contract_batched(Qg, f, *args, form="af_exact")
+    assert np.array_equal(Qg, Qr)
+    Qr = Q0.copy(order="F")
+    reference_lib.batch("rf", Qr, f, *args, nthreads=4)
+    Qg = Q0.copy(order="F")
+    cf_b200.contract_batched(Qg, f, *args, form="rf_exact")
+    assert np.array_equal(Qg, Qr)
+
+
+@pytest.mark.parametrize("L,K", [(4, 4), (6, 6), (8, 6), (10, 8), (6, 12), (4, 16), (3, 1)])
+def test_fast_forms_vs_oracle(L, K, cuda_available, oracle_lib):
+    """AF and RF fast forms vs the oracle on batches whose size is not a multiple of the tile."""
+    import cf_b200
+    from cf_b200 import geometry, workloads
+    from oracle import rtensor
+
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=L * 31 + K)
+    B = 37 if L <= 8 else 13
+    f = _cells_cm(workloads.maxwellian_cells(K, L, B, seed=L + K))
+    NQ = geo.n_q
+    args = (geo.labels, geo.vals, geo.ic_map, R, NQ, K)
+    Qo = np.zeros_like(f, order="F")
+    oracle_lib.af_batch(Qo, f, *args)
+    for form in ("af", "rf"):
+        Qg = np.zeros_like(f, order="F")
+        cf_b200.contract_batched(Qg, f, *args, form=form)
+        err = per_cell_err(Qg.transpose(2, 1, 0), Qo.transpose(2, 1, 0))
+        assert err <= TOL_FP64, f"{form} L={L} K={K}: {err:.3e}"
+
+
+@pytest.mark.parametrize("L,K", [(4, 4), (8, 8), (6, 12), (4, 16)])
+def test_jacobian_apply_vs_oracle(L, K, cuda_available, oracle_lib):
+    import cf_b200
+    from cf_b200 import geometry, workloads
+    from oracle import rtensor
+
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=5)
+    B = 35
+    f = _cells_cm(workloads.maxwellian_cells(K, L, B, seed=9))
+    rng = np.random.default_rng(2)
+    v = np.asfortranarray(rng.standard_normal(f.shape))
+    NQ = geo.n_q
+    args = (geo.labels, geo.vals, geo.ic_map, R, NQ, K)
+    ref = np.zeros_like(f, order="F")
+    oracle_lib.jv_batch(ref, f, v, *args)
+    out = np.zeros_like(f, order="F")
+    cf_b200.collision_jacobian_apply_mex(out, f, v, *args)
+    assert per_cell_err(out.transpose(2, 1, 0), ref.transpose(2, 1, 0)) <= TOL_FP64
+    if K <= 8:
+        out2 = np.zeros_like(f, order="F")
+        cf_b200.collision_jacobian_apply_mex(out2, f, v, *args, exact=True)
+        assert np.array_equal(out2, ref), "exact J.v must equal the oracle's operation order bit for bit"
+
+
+def test_unsorted_and_interleaved_coo(cuda_available, oracle_lib):
+    """Any entry order is accepted: runs of equal (t, q1) are summed in the caller's order."""
+    import cf_b200
+
+    d = load_op("cfg1_k3_l4_g0")
+    NQ, K = d["NQ"], d["K"]
+    rng = np.random.default_rng(1)
+    perm = rng.permutation(d["labels"].shape[0])
+    lab = np.asfortranarray(d["labels"][perm])
+    vals, ic = d["vals"][perm], d["ic_map"][perm]
+    Qo = np.zeros((NQ, K), order="F")
+    oracle_lib.af(Qo, d["f"], lab, vals, ic, d["R"], NQ, K)
+    Qg = np.zeros((NQ, K), order="F")
+    cf_b200.contract_batched(Qg, d["f"], lab, vals, ic, d["R"], NQ, K, form="af_exact")
+    assert np.array_equal(Qg, Qo)
+    Qg = np.zeros((NQ, K), order="F")
+    cf_b200.angular_first_collision_kernel_mex(Qg, d["f"], lab, vals, ic, d["R"], NQ, K)
+    assert normwise_err(Qg, Qo) <= TOL_FP64
+
+
+def test_edge_cases(cuda_available):
+    import cf_b200
+    from cf_b200 import CFError
+
+    d = load_op("wcu_k2_l2_g0")
+    NQ, K = d["NQ"], d["K"]
+    args = (d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"], d["R"], NQ, K)
+    # empty COO: Q unchanged
+    Q = np.full((NQ, K), 3.0, order="F")
+    cf_b200.angular_first_collision_kernel_mex(Q, d["f"], np.zeros((0, 3), order="F"), np.zeros(0), np.zeros(0),
+                                               d["R"], NQ, K)
+    assert np.all(Q == 3.0)
+    # empty batch
+    Qb = np.zeros((NQ, K, 0), order="F")
+    cf_b200.contract_batched(Qb, np.zeros((NQ, K, 0), order="F"), *args)
+    # one entry
+    lab1 = np.asfortranarray(d["labels_sorted"][5:6])
+    Q1 = np.zeros((NQ, K), order="F")
+    cf_b200.contract_batched(Q1, d["f"], lab1, d["vals_sorted"][5:6], d["ic_map_sorted"][5:6], d["R"], NQ, K,
+                             form="af_exact")
+    from oracle.reference import Oracle
+
+    Qo = np.zeros((NQ, K), order="F")
+    Oracle().af(Qo, d["f"], lab1, d["vals_sorted"][5:6], d["ic_map_sorted"][5:6], d["R"], NQ, K)
+    assert np.array_equal(Q1, Qo)
+    # bad indices are rejected with a status, not read out of bounds
+    bad = d["labels_sorted"].copy(order="F")
+    bad[3, 1] = NQ + 1
+    with pytest.raises(CFError) as e:
+        cf_b200.angular_first_collision_kernel_mex(np.zeros((NQ, K), order="F"), d["f"], bad, d["vals_sorted"],
+                                                   d["ic_map_sorted"], d["R"], NQ, K)
+    assert e.value.status == 3
+    badic = d["ic_map_sorted"].copy()
+    badic[0] = 999
+    with pytest.raises(CFError) as e:
+        cf_b200.angular_first_collision_kernel_mex(np.zeros((NQ, K), order="F"), d["f"], d["labels_sorted"],
+                                                   d["vals_sorted"], badic, d["R"], NQ, K)
+    assert e.value.status == 3
+    badv = d["vals_sorted"].copy()
+    badv[2] = np.nan
+    with pytest.raises(CFError) as e:
+        cf_b200.angular_first_collision_kernel_mex(np.zeros((NQ, K), order="F"), d["f"], d["labels_sorted"], badv,
+                                                   d["ic_map_sorted"], d["R"], NQ, K)
+    assert e.value.status == 4
+    with pytest.raises(CFError):
+        cf_b200.angular_first_collision_kernel_mex(np.zeros((NQ, K)), d["f"], *args)  # C-order Q_out rejected
+
+
+def test_conservation_rows_give_exact_zero_invariants(cuda_available):
+    """R rows of mass, momentum and energy are zero, so those Q entries are exactly 0 (src/GeneralCollisionTensor.m:184-191)."""
+    import torch
+
+    import cf_b200
+    from cf_b200 import workloads
+
+    d = load_op("hs_k4_l4_g1")
+    NQ, K = d["NQ"], d["K"]
+    op = cf_b200.CollisionOperator(d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"], d["R"], NQ, K)
+    f = torch.from_numpy(workloads.maxwellian_cells(K, d["L"], 100, seed=4, amplitude=0.1)).cuda()
+    Q = op.q(f)
+    inv = Q.reshape(100, -1)[:, [0, 1, 2, 3, NQ]].cpu().numpy()
+    assert np.all(inv == 0.0)
+
+
+def test_operator_device_api_and_determinism(cuda_available, oracle_lib):
+    import torch
+
+    import cf_b200
+    from cf_b200 import workloads
+
+    d = load_op("hs_k4_l4_g1")
+    NQ, K = d["NQ"], d["K"]
+    op = cf_b200.CollisionOperator(d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"], d["R"], NQ, K)
+    assert op.n_slices > 0 and op.flops_q > 0
+    cells = workloads.maxwellian_cells(K, d["L"], 70, seed=8)
+    f = torch.from_numpy(cells).cuda()
+    Q1 = op.q(f)
+    Q2 = op.q(f)
+    assert torch.equal(Q1, Q2), "the atomic-free path must be deterministic"
+    ws = torch.empty(op.workspace_bytes(70) // 8 + 1, dtype=torch.float64, device="cuda")
+    Q3 = op.q(f, workspace=ws)
+    assert torch.equal(Q1, Q3)
+    Qo = np.zeros((NQ, K, 70), order="F")
+    oracle_lib.af_batch(Qo, _cells_cm(cells), d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"], d["R"], NQ, K)
+    assert per_cell_err(Q1.cpu().numpy(), Qo.transpose(2, 1, 0)) <= TOL_FP64
+    # += semantics on device
+    Q4 = Q1.clone()
+    op.q(f, out=Q4)
+    assert torch.allclose(Q4, 2 * Q1, rtol=1e-14, atol=0)
+    # quadratic homogeneity Q(a f) = a^2 Q(f) and J(f) f = 2 Q(f)
+    Qa = op.q(3.0 * f)
+    assert torch.allclose(Qa, 9.0 * Q1, rtol=1e-12, atol=1e-15)
+    J = op.jv(f, f)
+    assert torch.allclose(J, 2.0 * Q1, rtol=1e-12, atol=1e-15)
+    op.close()
