@@ -29,7 +29,7 @@ EXPORTS = [
     "cf_angular_first", "cf_radial_first", "cf_contract_host", "cf_jacobian_apply_host",
     "cf_plan_create", "cf_plan_destroy", "cf_plan_get_info", "cf_plan_workspace_size",
     "cf_q_device", "cf_q_device_ws", "cf_jv_device",
-    "cf_pack_cells", "cf_unpack_cells", "cf_q_tiled", "cf_jv_tiled", "cf_fp64_fma_peak",
+    "cf_pack_cells", "cf_unpack_cells", "cf_q_tiled", "cf_jv_tiled", "cf_plan_set_kernel_path", "cf_fp64_fma_peak",
     "cf_status_string", "cf_last_error", "cf_launch_count", "cf_version",
 ]
 
@@ -78,6 +78,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_q_tiled.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]
     lib.cf_jv_tiled.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]
     lib.cf_fp64_fma_peak.argtypes = [_I32, C.POINTER(C.c_double)]
+    lib.cf_plan_set_kernel_path.argtypes = [C.c_void_p, _I32]
     lib.cf_status_string.restype = C.c_char_p
     lib.cf_status_string.argtypes = [C.c_int]
     lib.cf_last_error.restype = C.c_char_p

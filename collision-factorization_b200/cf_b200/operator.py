@@ -79,6 +79,11 @@ class CollisionOperator:
         _lib.check(_lib.load().cf_plan_get_info(self._h, C.byref(inf)))
         return {f: getattr(inf, f) for f, _ in inf._fields_}
 
+    def set_kernel_path(self, path: str) -> None:
+        """'auto' (default), 'gather', 'tile' or 'pair': the kernel family of the AF and J.v forms."""
+        code = {"auto": 0, "gather": 1, "tile": 2, "pair": 3}[path]
+        _lib.check(_lib.load().cf_plan_set_kernel_path(self._h, code))
+
     def workspace_bytes(self, B: int, jacobian: bool = False) -> int:
         n = C.c_size_t()
         _lib.check(_lib.load().cf_plan_workspace_size(self._h, int(B), int(jacobian), C.byref(n)))

@@ -2,41 +2,148 @@
 #pragma once
 #include "kernels.cuh"
 #include "launch.cuh"
+#include "tile_kernels.cuh"
+#include "pair_kernels.cuh"
 
 namespace cf {
 
 template <int K, int P, bool EXACT, bool JV>
 static LaunchResult launch_af(const LaunchArgs& a) {
     const int64_t warps = (int64_t)a.op.n_items * a.n_tiles * P;
-    if (warps == 0) return {0, 0, cudaSuccess};
+    if (warps == 0) return {0, 0, cudaSuccess, PATH_GATHER};
     const int64_t blocks = (warps + 3) / 4;
-    if (blocks > INT32_MAX) return {2, 0, cudaSuccess};
+    if (blocks > INT32_MAX) return {2, 0, cudaSuccess, PATH_GATHER};
     af_kernel<K, P, EXACT, JV><<<(unsigned)blocks, 128, 0, a.stream>>>(a.op, a.fT, a.vT, a.QT, (int)a.n_tiles);
     const cudaError_t e = cudaGetLastError();
-    return {e == cudaSuccess ? 0 : 5, 1, e};
+    return {e == cudaSuccess ? 0 : 5, 1, e, PATH_GATHER};
+}
+
+// Tile-resident persistent kernel.  Returns status -1 when it does not fit (shared memory or
+// occupancy), in which case the caller uses the gather kernel.
+template <int K, int W, bool EXACT, bool JV>
+static LaunchResult launch_tile(const LaunchArgs& a) {
+    const int M = a.op.n_q * K;
+    const size_t smem = tile_smem_bytes<K>(M, W, JV);
+    if (smem + 256 > a.max_smem || a.counter == nullptr) return {-1, 0, cudaSuccess, PATH_TILE};
+    auto kern = af_tile_kernel<K, W, EXACT, JV>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return {5, 0, e, PATH_TILE};
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem);
+    if (e != cudaSuccess) return {5, 0, e, PATH_TILE};
+    if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_TILE};
+    const int64_t ctas = (int64_t)per_sm * a.n_sms;
+    const int64_t n_ht = (a.n_cells + kTileCells - 1) / kTileCells;
+    TileSched sc;
+    sc.bin_begin = a.bin_begin;
+    sc.bin_q1 = a.bin_q1;
+    sc.n_ht = (int)n_ht;
+    const int64_t n_whole = n_ht > ctas ? n_ht - ctas : 0;
+    const int64_t rem = n_ht - n_whole;
+    sc.split = rem * 4 >= ctas ? 4 : 16;
+    sc.n_whole = (int)n_whole;
+    const int64_t n_units = n_whole + rem * sc.split;
+    if (n_units > INT32_MAX) return {2, 0, cudaSuccess, PATH_TILE};
+    sc.n_units = (int)n_units;
+    sc.counter = a.counter;
+    e = cudaMemsetAsync(a.counter, 0, sizeof(int), a.stream);
+    if (e != cudaSuccess) return {5, 0, e, PATH_TILE};
+    const unsigned grid = (unsigned)(n_units < ctas ? n_units : ctas);
+    kern<<<grid, W * 32, smem, a.stream>>>(a.op, sc, a.fT, a.vT, a.QT);
+    e = cudaGetLastError();
+    return {e == cudaSuccess ? 0 : 5, 1, e, PATH_TILE};
+}
+
+// Work-unit schedule shared by the persistent kernels: whole half-tiles while there are more
+// half-tiles than CTAs, then the last `ctas` half-tiles split into 4 (or 16) bins each.
+struct UnitPlan {
+    int n_ht, n_whole, split, n_units;
+};
+static inline UnitPlan plan_units(int64_t n_cells, int64_t ctas) {
+    const int64_t n_ht = (n_cells + kTileCells - 1) / kTileCells;
+    const int64_t n_whole = n_ht > ctas ? n_ht - ctas : 0;
+    const int64_t rem = n_ht - n_whole;
+    const int split = rem * 4 >= ctas ? 4 : 16;
+    return {(int)n_ht, (int)n_whole, split, (int)(n_whole + rem * split)};
+}
+
+template <int K, int W, bool EXACT, bool JV>
+static LaunchResult launch_pair(const LaunchArgs& a) {
+    const int M = a.op.n_q * K;
+    const size_t smem = pair_smem_bytes<K>(M, W, JV);
+    if (smem + 256 > a.max_smem || a.counter == nullptr || a.pitems == nullptr) return {-1, 0, cudaSuccess, PATH_PAIR};
+    auto kern = af_pair_kernel<K, W, EXACT, JV>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return {5, 0, e, PATH_PAIR};
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem);
+    if (e != cudaSuccess) return {5, 0, e, PATH_PAIR};
+    if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_PAIR};
+    const int64_t ctas = (int64_t)per_sm * a.n_sms;
+    if ((a.n_cells + kTileCells - 1) / kTileCells * 16 > INT32_MAX) return {2, 0, cudaSuccess, PATH_PAIR};
+    const UnitPlan up = plan_units(a.n_cells, ctas);
+    PairSched sc{a.pbin_begin, a.pbin_item, a.pitems, up.n_ht, up.n_whole, up.split, up.n_units, a.counter};
+    e = cudaMemsetAsync(a.counter, 0, sizeof(int), a.stream);
+    if (e != cudaSuccess) return {5, 0, e, PATH_PAIR};
+    const unsigned grid = (unsigned)(up.n_units < ctas ? up.n_units : ctas);
+    kern<<<grid, W * 32, smem, a.stream>>>(a.op, sc, a.fT, a.vT, a.QT);
+    e = cudaGetLastError();
+    return {e == cudaSuccess ? 0 : 5, 1, e, PATH_PAIR};
 }
 
 template <int K, bool EXACT>
 static LaunchResult launch_rf(const LaunchArgs& a) {
     const int64_t warps = (int64_t)a.op.n_items * a.n_tiles;
-    if (warps == 0) return {0, 0, cudaSuccess};
+    if (warps == 0) return {0, 0, cudaSuccess, PATH_GATHER};
     const int64_t blocks = (warps + 3) / 4;
-    if (blocks > INT32_MAX) return {2, 0, cudaSuccess};
+    if (blocks > INT32_MAX) return {2, 0, cudaSuccess, PATH_GATHER};
     rf_kernel<K, EXACT><<<(unsigned)blocks, 128, 0, a.stream>>>(a.op, a.fT, a.QT, (int)a.n_tiles);
     const cudaError_t e = cudaGetLastError();
-    return {e == cudaSuccess ? 0 : 5, 1, e};
+    return {e == cudaSuccess ? 0 : 5, 1, e, PATH_GATHER};
 }
+
+// Warps per CTA of the tile kernel (registers: 16 warps leave 128 per thread).
+constexpr int tile_W(int K, bool jv) { return jv ? (K >= 8 ? 12 : 16) : 16; }
 
 template <int K>
 static LaunchResult launch_for_k(const LaunchArgs& a) {
     if (a.what == OP_RF) return a.exact ? launch_rf<K, true>(a) : launch_rf<K, false>(a);
+    const bool jv = a.what == OP_JV;
+    if constexpr (K <= 8) {
+        if (a.path == PATH_AUTO || a.path == PATH_PAIR) {
+            LaunchResult r;
+            if (jv)
+                r = a.exact ? launch_pair<K, 8, true, true>(a) : launch_pair<K, 8, false, true>(a);
+            else
+                r = a.exact ? launch_pair<K, 8, true, false>(a) : launch_pair<K, 8, false, false>(a);
+            if (r.status != -1) return r;
+            if (a.path == PATH_PAIR) return {8, 0, cudaSuccess, PATH_PAIR};
+        }
+    } else {
+        if (a.path == PATH_PAIR) return {8, 0, cudaSuccess, PATH_PAIR};
+    }
+    if constexpr (K % 2 == 0 && K <= 8) {
+        if (a.path == PATH_AUTO || a.path == PATH_TILE) {
+            LaunchResult r;
+            if (jv)
+                r = a.exact ? launch_tile<K, tile_W(K, true), true, true>(a)
+                            : launch_tile<K, tile_W(K, true), false, true>(a);
+            else
+                r = a.exact ? launch_tile<K, tile_W(K, false), true, false>(a)
+                            : launch_tile<K, tile_W(K, false), false, false>(a);
+            if (r.status != -1) return r;
+            if (a.path == PATH_TILE) return {8, 0, cudaSuccess, PATH_TILE};
+        }
+    } else {
+        if (a.path == PATH_TILE) return {8, 0, cudaSuccess, PATH_TILE};
+    }
     if constexpr (K <= 8) {
         if (a.exact)
-            return a.what == OP_JV ? launch_af<K, 1, true, true>(a) : launch_af<K, 1, true, false>(a);
+            return jv ? launch_af<K, 1, true, true>(a) : launch_af<K, 1, true, false>(a);
     } else {
-        if (a.exact) return {8, 0, cudaSuccess};
+        if (a.exact) return {8, 0, cudaSuccess, PATH_GATHER};
     }
-    return a.what == OP_JV ? launch_af<K, jv_P(K), false, true>(a) : launch_af<K, af_P(K), false, false>(a);
+    return jv ? launch_af<K, jv_P(K), false, true>(a) : launch_af<K, af_P(K), false, false>(a);
 }
 
 }  // namespace cf

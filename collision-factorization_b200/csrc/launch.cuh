@@ -10,15 +10,30 @@ namespace cf {
 
 enum Op { OP_AF = 0, OP_RF = 1, OP_JV = 2 };
 
+// Kernel families for the angular-first / Jacobian forms.
+enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3 };
+
 struct LaunchArgs {
     DevOp op;
     const double* fT;
     const double* vT;
     double* QT;
     int64_t n_tiles;
+    int64_t n_cells;
     cudaStream_t stream;
     int what;    // Op
     bool exact;  // reference operation order, no FMA
+    int path;    // Path
+    // tile-resident kernels: q1 bins, work-queue counter, device limits
+    const int* bin_begin;
+    const int* bin_q1;
+    int* counter;
+    int n_sms;
+    size_t max_smem;
+    // pair kernels: bins over pair items, items (qa, qb)
+    const int* pbin_begin;
+    const int* pbin_item;
+    const int2* pitems;
 };
 
 // Status codes mirror cf_status: 0 ok, 5 CUDA error, 8 unsupported, 2 shape.
@@ -26,6 +41,7 @@ struct LaunchResult {
     int status;
     int launches;
     cudaError_t cuda;
+    int path;  // the kernel family that ran
 };
 
 #define CF_DECLARE_K(KK) LaunchResult launch_k##KK(const LaunchArgs& a);

@@ -68,6 +68,16 @@ struct cf_plan {
     double* d_e_g = nullptr;
     double* d_R = nullptr;
     int* d_item_q1 = nullptr;
+    int* d_bin_begin = nullptr;  // q1 bins of the tile kernel's work units (bin 0 = all, 1..4, 5..20)
+    int* d_bin_q1 = nullptr;
+    int* d_counter = nullptr;    // work-queue head of the tile kernel
+    int* d_pbin_begin = nullptr; // bins over pair items (same layout as the q1 bins)
+    int* d_pbin_item = nullptr;
+    int2* d_pitems = nullptr;    // (qa, qb) rows contracted by the two half-warps; qb = -1: no mirror
+    int n_pairs = 0, n_pair_items = 0;
+    int n_sms = 0;
+    size_t max_smem = 0;
+    int path = 0;  // cf::Path: 0 automatic, 1 gather kernels, 2 tile-resident kernels
     // scratch owned by the plan (tiled copies; device copies of host inputs)
     void* d_ws = nullptr;
     size_t ws_bytes = 0;
@@ -165,6 +175,12 @@ void free_plan_memory(cf_plan* p) {
     cudaFree(p->d_e_g);
     cudaFree(p->d_R);
     cudaFree(p->d_item_q1);
+    cudaFree(p->d_bin_begin);
+    cudaFree(p->d_bin_q1);
+    cudaFree(p->d_counter);
+    cudaFree(p->d_pbin_begin);
+    cudaFree(p->d_pbin_item);
+    cudaFree(p->d_pitems);
     cudaFree(p->d_ws);
     cudaFree(p->d_io);
     if (p->stream) cudaStreamDestroy(p->stream);
@@ -224,6 +240,70 @@ int build_plan(cf_plan* p, const double* labels, const double* vals, const doubl
     p->flops_q = (double)NG * (2.0 * K * K + K) + (double)S * 2.0 * K * K * K;
     p->flops_jv = (double)NG * (4.0 * K * K + 2.0 * K) + (double)S * 2.0 * K * K * K;
 
+    // q1 bins of the tile kernel: bin 0 = every q1 heaviest first; bins 1..4 and 5..20 split the
+    // q1 values into 4 and 16 bins of near-equal cost (longest-processing-time assignment)
+    std::vector<int> bin_begin(1, 0), bin_q1;
+    bin_q1.insert(bin_q1.end(), items.begin(), items.end());
+    bin_begin.push_back((int)bin_q1.size());
+    for (int nb : {4, 16}) {
+        std::vector<std::vector<int>> bins(nb);
+        std::vector<double> load(nb, 0.0);
+        for (int q : items) {
+            const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            bins[b].push_back(q);
+            load[b] += cost[q];
+        }
+        for (auto& bl : bins) {
+            bin_q1.insert(bin_q1.end(), bl.begin(), bl.end());
+            bin_begin.push_back((int)bin_q1.size());
+        }
+    }
+
+    // pair items: rows (l1,+m1) and (l1,-m1) whose slices have the same t sequence and lengths
+    std::vector<std::vector<std::pair<int, int>>> shape(NQ);
+    for (int q = 0; q < NQ; ++q)
+        for (int s = q1_begin[q]; s < q1_begin[q + 1]; ++s) shape[q].push_back({slice_t[s], slice_e[s + 1] - slice_e[s]});
+    std::vector<int2> pitems;
+    std::vector<double> pcost;
+    std::vector<char> used(NQ, 0);
+    for (int l = 0; l * l < NQ; ++l) {
+        for (int m = 1; m <= l; ++m) {
+            const int qa = l * l + l + m, qb = l * l + l - m;
+            if (qa >= NQ || qb >= NQ) continue;
+            if (!shape[qa].empty() && shape[qa] == shape[qb]) {
+                pitems.push_back(make_int2(qa, qb));
+                pcost.push_back(cost[qa]);
+                used[qa] = used[qb] = 1;
+            }
+        }
+    }
+    for (int q = 0; q < NQ; ++q)
+        if (!used[q] && !shape[q].empty()) {
+            pitems.push_back(make_int2(q, -1));
+            pcost.push_back(cost[q]);
+        }
+    std::vector<int> porder(pitems.size());
+    for (size_t i = 0; i < porder.size(); ++i) porder[i] = (int)i;
+    std::stable_sort(porder.begin(), porder.end(), [&](int a, int b) { return pcost[a] > pcost[b]; });
+    std::vector<int> pbin_begin(1, 0), pbin_item(porder.begin(), porder.end());
+    pbin_begin.push_back((int)pbin_item.size());
+    for (int nb : {4, 16}) {
+        std::vector<std::vector<int>> bins(nb);
+        std::vector<double> load(nb, 0.0);
+        for (int i : porder) {
+            const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+            bins[b].push_back(i);
+            load[b] += pcost[i];
+        }
+        for (auto& bl : bins) {
+            pbin_item.insert(pbin_item.end(), bl.begin(), bl.end());
+            pbin_begin.push_back((int)pbin_item.size());
+        }
+    }
+    p->n_pair_items = (int)pitems.size();
+    p->n_pairs = 0;
+    for (const int2& it : pitems) p->n_pairs += it.y >= 0;
+
     std::vector<double> Rv((size_t)K * K * K * p->n_l);
     if (NG > 0) std::memcpy(Rv.data(), R, Rv.size() * sizeof(double));
     int64_t bytes = 0;
@@ -234,6 +314,18 @@ int build_plan(cf_plan* p, const double* labels, const double* vals, const doubl
     CF_TRY(upload(&p->d_e_g, e_g, bytes));
     CF_TRY(upload(&p->d_R, Rv, bytes));
     CF_TRY(upload(&p->d_item_q1, items, bytes));
+    CF_TRY(upload(&p->d_bin_begin, bin_begin, bytes));
+    CF_TRY(upload(&p->d_bin_q1, bin_q1, bytes));
+    CF_TRY(upload(&p->d_pbin_begin, pbin_begin, bytes));
+    CF_TRY(upload(&p->d_pbin_item, pbin_item, bytes));
+    CF_TRY(upload(&p->d_pitems, pitems, bytes));
+    CF_CUDA(cudaMalloc((void**)&p->d_counter, sizeof(int)));
+    bytes += sizeof(int);
+    int dev = 0, optin = 0;
+    CF_CUDA(cudaGetDevice(&dev));
+    CF_CUDA(cudaDeviceGetAttribute(&p->n_sms, cudaDevAttrMultiProcessorCount, dev));
+    CF_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    p->max_smem = (size_t)optin;
     p->dev_bytes = bytes;
     return CF_OK;
 }
@@ -247,9 +339,11 @@ size_t tiled_bytes(const cf_plan* p, int64_t B) {
 // ------------------------------------------------------------------------------------------
 // Kernel dispatch over K (each K lives in its own translation unit, inst.cu)
 // ------------------------------------------------------------------------------------------
-int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const double* vT, double* QT, int64_t nt,
+int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const double* vT, double* QT, int64_t B,
              cudaStream_t st) {
-    cf::LaunchArgs a{p->op(), fT, vT, QT, nt, st, what, exact};
+    const int64_t nt = n_tiles_for(B);
+    cf::LaunchArgs a{p->op(), fT, vT, QT, nt, B, st, what, exact, p->path, p->d_bin_begin, p->d_bin_q1,
+                     p->d_counter, p->n_sms, p->max_smem, p->d_pbin_begin, p->d_pbin_item, p->d_pitems};
     cf::LaunchResult r{8, 0, cudaSuccess};
     switch (p->k) {
 #define CF_K(KK) \
@@ -262,7 +356,8 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
     g_launches += r.launches;
     if (r.status == CF_ECUDA) return fail(CF_ECUDA, "kernel launch: %s", cudaGetErrorString(r.cuda));
     if (r.status == CF_EUNSUPPORTED)
-        return fail(CF_EUNSUPPORTED, "form not built for K = %d (the exact angular-first order needs K <= 8)", p->k);
+        return fail(CF_EUNSUPPORTED, "form or kernel path not built for K = %d (exact angular-first needs K <= 8; "
+                    "the tile-resident kernels need an even K <= 8 and a tile that fits in shared memory)", p->k);
     if (r.status != CF_OK) return fail(r.status, "launch failed for K = %d", p->k);
     return CF_OK;
 }
@@ -306,7 +401,7 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
     CF_TRY(launch_pack(p, f_dev, fT, B, st));
     if (what == 2) CF_TRY(launch_pack(p, v_dev, vT, B, st));
     CF_TRY(launch_pack(p, q_dev, QT, B, st));
-    CF_TRY(dispatch(p, what, exact, fT, vT, QT, nt, st));
+    CF_TRY(dispatch(p, what, exact, fT, vT, QT, B, st));
     CF_TRY(launch_unpack(p, QT, q_dev, B, st));
     return CF_OK;
 }
@@ -604,7 +699,7 @@ int cf_q_tiled(cf_plan* plan, double* q_tiled, const double* f_tiled, int64_t b,
     if (b == 0 || plan->n_g == 0) return CF_OK;
     if (!q_tiled || !f_tiled) return fail(CF_EINVAL, "null device buffer");
     DeviceGuard guard(plan->device);
-    return dispatch(plan, what, exact, f_tiled, nullptr, q_tiled, n_tiles_for(b), (cudaStream_t)stream);
+    return dispatch(plan, what, exact, f_tiled, nullptr, q_tiled, b, (cudaStream_t)stream);
 }
 
 int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const double* v_tiled, int64_t b,
@@ -615,7 +710,17 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
     if (b == 0 || plan->n_g == 0) return CF_OK;
     if (!out_tiled || !f_tiled || !v_tiled) return fail(CF_EINVAL, "null device buffer");
     DeviceGuard guard(plan->device);
-    return dispatch(plan, cf::OP_JV, exact != 0, f_tiled, v_tiled, out_tiled, n_tiles_for(b), (cudaStream_t)stream);
+    return dispatch(plan, cf::OP_JV, exact != 0, f_tiled, v_tiled, out_tiled, b, (cudaStream_t)stream);
+}
+
+int cf_plan_set_kernel_path(cf_plan* plan, int32_t path) {
+    g_last_error.clear();
+    if (!plan) return fail(CF_EINVAL, "null plan");
+    if (path < 0 || path > 3)
+        return fail(CF_EINVAL, "kernel path %d is not 0 (auto), 1 (gather), 2 (tile) or 3 (pair)", path);
+    std::lock_guard<std::mutex> lk(plan->mu);
+    plan->path = path;
+    return CF_OK;
 }
 
 int cf_fp64_fma_peak(int32_t device, double* tflops) {

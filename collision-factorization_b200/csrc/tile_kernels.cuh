@@ -1,0 +1,269 @@
+// tile_kernels.cuh -- tile-resident angular-first kernels (persistent, device work queue).
+//
+// A CTA keeps the f (and, for J.v, the v) coefficients of a 16-cell half-tile resident in shared
+// memory and its W warps contract every q1 of those cells out of it:
+//
+//   * one warp per q1; each cell is handled by two lanes (lane = 16*part + cell) that split the
+//     K x K Phi accumulator by k3 column, so the f2 row is a broadcast between the two halves and a
+//     lane holds K*K/2 accumulators;
+//   * per (t, q1) slice the warp copies R_t into its own shared buffer with cp.async while it
+//     accumulates Phi, so the K^3 step reads R from shared memory (k3 slices padded by two doubles
+//     so the two lane halves hit different banks);
+//   * CTAs are persistent and pull work units from a device counter: whole half-tiles first, then
+//     half-tiles split into q1 bins, so the last wave is made of small units.  Inside a unit the
+//     warps pull q1 values (heaviest first) from a shared counter.
+//
+// The counter is the only inter-CTA interaction; nothing waits on another CTA.
+#pragma once
+#include "common.cuh"
+
+namespace cf {
+
+constexpr int kTileCells = 16;
+
+struct TileSched {
+    const int* bin_begin;  // bin b = q1 list bin_q1[bin_begin[b] .. bin_begin[b+1])
+    const int* bin_q1;     // bin 0: every q1, heaviest first; bins 1..4: quarters; bins 5..20: sixteenths
+    int n_ht;              // half-tiles: ceil(B / 16)
+    int n_whole;           // units [0, n_whole) are whole half-tiles
+    int split;             // later units split a half-tile into `split` bins (4 or 16)
+    int n_units;
+    int* counter;          // zeroed before the launch
+};
+
+__host__ __device__ constexpr int bin_base(int split) { return split == 4 ? 1 : 5; }
+
+template <int K>
+struct RBuf {
+    static constexpr int SL = K * K + 2;  // padded k3 slice (keeps 16-byte alignment for even K)
+    static constexpr int SIZE = K * SL;
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Contract every slice of one q1 for the resident half-tile.  qtc points at this lane's cell of
+// the tiled output; the result is accumulated into it (out += ...).
+template <int K, bool EXACT, bool JV>
+__device__ __forceinline__ void tile_q1(const DevOp& op, int q1, const double* __restrict__ fs,
+                                        const double* __restrict__ vs, double* rb, double* qtc, int lane) {
+    constexpr int KC = K / 2;
+    constexpr int SL = RBuf<K>::SL;
+    const int c = lane & 15;
+    const int part = lane >> 4;
+    const int k3b = part * KC;
+    const int owner = EXACT ? 1 : 0;  // the lane half that holds the caller's Q and writes it back
+
+    double acc[K];
+#pragma unroll
+    for (int k1 = 0; k1 < K; ++k1) acc[k1] = (part == owner) ? qtc[(size_t)(q1 * K + k1) * CF_TILE] : 0.0;
+
+    const int s0 = op.q1_begin[q1], s1 = op.q1_begin[q1 + 1];
+    for (int s = s0; s < s1; ++s) {
+        const int t = op.slice_t[s];
+        const int e0 = op.slice_e[s], e1 = op.slice_e[s + 1];
+        // stage R_t (K^3 doubles) into this warp's padded buffer while Phi accumulates
+        __syncwarp();
+        const double* __restrict__ Rt = op.R + (size_t)t * K * K * K;
+        for (int i = lane; i < K * K * K / 2; i += 32) {
+            const int j = (2 * i) / (K * K), w = (2 * i) % (K * K);
+            cp_async16(rb + j * SL + w, Rt + 2 * i);
+        }
+        cp_async_commit();
+
+        double phi[K][KC];
+#pragma unroll
+        for (int a = 0; a < K; ++a)
+#pragma unroll
+            for (int b = 0; b < KC; ++b) phi[a][b] = 0.0;
+
+        for (int eb = e0; eb < e1; eb += 32) {
+            const int n = min(32, e1 - eb);
+            uint32_t my_q23 = 0;
+            double my_g = 0.0;
+            if (lane < n) {
+                my_q23 = __ldg(op.e_q23 + eb + lane);
+                my_g = __ldg(op.e_g + eb + lane);
+            }
+            for (int j = 0; j < n; ++j) {
+                const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, j);
+                const double g = __shfl_sync(0xffffffffu, my_g, j);
+                const int r2 = (int)(q23 & 0xffffu) * K, r3 = (int)(q23 >> 16) * K + k3b;
+                double f2[K], f3[KC];
+#pragma unroll
+                for (int k = 0; k < K; ++k) f2[k] = fs[(r2 + k) * kTileCells + c];
+#pragma unroll
+                for (int b = 0; b < KC; ++b) f3[b] = fs[(r3 + b) * kTileCells + c];
+                if constexpr (JV) {
+                    double v2[K], v3[KC];
+#pragma unroll
+                    for (int k = 0; k < K; ++k) v2[k] = vs[(r2 + k) * kTileCells + c];
+#pragma unroll
+                    for (int b = 0; b < KC; ++b) v3[b] = vs[(r3 + b) * kTileCells + c];
+                    if constexpr (EXACT) {
+#pragma unroll
+                        for (int b = 0; b < KC; ++b)
+#pragma unroll
+                            for (int k2 = 0; k2 < K; ++k2)
+                                phi[k2][b] = __dadd_rn(
+                                    phi[k2][b],
+                                    __dmul_rn(g, __dadd_rn(__dmul_rn(v2[k2], f3[b]), __dmul_rn(f2[k2], v3[b]))));
+                    } else {
+#pragma unroll
+                        for (int b = 0; b < KC; ++b) {
+                            const double gf3 = g * f3[b], gv3 = g * v3[b];
+#pragma unroll
+                            for (int k2 = 0; k2 < K; ++k2) phi[k2][b] = fma(v2[k2], gf3, fma(f2[k2], gv3, phi[k2][b]));
+                        }
+                    }
+                } else if constexpr (EXACT) {
+                    double gf2[K];
+#pragma unroll
+                    for (int k2 = 0; k2 < K; ++k2) gf2[k2] = __dmul_rn(g, f2[k2]);
+#pragma unroll
+                    for (int b = 0; b < KC; ++b)
+#pragma unroll
+                        for (int k2 = 0; k2 < K; ++k2) phi[k2][b] = __dadd_rn(phi[k2][b], __dmul_rn(gf2[k2], f3[b]));
+                } else {
+#pragma unroll
+                    for (int b = 0; b < KC; ++b) {
+                        const double gf3 = g * f3[b];
+#pragma unroll
+                        for (int k2 = 0; k2 < K; ++k2) phi[k2][b] = fma(f2[k2], gf3, phi[k2][b]);
+                    }
+                }
+            }
+        }
+        cp_async_wait_all();
+        __syncwarp();
+
+        // K^3 step from the shared copy of R_t: element (k1,k2,k3) at rb[k3*SL + k2*K + k1]
+        if constexpr (EXACT) {
+            // the reference sums k3 = 0..K-1 (outer), k2 (inner) sequentially: half 0 sums its columns,
+            // hands the partial to half 1, which continues with its columns
+            double sp[K];
+            if (part == 0) {
+#pragma unroll
+                for (int k1 = 0; k1 < K; ++k1) {
+                    double sacc = 0.0;
+#pragma unroll
+                    for (int b = 0; b < KC; ++b)
+#pragma unroll
+                        for (int k2 = 0; k2 < K; ++k2) sacc = __dadd_rn(sacc, __dmul_rn(rb[b * SL + k2 * K + k1], phi[k2][b]));
+                    sp[k1] = sacc;
+                }
+            }
+#pragma unroll
+            for (int k1 = 0; k1 < K; ++k1) sp[k1] = __shfl_up_sync(0xffffffffu, sp[k1], 16);
+            if (part == 1) {
+#pragma unroll
+                for (int k1 = 0; k1 < K; ++k1) {
+                    double sacc = sp[k1];
+#pragma unroll
+                    for (int b = 0; b < KC; ++b)
+#pragma unroll
+                        for (int k2 = 0; k2 < K; ++k2)
+                            sacc = __dadd_rn(sacc, __dmul_rn(rb[(KC + b) * SL + k2 * K + k1], phi[k2][b]));
+                    acc[k1] = __dadd_rn(acc[k1], sacc);
+                }
+            }
+        } else {
+            const double* __restrict__ rk = rb + k3b * SL;
+#pragma unroll
+            for (int b = 0; b < KC; ++b) {
+#pragma unroll
+                for (int k2 = 0; k2 < K; ++k2) {
+                    const double2* r2v = reinterpret_cast<const double2*>(rk + b * SL + k2 * K);
+#pragma unroll
+                    for (int h = 0; h < K / 2; ++h) {
+                        const double2 r = r2v[h];
+                        acc[2 * h] = fma(r.x, phi[k2][b], acc[2 * h]);
+                        acc[2 * h + 1] = fma(r.y, phi[k2][b], acc[2 * h + 1]);
+                    }
+                }
+            }
+        }
+    }
+
+    if constexpr (!EXACT) {
+#pragma unroll
+        for (int k1 = 0; k1 < K; ++k1) acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], 16);
+    }
+    if (part == owner) {
+#pragma unroll
+        for (int k1 = 0; k1 < K; ++k1) qtc[(size_t)(q1 * K + k1) * CF_TILE] = acc[k1];
+    }
+}
+
+template <int K, int W, bool EXACT, bool JV>
+__global__ void __launch_bounds__(W * 32, 1)
+    af_tile_kernel(DevOp op, TileSched sc, const double* __restrict__ fT, const double* __restrict__ vT,
+                   double* __restrict__ QT) {
+    static_assert(K % 2 == 0, "the tile kernel splits Phi into two column halves");
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_unit, s_next;
+    const int M = op.n_q * K;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    double* fs = smem;
+    double* vs = JV ? smem + (size_t)M * kTileCells : nullptr;
+    double* rb = smem + (size_t)(JV ? 2 : 1) * M * kTileCells + (size_t)warp * RBuf<K>::SIZE;
+    int staged = -1;
+
+    for (;;) {
+        if (tid == 0) s_unit = atomicAdd(sc.counter, 1);
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= sc.n_units) break;
+        int ht, bin;
+        if (u < sc.n_whole) {
+            ht = u;
+            bin = 0;
+        } else {
+            const int v = u - sc.n_whole;
+            ht = sc.n_whole + v / sc.split;
+            bin = bin_base(sc.split) + v % sc.split;
+        }
+        const size_t tile_base = (size_t)(ht >> 1) * M * CF_TILE + (size_t)(ht & 1) * kTileCells;
+        if (ht != staged) {
+            // rows of 16 cells (128 B) from the tiled global layout, 8 x 16-byte copies per row
+            const double* srcf = fT + tile_base;
+            for (int i = tid; i < M * 8; i += W * 32) {
+                const int r = i >> 3, w = (i & 7) * 2;
+                cp_async16(fs + r * kTileCells + w, srcf + (size_t)r * CF_TILE + w);
+            }
+            if constexpr (JV) {
+                const double* srcv = vT + tile_base;
+                for (int i = tid; i < M * 8; i += W * 32) {
+                    const int r = i >> 3, w = (i & 7) * 2;
+                    cp_async16(vs + r * kTileCells + w, srcv + (size_t)r * CF_TILE + w);
+                }
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            staged = ht;
+        }
+        if (tid == 0) s_next = 0;
+        __syncthreads();
+        const int b0 = sc.bin_begin[bin], nb = sc.bin_begin[bin + 1] - b0;
+        double* qtc = QT + tile_base + (lane & 15);
+        for (;;) {
+            int i = 0;
+            if (lane == 0) i = atomicAdd(&s_next, 1);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= nb) break;
+            tile_q1<K, EXACT, JV>(op, sc.bin_q1[b0 + i], fs, vs, rb, qtc, lane);
+        }
+        __syncthreads();
+    }
+}
+
+template <int K>
+constexpr size_t tile_smem_bytes(int M, int W, bool jv) {
+    return sizeof(double) * ((size_t)(jv ? 2 : 1) * M * kTileCells + (size_t)W * RBuf<K>::SIZE);
+}
+
+}  // namespace cf

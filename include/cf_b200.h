@@ -139,6 +139,14 @@ int cf_q_tiled(cf_plan* plan, double* q_tiled, const double* f_tiled, int64_t b,
 int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const double* v_tiled, int64_t b,
                 int32_t exact, void* stream);
 
+/* Kernel family of a plan's angular-first and Jacobian contractions: 0 = automatic (the first of
+ * pair, tile, gather that fits), 1 = the gather kernel (warp per row and 32-cell tile, f read
+ * through L1/L2), 2 = the tile-resident kernel (16 cells in shared memory, Phi split over two
+ * lanes per cell), 3 = the pair kernel (16 cells in shared memory, the mirrored rows (l,+m) and
+ * (l,-m) on the two half-warps).  2 and 3 return CF_EUNSUPPORTED where they do not fit.  All
+ * families agree to rounding, and bit for bit in the exact forms. */
+int cf_plan_set_kernel_path(cf_plan* plan, int32_t path);
+
 /* Measured FP64 FMA throughput of `device` in TFLOP/s (independent DFMA chains on every SM, timed
  * with CUDA events): the peak the FP64 forms are compared against. */
 int cf_fp64_fma_peak(int32_t device, double* tflops);
