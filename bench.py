@@ -56,6 +56,8 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=20260)
+    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1"],
+                    help="kernel family of the angular-first contraction")
     ap.add_argument("--profile", action="store_true",
                     help="only build the workload and launch the contraction (steps+1 times); for ncu captures")
     return ap.parse_args(argv)
@@ -234,6 +236,7 @@ def run_ours(args):
     M = NQ * K
     cells = make_cells(L, K, B, seed=args.seed + rank)
     op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, NQ, K, device=local)
+    op.set_kernel_path(args.path)
     lib = _lib.load()
 
     f = torch.from_numpy(cells).to(dev)
@@ -298,13 +301,13 @@ def run_ours(args):
     kern_ms = timed(kernel_only, args.steps)
     rf_ms = timed(lambda: step("rf"), max(2, args.steps // 4))
     path_ms = {}
-    for path in ("pair", "tile", "gather"):
+    for path in ("pair", "pair_l1", "tile", "gather"):
         try:
             op.set_kernel_path(path)
             path_ms[path] = timed(step, max(2, args.steps // 4))
         except Exception:
             path_ms[path] = None
-    op.set_kernel_path("auto")
+    op.set_kernel_path(args.path)
     exact_ms = timed(lambda: step("af_exact"), max(2, args.steps // 4))
     clk = clocks.stop()
     torch.cuda.synchronize(dev)
@@ -521,6 +524,7 @@ def run_profile(args):
     L, K, B, gamma = WORKLOADS[args.workload]
     geo, R, _ = make_operator(L, K, gamma, args.seed)
     op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K, device=0)
+    op.set_kernel_path(args.path)
     lib = _lib.load()
     f = torch.from_numpy(make_cells(L, K, B, seed=args.seed)).cuda()
     M = geo.n_q * K

@@ -29,6 +29,9 @@ EXPORTS = [
     "cf_angular_first", "cf_radial_first", "cf_contract_host", "cf_jacobian_apply_host",
     "cf_plan_create", "cf_plan_destroy", "cf_plan_get_info", "cf_plan_workspace_size",
     "cf_q_device", "cf_q_device_ws", "cf_jv_device",
+    "cf_gmres_workspace_size", "cf_gmres_solve_tiled",
+    "cf_mlp_create", "cf_mlp_destroy", "cf_mlp_num_params", "cf_mlp_copy", "cf_mlp_forward", "cf_mlp_backward",
+    "cf_mlp_adam_step", "cf_precond_probe_loss", "cf_precond_assemble",
     "cf_pack_cells", "cf_unpack_cells", "cf_q_tiled", "cf_jv_tiled", "cf_plan_set_kernel_path", "cf_fp64_fma_peak",
     "cf_status_string", "cf_last_error", "cf_launch_count", "cf_version",
 ]
@@ -79,6 +82,20 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_jv_tiled.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]
     lib.cf_fp64_fma_peak.argtypes = [_I32, C.POINTER(C.c_double)]
     lib.cf_plan_set_kernel_path.argtypes = [C.c_void_p, _I32]
+    V = C.c_void_p
+    lib.cf_mlp_create.argtypes = [C.POINTER(V), _I32, _I32, _I32, _I32, C.c_uint64, _I32]
+    lib.cf_mlp_destroy.argtypes = [V]
+    lib.cf_mlp_num_params.argtypes = [V, C.POINTER(C.c_int64)]
+    lib.cf_mlp_copy.argtypes = [V, V, _I32]
+    lib.cf_mlp_forward.argtypes = [V, V, V, _I64, _I32, V]
+    lib.cf_mlp_backward.argtypes = [V, V, V, _I64, V]
+    lib.cf_mlp_adam_step.argtypes = [V, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, V]
+    lib.cf_precond_probe_loss.argtypes = [V, V, V, V, V, C.c_float, _I64, _I32, _I32, _I32, V, V, V]
+    lib.cf_precond_assemble.argtypes = [V, V, V, C.c_float, _I64, _I32, _I32, V]
+    lib.cf_gmres_workspace_size.argtypes = [C.c_void_p, _I64, _I32, C.POINTER(C.c_size_t)]
+    lib.cf_gmres_solve_tiled.argtypes = [C.c_void_p, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, _I64, _I32,
+                                         _I32, C.c_double, C.c_void_p, _I32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_size_t, C.c_void_p]
     lib.cf_status_string.restype = C.c_char_p
     lib.cf_status_string.argtypes = [C.c_int]
     lib.cf_last_error.restype = C.c_char_p

@@ -67,12 +67,12 @@ static inline UnitPlan plan_units(int64_t n_cells, int64_t ctas) {
     return {(int)n_ht, (int)n_whole, split, (int)(n_whole + rem * split)};
 }
 
-template <int K, int W, bool EXACT, bool JV>
+template <int K, int W, bool EXACT, bool JV, bool RG>
 static LaunchResult launch_pair(const LaunchArgs& a) {
     const int M = a.op.n_q * K;
-    const size_t smem = pair_smem_bytes<K>(M, W, JV);
+    const size_t smem = pair_smem_bytes<K>(M, W, JV, RG);
     if (smem + 256 > a.max_smem || a.counter == nullptr || a.pitems == nullptr) return {-1, 0, cudaSuccess, PATH_PAIR};
-    auto kern = af_pair_kernel<K, W, EXACT, JV>;
+    auto kern = af_pair_kernel<K, W, EXACT, JV, RG>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return {5, 0, e, PATH_PAIR};
     int per_sm = 0;
@@ -110,17 +110,24 @@ static LaunchResult launch_for_k(const LaunchArgs& a) {
     if (a.what == OP_RF) return a.exact ? launch_rf<K, true>(a) : launch_rf<K, false>(a);
     const bool jv = a.what == OP_JV;
     if constexpr (K <= 8) {
-        if (a.path == PATH_AUTO || a.path == PATH_PAIR) {
+        if (a.path == PATH_AUTO || a.path == PATH_PAIR || a.path == PATH_PAIR_L1) {
             LaunchResult r;
-            if (jv)
-                r = a.exact ? launch_pair<K, 8, true, true>(a) : launch_pair<K, 8, false, true>(a);
-            else
-                r = a.exact ? launch_pair<K, 8, true, false>(a) : launch_pair<K, 8, false, false>(a);
+            if (a.path == PATH_PAIR_L1) {
+                if (jv)
+                    r = a.exact ? launch_pair<K, 8, true, true, true>(a) : launch_pair<K, 8, false, true, true>(a);
+                else
+                    r = a.exact ? launch_pair<K, 8, true, false, true>(a) : launch_pair<K, 8, false, false, true>(a);
+            } else {
+                if (jv)
+                    r = a.exact ? launch_pair<K, 8, true, true, false>(a) : launch_pair<K, 8, false, true, false>(a);
+                else
+                    r = a.exact ? launch_pair<K, 8, true, false, false>(a) : launch_pair<K, 8, false, false, false>(a);
+            }
             if (r.status != -1) return r;
-            if (a.path == PATH_PAIR) return {8, 0, cudaSuccess, PATH_PAIR};
+            if (a.path != PATH_AUTO) return {8, 0, cudaSuccess, a.path};
         }
     } else {
-        if (a.path == PATH_PAIR) return {8, 0, cudaSuccess, PATH_PAIR};
+        if (a.path == PATH_PAIR || a.path == PATH_PAIR_L1) return {8, 0, cudaSuccess, a.path};
     }
     if constexpr (K % 2 == 0 && K <= 8) {
         if (a.path == PATH_AUTO || a.path == PATH_TILE) {

@@ -38,7 +38,10 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
-template <int K, bool EXACT, bool JV>
+// RG = false: R_t is staged into the warp's shared buffer with cp.async.  RG = true: R_t is read
+// straight from global memory with warp-uniform loads through L1 (prefetched into L1 at the start
+// of the slice), which keeps the K^3 step off the shared-memory wavefront budget.
+template <int K, bool EXACT, bool JV, bool RG>
 __device__ __forceinline__ void pair_item(const DevOp& op, int2 item, const double* __restrict__ fs,
                                           const double* __restrict__ vs, double* rb, double* qtc, int lane) {
     const int half = lane >> 4;
@@ -60,14 +63,20 @@ __device__ __forceinline__ void pair_item(const DevOp& op, int2 item, const doub
         const int eb_ = op.slice_e[sb];
         const int my_e0 = half == 0 ? ea : eb_;
 
-        __syncwarp();
         const double* __restrict__ Rt = op.R + (size_t)t * K * K * K;
-        if constexpr (K % 2 == 0) {
-            for (int j = lane; j < K * K * K / 2; j += 32) cp_async16(rb + 2 * j, Rt + 2 * j);
+        if constexpr (RG) {
+            const char* rbytes = reinterpret_cast<const char*>(Rt);
+            for (int off = lane * 128; off < K * K * K * 8; off += 32 * 128)
+                asm volatile("prefetch.global.L1 [%0];\n" ::"l"(rbytes + off));
         } else {
-            for (int j = lane; j < K * K * K; j += 32) cp_async8(rb + j, Rt + j);
+            __syncwarp();
+            if constexpr (K % 2 == 0) {
+                for (int j = lane; j < K * K * K / 2; j += 32) cp_async16(rb + 2 * j, Rt + 2 * j);
+            } else {
+                for (int j = lane; j < K * K * K; j += 32) cp_async8(rb + j, Rt + j);
+            }
+            cp_async_commit();
         }
-        cp_async_commit();
 
         double phi[K][K];
 #pragma unroll
@@ -134,10 +143,13 @@ __device__ __forceinline__ void pair_item(const DevOp& op, int2 item, const doub
                 }
             }
         }
-        cp_async_wait_all();
-        __syncwarp();
+        if constexpr (!RG) {
+            cp_async_wait_all();
+            __syncwarp();
+        }
+        const double* __restrict__ rsrc = RG ? Rt : rb;
 
-        // K^3 step: R_t element (k1,k2,k3) at rb[k1 + K k2 + K^2 k3]; the address is warp-uniform
+        // K^3 step: R_t element (k1,k2,k3) at rsrc[k1 + K k2 + K^2 k3]; the address is warp-uniform
         if constexpr (EXACT) {
 #pragma unroll
             for (int k1 = 0; k1 < K; ++k1) {
@@ -145,7 +157,10 @@ __device__ __forceinline__ void pair_item(const DevOp& op, int2 item, const doub
 #pragma unroll
                 for (int b = 0; b < K; ++b)
 #pragma unroll
-                    for (int a = 0; a < K; ++a) sacc = __dadd_rn(sacc, __dmul_rn(rb[k1 + K * a + K * K * b], phi[a][b]));
+                    for (int a = 0; a < K; ++a) {
+                        const double r = RG ? __ldg(rsrc + k1 + K * a + K * K * b) : rsrc[k1 + K * a + K * K * b];
+                        sacc = __dadd_rn(sacc, __dmul_rn(r, phi[a][b]));
+                    }
                 acc[k1] = __dadd_rn(acc[k1], sacc);
             }
         } else if constexpr (K % 2 == 0) {
@@ -153,10 +168,10 @@ __device__ __forceinline__ void pair_item(const DevOp& op, int2 item, const doub
             for (int b = 0; b < K; ++b)
 #pragma unroll
                 for (int a = 0; a < K; ++a) {
-                    const double2* r2v = reinterpret_cast<const double2*>(rb + K * a + K * K * b);
+                    const double2* r2v = reinterpret_cast<const double2*>(rsrc + K * a + K * K * b);
 #pragma unroll
                     for (int h = 0; h < K / 2; ++h) {
-                        const double2 r = r2v[h];
+                        const double2 r = RG ? __ldg(r2v + h) : r2v[h];
                         acc[2 * h] = fma(r.x, phi[a][b], acc[2 * h]);
                         acc[2 * h + 1] = fma(r.y, phi[a][b], acc[2 * h + 1]);
                     }
@@ -167,7 +182,10 @@ __device__ __forceinline__ void pair_item(const DevOp& op, int2 item, const doub
 #pragma unroll
                 for (int a = 0; a < K; ++a)
 #pragma unroll
-                    for (int k1 = 0; k1 < K; ++k1) acc[k1] = fma(rb[k1 + K * a + K * K * b], phi[a][b], acc[k1]);
+                    for (int k1 = 0; k1 < K; ++k1) {
+                        const double r = RG ? __ldg(rsrc + k1 + K * a + K * K * b) : rsrc[k1 + K * a + K * K * b];
+                        acc[k1] = fma(r, phi[a][b], acc[k1]);
+                    }
         }
     }
     if (active) {
@@ -176,7 +194,7 @@ __device__ __forceinline__ void pair_item(const DevOp& op, int2 item, const doub
     }
 }
 
-template <int K, int W, bool EXACT, bool JV>
+template <int K, int W, bool EXACT, bool JV, bool RG>
 __global__ void __launch_bounds__(W * 32, 1)
     af_pair_kernel(DevOp op, PairSched sc, const double* __restrict__ fT, const double* __restrict__ vT,
                    double* __restrict__ QT) {
@@ -230,15 +248,15 @@ __global__ void __launch_bounds__(W * 32, 1)
             if (lane == 0) i = atomicAdd(&s_next, 1);
             i = __shfl_sync(0xffffffffu, i, 0);
             if (i >= nb) break;
-            pair_item<K, EXACT, JV>(op, sc.items[sc.bin_item[b0 + i]], fs, vs, rb, qtc, lane);
+            pair_item<K, EXACT, JV, RG>(op, sc.items[sc.bin_item[b0 + i]], fs, vs, rb, qtc, lane);
         }
         __syncthreads();
     }
 }
 
 template <int K>
-constexpr size_t pair_smem_bytes(int M, int W, bool jv) {
-    return sizeof(double) * ((size_t)(jv ? 2 : 1) * M * kTileCells + (size_t)W * RPair<K>::SIZE);
+constexpr size_t pair_smem_bytes(int M, int W, bool jv, bool rg) {
+    return sizeof(double) * ((size_t)(jv ? 2 : 1) * M * kTileCells + (rg ? 0 : (size_t)W * RPair<K>::SIZE));
 }
 
 }  // namespace cf

@@ -50,6 +50,9 @@ constexpr int kMaxK = 16;
 
 }  // namespace
 
+// Lets the other translation units of the library report through cf_last_error().
+__attribute__((visibility("hidden"))) void cf_set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
 // ------------------------------------------------------------------------------------------
 // The plan: one operator resident on one device
 // ------------------------------------------------------------------------------------------
@@ -716,8 +719,9 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    if (path < 0 || path > 3)
-        return fail(CF_EINVAL, "kernel path %d is not 0 (auto), 1 (gather), 2 (tile) or 3 (pair)", path);
+    if (path < 0 || path > 4)
+        return fail(CF_EINVAL, "kernel path %d is not 0 (auto), 1 (gather), 2 (tile), 3 (pair) or 4 (pair, R via L1)",
+                    path);
     std::lock_guard<std::mutex> lk(plan->mu);
     plan->path = path;
     return CF_OK;

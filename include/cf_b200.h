@@ -143,13 +143,62 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
  * pair, tile, gather that fits), 1 = the gather kernel (warp per row and 32-cell tile, f read
  * through L1/L2), 2 = the tile-resident kernel (16 cells in shared memory, Phi split over two
  * lanes per cell), 3 = the pair kernel (16 cells in shared memory, the mirrored rows (l,+m) and
- * (l,-m) on the two half-warps).  2 and 3 return CF_EUNSUPPORTED where they do not fit.  All
- * families agree to rounding, and bit for bit in the exact forms. */
+ * (l,-m) on the two half-warps), 4 = the pair kernel reading R through L1 instead of shared
+ * memory.  2-4 return CF_EUNSUPPORTED where they do not fit.  All families agree to rounding, and
+ * bit for bit in the exact forms. */
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path);
 
 /* Measured FP64 FMA throughput of `device` in TFLOP/s (independent DFMA chains on every SM, timed
  * with CUDA events): the peak the FP64 forms are compared against. */
 int cf_fp64_fma_peak(int32_t device, double* tflops);
+
+/* ------------------------------------------------------------------------------------------
+ * Implicit solves: (I - dt J(f)) x = b per cell with restarted GMRES, FP64.  No counterpart in
+ * the reference (it steps only explicitly, with a dense tensor: tutorial_stress_relaxation.m:77-91).
+ * All vectors are device arrays in the tiled layout (cf_pack_cells).  x holds the initial guess on
+ * entry.  Preconditioning is on the right with block-Jacobi over the angular modes: `precond` is
+ * NULL (none), N_Q blocks of K x K shared by all cells (precond_per_cell = 0), or B sets of N_Q
+ * blocks (precond_per_cell = 1); block q maps rows q*K..q*K+K-1 (row-major, [out][in]).  A cell
+ * is done when |b - A x| <= tol |b| in FP64.  iters_out[B] (host, may be NULL) receives the
+ * Arnoldi steps each cell used, relres_out[B] (host, may be NULL) the final relative residuals.
+ * Returns CF_ETIMEOUT if some cell is still above tol after max_iters steps.
+ * ------------------------------------------------------------------------------------------ */
+int cf_gmres_workspace_size(const cf_plan* plan, int64_t b, int32_t restart, size_t* bytes);
+int cf_gmres_solve_tiled(cf_plan* plan, const double* f_tiled, double dt, const double* b_tiled,
+                         double* x_tiled, int64_t b, int32_t restart, int32_t max_iters, double tol,
+                         const double* precond, int32_t precond_per_cell, int32_t* iters_out,
+                         double* relres_out, void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Learned block preconditioner (no counterpart in the reference).  A small FP32 network maps a
+ * cell's features (its coefficients and log10(dt nu)) to a correction Delta of the Maxwellian
+ * blocks: P_q = P_eq,q + scale * Delta_q.  x -> Linear -> GELU -> Linear -> GELU -> Linear,
+ * weights [out][in]; all products are this library's SGEMM kernels; Adam trains it.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct cf_mlp cf_mlp;
+int cf_mlp_create(cf_mlp** mlp, int32_t n_in, int32_t n_hidden, int32_t n_out, int32_t max_batch,
+                  uint64_t seed, int32_t device);
+int cf_mlp_destroy(cf_mlp* mlp);
+int cf_mlp_num_params(const cf_mlp* mlp, int64_t* n);
+/* dir 0: parameters device -> host, 1: host -> device, 2: gradients device -> host (flat layout
+ * W1, b1, W2, b2, W3, b3, each padded to a multiple of 64 floats). */
+int cf_mlp_copy(cf_mlp* mlp, float* host, int32_t dir);
+/* y[n][n_out] = net(x[n][n_in]) (device arrays); train != 0 keeps the activations for backward. */
+int cf_mlp_forward(cf_mlp* mlp, const float* x, float* y, int64_t n, int32_t train, void* stream);
+/* Parameter gradients of sum(dy .* y) for the last training forward pass on the same x. */
+int cf_mlp_backward(cf_mlp* mlp, const float* x, const float* dy, int64_t n, void* stream);
+int cf_mlp_adam_step(cf_mlp* mlp, float lr, float beta1, float beta2, float eps, float weight_decay,
+                     void* stream);
+/* Probe loss of P = P_eq + scale * Delta for n cells: with probe pairs v_p and a_p = A v_p
+ * (av, v: [n][n_probes][N_Q*K] FP32, block q at q*K; vnorm2: [n][n_probes] = |v_p|^2),
+ * L = mean over cells of (1/n_p) sum_p sum_q |P_q a_pq - v_pq|^2 / |v_p|^2, accumulated into
+ * *loss_dev (device), and dL/dDelta into grad [n][N_Q][K][K]. */
+int cf_precond_probe_loss(const float* delta, const double* peq, const float* av, const float* v,
+                          const float* vnorm2, float scale, int64_t n, int32_t n_probes, int32_t n_q,
+                          int32_t k, float* grad, double* loss_dev, void* stream);
+/* P [n][N_Q][K][K] (FP64) = P_eq + scale * Delta: the per-cell blocks cf_gmres_solve_tiled applies. */
+int cf_precond_assemble(const float* delta, const double* peq, double* P, float scale, int64_t n,
+                        int32_t n_q, int32_t k, void* stream);
 
 /* ------------------------------------------------------------------------------------------
  * Status and introspection

@@ -260,7 +260,7 @@ def test_kernel_paths_agree(L, K, B, cuda_available, oracle_lib):
     oracle_lib.af_batch(Qo, _cells_cm(cells), geo.labels, geo.vals, geo.ic_map, R, NQ, K)
     ref = Qo.transpose(2, 1, 0)
     outs = {}
-    for path in ("pair", "tile", "gather"):
+    for path in ("pair", "pair_l1", "tile", "gather"):
         op.set_kernel_path(path)
         Qf = op.q(f).cpu().numpy()
         assert per_cell_err(Qf, ref) <= TOL_FP64, f"{path}: {per_cell_err(Qf, ref):.3e}"
@@ -288,7 +288,7 @@ def test_tile_path_jacobian(L, K, B, cuda_available, oracle_lib):
     ref = ref.transpose(2, 1, 0)
     op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, NQ, K)
     ft, vt = torch.from_numpy(cells).cuda(), torch.from_numpy(v).cuda()
-    for path in ("pair", "tile"):
+    for path in ("pair", "pair_l1", "tile"):
         op.set_kernel_path(path)
         assert per_cell_err(op.jv(ft, vt).cpu().numpy(), ref) <= TOL_FP64
         assert np.array_equal(op.jv(ft, vt, exact=True).cpu().numpy(), ref)
