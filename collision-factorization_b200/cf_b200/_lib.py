@@ -28,7 +28,7 @@ FORMS = {"af": FORM_AF, "rf": FORM_RF, "af_exact": FORM_AF_EXACT, "rf_exact": FO
 EXPORTS = [
     "cf_angular_first", "cf_radial_first", "cf_contract_host", "cf_jacobian_apply_host",
     "cf_plan_create", "cf_plan_destroy", "cf_plan_get_info", "cf_plan_workspace_size",
-    "cf_q_device", "cf_q_device_ws", "cf_jv_device",
+    "cf_q_device", "cf_q_device_ws", "cf_jv_device", "cf_q_device_noalloc",
     "cf_gmres_workspace_size", "cf_gmres_solve_tiled",
     "cf_mlp_create", "cf_mlp_destroy", "cf_mlp_num_params", "cf_mlp_copy", "cf_mlp_forward", "cf_mlp_backward",
     "cf_mlp_adam_step", "cf_precond_probe_loss", "cf_precond_assemble",
@@ -76,6 +76,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_q_device_ws.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p, C.c_size_t,
                                    C.c_void_p]
     lib.cf_jv_device.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]
+    lib.cf_q_device_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]
     lib.cf_pack_cells.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, C.c_void_p]
     lib.cf_unpack_cells.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, C.c_void_p]
     lib.cf_q_tiled.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]

@@ -1,0 +1,82 @@
+// noalloc.cu -- the allocation-free variant of the batched Q(f) contraction.
+//
+// cf_q_device needs device scratch (the tiled copies of f and Q) and allocates it inside the plan
+// on first use.  Some callers cannot let a library call cudaMalloc: a host that owns every byte of
+// device memory through its own allocator, or a caller about to record its work into a stream
+// capture.  For them, cf_q_device_noalloc runs the same contraction with its scratch in the
+// file-scope array below instead.  The array is a fixed CF_NOALLOC_SCRATCH_BYTES on every device
+// that loads this module and stays allocated until the process exits.
+//
+// Host code may not pass g_noalloc_scratch to a kernel directly: on the host the symbol is a
+// host-side stand-in, not a device address.  The device address is looked up once per device,
+// with that device current, by cudaGetSymbolAddress on the first call made on that device.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "../../include/cf_b200.h"
+
+// Sets the message cf_last_error() returns (plan.cu; not part of the C ABI).
+void cf_set_last_error(const char* msg);
+
+namespace {
+
+constexpr size_t kScratchBytes = CF_NOALLOC_SCRATCH_BYTES;
+constexpr int kMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+std::mutex g_mu;
+void* g_scratch_ptr[kMaxDevices] = {};
+
+int scratch_for_device(int device, void** out) {
+    if (device < 0 || device >= kMaxDevices) {
+        cf_set_last_error("cf_q_device_noalloc: device index out of range");
+        return CF_ENODEVICE;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_scratch_ptr[device] == nullptr) {
+        int prev = -1;
+        if (cudaGetDevice(&prev) != cudaSuccess) return CF_ECUDA;
+        if (prev != device && cudaSetDevice(device) != cudaSuccess) return CF_ENODEVICE;
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (prev != device) cudaSetDevice(prev);
+        if (e != cudaSuccess || p == nullptr) {
+            cf_set_last_error((std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e)).c_str());
+            return CF_ECUDA;
+        }
+        g_scratch_ptr[device] = p;
+    }
+    *out = g_scratch_ptr[device];
+    return CF_OK;
+}
+
+}  // namespace
+
+extern "C" int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form,
+                                   void* stream) {
+    if (!plan) return CF_EINVAL;
+    cf_plan_info info;
+    int st = cf_plan_get_info(plan, &info);
+    if (st != CF_OK) return st;
+    size_t need = 0;
+    st = cf_plan_workspace_size(plan, b, 0, &need);
+    if (st != CF_OK) return st;
+    if (need > kScratchBytes) {
+        char msg[256];
+        snprintf(msg, sizeof(msg),
+                 "cf_q_device_noalloc: B = %lld cells of N_Q*K = %d need %zu bytes of scratch, more than the "
+                 "fixed %zu (use cf_q_device or cf_q_device_ws for larger batches)",
+                 (long long)b, info.n_q * info.k, need, kScratchBytes);
+        cf_set_last_error(msg);
+        return CF_ESHAPE;
+    }
+    void* scratch = nullptr;
+    st = scratch_for_device(info.device, &scratch);
+    if (st != CF_OK) return st;
+    return cf_q_device_ws(plan, q_dev, f_dev, b, form, scratch, kScratchBytes, stream);
+}
+

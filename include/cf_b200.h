@@ -152,6 +152,22 @@ int cf_plan_set_kernel_path(cf_plan* plan, int32_t path);
  * with CUDA events): the peak the FP64 forms are compared against. */
 int cf_fp64_fma_peak(int32_t device, double* tflops);
 
+/* Q_dev += Q(f_dev) for B cells without allocating anything: no cudaMalloc, cudaFree or other
+ * allocating routine runs inside this call.  No counterpart in the reference (its MEX kernels
+ * run on the host).  It is for callers that cannot let a library allocate device memory -- a
+ * host whose device memory is all owned by its own allocator, or code about to record work into
+ * a stream capture -- which cf_q_device does on its first use of a batch size.  The scratch (the
+ * tiled copies of f and Q) lives in a fixed array of CF_NOALLOC_SCRATCH_BYTES inside the library,
+ * which each device holds from the first call on that device until the process exits; batches
+ * whose 2 * ceil(B/32) * 32 * N_Q * K doubles do not fit are rejected with CF_ESHAPE (about 4300
+ * cells at N_Q*K = 968).  The first call on a device looks up the array's device address with
+ * that device current; make that first call before any stream capture.  All calls share the one
+ * array, so calls that overlap on the GPU (other streams, other host threads) race on it.  The
+ * plan itself is created beforehand with cf_plan_create, which does allocate. */
+#define CF_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
+int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form,
+                        void* stream);
+
 /* ------------------------------------------------------------------------------------------
  * Implicit solves: (I - dt J(f)) x = b per cell with restarted GMRES, FP64.  No counterpart in
  * the reference (it steps only explicitly, with a dense tensor: tutorial_stress_relaxation.m:77-91).
