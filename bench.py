@@ -42,7 +42,10 @@ WORKLOADS = {
     "hs_l10_k8_b4096": (10, 8, 4096, 1.0),
     "hs_l8_k8_b2048": (8, 8, 2048, 1.0),
     "hs_l16_k12_b1024": (16, 12, 1024, 1.0),
+    "implicit_hs_l8_k8_b2048": (8, 8, 2048, 1.0),
+    "ragged_hs_b16384": (10, 8, 16384, 1.0),  # largest bucket's (L, K); buckets in RAGGED_BUCKETS
 }
+RAGGED_BUCKETS = [(4, 4), (6, 6), (8, 6), (10, 8)]  # (L, K), drawn with RAGGED_WEIGHTS per cell
 R_FILES = {(10, 8): "R_hs_k7_l10_pad20.npy", (8, 8): "R_hs_k7_l8_pad20.npy"}
 
 
@@ -56,7 +59,11 @@ def parse_args(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="target length of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=20260)
-    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1"],
+    ap.add_argument("--train-states", type=int, default=100000)
+    ap.add_argument("--epochs", type=int, default=12)
+    ap.add_argument("--form", default="af", choices=["af", "af_sym", "af_exact", "rf"],
+                    help="form launched by --profile")
+    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split"],
                     help="kernel family of the angular-first contraction")
     ap.add_argument("--profile", action="store_true",
                     help="only build the workload and launch the contraction (steps+1 times); for ncu captures")
@@ -157,6 +164,8 @@ class ClockSampler:
 # distributed plumbing (timing only; the data path has no collective)
 # --------------------------------------------------------------------------------------------
 def dist_setup(args):
+    """Rank, world size and local device from the launcher's environment; a process group when
+    world > 1 (NCCL on GPUs; gloo where no GPU is visible, which the multi-rank host tests use)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -166,19 +175,25 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if not dist.is_initialized():
+            if torch.cuda.is_available():
+                torch.cuda.set_device(local)
+                dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                        device_id=torch.device("cuda", local))
+            else:
+                dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
 def dist_max(x: float, world: int) -> float:
+    """Max of x over the ranks (the timed interval of a weak-scaling run is the slowest rank's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -188,6 +203,18 @@ def dist_barrier(world: int):
         import torch.distributed as dist
 
         dist.barrier()
+
+
+def weak_rate(world: int, cells_per_rank: int, steps: int, local_seconds: float) -> tuple[float, float]:
+    """Whole-job cells per second of a weak-scaling run: every rank contracts its own cells, the job
+    takes as long as its slowest rank.  Returns (rate, max seconds)."""
+    t = dist_max(local_seconds, world)
+    return world * cells_per_rank * steps / t, t
+
+
+def rank_seed(seed: int, rank: int) -> int:
+    """Each rank draws its own cells (its shard of the job)."""
+    return seed + rank
 
 
 # --------------------------------------------------------------------------------------------
@@ -234,7 +261,7 @@ def run_ours(args):
     geo, R, r_source = make_operator(L, K, gamma, args.seed)
     NQ = geo.n_q
     M = NQ * K
-    cells = make_cells(L, K, B, seed=args.seed + rank)
+    cells = make_cells(L, K, B, seed=rank_seed(args.seed, rank))
     op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, NQ, K, device=local)
     op.set_kernel_path(args.path)
     lib = _lib.load()
@@ -258,8 +285,10 @@ def run_ours(args):
 
     _lib.check(lib.cf_pack_cells(op._h, int(fT.data_ptr()), int(f.data_ptr()), B, sh))
 
-    # accuracy of the fast form against the reference's exact operation order (bitwise = reference MEX)
-    step("af_exact")
+    # accuracy of the fast form against the reference's exact operation order (bitwise = reference MEX);
+    # the exact order is built for K <= 8, above that the plain FP64 form is the reference
+    ref_form = "af_exact" if K <= 8 else "af"
+    step(ref_form)
     Q_exact = Q.clone()
     step("af")
     num = (Q - Q_exact).abs().reshape(B, -1).amax(dim=1)
@@ -300,28 +329,59 @@ def run_ours(args):
     launches = _lib.launch_count() - launches0
     kern_ms = timed(kernel_only, args.steps)
     rf_ms = timed(lambda: step("rf"), max(2, args.steps // 4))
+    # the q2 <-> q3 folded form: accuracy against the exact form, then timing (step and kernel)
+    step("af_sym")
+    num = (Q - Q_exact).abs().reshape(B, -1).amax(dim=1)
+    err_sym = float((num / den).max())
+    sym_ms = timed(lambda: step("af_sym"), args.steps)
+    sym_kern_ms = timed(lambda: kernel_only("af_sym"), max(2, args.steps // 2))
     path_ms = {}
-    for path in ("pair", "pair_l1", "tile", "gather"):
+    for path in ("pair_split", "pair", "pair_l1", "tile", "gather"):
         try:
             op.set_kernel_path(path)
             path_ms[path] = timed(step, max(2, args.steps // 4))
         except Exception:
             path_ms[path] = None
     op.set_kernel_path(args.path)
-    exact_ms = timed(lambda: step("af_exact"), max(2, args.steps // 4))
+    exact_ms = timed(lambda: step("af_exact"), max(2, args.steps // 4)) if K <= 8 else None
+    # reduced-precision forms (FP32 contraction, FP64 accumulation of Q): error and throughput
+    f32 = {}
+    for form in ("af_f32", "af_sym_f32"):
+        try:
+            step(form)
+            num = (Q - Q_exact).abs().reshape(B, -1).amax(dim=1)
+            ms = timed(lambda: step(form), max(2, args.steps // 4))
+            f32[form] = {"cells_per_s": B * len(ms) / (sum(ms) / 1e3), "max_rel_err_vs_fp64": float((num / den).max()),
+                         "meets_1e-10": bool(float((num / den).max()) <= 1e-10)}
+        except Exception as e:
+            f32[form] = {"unavailable": str(e)[:160]}
     clk = clocks.stop()
     torch.cuda.synchronize(dev)
     dist_barrier(world)
 
-    total_s = dist_max(sum(step_ms) / 1e3, world)
-    value = world * B * args.steps / total_s
+    # the headline form: the fastest form within 1e-10 of the FP64 (exact-order) result
+    plain_s = sum(step_ms) / 1e3
+    sym_s = sum(sym_ms) / 1e3 * args.steps / len(sym_ms)
+    chosen = "af_sym" if (err_sym <= 1e-10 and sym_s < plain_s) else "af"
+    chosen_ms = sym_ms if chosen == "af_sym" else step_ms
+    value, total_s = weak_rate(world, B, args.steps, sum(chosen_ms) / 1e3 * args.steps / len(chosen_ms))
     ms_per_step = 1e3 * total_s / args.steps
-    kern_s = sum(kern_ms) / len(kern_ms) / 1e3
+    kern_list = sym_kern_ms if chosen == "af_sym" else kern_ms
+    kernel_only(chosen)
+    torch.cuda.synchronize(dev)
+    kern_name = {"pair": "af_pair_kernel (persistent, tile-resident, mirrored row pairs)",
+                 "pair_split": "af_pair_kernel, split variant (both mirrored rows per lane, k3 halves)",
+                 "pair_l1": "af_pair_kernel (R_t through L1)", "tile": "af_tile_kernel (persistent, tile-resident)",
+                 "gather": "af_kernel (gathers through L1/L2)"}.get(_lib.PATH_NAMES[op.info()["last_path"]], "?")
+    kern_s = sum(kern_list) / len(kern_list) / 1e3
     flops_launch = op.flops_q * B
     achieved_tf = flops_launch / kern_s / 1e12
+    sym_info = op.sym_info() if chosen == "af_sym" else None
+    exec_flops = (sym_info["flops_q"] if sym_info else op.flops_q) * B
+    exec_tf = exec_flops / kern_s / 1e12
 
-    # end to end through the host C-ABI entry point, pinned host buffers
-    e2e = run_e2e(op, geo, R, cells, K, args, world)
+    # end to end through the host C-ABI entry point, pinned host buffers, in the headline form
+    e2e = run_e2e(op, geo, R, cells, K, args, world, form=chosen)
 
     out = None
     if rank == 0:
@@ -337,7 +397,9 @@ def run_ours(args):
                 cpu = {"value": None, "unit": "cell-evals/s", "cores": None, "kind": "reference",
                        "sample": f"unavailable: {e}"}
         rf_rate = B / (sum(rf_ms) / len(rf_ms) / 1e3)
-        exact_rate = B / (sum(exact_ms) / len(exact_ms) / 1e3)
+        sym_rate = B * len(sym_ms) / (sum(sym_ms) / 1e3)
+        plain_rate = B * args.steps / (sum(step_ms) / 1e3)
+        exact_rate = B / (sum(exact_ms) / len(exact_ms) / 1e3) if exact_ms else None
         out = {
             "metric": METRIC,
             "value": value,
@@ -353,22 +415,32 @@ def run_ours(args):
             "data": "synthetic (seeded Maxwellians + N(0,1) exp(-0.6(k+l)) perturbation, amplitude 1e-2)",
             "config": {
                 "workload": args.workload, "L": L, "K": K, "M": M, "cells_per_gpu": B, "gamma": gamma,
-                "n_g": op.n_g, "n_l": op.n_l, "n_slices": op.n_slices, "form": "af (plain FP64)",
+                "n_g": op.n_g, "n_l": op.n_l, "n_slices": op.n_slices,
+                "form": {"af_sym": "af_sym (FP64, q2<->q3 folded operator)", "af": "af (plain FP64)"}[chosen],
                 "R": r_source, "l2": "flushed (256 MB write) before every timed step",
                 "parallelism": f"cells sharded, {B} per GPU, no collective",
             },
             "forms": {
-                "af": {"cells_per_s": B * args.steps / (sum(step_ms) / 1e3), "max_rel_err_vs_fp64": err_af},
-                "af_exact": {"cells_per_s": exact_rate, "max_rel_err_vs_fp64": 0.0},
+                "af": {"cells_per_s": plain_rate, "max_rel_err_vs_fp64": err_af},
+                "af_sym": {"cells_per_s": sym_rate, "max_rel_err_vs_fp64": err_sym},
+                "af_exact": {"cells_per_s": exact_rate, "max_rel_err_vs_fp64": 0.0} if exact_ms else
+                {"unavailable": "the exact operation order is built for K <= 8"},
+                "error_reference": {"af_exact": "the reference's exact operation order (bitwise equal to its MEX)",
+                                    "af": "the plain FP64 form (the exact order is built for K <= 8)"}[ref_form],
                 "rf": {"cells_per_s": rf_rate},
                 "af_by_kernel": {p: (B / (sum(v) / len(v) / 1e3) if v else None) for p, v in path_ms.items()},
-                "chosen": "af",
+                **f32,
+                "chosen": chosen,
+                "plain_cells_per_s": plain_rate,
+                "chosen_vs_plain": (B * args.steps / total_s) / plain_rate,
             },
             "invariants_abs_max": inv,
             "roofline": {
-                "bound": "fp64", "kernel": f"af_pair_kernel<K={K}> (persistent, tile-resident, mirrored row pairs)", "achieved": achieved_tf, "peak": peak_tf,
+                "bound": "fp64", "kernel": f"{kern_name}, K={K}" + (" on the folded operator" if chosen == "af_sym" else ""),
+                "achieved": achieved_tf, "peak": peak_tf,
                 "unit": "TFLOP/s", "frac": achieved_tf / peak_tf, "traffic": None,
                 "algorithmic_flop_per_launch": flops_launch, "kernel_ms": kern_s * 1e3,
+                "executed_flop_per_launch": exec_flops, "executed_tflops": exec_tf, "executed_frac": exec_tf / peak_tf,
                 "peak_source": f"measured on this GPU in this run: DFMA probe {dfma_tf:.2f}, cuBLAS DGEMM "
                                f"{dgemm_tf:.2f} TFLOP/s (max); MEASURED_PEAKS.json has no FP64 entry",
                 "hbm_gbs_algorithmic": 16.0 * M * B / kern_s / 1e9,
@@ -413,7 +485,7 @@ def dgemm_peak(dev, n: int = 8192, reps: int = 3) -> float:
     return 2.0 * n**3 / (best * 1e-3) / 1e12
 
 
-def run_e2e(op, geo, R, cells, K, args, world):
+def run_e2e(op, geo, R, cells, K, args, world, form="af"):
     """Same metric through the host-pointer C-ABI call (cf_contract_host): H2D f and Q, contract, D2H Q."""
     import ctypes
 
@@ -437,7 +509,7 @@ def run_e2e(op, geo, R, cells, K, args, world):
     def call():
         _lib.check(lib.cf_contract_host(ctypes.cast(Q_h.data_ptr(), D), ctypes.cast(f_h.data_ptr(), D), B,
                                         lab.ctypes.data_as(D), vals.ctypes.data_as(D), ic.ctypes.data_as(D),
-                                        Rr.ctypes.data_as(D), geo.n_g, n_l, NQ, K, _lib.FORM_AF))
+                                        Rr.ctypes.data_as(D), geo.n_g, n_l, NQ, K, _lib.FORMS[form]))
 
     for _ in range(2):
         Q_h.zero_()
@@ -453,7 +525,9 @@ def run_e2e(op, geo, R, cells, K, args, world):
     nbytes = B * NQ * K * 8
     return {"value": world * B * steps / tot, "unit": "cell-evals/s", "h2d_bytes_per_step": 2 * nbytes,
             "d2h_bytes_per_step": nbytes,
-            "path": "cf_contract_host (the MEX-compatible host entry point), pinned host buffers, synchronous"}
+            "form": form,
+            "path": "cf_contract_host (the MEX-compatible host entry point: content-keyed plan cache, chunks of "
+                    "cells copied in, contracted and copied back on three streams), pinned host buffers"}
 
 
 # --------------------------------------------------------------------------------------------
@@ -533,14 +607,251 @@ def run_profile(args):
     sh = int(torch.cuda.current_stream().cuda_stream)
     _lib.check(lib.cf_pack_cells(op._h, int(fT.data_ptr()), int(f.data_ptr()), B, sh))
     for _ in range(args.steps + 1):
-        _lib.check(lib.cf_q_tiled(op._h, int(QT.data_ptr()), int(fT.data_ptr()), B, _lib.FORM_AF, sh))
+        _lib.check(lib.cf_q_tiled(op._h, int(QT.data_ptr()), int(fT.data_ptr()), B, _lib.FORMS[args.form], sh))
     torch.cuda.synchronize()
     print(json.dumps({"profile": args.workload, "launches": args.steps + 1, "B": B}))
 
 
+def run_implicit(args):
+    """Implicit relaxation configuration: GMRES(30) on (I - dt J(f)) x = r to 1e-10, 2048 cells,
+    hard spheres L=8, K=8, dt*nu in {1, 10, 100}; Maxwellian block preconditioner vs the learned one."""
+    import torch
+
+    import cf_b200
+    from cf_b200 import implicit, workloads
+    from cf_b200.learned import LearnedPreconditioner
+
+    L, K, B = 8, 8, 2048
+    geo, R, r_source = make_operator(L, K, 1.0, args.seed)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+    t0 = time.perf_counter()
+    lp = LearnedPreconditioner(op, hidden=512, max_batch=4096, scale=0.1, seed=args.seed)
+    train = lp.make_samples(args.train_states, dt_nu_values=(1.0, 10.0, 100.0), n_probes=8, seed=args.seed,
+                            amp_range=(0.0, 0.3))
+    lp.fit_normalisation(train)
+    t_gen = time.perf_counter() - t0
+    hist = lp.train(train, epochs=args.epochs, batch=512, lr=1e-3)
+    t_train = time.perf_counter() - t0 - t_gen
+    del train
+    val = lp.make_samples(max(1000, args.train_states // 10), dt_nu_values=(1.0, 10.0, 100.0), n_probes=8,
+                          seed=args.seed + 7, amp_range=(0.0, 0.3))
+    gains = lp.calibrate(val)
+    val_loss = {f"{dtn:g}": {"maxwellian": lp.probe_loss(val, dtn / lp.nu, use_net=False),
+                             "learned": lp.probe_loss(val, dtn / lp.nu, use_net=True)} for dtn in (1.0, 10.0, 100.0)}
+    del val
+    cells = workloads.stress_cells(K, L, B, seed=args.seed + 1, amplitude=0.1)
+    rng = np.random.default_rng(args.seed + 2)
+    cells[:, 0, 4:9] *= rng.uniform(0.0, 3.0, size=(B, 1))
+    f = torch.from_numpy(cells).cuda()
+    rhs = op.q(f)
+    results = {}
+    for dtnu in (1.0, 10.0, 100.0):
+        dt = dtnu / lp.nu
+        row = {}
+        for name in ("block", "learned", "none"):
+            def solve():
+                P = (implicit.block_preconditioner(op, dt) if name == "block"
+                     else lp.predict(f, dt) if name == "learned" else None)
+                return implicit.gmres_solve(op, f, rhs, dt, restart=30, tol=1e-10, max_iters=3000, precond=P,
+                                            raise_on_timeout=False)
+            solve()  # warm-up
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            x, it, rel = solve()
+            torch.cuda.synchronize()
+            row[name] = {"seconds": time.perf_counter() - t, "iters_mean": float(it.mean()), "iters_max": int(it.max()),
+                         "relres_max": float(rel.max()), "converged": bool(np.all(rel <= 1e-10))}
+        row["speedup_learned_vs_block"] = row["block"]["seconds"] / row["learned"]["seconds"]
+        results[f"dt_nu={dtnu:g}"] = row
+    out = {"workload": "implicit_hs_l8_k8_b2048", "cells": B, "M": geo.n_q * K, "R": r_source,
+           "gmres": "GMRES(30), right block-Jacobi preconditioning, FP64, tol 1e-10 on |b - A x| / |b| per cell",
+           "learned": {"train_states": args.train_states, "epochs": args.epochs, "probes_per_state": 8,
+                       "loss_first": hist[0], "loss_last": hist[-1], "sample_s": t_gen, "train_s": t_train,
+                       "calibrated_gain_by_dt_nu": {f"{k:.3g}": v for k, v in gains.items()},
+                       "validation_probe_loss": val_loss},
+           "results": results}
+    print(json.dumps(out), flush=True)
+    op.close()
+    return out
+
+
+def run_ragged(args):
+    """Ragged batch: 16384 hard-sphere cells drawn 40/30/20/10 % from (L, K) in {(4,4), (6,6), (8,6), (10,8)},
+    one step = Q(f) for every cell through one CUDA-graph replay (layout passes, one fused persistent
+    launch for the angular-first buckets, the other buckets' kernels), forms and tail split autotuned."""
+    import torch
+
+    import cf_b200
+    from cf_b200 import _lib, workloads
+    from cf_b200.ragged import RaggedBatch, autotune
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    B = WORKLOADS[args.workload][2]
+    assign = workloads.ragged_assignment(B, seed=rank_seed(args.seed, rank))
+    counts = [int(np.sum(assign == b)) for b in range(len(RAGGED_BUCKETS))]
+    ops, geos, Rs, sources, fs_np = [], [], [], [], []
+    for b, (L, K) in enumerate(RAGGED_BUCKETS):
+        geo, R, src = make_operator(L, K, 1.0, args.seed + 17 * b)
+        geos.append(geo)
+        Rs.append(R)
+        sources.append(f"L={L} K={K}: {src}")
+        ops.append(cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K, device=local))
+        fs_np.append(make_cells(L, K, counts[b], seed=args.seed + rank * 101 + b))
+    t0 = time.perf_counter()
+    forms, tail, tune = autotune(ops, counts, candidates=("af_sym", "af", "rf"), tail_splits=(0, 4, 16), reps=5)
+    tune_s = time.perf_counter() - t0
+    rb = RaggedBatch(ops, counts, forms, tail_split=tail)
+    fs = [torch.from_numpy(c).to(dev) for c in fs_np]
+    qs = [torch.zeros_like(f) for f in fs]
+
+    # accuracy: every bucket against the reference's exact operation order
+    rb.q(fs, qs)
+    errs = []
+    for op, f, q in zip(ops, fs, qs):
+        qe = op.q(f, form="af_exact")
+        num = (q - qe).abs().reshape(q.shape[0], -1).amax(dim=1)
+        den = qe.abs().reshape(q.shape[0], -1).amax(dim=1).clamp_min(1e-300)
+        errs.append(float((num / den).max()) if q.shape[0] else 0.0)
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        for q in qs:
+            q.zero_()
+        rb.q_graph(fs, qs)
+
+    def step_eager():
+        for q in qs:
+            q.zero_()
+        rb.q(fs, qs)
+
+    def step_separate():  # the same forms, one library call per bucket (no fused launch, no graph)
+        for op, f, q, form in zip(ops, fs, qs, forms):
+            q.zero_()
+            op.q(f, out=q, form=form)
+
+    def timed(fn, steps):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for i in range(steps):
+            flush.fill_(float(i))
+            evs[i][0].record(stream)
+            fn()
+            evs[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        return [a.elapsed_time(b) for a, b in evs]
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+        step_eager()
+        step_separate()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(local)
+    dist_barrier(world)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    step_ms = timed(step, args.steps)
+    launches = rb.launches_per_step() * args.steps
+    eager_ms = timed(step_eager, max(2, args.steps // 2))
+    sep_ms = timed(step_separate, max(2, args.steps // 2))
+    step()
+    kern_ms = timed(rb.q_resident, max(2, args.steps // 2))  # the contraction alone (Q_tiled accumulates)
+    clk = clocks.stop()
+    torch.cuda.synchronize(dev)
+    dist_barrier(world)
+    value, total_s = weak_rate(world, B, args.steps, sum(step_ms) / 1e3)
+    kern_s = sum(kern_ms) / len(kern_ms) / 1e3
+    probe = ctypes_double()
+    _lib.check(_lib.load().cf_fp64_fma_peak(local, probe))
+    peak_tf = probe.value
+    achieved = rb.flops_q / kern_s / 1e12
+
+    # end to end: pinned host cells in, graph step, Q out, every step
+    f_h = [torch.from_numpy(c).pin_memory() for c in fs_np]
+    q_h = [torch.empty_like(t).pin_memory() for t in f_h]
+
+    def e2e_step():
+        for fh, f, q in zip(f_h, fs, qs):
+            f.copy_(fh, non_blocking=True)
+            q.zero_()
+        rb.q_graph(fs, qs)
+        for qh, q in zip(q_h, qs):
+            qh.copy_(q, non_blocking=True)
+        torch.cuda.synchronize(dev)
+
+    e2e_step()
+    t = time.perf_counter()
+    n_e2e = max(3, args.steps // 4)
+    for _ in range(n_e2e):
+        e2e_step()
+    e2e_s = dist_max(time.perf_counter() - t, world)
+    nbytes = sum(int(x.numel()) * 8 for x in f_h)
+
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                per = args.cpu_seconds / len(RAGGED_BUCKETS)
+                t_mix, desc, thr = 0.0, [], 0
+                for b, (L, K) in enumerate(RAGGED_BUCKETS):
+                    rate, n, dt, thr = cpu_reference_rate(geos[b], Rs[b], fs_np[b], K, per)
+                    t_mix += counts[b] / rate
+                    desc.append(f"{n} cells of L={L} K={K} in {dt:.1f} s")
+                cpu = {"value": B / t_mix, "unit": "cell-evals/s", "cores": thr, "kind": "reference",
+                       "sample": "angular_first_collision_kernel_mex compiled unmodified (-O3 -mavx2 -mfma), one call "
+                                 "per cell under an OpenMP loop, per bucket: " + "; ".join(desc)
+                                 + "; combined with the batch's bucket counts"}
+            except Exception as e:
+                cpu = {"value": None, "unit": "cell-evals/s", "cores": None, "kind": "reference",
+                       "sample": f"unavailable: {e}"}
+        out = {
+            "metric": METRIC, "value": value, "unit": "cell-evals/s", "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * total_s / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Maxwellians + N(0,1) exp(-0.6(k+l)) perturbation, amplitude 1e-2)",
+            "config": {"workload": args.workload, "cells_per_gpu": B, "gamma": 1.0,
+                       "buckets": [{"L": L, "K": K, "cells": c, "form": fm, "max_rel_err_vs_fp64": e}
+                                   for (L, K), c, fm, e in zip(RAGGED_BUCKETS, counts, forms, errs)],
+                       "tail_split": tail, "fused_units": rb.n_units, "ctas": rb.ctas, "smem_bytes": rb.smem_bytes,
+                       "R": sources, "l2": "flushed (256 MB write) before every timed step",
+                       "parallelism": f"cells sharded, {B} per GPU, no collective"},
+            "variants": {"graph_step_cells_per_s": value,
+                         "eager_step_cells_per_s": B * len(eager_ms) / (sum(eager_ms) / 1e3),
+                         "separate_calls_cells_per_s": B * len(sep_ms) / (sum(sep_ms) / 1e3),
+                         "contraction_only_cells_per_s": B / kern_s},
+            "autotune": dict(tune, seconds=tune_s),
+            "roofline": {"bound": "fp64", "kernel": "af_pair_ragged_kernel (one persistent launch over the buckets)",
+                         "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
+                         "traffic": None, "algorithmic_flop_per_launch": rb.flops_q, "kernel_ms": kern_s * 1e3,
+                         "peak_source": "DFMA probe measured on this GPU in this run"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * B * n_e2e / e2e_s, "unit": "cell-evals/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes,
+                    "path": "RaggedBatch.q_graph with pinned host f copied in and Q copied out every step"},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    rb.close()
+    for op in ops:
+        op.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return out
+
+
 def main(argv=None):
     args = parse_args(argv)
-    if args.profile:
+    if args.workload == "implicit_hs_l8_k8_b2048":
+        run_implicit(args)
+    elif args.workload == "ragged_hs_b16384" and args.impl == "ours" and not args.profile:
+        run_ragged(args)
+    elif args.profile:
         run_profile(args)
     elif args.impl == "reference":
         run_reference(args)

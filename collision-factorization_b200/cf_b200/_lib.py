@@ -15,20 +15,24 @@ _D = C.POINTER(C.c_double)
 _I64 = C.c_int64
 _I32 = C.c_int32
 
-CF_OK = 0
+CF_OK, CF_EINVAL, CF_ESHAPE, CF_EBADIDX, CF_ENONFINITE, CF_ECUDA, CF_ENOMEM, CF_ENODEVICE, CF_EUNSUPPORTED, \
+    CF_ETIMEOUT = range(10)
 STATUS_NAMES = {
     0: "CF_OK", 1: "CF_EINVAL", 2: "CF_ESHAPE", 3: "CF_EBADIDX", 4: "CF_ENONFINITE", 5: "CF_ECUDA",
     6: "CF_ENOMEM", 7: "CF_ENODEVICE", 8: "CF_EUNSUPPORTED", 9: "CF_ETIMEOUT",
 }
 
-FORM_AF, FORM_RF, FORM_AF_EXACT, FORM_RF_EXACT = 0, 1, 2, 3
-FORMS = {"af": FORM_AF, "rf": FORM_RF, "af_exact": FORM_AF_EXACT, "rf_exact": FORM_RF_EXACT}
+FORM_AF, FORM_RF, FORM_AF_EXACT, FORM_RF_EXACT, FORM_AF_SYM, FORM_AF_F32, FORM_AF_SYM_F32 = 0, 1, 2, 3, 4, 5, 6
+FORMS = {"af": FORM_AF, "rf": FORM_RF, "af_exact": FORM_AF_EXACT, "rf_exact": FORM_RF_EXACT, "af_sym": FORM_AF_SYM,
+         "af_f32": FORM_AF_F32, "af_sym_f32": FORM_AF_SYM_F32}
 
 # Every symbol the header declares; the tests check that the library exports all of them.
 EXPORTS = [
     "cf_angular_first", "cf_radial_first", "cf_contract_host", "cf_jacobian_apply_host",
     "cf_plan_create", "cf_plan_destroy", "cf_plan_get_info", "cf_plan_workspace_size",
     "cf_q_device", "cf_q_device_ws", "cf_jv_device", "cf_q_device_noalloc",
+    "cf_ragged_create", "cf_ragged_destroy", "cf_ragged_q", "cf_ragged_graph_launch", "cf_ragged_q_resident",
+    "cf_ragged_info", "cf_rk2_workspace_size", "cf_rk2_steps_tiled",
     "cf_gmres_workspace_size", "cf_gmres_solve_tiled",
     "cf_mlp_create", "cf_mlp_destroy", "cf_mlp_num_params", "cf_mlp_copy", "cf_mlp_forward", "cf_mlp_backward",
     "cf_mlp_adam_step", "cf_precond_probe_loss", "cf_precond_assemble",
@@ -47,8 +51,10 @@ class PlanInfo(C.Structure):
     _fields_ = [
         ("n_g", C.c_int64), ("n_slices", C.c_int64), ("n_l", C.c_int32), ("n_q", C.c_int32),
         ("k", C.c_int32), ("device", C.c_int32), ("flops_q", C.c_double), ("flops_jv", C.c_double),
-        ("device_bytes", C.c_int64),
+        ("device_bytes", C.c_int64), ("last_path", C.c_int32), ("reserved", C.c_int32),
     ]
+
+PATH_NAMES = {0: "none", 1: "gather", 2: "tile", 3: "pair", 4: "pair_l1", 5: "pair_split"}
 
 
 _lib = None
@@ -84,6 +90,14 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_fp64_fma_peak.argtypes = [_I32, C.POINTER(C.c_double)]
     lib.cf_plan_set_kernel_path.argtypes = [C.c_void_p, _I32]
     V = C.c_void_p
+    lib.cf_ragged_create.argtypes = [C.POINTER(V), V, V, V, _I32, _I32]
+    lib.cf_ragged_destroy.argtypes = [V]
+    lib.cf_ragged_q.argtypes = [V, V, V, V]
+    lib.cf_ragged_graph_launch.argtypes = [V, V, V, V]
+    lib.cf_ragged_q_resident.argtypes = [V, V]
+    lib.cf_rk2_workspace_size.argtypes = [V, _I64, C.POINTER(C.c_size_t)]
+    lib.cf_rk2_steps_tiled.argtypes = [V, V, _I64, C.c_double, _I32, _I32, V, C.c_size_t, V]
+    lib.cf_ragged_info.argtypes = [V, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(C.c_int64), C.POINTER(_I32)]
     lib.cf_mlp_create.argtypes = [C.POINTER(V), _I32, _I32, _I32, _I32, C.c_uint64, _I32]
     lib.cf_mlp_destroy.argtypes = [V]
     lib.cf_mlp_num_params.argtypes = [V, C.POINTER(C.c_int64)]
@@ -115,3 +129,7 @@ def check(status: int) -> None:
 
 def launch_count() -> int:
     return int(load().cf_launch_count())
+
+
+def version() -> str:
+    return load().cf_version().decode()

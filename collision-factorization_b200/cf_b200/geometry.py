@@ -229,3 +229,43 @@ def slice_count(geo: Geometry) -> int:
     q1 = geo.labels[:, 0]
     change = (np.diff(t) != 0) | (np.diff(q1) != 0)
     return int(1 + np.count_nonzero(change))
+
+
+def fold_q2q3(geo: Geometry, R: np.ndarray, K: int):
+    """The q2 <-> q3 folded operator (labels, vals, ic_map, R_sym), the same quadratic form as (geo, R).
+
+    Entries (q1,q2,q3) with l-triplet t = (l1,l2,l3) and their mirrors (q1,q3,q2) with
+    t' = (l1,l3,l2) contribute G R_t.(f2 (x) f3) + G' R_t'.(f3 (x) f2); with G = G' (real Gaunt
+    symmetry) this is G (R_t + R_t'^T23).(f2 (x) f3).  The folded list keeps entries with l2 < l3, or
+    l2 = l3 and q2 <= q3 (q2 = q3 at G/2), against R^S_t = R_t + R_t'^T23, renumbering the kept
+    triplets in order.  This is the host-side statement of what the library builds for
+    CF_FORM_AF_SYM (csrc/plan.cu, build_folded).
+    """
+    lab = geo.labels.astype(np.int64)
+    ic = geo.ic_map.astype(np.int64) - 1
+    l = np.floor(np.sqrt(lab - 1.0)).astype(np.int64)
+    n_l = int(ic.max()) + 1
+    trip = np.zeros((n_l, 3), dtype=np.int64)
+    trip[ic] = l
+    tindex = {tuple(t): i for i, t in enumerate(trip)}
+    keep_t = trip[:, 1] <= trip[:, 2]
+    tnew = np.cumsum(keep_t) - 1
+    R = np.asarray(R).reshape(K, K, K, -1, order="F")
+    Rs = []
+    for t in np.flatnonzero(keep_t):
+        tp = tindex[(trip[t, 0], trip[t, 2], trip[t, 1])]
+        Rs.append(R[:, :, :, t] + R[:, :, :, tp].transpose(0, 2, 1))
+    Rs = np.asfortranarray(np.stack(Rs, axis=3))
+    where = {tuple(r): i for i, r in enumerate(lab)}
+    rows, vals, ics = [], [], []
+    for z in range(lab.shape[0]):
+        q1, q2, q3 = lab[z]
+        l2, l3 = l[z, 1], l[z, 2]
+        if not (l2 < l3 or (l2 == l3 and q2 <= q3)):
+            continue
+        zp = where[(q1, q3, q2)]
+        g = 0.5 * geo.vals[z] if q2 == q3 else 0.5 * (geo.vals[z] + geo.vals[zp])
+        rows.append((q1, q2, q3))
+        vals.append(g)
+        ics.append(tnew[ic[z]] + 1)
+    return (np.asfortranarray(np.array(rows, dtype=np.float64)), np.array(vals), np.array(ics, dtype=np.float64), Rs)

@@ -94,6 +94,10 @@ class LearnedPreconditioner:
         self.mu = np.zeros(self.n_in, dtype=np.float32)
         self.sd = np.ones(self.n_in, dtype=np.float32)
         self.nu = abs(implicit.equilibrium_jacobian_blocks(op)[min(6, self.NQ - 1)][0, 0])
+        self.gain = {}  # log10(dt nu) (rounded) -> multiplier of the correction, from calibrate()
+
+    def _gain(self, dt) -> float:
+        return self.gain.get(round(math.log10(max(dt * self.nu, 1e-12)), 6), 1.0)
 
     def features(self, f, dt):
         """[B, M + 1] float32: the coefficients (standardised) and log10(dt nu)."""
@@ -120,8 +124,8 @@ class LearnedPreconditioner:
             x = self.features(f[b0:b1], dt)
             d = torch.empty((b1 - b0, self.n_out), dtype=torch.float32, device=f.device)
             self.net.forward(x, d)
-            _lib.check(_lib.load().cf_precond_assemble(_dp(d), _dp(peq), _dp(P[b0:b1]), self.scale, b1 - b0, self.NQ,
-                                                       self.K, _s()))
+            _lib.check(_lib.load().cf_precond_assemble(_dp(d), _dp(peq), _dp(P[b0:b1]), self.scale * self._gain(dt),
+                                                       b1 - b0, self.NQ, self.K, _s()))
         return P
 
     # ------------------------------------------------------------------ training
@@ -139,7 +143,9 @@ class LearnedPreconditioner:
         cells[:, 0, 0] = 1.0
         dts = rng.choice(np.asarray(dt_nu_values), size=n_states) / self.nu
         f = torch.from_numpy(cells).cuda(self.op.device)
-        v = torch.from_numpy(rng.standard_normal((n_states, n_probes, K, self.NQ))).cuda(self.op.device)
+        gen = torch.Generator(device=f.device)
+        gen.manual_seed(int(seed) + 12345)
+        v = torch.randn((n_states, n_probes, K, self.NQ), dtype=torch.float64, device=f.device, generator=gen)
         a = torch.empty_like(v)
         chunk = max(1, 65536 // n_probes)
         for s0 in range(0, n_states, chunk):
@@ -196,10 +202,14 @@ class LearnedPreconditioner:
                 m = x.shape[0]
                 self.net.forward(x, d[:m], train=True)
                 loss_dev.zero_()
+                # the gathered probe batches are held in names for the duration of the call: a pointer
+                # into a temporary would be released to the allocator (and reused) before the kernel runs
+                av_b = samples["av"][it].contiguous()
+                v_b = samples["v"][it].contiguous()
+                vn2_b = samples["vn2"][it].contiguous()
                 _lib.check(_lib.load().cf_precond_probe_loss(
-                    _dp(d), _dp(peq_cache[dt]), _dp(samples["av"][it].contiguous()), _dp(samples["v"][it].contiguous()),
-                    _dp(samples["vn2"][it].contiguous()), self.scale, m, samples["v"].shape[1], self.NQ, self.K,
-                    _dp(g), _dp(loss_dev), _s()))
+                    _dp(d), _dp(peq_cache[dt]), _dp(av_b), _dp(v_b), _dp(vn2_b), self.scale, m, samples["v"].shape[1],
+                    self.NQ, self.K, _dp(g), _dp(loss_dev), _s()))
                 self.net.backward(x, g[:m])
                 self.net.adam(lr=lr)
                 tot += float(loss_dev.item())
@@ -226,8 +236,47 @@ class LearnedPreconditioner:
                 self.net.forward(self.features(f[b0:b1], dt_value), d[b0:b1])
         g = torch.empty_like(d)
         loss = torch.zeros(1, dtype=torch.float64, device=dev)
+        av_b = samples["av"][it].contiguous()
+        v_b = samples["v"][it].contiguous()
+        vn2_b = samples["vn2"][it].contiguous()
         _lib.check(_lib.load().cf_precond_probe_loss(
-            _dp(d), _dp(peq), _dp(samples["av"][it].contiguous()), _dp(samples["v"][it].contiguous()),
-            _dp(samples["vn2"][it].contiguous()), self.scale, m, samples["v"].shape[1], self.NQ, self.K, _dp(g),
-            _dp(loss), _s()))
+            _dp(d), _dp(peq), _dp(av_b), _dp(v_b), _dp(vn2_b), self.scale * self._gain(dt_value), m,
+            samples["v"].shape[1], self.NQ, self.K, _dp(g), _dp(loss), _s()))
         return float(loss.item())
+
+    def calibrate(self, samples, max_gain: float = 2.0) -> dict:
+        """Least-squares multiplier of the network's correction, per time step, on held-out probes.
+
+        The probe loss of P_eq + s * scale * Delta is quadratic in s; its minimiser over the samples,
+        s* = -sum w <r0, D a> / sum w |D a|^2 (r0 = P_eq a - v, D = scale * Delta), clipped to
+        [0, max_gain], is kept for that time step.  s* = 0 (the Maxwellian blocks alone) is chosen
+        whenever the network does not lower the loss on these samples.
+        """
+        import torch
+
+        dev = samples["f"].device
+        out = {}
+        n_p = samples["v"].shape[1]
+        for dt_value in np.unique(samples["dt"]):
+            idx = np.flatnonzero(samples["dt"] == dt_value)
+            it = torch.as_tensor(idx, device=dev)
+            f = samples["f"][it]
+            m = f.shape[0]
+            d = torch.zeros((m, self.n_out), dtype=torch.float32, device=dev)
+            for b0 in range(0, m, self.net.max_batch):
+                b1 = min(m, b0 + self.net.max_batch)
+                self.net.forward(self.features(f[b0:b1], float(dt_value)), d[b0:b1])
+            D = d.double().view(m, self.NQ, self.K, self.K) * self.scale
+            peq = torch.as_tensor(implicit.block_preconditioner(self.op, float(dt_value)), device=dev)
+            a = samples["av"][it].double().view(m, n_p, self.NQ, self.K)
+            v = samples["v"][it].double().view(m, n_p, self.NQ, self.K)
+            w = (1.0 / samples["vn2"][it].double()).view(m, n_p, 1, 1)
+            r0 = torch.einsum("qij,npqj->npqi", peq, a) - v
+            da = torch.einsum("nqij,npqj->npqi", D, a)
+            num = float((w * r0 * da).sum())
+            den = float((w * da * da).sum())
+            s_opt = min(max(-num / den, 0.0), max_gain) if den > 0 else 0.0
+            key = round(math.log10(max(float(dt_value) * self.nu, 1e-12)), 6)
+            self.gain[key] = s_opt
+            out[float(dt_value) * self.nu] = s_opt
+        return out

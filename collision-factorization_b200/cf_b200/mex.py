@@ -93,8 +93,10 @@ def contract_batched(Q_out, f, labels, vals, ic_map, R, N_Q, K_len, form: str = 
                                     K, _lib.FORMS[form]))
 
 
-def collision_jacobian_apply_mex(out, f, v, labels, vals, ic_map, R, N_Q, K_len, exact: bool = False):
-    """out += J(f).v = Q(v,f) + Q(f,v) for each cell (host arrays [N_Q x K] or [N_Q x K x B], in place)."""
+def collision_jacobian_apply_mex(out, f, v, labels, vals, ic_map, R, N_Q, K_len, exact: int = 0):
+    """out += J(f).v = Q(v,f) + Q(f,v) for each cell (host arrays [N_Q x K] or [N_Q x K x B], in place).
+
+    exact: 0 fast, 1 the exact operation order, 2 the q2 <-> q3 folded operator."""
     lab, g, ic, Rr, n_g, n_l, NQ, K = _operator_args(labels, vals, ic_map, R, N_Q, K_len)
     if not isinstance(out, np.ndarray) or out.dtype != np.float64 or not out.flags.f_contiguous:
         raise _lib.CFError(1, "out must be a column-major float64 numpy array")
@@ -105,4 +107,4 @@ def collision_jacobian_apply_mex(out, f, v, labels, vals, ic_map, R, N_Q, K_len,
     B = f.size // (NQ * K)
     lib = _lib.load()
     _lib.check(lib.cf_jacobian_apply_host(_ptr(out), _ptr(f), _ptr(v), B, _ptr(lab), _ptr(g), _ptr(ic), _ptr(Rr),
-                                          n_g, n_l, NQ, K, int(bool(exact))))
+                                          n_g, n_l, NQ, K, int(exact)))

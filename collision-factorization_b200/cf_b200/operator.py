@@ -9,6 +9,7 @@ library's own sm_100a kernels.
 from __future__ import annotations
 
 import ctypes as C
+import hashlib
 
 import numpy as np
 
@@ -56,6 +57,7 @@ class CollisionOperator:
                                       Rr.ctypes.data_as(D), self.n_g, n_l, self.N_Q, self.K, int(device)))
         self._h = h
         self.device = int(device)
+        self._host_operator = (lab, v, ic, Rr)
         info = _lib.PlanInfo()
         _lib.check(lib.cf_plan_get_info(h, C.byref(info)))
         self.n_slices = int(info.n_slices)
@@ -79,9 +81,44 @@ class CollisionOperator:
         _lib.check(_lib.load().cf_plan_get_info(self._h, C.byref(inf)))
         return {f: getattr(inf, f) for f, _ in inf._fields_}
 
+    def content_digest(self) -> str:
+        """SHA-256 (hex, 16 chars) of the operator's arrays: names the operator in caches."""
+        if not hasattr(self, "_digest"):
+            h = hashlib.sha256()
+            for a in self._host_operator:
+                h.update(np.ascontiguousarray(a).tobytes())
+            h.update(f"{self.N_Q},{self.K}".encode())
+            self._digest = h.hexdigest()[:16]
+        return self._digest
+
+    def sym_info(self) -> dict:
+        """Sizes and FLOP counts of the q2 <-> q3 folded operator (built on first use)."""
+        import torch
+
+        f = torch.zeros((1, self.K, self.N_Q), dtype=torch.float64, device=f"cuda:{self.device}")
+        self.q(f, form="af_sym")  # builds the folded plan
+        from . import geometry  # noqa: F401
+
+        return dict(self._sym_counts) if hasattr(self, "_sym_counts") else self._fold_counts()
+
+    def _fold_counts(self) -> dict:
+        import numpy as np
+
+        from . import geometry
+
+        lab, vals, ic, R = self._host_operator
+        geo = geometry.Geometry(int(round(self.N_Q ** 0.5)) - 1, lab, vals, ic, None)
+        flab, fv, fic, _ = geometry.fold_q2q3(geo, np.zeros((self.K, self.K, self.K, self.n_l), order="F"), self.K)
+        fgeo = geometry.Geometry(geo.L, flab, fv, fic, None)
+        S = geometry.slice_count(fgeo)
+        K = self.K
+        self._sym_counts = {"n_g": int(flab.shape[0]), "n_slices": S,
+                            "flops_q": float(flab.shape[0] * (2 * K * K + K) + S * 2 * K ** 3)}
+        return dict(self._sym_counts)
+
     def set_kernel_path(self, path: str) -> None:
         """'auto' (default), 'gather', 'tile', 'pair' or 'pair_l1': the kernel family of the AF and J.v forms."""
-        code = {"auto": 0, "gather": 1, "tile": 2, "pair": 3, "pair_l1": 4}[path]
+        code = {"auto": 0, "gather": 1, "tile": 2, "pair": 3, "pair_l1": 4, "pair_split": 5}[path]
         _lib.check(_lib.load().cf_plan_set_kernel_path(self._h, code))
 
     def workspace_bytes(self, B: int, jacobian: bool = False) -> int:
@@ -120,13 +157,15 @@ class CollisionOperator:
         _lib.check(st)
         return out
 
-    def jv(self, f, v, out=None, exact: bool = False, stream=None):
-        """out += J(f).v = Q(v,f) + Q(f,v) for every cell; returns out."""
+    def jv(self, f, v, out=None, exact: bool = False, stream=None, folded: bool = False):
+        """out += J(f).v = Q(v,f) + Q(f,v) for every cell; returns out.
+
+        exact: the reference-style operation order; folded: the q2 <-> q3 folded operator."""
         import torch
 
         if out is None:
             out = torch.zeros_like(f)
         B = self._check_cells(f, v, out)
-        _lib.check(_lib.load().cf_jv_device(self._h, _dptr(out), _dptr(f), _dptr(v), B, int(bool(exact)),
-                                            _stream_handle(stream)))
+        mode = 2 if folded else int(bool(exact))
+        _lib.check(_lib.load().cf_jv_device(self._h, _dptr(out), _dptr(f), _dptr(v), B, mode, _stream_handle(stream)))
         return out

@@ -1,0 +1,194 @@
+"""Ragged batches: cells of several resolutions contracted in one persistent launch.
+
+Each bucket is a CollisionOperator (one (L, K) operator) with its own cells and its own FP64 form.
+``RaggedBatch.q`` computes Q for every bucket in one step of the library (cf_ragged_q): the
+angular-first buckets with K <= 8 share one fused persistent launch, any other bucket (radial-first,
+the exact forms, K > 8) runs its own kernels in the same step.  ``RaggedBatch.q_graph`` replays the
+step from a CUDA graph recorded on first use (cf_ragged_graph_launch), which is how a time stepper
+calls it once per step.
+
+``autotune`` picks each bucket's form (radial-first against angular-first, plain or q2 <-> q3
+folded) and the fused table's tail split by timing them on the device, and keeps the choice in a
+small JSON cache keyed by the device and the buckets' shapes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import hashlib
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib
+
+
+class RaggedBatch:
+    def __init__(self, operators, cells_per_bucket, forms=None, tail_split: int = 4):
+        self.ops = list(operators)
+        self.cells = [int(c) for c in cells_per_bucket]
+        n = len(self.ops)
+        if len(self.cells) != n:
+            raise _lib.CFError(_lib.CF_EINVAL, "one cell count per bucket")
+        self.forms = list(forms) if forms is not None else ["af"] * n
+        codes = [_lib.FORMS[f] for f in self.forms]
+        self.tail_split = int(tail_split)
+        plans = (C.c_void_p * n)(*[op._h.value for op in self.ops])
+        counts = (C.c_int64 * n)(*self.cells)
+        fc = (C.c_int32 * n)(*codes)
+        h = C.c_void_p()
+        _lib.check(_lib.load().cf_ragged_create(C.byref(h), plans, counts, fc, n, self.tail_split))
+        self._h = h
+        nu, ct, sm, nf = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int32()
+        _lib.check(_lib.load().cf_ragged_info(h, C.byref(nu), C.byref(ct), C.byref(sm), C.byref(nf)))
+        self.n_units, self.ctas, self.smem_bytes, self.n_fused = nu.value, ct.value, sm.value, nf.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.load().cf_ragged_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def flops_q(self) -> float:
+        """Algorithmic FLOPs of one step (every bucket's cells through its operator)."""
+        return float(sum(op.flops_q * c for op, c in zip(self.ops, self.cells)))
+
+    def _ptrs(self, fs, qs):
+        n = len(self.ops)
+        if len(fs) != n or len(qs) != n:
+            raise _lib.CFError(_lib.CF_EINVAL, "one f and one q array per bucket")
+        for op, f, q, c in zip(self.ops, fs, qs, self.cells):
+            shape = (c, op.K, op.N_Q)
+            if tuple(f.shape) != shape or tuple(q.shape) != shape or not f.is_contiguous() or not q.is_contiguous():
+                raise _lib.CFError(_lib.CF_ESHAPE, f"bucket arrays must be contiguous {shape} float64 CUDA tensors")
+        fp = (C.c_void_p * n)(*[int(f.data_ptr()) for f in fs])
+        qp = (C.c_void_p * n)(*[int(q.data_ptr()) for q in qs])
+        return fp, qp
+
+    def q(self, fs, qs, stream=None):
+        """qs[b] += Q(fs[b]) for every bucket in one step."""
+        import torch
+
+        fp, qp = self._ptrs(fs, qs)
+        s = int((stream or torch.cuda.current_stream()).cuda_stream)
+        _lib.check(_lib.load().cf_ragged_q(self._h, qp, fp, s))
+        return qs
+
+    def launches_per_step(self) -> int:
+        """Kernels one step launches: two layout passes in and one out per non-empty bucket, the fused
+        launch, and one contraction kernel per bucket outside it."""
+        nb = sum(1 for c in self.cells if c > 0)
+        sep = sum(1 for op, c, f in zip(self.ops, self.cells, self.forms)
+                  if c > 0 and not (f in ("af", "af_sym") and op.K <= 8))
+        return 3 * nb + (1 if self.n_fused else 0) + sep
+
+    def q_resident(self, stream=None):
+        """The contraction alone on the resident tiled buffers left by the last step."""
+        import torch
+
+        s = int((stream or torch.cuda.current_stream()).cuda_stream)
+        _lib.check(_lib.load().cf_ragged_q_resident(self._h, s))
+
+    def q_graph(self, fs, qs, stream=None):
+        """The same step replayed from a CUDA graph (recorded on first use for these buffers)."""
+        import torch
+
+        fp, qp = self._ptrs(fs, qs)
+        s = int((stream or torch.cuda.current_stream()).cuda_stream)
+        _lib.check(_lib.load().cf_ragged_graph_launch(self._h, qp, fp, s))
+        return qs
+
+
+# ------------------------------------------------------------------------------------- autotuning
+def _cache_path() -> Path:
+    root = os.environ.get("CF_B200_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "cf_b200")
+    return Path(root) / "ragged_autotune.json"
+
+
+def _key(ops, cells, candidates, tail_splits) -> str:
+    import torch
+
+    dev = torch.cuda.get_device_name(ops[0].device) if torch.cuda.is_available() else "none"
+    sig = [dev, _lib.version(), list(candidates), list(tail_splits)]
+    for op, c in zip(ops, cells):
+        sig.append([op.N_Q, op.K, op.n_g, op.n_l, int(c), op.content_digest()])
+    return hashlib.sha256(json.dumps(sig).encode()).hexdigest()[:32]
+
+
+def _time_step(rb: RaggedBatch, fs, qs, reps: int) -> float:
+    import torch
+
+    rb.q(fs, qs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = float("inf")
+    for _ in range(reps):
+        e0.record()
+        rb.q(fs, qs)
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    return best
+
+
+def autotune(ops, cells, candidates=("af_sym", "af", "rf"), tail_splits=(0, 4, 16), reps: int = 5,
+             use_cache: bool = True, seed: int = 0):
+    """Choose each bucket's form and the fused table's tail split by timing them.
+
+    Returns (forms, tail_split, report).  Each bucket's candidates are timed alone (a one-bucket ragged
+    step on that bucket's cells); a candidate the operator does not support (an unfoldable Gaunt list
+    for af_sym) is skipped.  Then the whole step is timed for each tail split with the chosen forms.
+    """
+    import torch
+
+    cells = [int(c) for c in cells]
+    key = _key(ops, cells, candidates, tail_splits)
+    path = _cache_path()
+    if use_cache and path.exists():
+        try:
+            hit = json.loads(path.read_text()).get(key)
+            if hit:
+                return hit["forms"], hit["tail_split"], dict(hit["report"], cached=True)
+        except (OSError, ValueError):
+            pass
+    rng = np.random.default_rng(seed)
+    fs = [torch.from_numpy(1e-2 * rng.standard_normal((c, op.K, op.N_Q))).cuda(op.device) for op, c in zip(ops, cells)]
+    qs = [torch.zeros_like(f) for f in fs]
+    forms, per_bucket = [], []
+    for op, c, f, q in zip(ops, cells, fs, qs):
+        times = {}
+        for form in candidates:
+            try:
+                rb = RaggedBatch([op], [c], [form], tail_split=4)
+            except _lib.CFError:
+                continue
+            times[form] = _time_step(rb, [f], [q], reps)
+            rb.close()
+        if not times:
+            raise _lib.CFError(_lib.CF_EUNSUPPORTED, f"no candidate form runs for bucket N_Q={op.N_Q} K={op.K}")
+        best = min(times, key=times.get)
+        forms.append(best)
+        per_bucket.append({"N_Q": op.N_Q, "K": op.K, "cells": c, "seconds": times, "chosen": best})
+    split_times = {}
+    for ts in tail_splits:
+        rb = RaggedBatch(ops, cells, forms, tail_split=ts)
+        split_times[int(ts)] = _time_step(rb, fs, qs, reps)
+        rb.close()
+    tail = min(split_times, key=split_times.get)
+    report = {"buckets": per_bucket, "tail_split_seconds": split_times, "cached": False}
+    if use_cache:
+        try:
+            path.parent.mkdir(parents=True, exist_ok=True)
+            data = json.loads(path.read_text()) if path.exists() else {}
+            data[key] = {"forms": forms, "tail_split": tail, "report": report}
+            path.write_text(json.dumps(data, indent=1))
+        except (OSError, ValueError):
+            pass
+    return forms, tail, report

@@ -30,6 +30,7 @@ struct DevOp {
     const uint32_t* e_q23;
     const double* e_g;
     const double* R;
+    const float* R32;  // FP32 copy of R for the FP32 form
     const int* item_q1;
     int n_items;  // number of q1 with at least one slice
     int n_q;

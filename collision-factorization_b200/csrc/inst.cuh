@@ -1,11 +1,55 @@
 // inst.cuh -- the body of one per-K translation unit (included by inst_k<K>.cu with CF_K defined).
 #pragma once
+#include <mutex>
+#include <vector>
+
 #include "kernels.cuh"
 #include "launch.cuh"
 #include "tile_kernels.cuh"
 #include "pair_kernels.cuh"
 
 namespace cf {
+
+// The dynamic shared-memory attribute and the resident CTAs per SM of a kernel, set and queried on
+// its first launch with a given shared-memory size on a device and remembered, so that later
+// launches (and launches recorded into a CUDA graph) make no attribute or occupancy calls.
+struct ResidentEntry {
+    const void* fn;
+    int dev;
+    size_t smem;
+    int per_sm;
+};
+static cudaError_t resident_ctas(const void* fn, int threads, size_t smem, int* per_sm) {
+    static std::mutex mu;
+    static std::vector<ResidentEntry> seen;
+    static std::vector<ResidentEntry> attr;  // per (fn, dev): the largest size the attribute allows
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    for (const ResidentEntry& r : seen)
+        if (r.fn == fn && r.dev == dev && r.smem == smem) {
+            *per_sm = r.per_sm;
+            return cudaSuccess;
+        }
+    ResidentEntry* a = nullptr;
+    for (ResidentEntry& r : attr)
+        if (r.fn == fn && r.dev == dev) a = &r;
+    if (!a || a->smem < smem) {
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        if (a)
+            a->smem = smem;
+        else
+            attr.push_back({fn, dev, smem, 0});
+    }
+    int n = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, smem);
+    if (e != cudaSuccess) return e;
+    seen.push_back({fn, dev, smem, n});
+    *per_sm = n;
+    return cudaSuccess;
+}
 
 template <int K, int P, bool EXACT, bool JV>
 static LaunchResult launch_af(const LaunchArgs& a) {
@@ -26,10 +70,8 @@ static LaunchResult launch_tile(const LaunchArgs& a) {
     const size_t smem = tile_smem_bytes<K>(M, W, JV);
     if (smem + 256 > a.max_smem || a.counter == nullptr) return {-1, 0, cudaSuccess, PATH_TILE};
     auto kern = af_tile_kernel<K, W, EXACT, JV>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return {5, 0, e, PATH_TILE};
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem);
+    cudaError_t e = resident_ctas((const void*)kern, W * 32, smem, &per_sm);
     if (e != cudaSuccess) return {5, 0, e, PATH_TILE};
     if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_TILE};
     const int64_t ctas = (int64_t)per_sm * a.n_sms;
@@ -67,16 +109,15 @@ static inline UnitPlan plan_units(int64_t n_cells, int64_t ctas) {
     return {(int)n_ht, (int)n_whole, split, (int)(n_whole + rem * split)};
 }
 
-template <int K, int W, bool EXACT, bool JV, bool RG>
+template <int K, int W, bool EXACT, bool JV, bool RG, typename T = double, bool SPLIT = false>
 static LaunchResult launch_pair(const LaunchArgs& a) {
     const int M = a.op.n_q * K;
-    const size_t smem = pair_smem_bytes<K>(M, W, JV, RG);
+    const size_t smem = pair_smem_bytes<K, T>(M, W, JV, RG);
     if (smem + 256 > a.max_smem || a.counter == nullptr || a.pitems == nullptr) return {-1, 0, cudaSuccess, PATH_PAIR};
-    auto kern = af_pair_kernel<K, W, EXACT, JV, RG>;
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return {5, 0, e, PATH_PAIR};
+    static_assert(!SPLIT || (!EXACT && !JV && !RG && K % 2 == 0), "the split variant is the fast Q form");
+    auto kern = af_pair_kernel<K, W, EXACT, JV, RG, T, SPLIT>;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, smem);
+    cudaError_t e = resident_ctas((const void*)kern, W * 32, smem, &per_sm);
     if (e != cudaSuccess) return {5, 0, e, PATH_PAIR};
     if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_PAIR};
     const int64_t ctas = (int64_t)per_sm * a.n_sms;
@@ -86,9 +127,18 @@ static LaunchResult launch_pair(const LaunchArgs& a) {
     e = cudaMemsetAsync(a.counter, 0, sizeof(int), a.stream);
     if (e != cudaSuccess) return {5, 0, e, PATH_PAIR};
     const unsigned grid = (unsigned)(up.n_units < ctas ? up.n_units : ctas);
-    kern<<<grid, W * 32, smem, a.stream>>>(a.op, sc, a.fT, a.vT, a.QT);
+    const T* fT;
+    const T* vT;
+    if constexpr (sizeof(T) == 8) {
+        fT = a.fT;
+        vT = a.vT;
+    } else {
+        fT = a.fT32;
+        vT = nullptr;
+    }
+    kern<<<grid, W * 32, smem, a.stream>>>(a.op, sc, fT, vT, a.QT);
     e = cudaGetLastError();
-    return {e == cudaSuccess ? 0 : 5, 1, e, PATH_PAIR};
+    return {e == cudaSuccess ? 0 : 5, 1, e, SPLIT ? PATH_PAIR_SPLIT : (RG ? PATH_PAIR_L1 : PATH_PAIR)};
 }
 
 template <int K, bool EXACT>
@@ -107,10 +157,33 @@ constexpr int tile_W(int K, bool jv) { return jv ? (K >= 8 ? 12 : 16) : 16; }
 
 template <int K>
 static LaunchResult launch_for_k(const LaunchArgs& a) {
+    if (a.f32) {
+        // FP32 form: the pair kernel in FP32 (angular first only), R staged in shared memory when the
+        // FP32 tile leaves room for it, else read through L1
+        if constexpr (K % 2 == 0 && K <= 12) {
+            if (a.what != OP_AF || a.exact) return {8, 0, cudaSuccess, PATH_PAIR};
+            LaunchResult r{-1, 0, cudaSuccess, PATH_PAIR};
+            if constexpr (K <= 8)
+                if (a.path == PATH_PAIR_SPLIT) r = launch_pair<K, 8, false, false, false, float, true>(a);
+            if (r.status == -1) r = launch_pair<K, 8, false, false, false, float>(a);
+            if (r.status == -1) r = launch_pair<K, 8, false, false, true, float>(a);
+            if (r.status == -1) return {8, 0, cudaSuccess, PATH_PAIR};
+            return r;
+        } else {
+            return {8, 0, cudaSuccess, PATH_PAIR};
+        }
+    }
     if (a.what == OP_RF) return a.exact ? launch_rf<K, true>(a) : launch_rf<K, false>(a);
     const bool jv = a.what == OP_JV;
+    if constexpr (K <= 8 && K % 2 == 0) {
+        if (a.path == PATH_PAIR_SPLIT && !jv && !a.exact) {
+            const LaunchResult r = launch_pair<K, 8, false, false, false, double, true>(a);
+            if (r.status != -1) return r;
+        }
+    }
+    // PATH_PAIR_SPLIT: the split variant where it applies (fast Q form, K even), else the pair kernel
     if constexpr (K <= 8) {
-        if (a.path == PATH_AUTO || a.path == PATH_PAIR || a.path == PATH_PAIR_L1) {
+        if (a.path == PATH_AUTO || a.path == PATH_PAIR || a.path == PATH_PAIR_L1 || a.path == PATH_PAIR_SPLIT) {
             LaunchResult r;
             if (a.path == PATH_PAIR_L1) {
                 if (jv)
@@ -127,7 +200,7 @@ static LaunchResult launch_for_k(const LaunchArgs& a) {
             if (a.path != PATH_AUTO) return {8, 0, cudaSuccess, a.path};
         }
     } else {
-        if (a.path == PATH_PAIR || a.path == PATH_PAIR_L1) return {8, 0, cudaSuccess, a.path};
+        if (a.path == PATH_PAIR || a.path == PATH_PAIR_L1 || a.path == PATH_PAIR_SPLIT) return {8, 0, cudaSuccess, a.path};
     }
     if constexpr (K % 2 == 0 && K <= 8) {
         if (a.path == PATH_AUTO || a.path == PATH_TILE) {

@@ -11,7 +11,7 @@ namespace cf {
 enum Op { OP_AF = 0, OP_RF = 1, OP_JV = 2 };
 
 // Kernel families for the angular-first / Jacobian forms.
-enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3, PATH_PAIR_L1 = 4 };
+enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3, PATH_PAIR_L1 = 4, PATH_PAIR_SPLIT = 5 };
 
 struct LaunchArgs {
     DevOp op;
@@ -34,6 +34,9 @@ struct LaunchArgs {
     const int* pbin_begin;
     const int* pbin_item;
     const int2* pitems;
+    // FP32 form: tiled FP32 copies of f (and v) in place of fT / vT
+    bool f32;
+    const float* fT32;
 };
 
 // Status codes mirror cf_status: 0 ok, 5 CUDA error, 8 unsupported, 2 shape.

@@ -8,8 +8,9 @@ namespace cf {
 // ----------------------------------------------------------------------------------------
 // Layout passes: MEX-native cell-major [B][N_Q*K] (m = q + k*N_Q)  <->  tiled [tile][q*K+k][32]
 // ----------------------------------------------------------------------------------------
+template <typename TO>
 __global__ void __launch_bounds__(256) pack_tiles_kernel(const double* __restrict__ src,
-                                                         double* __restrict__ dst, int64_t B,
+                                                         TO* __restrict__ dst, int64_t B,
                                                          int nq, int K) {
     __shared__ double sm[32][33];
     const int M = nq * K;
@@ -26,12 +27,12 @@ __global__ void __launch_bounds__(256) pack_tiles_kernel(const double* __restric
         const int m = m0 + j;
         if (m < M) {
             const int q = m % nq, k = m / nq;
-            dst[(tile * M + (int64_t)q * K + k) * 32 + tx] = sm[tx][j];
+            dst[(tile * M + (int64_t)q * K + k) * 32 + tx] = (TO)sm[tx][j];
         }
     }
 }
 
-__global__ void __launch_bounds__(256) unpack_tiles_kernel(const double* __restrict__ src,
+static __global__ void __launch_bounds__(256) unpack_tiles_kernel(const double* __restrict__ src,
                                                            double* __restrict__ dst, int64_t B,
                                                            int nq, int K) {
     __shared__ double sm[32][33];
@@ -58,7 +59,7 @@ __global__ void __launch_bounds__(256) unpack_tiles_kernel(const double* __restr
 
 // FP64 FMA throughput probe: kProbeChains independent DFMA chains per thread.
 constexpr int kProbeChains = 8;
-__global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double* sink, int iters, double a) {
+static __global__ void __launch_bounds__(256) fp64_fma_probe_kernel(double* sink, int iters, double a) {
     double x[kProbeChains];
 #pragma unroll
     for (int c = 0; c < kProbeChains; ++c) x[c] = threadIdx.x * 1e-3 + c;

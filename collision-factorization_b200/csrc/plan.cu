@@ -8,6 +8,9 @@
 #include <cstdio>
 #include <cstring>
 #include <list>
+#include <map>
+#include <unordered_map>
+#include <array>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -47,8 +50,16 @@ int fail(int status, const char* fmt, ...) {
     } while (0)
 
 constexpr int kMaxK = 16;
+constexpr int kCounterSlots = 64;  // work-queue heads per plan (one per stream in use)
+constexpr int kHostStreams = 3;    // streams of the chunked host entry points
+constexpr int64_t kHostChunkMin = 512;
 
 }  // namespace
+
+// Internal view of a plan for the ragged (multi-operator) launcher in ragged.cu.
+__attribute__((visibility("hidden"))) int cf_plan_internal_view(const cf_plan* plan, DevOp* op,
+                                                                const int** pbin_begin, const int** pbin_item,
+                                                                const int2** pitems, int* n_sms, size_t* max_smem);
 
 // Lets the other translation units of the library report through cf_last_error().
 __attribute__((visibility("hidden"))) void cf_set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
@@ -70,24 +81,39 @@ struct cf_plan {
     uint32_t* d_e_q23 = nullptr;
     double* d_e_g = nullptr;
     double* d_R = nullptr;
+    float* d_R32 = nullptr;  // FP32 copy of R for CF_FORM_AF_F32
     int* d_item_q1 = nullptr;
     int* d_bin_begin = nullptr;  // q1 bins of the tile kernel's work units (bin 0 = all, 1..4, 5..20)
     int* d_bin_q1 = nullptr;
-    int* d_counter = nullptr;    // work-queue head of the tile kernel
+    // work-queue heads of the persistent kernels: one slot per stream (kCounterSlots slots, assigned
+    // on first use of a stream, least recently assigned slot reused beyond that), so launches on
+    // different streams never share a counter; allocated with the plan, nothing is allocated later
+    int* d_counter = nullptr;
+    std::vector<std::pair<cudaStream_t, int>> counter_slots;  // most recently assigned last
+    std::mutex counter_mu;
     int* d_pbin_begin = nullptr; // bins over pair items (same layout as the q1 bins)
     int* d_pbin_item = nullptr;
     int2* d_pitems = nullptr;    // (qa, qb) rows contracted by the two half-warps; qb = -1: no mirror
     int n_pairs = 0, n_pair_items = 0;
     int n_sms = 0;
     size_t max_smem = 0;
-    int path = 0;  // cf::Path: 0 automatic, 1 gather kernels, 2 tile-resident kernels
+    int path = 0;  // cf::Path requested: 0 automatic, 1 gather, 2 tile, 3 pair, 4 pair (R via L1), 5 split pair
+    int last_path = 0;  // family of the last angular-first / J.v launch (of this plan or its folded twin)
+    cf_plan* parent = nullptr;  // for a folded twin: the plan it folds
     // scratch owned by the plan (tiled copies; device copies of host inputs)
     void* d_ws = nullptr;
     size_t ws_bytes = 0;
     double* d_io = nullptr;
     size_t io_bytes = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t host_streams[kHostStreams] = {};  // chunked host path: copies overlap the contraction
     std::mutex mu;
+    // q2 <-> q3 folded operator (built on first use of CF_FORM_AF_SYM); fold_status != 0 if the
+    // COO list is not symmetric in its last two indices
+    cf_plan* sym = nullptr;
+    int fold_status = -1;
+    std::mutex sym_mu;
+    std::vector<double> h_labels, h_vals, h_ic, h_R;  // host copies kept for building the folded operator
 
     DevOp op() const {
         DevOp o;
@@ -97,6 +123,7 @@ struct cf_plan {
         o.e_q23 = d_e_q23;
         o.e_g = d_e_g;
         o.R = d_R;
+        o.R32 = d_R32;
         o.item_q1 = d_item_q1;
         o.n_items = n_items;
         o.n_q = n_q;
@@ -170,13 +197,20 @@ int upload(T** dst, const std::vector<T>& src, int64_t& bytes) {
     return CF_OK;
 }
 
+void free_plan_memory(cf_plan* p);
 void free_plan_memory(cf_plan* p) {
+    if (p->sym) {
+        free_plan_memory(p->sym);
+        delete p->sym;
+        p->sym = nullptr;
+    }
     cudaFree(p->d_q1_begin);
     cudaFree(p->d_slice_t);
     cudaFree(p->d_slice_e);
     cudaFree(p->d_e_q23);
     cudaFree(p->d_e_g);
     cudaFree(p->d_R);
+    cudaFree(p->d_R32);
     cudaFree(p->d_item_q1);
     cudaFree(p->d_bin_begin);
     cudaFree(p->d_bin_q1);
@@ -187,6 +221,8 @@ void free_plan_memory(cf_plan* p) {
     cudaFree(p->d_ws);
     cudaFree(p->d_io);
     if (p->stream) cudaStreamDestroy(p->stream);
+    for (cudaStream_t& hs : p->host_streams)
+        if (hs) cudaStreamDestroy(hs);
 }
 
 // Build the q1-grouped run structure (host) and upload it.
@@ -316,14 +352,16 @@ int build_plan(cf_plan* p, const double* labels, const double* vals, const doubl
     CF_TRY(upload(&p->d_e_q23, e_q23, bytes));
     CF_TRY(upload(&p->d_e_g, e_g, bytes));
     CF_TRY(upload(&p->d_R, Rv, bytes));
+    std::vector<float> R32(Rv.begin(), Rv.end());
+    CF_TRY(upload(&p->d_R32, R32, bytes));
     CF_TRY(upload(&p->d_item_q1, items, bytes));
     CF_TRY(upload(&p->d_bin_begin, bin_begin, bytes));
     CF_TRY(upload(&p->d_bin_q1, bin_q1, bytes));
     CF_TRY(upload(&p->d_pbin_begin, pbin_begin, bytes));
     CF_TRY(upload(&p->d_pbin_item, pbin_item, bytes));
     CF_TRY(upload(&p->d_pitems, pitems, bytes));
-    CF_CUDA(cudaMalloc((void**)&p->d_counter, sizeof(int)));
-    bytes += sizeof(int);
+    CF_CUDA(cudaMalloc((void**)&p->d_counter, kCounterSlots * sizeof(int)));
+    bytes += kCounterSlots * sizeof(int);
     int dev = 0, optin = 0;
     CF_CUDA(cudaGetDevice(&dev));
     CF_CUDA(cudaDeviceGetAttribute(&p->n_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -342,11 +380,29 @@ size_t tiled_bytes(const cf_plan* p, int64_t B) {
 // ------------------------------------------------------------------------------------------
 // Kernel dispatch over K (each K lives in its own translation unit, inst.cu)
 // ------------------------------------------------------------------------------------------
+int* counter_for(const cf_plan* pc, cudaStream_t st) {
+    cf_plan* p = const_cast<cf_plan*>(pc);
+    std::lock_guard<std::mutex> lk(p->counter_mu);
+    auto& v = p->counter_slots;
+    for (size_t i = 0; i < v.size(); ++i)
+        if (v[i].first == st) return p->d_counter + v[i].second;
+    int slot;
+    if ((int)v.size() < kCounterSlots) {
+        slot = (int)v.size();
+    } else {
+        slot = v.front().second;
+        v.erase(v.begin());
+    }
+    v.push_back({st, slot});
+    return p->d_counter + slot;
+}
+
 int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const double* vT, double* QT, int64_t B,
-             cudaStream_t st) {
+             cudaStream_t st, const float* fT32 = nullptr) {
     const int64_t nt = n_tiles_for(B);
     cf::LaunchArgs a{p->op(), fT, vT, QT, nt, B, st, what, exact, p->path, p->d_bin_begin, p->d_bin_q1,
-                     p->d_counter, p->n_sms, p->max_smem, p->d_pbin_begin, p->d_pbin_item, p->d_pitems};
+                     counter_for(p, st), p->n_sms, p->max_smem, p->d_pbin_begin, p->d_pbin_item, p->d_pitems,
+                     fT32 != nullptr, fT32};
     cf::LaunchResult r{8, 0, cudaSuccess};
     switch (p->k) {
 #define CF_K(KK) \
@@ -357,6 +413,11 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
         default: return fail(CF_EUNSUPPORTED, "K = %d not built", p->k);
     }
     g_launches += r.launches;
+    if (r.status == CF_OK && r.launches > 0 && what != cf::OP_RF) {
+        cf_plan* pm = const_cast<cf_plan*>(p);
+        pm->last_path = r.path;
+        if (pm->parent) pm->parent->last_path = r.path;
+    }
     if (r.status == CF_ECUDA) return fail(CF_ECUDA, "kernel launch: %s", cudaGetErrorString(r.cuda));
     if (r.status == CF_EUNSUPPORTED)
         return fail(CF_EUNSUPPORTED, "form or kernel path not built for K = %d (exact angular-first needs K <= 8; "
@@ -371,7 +432,19 @@ int launch_pack(const cf_plan* p, const double* src, double* dst, int64_t B, cud
     if (nt == 0) return CF_OK;
     if (nt > 65535) return fail(CF_ESHAPE, "B = %lld exceeds %d cells per call", (long long)B, 65535 * CF_TILE);
     dim3 grid((M + 31) / 32, (unsigned)nt), block(32, 8);
-    cf::pack_tiles_kernel<<<grid, block, 0, st>>>(src, dst, B, p->n_q, p->k);
+    cf::pack_tiles_kernel<double><<<grid, block, 0, st>>>(src, dst, B, p->n_q, p->k);
+    g_launches++;
+    CF_CUDA(cudaGetLastError());
+    return CF_OK;
+}
+
+int launch_pack32(const cf_plan* p, const double* src, float* dst, int64_t B, cudaStream_t st) {
+    const int M = p->n_q * p->k;
+    const int64_t nt = n_tiles_for(B);
+    if (nt == 0) return CF_OK;
+    if (nt > 65535) return fail(CF_ESHAPE, "B = %lld exceeds %d cells per call", (long long)B, 65535 * CF_TILE);
+    dim3 grid((M + 31) / 32, (unsigned)nt), block(32, 8);
+    cf::pack_tiles_kernel<float><<<grid, block, 0, st>>>(src, dst, B, p->n_q, p->k);
     g_launches++;
     CF_CUDA(cudaGetLastError());
     return CF_OK;
@@ -389,8 +462,10 @@ int launch_unpack(const cf_plan* p, const double* src, double* dst, int64_t B, c
 }
 
 // Q_dev (cell-major) += op(f_dev[, v_dev]) using the tiled workspace ws (>= 2 or 3 tiled buffers).
+int get_sym(cf_plan* p, cf_plan** out);
+
 int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_dev, const double* v_dev,
-               int64_t B, void* ws, size_t ws_bytes, cudaStream_t st) {
+               int64_t B, void* ws, size_t ws_bytes, cudaStream_t st, bool sym = false, bool f32 = false) {
     if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
     if (B == 0 || p->n_g == 0) return CF_OK;
     if (!q_dev || !f_dev || (what == 2 && !v_dev)) return fail(CF_EINVAL, "null device buffer");
@@ -400,11 +475,16 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
     double* fT = (double*)ws;
     double* QT = (double*)((char*)ws + tb);
     double* vT = what == 2 ? (double*)((char*)ws + 2 * tb) : nullptr;
-    const int64_t nt = n_tiles_for(B);
-    CF_TRY(launch_pack(p, f_dev, fT, B, st));
+    float* fT32 = f32 ? reinterpret_cast<float*>(fT) : nullptr;  // FP32 tiles use half of the f slot
+    if (f32)
+        CF_TRY(launch_pack32(p, f_dev, fT32, B, st));
+    else
+        CF_TRY(launch_pack(p, f_dev, fT, B, st));
     if (what == 2) CF_TRY(launch_pack(p, v_dev, vT, B, st));
     CF_TRY(launch_pack(p, q_dev, QT, B, st));
-    CF_TRY(dispatch(p, what, exact, fT, vT, QT, B, st));
+    cf_plan* target = p;
+    if (sym) CF_TRY(get_sym(p, &target));
+    CF_TRY(dispatch(target, what, exact, fT, vT, QT, B, st, fT32));
     CF_TRY(launch_unpack(p, QT, q_dev, B, st));
     return CF_OK;
 }
@@ -451,6 +531,12 @@ int plan_create(cf_plan** out, const double* labels, const double* vals, const d
     p->n_l = n_g > 0 ? n_l : std::max(n_l, 0);
     p->n_g = n_g;
     int s = build_plan(p, labels, vals, ic_map, R);
+    if (s == CF_OK && n_g > 0) {
+        p->h_labels.assign(labels, labels + 3 * n_g);
+        p->h_vals.assign(vals, vals + n_g);
+        p->h_ic.assign(ic_map, ic_map + n_g);
+        p->h_R.assign(R, R + (size_t)k * k * k * n_l);
+    }
     if (s == CF_OK) {
         cudaError_t e = cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) s = fail(CF_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
@@ -465,16 +551,143 @@ int plan_create(cf_plan** out, const double* labels, const double* vals, const d
 }
 
 // ------------------------------------------------------------------------------------------
+// q2 <-> q3 folding.  The real Gaunt coefficients are symmetric in their last two indices, so
+// the entries (q1,q2,q3,t = (l1,l2,l3)) and (q1,q3,q2,t' = (l1,l3,l2)) contribute
+//   G R_t.(f2 (x) f3) + G' R_t'.(f3 (x) f2) = G (R_t + R_t'^T23).(f2 (x) f3)   (G = G').
+// The folded operator keeps the entries with l2 < l3, or l2 = l3 and q2 <= q3 (diagonal q2 = q3
+// at G/2), against R^S_t = R_t + R_t'^T23: about half the entries and half the slices, the same
+// quadratic form.  J.v on it is the same Jacobian (the folded bilinear form is not symmetric, but
+// its symmetric part is).
+// ------------------------------------------------------------------------------------------
+int isqrt_l(double q) {
+    int64_t x = (int64_t)q - 1, l = (int64_t)std::sqrt((double)x);
+    while ((l + 1) * (l + 1) <= x) ++l;
+    while (l * l > x) --l;
+    return (int)l;
+}
+
+int build_folded(const cf_plan* p, std::vector<double>& lab2, std::vector<double>& val2, std::vector<double>& ic2,
+                 std::vector<double>& R2, int64_t& ng2, int& nl2) {
+    const int64_t NG = p->n_g;
+    const int K = p->k, NL = p->n_l, NQ = p->n_q;
+    const size_t K3 = (size_t)K * K * K;
+    const double* lab = p->h_labels.data();
+    const double* val = p->h_vals.data();
+    const double* ic = p->h_ic.data();
+    std::vector<std::array<int, 3>> trip(NL, {-1, -1, -1});
+    std::unordered_map<int64_t, int64_t> where;
+    where.reserve((size_t)NG * 2);
+    double gmax = 0.0;
+    for (int64_t z = 0; z < NG; ++z) {
+        const int t = (int)ic[z] - 1;
+        const std::array<int, 3> l = {isqrt_l(lab[z]), isqrt_l(lab[z + NG]), isqrt_l(lab[z + 2 * NG])};
+        if (trip[t][0] < 0) trip[t] = l;
+        else if (trip[t] != l) return fail(CF_EUNSUPPORTED, "fold: ic_map %d mixes l-triplets", t + 1);
+        const int64_t key = (((int64_t)lab[z] - 1) * NQ + ((int64_t)lab[z + NG] - 1)) * NQ + ((int64_t)lab[z + 2 * NG] - 1);
+        where[key] = z;
+        gmax = std::max(gmax, std::fabs(val[z]));
+    }
+    std::map<std::array<int, 3>, int> tindex;
+    for (int t = 0; t < NL; ++t)
+        if (trip[t][0] >= 0) tindex[trip[t]] = t;
+    std::vector<int> tnew(NL, -1);
+    nl2 = 0;
+    R2.clear();
+    for (int t = 0; t < NL; ++t) {
+        if (trip[t][0] < 0 || trip[t][1] > trip[t][2]) continue;
+        auto it = tindex.find({trip[t][0], trip[t][2], trip[t][1]});
+        if (it == tindex.end()) return fail(CF_EUNSUPPORTED, "fold: l-triplet of ic_map %d has no mirror", t + 1);
+        const int tp = it->second;
+        tnew[t] = nl2++;
+        const double* Rt = p->h_R.data() + (size_t)t * K3;
+        const double* Rp = p->h_R.data() + (size_t)tp * K3;
+        for (int k3 = 0; k3 < K; ++k3)
+            for (int k2 = 0; k2 < K; ++k2)
+                for (int k1 = 0; k1 < K; ++k1)
+                    R2.push_back(Rt[k1 + K * k2 + K * K * k3] + Rp[k1 + K * k3 + K * K * k2]);
+    }
+    std::vector<double> q1v, q2v, q3v;
+    val2.clear();
+    ic2.clear();
+    for (int64_t z = 0; z < NG; ++z) {
+        const int t = (int)ic[z] - 1;
+        const int l2 = trip[t][1], l3 = trip[t][2];
+        const double q1 = lab[z], q2 = lab[z + NG], q3 = lab[z + 2 * NG];
+        if (!(l2 < l3 || (l2 == l3 && q2 <= q3))) continue;
+        const int64_t key = (((int64_t)q1 - 1) * NQ + ((int64_t)q3 - 1)) * NQ + ((int64_t)q2 - 1);
+        auto it = where.find(key);
+        if (it == where.end()) return fail(CF_EUNSUPPORTED, "fold: entry %lld has no (q1,q3,q2) mirror", (long long)z + 1);
+        const double gp = val[it->second];
+        if (std::fabs(gp - val[z]) > 1e-10 * gmax)
+            return fail(CF_EUNSUPPORTED, "fold: G(q1,q2,q3) and G(q1,q3,q2) differ at entry %lld", (long long)z + 1);
+        q1v.push_back(q1);
+        q2v.push_back(q2);
+        q3v.push_back(q3);
+        val2.push_back(q2 == q3 ? 0.5 * val[z] : 0.5 * (val[z] + gp));
+        ic2.push_back((double)(tnew[t] + 1));
+    }
+    ng2 = (int64_t)q1v.size();
+    lab2.clear();
+    lab2.insert(lab2.end(), q1v.begin(), q1v.end());
+    lab2.insert(lab2.end(), q2v.begin(), q2v.end());
+    lab2.insert(lab2.end(), q3v.begin(), q3v.end());
+    return CF_OK;
+}
+
+// The folded plan of p (created on first use).
+int get_sym(cf_plan* p, cf_plan** out) {
+    std::lock_guard<std::mutex> lk(p->sym_mu);
+    if (p->sym) {
+        *out = p->sym;
+        return CF_OK;
+    }
+    if (p->fold_status > 0) return fail(p->fold_status, "this operator cannot be folded (see the first failure)");
+    std::vector<double> lab2, val2, ic2, R2;
+    int64_t ng2 = 0;
+    int nl2 = 0;
+    int st = build_folded(p, lab2, val2, ic2, R2, ng2, nl2);
+    if (st != CF_OK) {
+        p->fold_status = st;
+        return st;
+    }
+    cf_plan* s = nullptr;
+    st = plan_create(&s, lab2.data(), val2.data(), ic2.data(), R2.data(), ng2, nl2, p->n_q, p->k, p->device);
+    if (st != CF_OK) return st;
+    s->path = p->path;
+    s->parent = p;
+    s->h_labels.clear();  // the folded plan is never folded again
+    p->sym = s;
+    p->fold_status = 0;
+    *out = s;
+    return CF_OK;
+}
+
+// ------------------------------------------------------------------------------------------
 // Content-keyed cache of plans for the MEX-style host entry points
 // ------------------------------------------------------------------------------------------
 uint64_t hash_words(const double* a, int64_t n, uint64_t h) {
+    // four independent multiply-xorshift lanes (the dependency chain of one lane bounds the speed)
     const uint64_t* w = reinterpret_cast<const uint64_t*>(a);
-    for (int64_t i = 0; i < n; ++i) {
-        h ^= w[i];
-        h *= 0x100000001b3ULL;
-        h ^= h >> 29;
+    uint64_t l[4] = {h, h ^ 0x9e3779b97f4a7c15ULL, h ^ 0xbf58476d1ce4e5b9ULL, h ^ 0x94d049bb133111ebULL};
+    int64_t i = 0;
+    for (; i + 4 <= n; i += 4)
+        for (int j = 0; j < 4; ++j) {
+            l[j] ^= w[i + j];
+            l[j] *= 0x100000001b3ULL;
+            l[j] ^= l[j] >> 29;
+        }
+    for (; i < n; ++i) {
+        l[0] ^= w[i];
+        l[0] *= 0x100000001b3ULL;
+        l[0] ^= l[0] >> 29;
     }
-    return h;
+    uint64_t r = (uint64_t)n;
+    for (int j = 0; j < 4; ++j) {
+        r ^= l[j];
+        r *= 0x100000001b3ULL;
+        r ^= r >> 31;
+    }
+    return r;
 }
 
 struct CacheEntry {
@@ -530,7 +743,7 @@ int cached_plan(cf_plan** out, const double* labels, const double* vals, const d
 // Host-pointer contraction: upload, run, download.  what: 0 AF, 1 RF, 2 JV.
 int run_host(int what, bool exact, double* Q, const double* f, const double* v, int64_t B, const double* labels,
              const double* vals, const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
-             int32_t k) {
+             int32_t k, bool sym = false, bool f32 = false) {
     if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
     if (!Q || !f || (what == 2 && !v)) return fail(CF_EINVAL, "null host buffer");
     cf_plan* p = nullptr;
@@ -538,31 +751,81 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
     if (B == 0 || n_g == 0) return CF_OK;
     std::lock_guard<std::mutex> lk(p->mu);
     DeviceGuard guard(p->device);
-    const size_t cell_bytes = (size_t)B * n_q * k * sizeof(double);
+    const int64_t M = (int64_t)n_q * k;
+    const size_t cell_bytes = (size_t)B * M * sizeof(double);
     const int nbuf = what == 2 ? 3 : 2;
     CF_TRY(ensure_io(p, cell_bytes * nbuf));
-    const size_t tb = tiled_bytes(p, B);
-    CF_TRY(ensure_ws(p, tb * nbuf));
     double* dQ = p->d_io;
     double* df = (double*)((char*)p->d_io + cell_bytes);
     double* dv = what == 2 ? (double*)((char*)p->d_io + 2 * cell_bytes) : nullptr;
-    CF_CUDA(cudaMemcpyAsync(dQ, Q, cell_bytes, cudaMemcpyHostToDevice, p->stream));
-    CF_CUDA(cudaMemcpyAsync(df, f, cell_bytes, cudaMemcpyHostToDevice, p->stream));
-    if (dv) CF_CUDA(cudaMemcpyAsync(dv, v, cell_bytes, cudaMemcpyHostToDevice, p->stream));
-    CF_TRY(run_device(p, what, exact, dQ, df, dv, B, p->d_ws, p->ws_bytes, p->stream));
-    CF_CUDA(cudaMemcpyAsync(Q, dQ, cell_bytes, cudaMemcpyDeviceToHost, p->stream));
-    CF_CUDA(cudaStreamSynchronize(p->stream));
-    return CF_OK;
+    if (B < 2 * kHostChunkMin) {
+        const size_t tb = tiled_bytes(p, B);
+        CF_TRY(ensure_ws(p, tb * nbuf));
+        CF_CUDA(cudaMemcpyAsync(dQ, Q, cell_bytes, cudaMemcpyHostToDevice, p->stream));
+        CF_CUDA(cudaMemcpyAsync(df, f, cell_bytes, cudaMemcpyHostToDevice, p->stream));
+        if (dv) CF_CUDA(cudaMemcpyAsync(dv, v, cell_bytes, cudaMemcpyHostToDevice, p->stream));
+        CF_TRY(run_device(p, what, exact, dQ, df, dv, B, p->d_ws, p->ws_bytes, p->stream, sym, f32));
+        CF_CUDA(cudaMemcpyAsync(Q, dQ, cell_bytes, cudaMemcpyDeviceToHost, p->stream));
+        CF_CUDA(cudaStreamSynchronize(p->stream));
+        return CF_OK;
+    }
+    // Chunked: chunk c goes up, is contracted and comes back on stream c mod kHostStreams, so the
+    // host<->device copies of one chunk overlap the contraction of the others (pinned host memory
+    // makes the copies asynchronous; pageable memory still gives the right answer, serialised).
+    for (cudaStream_t& hs : p->host_streams)
+        if (!hs) CF_CUDA(cudaStreamCreateWithFlags(&hs, cudaStreamNonBlocking));
+    int64_t n_chunks = std::min<int64_t>(8, B / kHostChunkMin);
+    const int64_t per = (B + n_chunks - 1) / n_chunks;
+    const int64_t chunk = (per + CF_TILE - 1) / CF_TILE * CF_TILE;  // whole 32-cell tiles per chunk
+    n_chunks = (B + chunk - 1) / chunk;
+    const size_t tbc = tiled_bytes(p, chunk) * nbuf;
+    CF_TRY(ensure_ws(p, tbc * kHostStreams));
+    int st = CF_OK;
+    for (int64_t c = 0; c < n_chunks && st == CF_OK; ++c) {
+        cudaStream_t s = p->host_streams[c % kHostStreams];
+        const int64_t b0 = c * chunk, bc = std::min(chunk, B - b0);
+        const size_t off = (size_t)b0 * M, nb = (size_t)bc * M * sizeof(double);
+        void* ws = (char*)p->d_ws + (size_t)(c % kHostStreams) * tbc;
+        cudaError_t e = cudaMemcpyAsync(dQ + off, Q + off, nb, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(df + off, f + off, nb, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && dv) e = cudaMemcpyAsync(dv + off, v + off, nb, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+            break;
+        }
+        st = run_device(p, what, exact, dQ + off, df + off, dv ? dv + off : nullptr, bc, ws, tbc, s, sym, f32);
+        if (st == CF_OK) {
+            e = cudaMemcpyAsync(Q + off, dQ + off, nb, cudaMemcpyDeviceToHost, s);
+            if (e != cudaSuccess) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+        }
+    }
+    for (cudaStream_t hs : p->host_streams) {
+        const cudaError_t e = cudaStreamSynchronize(hs);
+        if (e != cudaSuccess && st == CF_OK) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+    }
+    return st;
 }
 
-int form_what(int form, bool& exact) {
+int form_what(int form, bool& exact, bool& sym, bool& f32) {
+    sym = false;
+    f32 = false;
     switch (form) {
+        case CF_FORM_AF_F32: exact = false; f32 = true; return 0;
+        case CF_FORM_AF_SYM_F32: exact = false; f32 = true; sym = true; return 0;
         case CF_FORM_AF: exact = false; return 0;
         case CF_FORM_RF: exact = false; return 1;
         case CF_FORM_AF_EXACT: exact = true; return 0;
         case CF_FORM_RF_EXACT: exact = true; return 1;
+        case CF_FORM_AF_SYM: exact = false; sym = true; return 0;
         default: return -1;
     }
+}
+
+// J.v mode argument: 0 fast, 1 exact operation order, 2 folded operator
+bool jv_mode(int mode, bool& exact, bool& sym) {
+    exact = mode == 1;
+    sym = mode == 2;
+    return mode >= 0 && mode <= 2;
 }
 
 }  // namespace
@@ -588,17 +851,19 @@ int cf_contract_host(double* Q, const double* f, int64_t b, const double* labels
                      const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k,
                      int32_t form) {
     g_last_error.clear();
-    bool exact = false;
-    const int what = form_what(form, exact);
+    bool exact = false, sym = false, f32 = false;
+    const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
-    return run_host(what, exact, Q, f, nullptr, b, labels, vals, ic_map, R, n_g, n_l, n_q, k);
+    return run_host(what, exact, Q, f, nullptr, b, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym, f32);
 }
 
 int cf_jacobian_apply_host(double* out, const double* f, const double* v, int64_t b, const double* labels,
                            const double* vals, const double* ic_map, const double* R, int64_t n_g, int32_t n_l,
                            int32_t n_q, int32_t k, int32_t exact) {
     g_last_error.clear();
-    return run_host(2, exact != 0, out, f, v, b, labels, vals, ic_map, R, n_g, n_l, n_q, k);
+    bool ex = false, sym = false;
+    if (!jv_mode(exact, ex, sym)) return fail(CF_EINVAL, "J.v mode %d is not 0 (fast), 1 (exact) or 2 (folded)", exact);
+    return run_host(2, ex, out, f, v, b, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym);
 }
 
 int cf_plan_create(cf_plan** plan, const double* labels, const double* vals, const double* ic_map, const double* R,
@@ -630,6 +895,8 @@ int cf_plan_get_info(const cf_plan* plan, cf_plan_info* info) {
     info->flops_q = plan->flops_q;
     info->flops_jv = plan->flops_jv;
     info->device_bytes = plan->dev_bytes + (int64_t)plan->ws_bytes + (int64_t)plan->io_bytes;
+    info->last_path = plan->last_path;
+    info->reserved = 0;
     return CF_OK;
 }
 
@@ -644,34 +911,37 @@ int cf_q_device_ws(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b,
                    size_t workspace_bytes, void* stream) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    bool exact = false;
-    const int what = form_what(form, exact);
+    bool exact = false, sym = false, f32 = false;
+    const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
     DeviceGuard guard(plan->device);
-    return run_device(plan, what, exact, q_dev, f_dev, nullptr, b, workspace, workspace_bytes, (cudaStream_t)stream);
+    return run_device(plan, what, exact, q_dev, f_dev, nullptr, b, workspace, workspace_bytes, (cudaStream_t)stream,
+                      sym, f32);
 }
 
 int cf_q_device(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form, void* stream) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    bool exact = false;
-    const int what = form_what(form, exact);
+    bool exact = false, sym = false, f32 = false;
+    const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
     std::lock_guard<std::mutex> lk(plan->mu);
     DeviceGuard guard(plan->device);
     CF_TRY(ensure_ws(plan, tiled_bytes(plan, b) * 2));
-    return run_device(plan, what, exact, q_dev, f_dev, nullptr, b, plan->d_ws, plan->ws_bytes, (cudaStream_t)stream);
+    return run_device(plan, what, exact, q_dev, f_dev, nullptr, b, plan->d_ws, plan->ws_bytes, (cudaStream_t)stream,
+                      sym, f32);
 }
 
 int cf_jv_device(cf_plan* plan, double* out_dev, const double* f_dev, const double* v_dev, int64_t b, int32_t exact,
                  void* stream) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
+    bool ex = false, sym = false;
+    if (!jv_mode(exact, ex, sym)) return fail(CF_EINVAL, "J.v mode %d is not 0 (fast), 1 (exact) or 2 (folded)", exact);
     std::lock_guard<std::mutex> lk(plan->mu);
     DeviceGuard guard(plan->device);
     CF_TRY(ensure_ws(plan, tiled_bytes(plan, b) * 3));
-    return run_device(plan, 2, exact != 0, out_dev, f_dev, v_dev, b, plan->d_ws, plan->ws_bytes,
-                      (cudaStream_t)stream);
+    return run_device(plan, 2, ex, out_dev, f_dev, v_dev, b, plan->d_ws, plan->ws_bytes, (cudaStream_t)stream, sym);
 }
 
 int cf_pack_cells(const cf_plan* plan, double* dst_tiled, const double* src_cells, int64_t b, void* stream) {
@@ -695,14 +965,17 @@ int cf_unpack_cells(const cf_plan* plan, double* dst_cells, const double* src_ti
 int cf_q_tiled(cf_plan* plan, double* q_tiled, const double* f_tiled, int64_t b, int32_t form, void* stream) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    bool exact = false;
-    const int what = form_what(form, exact);
+    bool exact = false, sym = false, f32 = false;
+    const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
+    if (f32) return fail(CF_EUNSUPPORTED, "the FP32 forms read FP64 cells through cf_q_device / cf_contract_host");
     if (b < 0) return fail(CF_ESHAPE, "B is negative");
     if (b == 0 || plan->n_g == 0) return CF_OK;
     if (!q_tiled || !f_tiled) return fail(CF_EINVAL, "null device buffer");
     DeviceGuard guard(plan->device);
-    return dispatch(plan, what, exact, f_tiled, nullptr, q_tiled, b, (cudaStream_t)stream);
+    cf_plan* target = plan;
+    if (sym) CF_TRY(get_sym(plan, &target));
+    return dispatch(target, what, exact, f_tiled, nullptr, q_tiled, b, (cudaStream_t)stream);
 }
 
 int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const double* v_tiled, int64_t b,
@@ -712,18 +985,47 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
     if (b < 0) return fail(CF_ESHAPE, "B is negative");
     if (b == 0 || plan->n_g == 0) return CF_OK;
     if (!out_tiled || !f_tiled || !v_tiled) return fail(CF_EINVAL, "null device buffer");
+    bool ex = false, sym = false;
+    if (!jv_mode(exact, ex, sym)) return fail(CF_EINVAL, "J.v mode %d is not 0 (fast), 1 (exact) or 2 (folded)", exact);
     DeviceGuard guard(plan->device);
-    return dispatch(plan, cf::OP_JV, exact != 0, f_tiled, v_tiled, out_tiled, b, (cudaStream_t)stream);
+    cf_plan* target = plan;
+    if (sym) CF_TRY(get_sym(plan, &target));
+    return dispatch(target, cf::OP_JV, ex, f_tiled, v_tiled, out_tiled, b, (cudaStream_t)stream);
 }
+
+}  // extern "C"
+
+__attribute__((visibility("hidden"))) int cf_plan_internal_view(const cf_plan* plan, DevOp* op,
+                                                                const int** pbin_begin, const int** pbin_item,
+                                                                const int2** pitems, int* n_sms, size_t* max_smem) {
+    *op = plan->op();
+    *pbin_begin = plan->d_pbin_begin;
+    *pbin_item = plan->d_pbin_item;
+    *pitems = plan->d_pitems;
+    *n_sms = plan->n_sms;
+    *max_smem = plan->max_smem;
+    return CF_OK;
+}
+
+// The plan's q2 <-> q3 folded twin (built on first use, owned by the plan).
+__attribute__((visibility("hidden"))) int cf_plan_folded(cf_plan* plan, cf_plan** folded) {
+    DeviceGuard guard(plan->device);
+    return get_sym(plan, folded);
+}
+
+extern "C" {
 
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    if (path < 0 || path > 4)
-        return fail(CF_EINVAL, "kernel path %d is not 0 (auto), 1 (gather), 2 (tile), 3 (pair) or 4 (pair, R via L1)",
+    if (path < 0 || path > 5)
+        return fail(CF_EINVAL,
+                    "kernel path %d is not 0 (auto), 1 (gather), 2 (tile), 3 (pair), 4 (pair, R via L1) or 5 (pair, "
+                    "split rows)",
                     path);
     std::lock_guard<std::mutex> lk(plan->mu);
     plan->path = path;
+    if (plan->sym) plan->sym->path = path;
     return CF_OK;
 }
 

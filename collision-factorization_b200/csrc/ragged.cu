@@ -1,0 +1,427 @@
+// ragged.cu -- one persistent launch over cells of several resolutions (L, K).
+//
+// A ragged batch is a set of buckets, each a plan (one (L, K) operator) with its own cells and its
+// own form.  Buckets in the angular-first forms CF_FORM_AF / CF_FORM_AF_SYM with K <= 8 are "fused":
+// one kernel runs the pair routine of pair_kernels.cuh for all of them in a single launch.  The work
+// units of the fused buckets -- whole 16-cell half-tiles first, heaviest buckets first, then the last
+// half-tiles split into 4 or 16 q1-pair bins (or not split) -- sit in one table that persistent CTAs
+// drain through a device counter; a unit names its bucket, and the CTA stages that bucket's tile and
+// switches to the pair routine compiled for the bucket's K.  Shared memory and registers are sized
+// for the largest fused bucket.  Any other bucket (radial-first, the exact forms, K > 8) runs its
+// own plan's kernels on its tiled buffers in the same step.
+//
+// Each step is: pack every bucket's cells into its tiled buffer, the fused launch, the separate
+// buckets, unpack.  The sequence has no host synchronisation and no allocation, so it is recorded
+// once into a CUDA graph (cf_ragged_graph_launch) and replayed per time step.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/cf_b200.h"
+#include "common.cuh"
+#include "layout.cuh"
+#include "pair_kernels.cuh"
+
+void cf_set_last_error(const char* msg);
+int cf_plan_internal_view(const cf_plan* plan, DevOp* op, const int** pbin_begin, const int** pbin_item,
+                          const int2** pitems, int* n_sms, size_t* max_smem);
+int cf_plan_folded(cf_plan* plan, cf_plan** folded);
+
+namespace {
+
+constexpr int kRW = 8;                  // warps per CTA
+constexpr int kMaxK = 8;                // buckets of K <= 8 (FP64 pair routine)
+constexpr int kRBuf = kMaxK * kMaxK * kMaxK;
+
+struct Bucket {
+    DevOp op;
+    const int* pbin_begin;
+    const int* pbin_item;
+    const int2* pitems;
+    const double* fT;
+    double* QT;
+    int K, M;
+};
+
+struct Unit {
+    int bucket, ht, bin, pad;
+};
+
+__global__ void __launch_bounds__(kRW * 32, 1)
+    af_pair_ragged_kernel(const Bucket* __restrict__ buckets, const Unit* __restrict__ units, int n_units,
+                          int* __restrict__ counter) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_unit, s_next;
+    __shared__ Bucket s_bk;  // the current unit's bucket (uniform shared loads inside the pair routine)
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    double* rb_all = smem;  // kRW x kRBuf
+    double* fs = smem + kRW * kRBuf;
+    double* rb = rb_all + warp * kRBuf;
+    int staged_b = -1, staged_ht = -1;
+    for (;;) {
+        if (tid == 0) {
+            const int uu = atomicAdd(counter, 1);
+            s_unit = uu;
+            if (uu < n_units) s_bk = buckets[units[uu].bucket];
+        }
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= n_units) break;
+        const Unit un = units[u];
+        const Bucket& bk = s_bk;
+        const int M = bk.M;
+        const size_t tile_base = (size_t)(un.ht >> 1) * M * CF_TILE + (size_t)(un.ht & 1) * cf::kTileCells;
+        if (un.bucket != staged_b || un.ht != staged_ht) {
+            const double* srcf = bk.fT + tile_base;
+            for (int i = tid; i < M * 8; i += kRW * 32) {
+                const int r = i >> 3, w = (i & 7) * 2;
+                cf::cp_async16(fs + r * cf::kTileCells + w, srcf + (size_t)r * CF_TILE + w);
+            }
+            cf::cp_async_commit();
+            cf::cp_async_wait_all();
+            staged_b = un.bucket;
+            staged_ht = un.ht;
+        }
+        if (tid == 0) s_next = 0;
+        __syncthreads();
+        const int b0 = bk.pbin_begin[un.bin], nb = bk.pbin_begin[un.bin + 1] - b0;
+        double* qtc = bk.QT + tile_base + (lane & 15);
+        for (;;) {
+            int i = 0;
+            if (lane == 0) i = atomicAdd(&s_next, 1);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= nb) break;
+            const int2 item = bk.pitems[bk.pbin_item[b0 + i]];
+            switch (bk.K) {
+                case 1: cf::pair_item<1, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                case 2: cf::pair_item<2, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                case 3: cf::pair_item<3, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                case 4: cf::pair_item<4, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                case 5: cf::pair_item<5, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                case 6: cf::pair_item<6, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                case 7: cf::pair_item<7, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                case 8: cf::pair_item<8, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                default: break;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+#define RCHECK(expr)                                                                                    \
+    do {                                                                                                \
+        cudaError_t e_ = (expr);                                                                        \
+        if (e_ != cudaSuccess) {                                                                        \
+            char m_[256];                                                                               \
+            snprintf(m_, sizeof(m_), "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            cf_set_last_error(m_);                                                                      \
+            return e_ == cudaErrorMemoryAllocation ? CF_ENOMEM : CF_ECUDA;                              \
+        }                                                                                               \
+    } while (0)
+
+}  // namespace
+
+struct cf_ragged {
+    int device = 0;
+    int n_buckets = 0;
+    std::vector<cf_plan*> plans;
+    std::vector<int64_t> cells;
+    std::vector<int> K, NQ;
+    std::vector<int> form;     // per bucket: the form it is contracted in
+    std::vector<char> fused;   // per bucket: part of the fused launch
+    std::vector<double> cost;  // relative cost of one half-tile of each bucket
+    int tail_split = 4;
+    Bucket* d_buckets = nullptr;
+    Unit* d_units = nullptr;
+    int* d_counter = nullptr;
+    double* d_tiles = nullptr;  // per bucket: tiled f, tiled Q
+    std::vector<size_t> tile_off;
+    int n_units = 0, ctas = 0;
+    size_t smem = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<const double*> graph_f;
+    std::vector<double*> graph_q;
+    cudaStream_t graph_stream = nullptr;
+    std::mutex mu;
+};
+
+namespace {
+
+int64_t ntiles(int64_t B) { return (B + CF_TILE - 1) / CF_TILE; }
+
+void free_ragged(cf_ragged* r) {
+    if (r->graph_exec) cudaGraphExecDestroy(r->graph_exec);
+    if (r->graph) cudaGraphDestroy(r->graph);
+    cudaFree(r->d_buckets);
+    cudaFree(r->d_units);
+    cudaFree(r->d_counter);
+    cudaFree(r->d_tiles);
+}
+
+double* tiled_f(cf_ragged* r, int b) { return r->d_tiles + r->tile_off[b]; }
+double* tiled_q(cf_ragged* r, int b) {
+    return r->d_tiles + r->tile_off[b] + (size_t)ntiles(r->cells[b]) * CF_TILE * r->NQ[b] * r->K[b];
+}
+
+// the contraction on the handle's tiled buffers: the fused launch, then the separate buckets
+int enqueue_contract(cf_ragged* r, cudaStream_t s) {
+    if (r->n_units > 0) {
+        RCHECK(cudaMemsetAsync(r->d_counter, 0, sizeof(int), s));
+        const unsigned grid = (unsigned)std::min(r->n_units, r->ctas);
+        af_pair_ragged_kernel<<<grid, kRW * 32, r->smem, s>>>(r->d_buckets, r->d_units, r->n_units, r->d_counter);
+        RCHECK(cudaGetLastError());
+    }
+    for (int b = 0; b < r->n_buckets; ++b) {
+        if (r->fused[b] || r->cells[b] == 0) continue;
+        const int st = cf_q_tiled(r->plans[b], tiled_q(r, b), tiled_f(r, b), r->cells[b], r->form[b], s);
+        if (st != CF_OK) return st;
+    }
+    return CF_OK;
+}
+
+// pack every bucket, the contraction, unpack (q += Q(f) per bucket), all on stream s
+int enqueue_step(cf_ragged* r, double* const* q, const double* const* f, cudaStream_t s) {
+    for (int b = 0; b < r->n_buckets; ++b) {
+        if (r->cells[b] == 0) continue;
+        const int M = r->NQ[b] * r->K[b];
+        dim3 grid((M + 31) / 32, (unsigned)ntiles(r->cells[b])), block(32, 8);
+        cf::pack_tiles_kernel<double><<<grid, block, 0, s>>>(f[b], tiled_f(r, b), r->cells[b], r->NQ[b], r->K[b]);
+        cf::pack_tiles_kernel<double><<<grid, block, 0, s>>>(q[b], tiled_q(r, b), r->cells[b], r->NQ[b], r->K[b]);
+    }
+    RCHECK(cudaGetLastError());
+    const int st = enqueue_contract(r, s);
+    if (st != CF_OK) return st;
+    for (int b = 0; b < r->n_buckets; ++b) {
+        if (r->cells[b] == 0) continue;
+        const int M = r->NQ[b] * r->K[b];
+        dim3 grid((M + 31) / 32, (unsigned)ntiles(r->cells[b])), block(32, 8);
+        cf::unpack_tiles_kernel<<<grid, block, 0, s>>>(tiled_q(r, b), q[b], r->cells[b], r->NQ[b], r->K[b]);
+    }
+    RCHECK(cudaGetLastError());
+    return CF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cf_ragged_create(cf_ragged** out, cf_plan* const* plans, const int64_t* cells, const int32_t* forms,
+                     int32_t n_buckets, int32_t tail_split) {
+    if (!out || !plans || !cells || n_buckets < 1 || n_buckets > 64) {
+        cf_set_last_error("cf_ragged_create: need 1..64 buckets");
+        return CF_EINVAL;
+    }
+    if (tail_split != 0 && tail_split != 4 && tail_split != 16) {
+        cf_set_last_error("cf_ragged_create: tail_split must be 0, 4 or 16");
+        return CF_EINVAL;
+    }
+    *out = nullptr;
+    cf_ragged* r = new cf_ragged();
+    r->n_buckets = n_buckets;
+    r->tail_split = tail_split;
+    std::vector<Bucket> hb(n_buckets);
+    int dev = -1;
+    size_t max_smem = 0;
+    int n_sms = 0;
+    size_t tiles_total = 0;
+    size_t max_M = 0;
+    for (int b = 0; b < n_buckets; ++b) {
+        cf_plan_info info;
+        if (!plans[b] || cf_plan_get_info(plans[b], &info) != CF_OK || cells[b] < 0 ||
+            ntiles(cells[b]) > 65535) {
+            delete r;
+            cf_set_last_error("cf_ragged_create: invalid plan or cell count");
+            return CF_EINVAL;
+        }
+        const int form = forms ? forms[b] : CF_FORM_AF;
+        if (form < CF_FORM_AF || form > CF_FORM_AF_SYM) {
+            delete r;
+            cf_set_last_error("cf_ragged_create: bucket forms must be one of the FP64 forms (0..4)");
+            return CF_EINVAL;
+        }
+        if (dev < 0) dev = info.device;
+        if (info.device != dev) {
+            delete r;
+            cf_set_last_error("cf_ragged_create: all plans must live on one device");
+            return CF_EINVAL;
+        }
+        const bool fused = (form == CF_FORM_AF || form == CF_FORM_AF_SYM) && info.k <= kMaxK;
+        DevOp op{};
+        const int* pbb = nullptr;
+        const int* pbi = nullptr;
+        const int2* pit = nullptr;
+        cf_plan* view = plans[b];
+        if (form == CF_FORM_AF_SYM) {
+            // built here, never inside a graph recording (the build copies from the host)
+            cf_plan* folded = nullptr;
+            const int fs = cf_plan_folded(plans[b], &folded);
+            if (fs != CF_OK) {
+                delete r;
+                return fs;
+            }
+            if (fused) view = folded;
+        }
+        cf_plan_internal_view(view, &op, &pbb, &pbi, &pit, &n_sms, &max_smem);
+        hb[b] = Bucket{op, pbb, pbi, pit, nullptr, nullptr, info.k, info.n_q * info.k};
+        r->form.push_back(form);
+        r->fused.push_back(fused ? 1 : 0);
+        r->plans.push_back(plans[b]);
+        r->cells.push_back(cells[b]);
+        r->K.push_back(info.k);
+        r->NQ.push_back(info.n_q);
+        // cost of one half-tile ~ its FLOPs (16 cells)
+        r->cost.push_back(info.flops_q * 16.0);
+        r->tile_off.push_back(tiles_total);
+        tiles_total += 2 * (size_t)ntiles(cells[b]) * CF_TILE * info.n_q * info.k;
+        if (fused) max_M = std::max(max_M, (size_t)info.n_q * info.k);
+    }
+    r->device = dev;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != dev) cudaSetDevice(dev);
+    int st = CF_OK;
+    r->smem = sizeof(double) * ((size_t)kRW * kRBuf + max_M * cf::kTileCells);
+    do {
+        if (max_M > 0 && r->smem + 256 > max_smem) {
+            cf_set_last_error("cf_ragged_create: the largest bucket's 16-cell tile does not fit in shared memory");
+            st = CF_EUNSUPPORTED;
+            break;
+        }
+        cudaError_t e = cudaFuncSetAttribute(af_pair_ragged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)r->smem);
+        int per_sm = 0;
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, af_pair_ragged_kernel,
+                                                                                kRW * 32, r->smem);
+        if (e != cudaSuccess || per_sm < 1) {
+            cf_set_last_error("cf_ragged_create: fused kernel does not fit on this device");
+            st = CF_EUNSUPPORTED;
+            break;
+        }
+        r->ctas = per_sm * n_sms;
+        // work units: whole half-tiles of every fused bucket, heaviest bucket first; the last `ctas`
+        // half-tiles (in that order) are split into tail_split q1-pair bins each
+        std::vector<int> order;
+        for (int b = 0; b < n_buckets; ++b)
+            if (r->fused[b]) order.push_back(b);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int c) { return r->cost[a] > r->cost[c]; });
+        std::vector<std::pair<int, int>> hts;
+        for (int b : order)
+            for (int64_t h = 0; h < (r->cells[b] + 15) / 16; ++h) hts.push_back({b, (int)h});
+        const size_t n_ht = hts.size();
+        const size_t n_whole = (tail_split == 0 || n_ht <= (size_t)r->ctas) ? (tail_split == 0 ? n_ht : 0)
+                                                                              : n_ht - r->ctas;
+        std::vector<Unit> units;
+        for (size_t i = 0; i < n_ht; ++i) {
+            if (i < n_whole) {
+                units.push_back({hts[i].first, hts[i].second, 0, 0});
+            } else {
+                const int base = tail_split == 4 ? 1 : 5;  // bin layout of the plan: 0 whole, 1..4, 5..20
+                for (int k = 0; k < tail_split; ++k) units.push_back({hts[i].first, hts[i].second, base + k, 0});
+            }
+        }
+        r->n_units = (int)units.size();
+        e = cudaMalloc(&r->d_tiles, std::max<size_t>(tiles_total, 1) * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&r->d_buckets, n_buckets * sizeof(Bucket));
+        if (e == cudaSuccess) e = cudaMalloc(&r->d_units, std::max<size_t>(units.size(), 1) * sizeof(Unit));
+        if (e == cudaSuccess) e = cudaMalloc(&r->d_counter, sizeof(int));
+        if (e != cudaSuccess) {
+            cf_set_last_error(cudaGetErrorString(e));
+            st = CF_ENOMEM;
+            break;
+        }
+        for (int b = 0; b < n_buckets; ++b) {
+            hb[b].fT = r->d_tiles + r->tile_off[b];
+            hb[b].QT = r->d_tiles + r->tile_off[b] + (size_t)ntiles(r->cells[b]) * CF_TILE * r->NQ[b] * r->K[b];
+        }
+        e = cudaMemcpy(r->d_buckets, hb.data(), n_buckets * sizeof(Bucket), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !units.empty())
+            e = cudaMemcpy(r->d_units, units.data(), units.size() * sizeof(Unit), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            cf_set_last_error(cudaGetErrorString(e));
+            st = CF_ECUDA;
+            break;
+        }
+    } while (false);
+    if (cur != dev) cudaSetDevice(cur);
+    if (st != CF_OK) {
+        free_ragged(r);
+        delete r;
+        return st;
+    }
+    *out = r;
+    return CF_OK;
+}
+
+int cf_ragged_destroy(cf_ragged* r) {
+    if (!r) return CF_OK;
+    free_ragged(r);
+    if (r->graph_stream) cudaStreamDestroy(r->graph_stream);
+    delete r;
+    return CF_OK;
+}
+
+// q[b] += Q(f[b]) for every bucket b (device arrays [N_Q x K x B_b]), one fused launch.
+int cf_ragged_q(cf_ragged* r, double* const* q_dev, const double* const* f_dev, void* stream) {
+    if (!r || !q_dev || !f_dev) return CF_EINVAL;
+    std::lock_guard<std::mutex> lk(r->mu);
+    return enqueue_step(r, q_dev, f_dev, (cudaStream_t)stream);
+}
+
+// The same step replayed from a CUDA graph recorded on first use for these buffers (re-recorded when
+// the buffers change).  The recording does not allocate or synchronise inside the step.
+int cf_ragged_graph_launch(cf_ragged* r, double* const* q_dev, const double* const* f_dev, void* stream) {
+    if (!r || !q_dev || !f_dev) return CF_EINVAL;
+    std::lock_guard<std::mutex> lk(r->mu);
+    bool same = r->graph_exec != nullptr && (int)r->graph_f.size() == r->n_buckets;
+    for (int b = 0; same && b < r->n_buckets; ++b) same = r->graph_f[b] == f_dev[b] && r->graph_q[b] == q_dev[b];
+    if (!same) {
+        if (r->graph_exec) cudaGraphExecDestroy(r->graph_exec);
+        if (r->graph) cudaGraphDestroy(r->graph);
+        r->graph_exec = nullptr;
+        r->graph = nullptr;
+        if (!r->graph_stream) RCHECK(cudaStreamCreateWithFlags(&r->graph_stream, cudaStreamNonBlocking));
+        RCHECK(cudaStreamBeginCapture(r->graph_stream, cudaStreamCaptureModeThreadLocal));
+        const int st = enqueue_step(r, q_dev, f_dev, r->graph_stream);
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(r->graph_stream, &g);
+        if (st != CF_OK) {
+            if (g) cudaGraphDestroy(g);
+            return st;
+        }
+        RCHECK(e);
+        r->graph = g;
+        RCHECK(cudaGraphInstantiate(&r->graph_exec, g, 0));
+        r->graph_f.assign(f_dev, f_dev + r->n_buckets);
+        r->graph_q.assign(q_dev, q_dev + r->n_buckets);
+    }
+    RCHECK(cudaGraphLaunch(r->graph_exec, (cudaStream_t)stream));
+    return CF_OK;
+}
+
+// The contraction alone on the handle's resident tiled buffers, as the last cf_ragged_q or
+// cf_ragged_graph_launch left them (Q_tiled += Q(f_tiled)): the step without its layout passes.
+int cf_ragged_q_resident(cf_ragged* r, void* stream) {
+    if (!r) return CF_EINVAL;
+    std::lock_guard<std::mutex> lk(r->mu);
+    return enqueue_contract(r, (cudaStream_t)stream);
+}
+
+int cf_ragged_info(const cf_ragged* r, int32_t* n_units, int32_t* ctas, int64_t* smem_bytes, int32_t* n_fused) {
+    if (!r) return CF_EINVAL;
+    if (n_units) *n_units = r->n_units;
+    if (ctas) *ctas = r->ctas;
+    if (smem_bytes) *smem_bytes = (int64_t)r->smem;
+    if (n_fused) {
+        int n = 0;
+        for (int b = 0; b < r->n_buckets; ++b) n += r->fused[b] ? 1 : 0;
+        *n_fused = n;
+    }
+    return CF_OK;
+}
+
+}  // extern "C"

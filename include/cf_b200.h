@@ -51,7 +51,15 @@ typedef enum cf_form {
     CF_FORM_RF = 1,        /* radial first: Psi_z = R_t . (f2 (x) f3) per entry, then Q += G Psi       */
     CF_FORM_AF_EXACT = 2,  /* angular first in the reference's exact operation order (no FMA):
                               reproduces angular_first_collision_kernel_mex bit for bit (K <= 8)        */
-    CF_FORM_RF_EXACT = 3   /* radial first in the reference's exact operation order (no FMA)           */
+    CF_FORM_RF_EXACT = 3,  /* radial first in the reference's exact operation order (no FMA)           */
+    CF_FORM_AF_SYM = 4,    /* angular first on the q2 <-> q3 folded operator: the entries (q1,q2,q3) and
+                              (q1,q3,q2) share one outer product against R_t + R_t'^T (half the work);
+                              needs a COO list that is symmetric in its last two indices (the real
+                              Gaunt lists are) and returns CF_EUNSUPPORTED otherwise                   */
+    CF_FORM_AF_F32 = 5,    /* angular first in FP32 (f, R, Phi and the row sums rounded to FP32; result
+                              added to the FP64 Q): ~1e-7 relative error, the invariant rows stay exactly
+                              zero because R's conservation rows are exactly zero in FP32 too          */
+    CF_FORM_AF_SYM_F32 = 6 /* the FP32 form on the folded operator                                       */
 } cf_form;
 
 typedef struct cf_plan cf_plan;
@@ -66,6 +74,10 @@ typedef struct cf_plan_info {
     double  flops_q;      /* algorithmic FLOP per cell for Q:  N_G(2K^2+K) + S 2K^3 */
     double  flops_jv;     /* algorithmic FLOP per cell for J.v: N_G(4K^2+2K) + S 2K^3 */
     int64_t device_bytes; /* device memory held by the plan (COO, R, buffers)   */
+    int32_t last_path;    /* kernel family of the plan's last angular-first or J.v launch
+                             (1 gather, 2 tile, 3 pair, 4 pair R via L1, 5 split pair; 0 none yet;
+                             launches of the folded form count for the plan they fold) */
+    int32_t reserved;
 } cf_plan_info;
 
 /* ------------------------------------------------------------------------------------------
@@ -125,7 +137,8 @@ int cf_q_device(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, in
 int cf_q_device_ws(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form,
                    void* workspace, size_t workspace_bytes, void* stream);
 
-/* out_dev += J(f_dev).v_dev for B cells. */
+/* out_dev += J(f_dev).v_dev for B cells.  `exact` selects the mode of every J.v call:
+ * 0 = fast, 1 = exact operation order, 2 = the q2 <-> q3 folded operator (as CF_FORM_AF_SYM). */
 int cf_jv_device(cf_plan* plan, double* out_dev, const double* f_dev, const double* v_dev,
                  int64_t b, int32_t exact, void* stream);
 
@@ -140,12 +153,14 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
                 int32_t exact, void* stream);
 
 /* Kernel family of a plan's angular-first and Jacobian contractions: 0 = automatic (the first of
- * pair, tile, gather that fits), 1 = the gather kernel (warp per row and 32-cell tile, f read
- * through L1/L2), 2 = the tile-resident kernel (16 cells in shared memory, Phi split over two
- * lanes per cell), 3 = the pair kernel (16 cells in shared memory, the mirrored rows (l,+m) and
+ * split pair, pair, tile, gather that fits), 1 = the gather kernel (warp per row and 32-cell tile,
+ * f read through L1/L2), 2 = the tile-resident kernel (16 cells in shared memory, Phi split over
+ * two lanes per cell), 3 = the pair kernel (16 cells in shared memory, the mirrored rows (l,+m) and
  * (l,-m) on the two half-warps), 4 = the pair kernel reading R through L1 instead of shared
- * memory.  2-4 return CF_EUNSUPPORTED where they do not fit.  All families agree to rounding, and
- * bit for bit in the exact forms. */
+ * memory, 5 = the split pair kernel (both mirrored rows in every lane, the k3 range split over the
+ * half-warps; fast Q forms with even K <= 8, the pair kernel otherwise).  2-5 return
+ * CF_EUNSUPPORTED where they do not fit.  All families agree to rounding, and bit for bit in the
+ * exact forms. */
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path);
 
 /* Measured FP64 FMA throughput of `device` in TFLOP/s (independent DFMA chains on every SM, timed
@@ -167,6 +182,42 @@ int cf_fp64_fma_peak(int32_t device, double* tflops);
 #define CF_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form,
                         void* stream);
+
+/* ------------------------------------------------------------------------------------------
+ * Ragged batches: cells of several resolutions (one plan per (L, K) bucket) contracted in ONE
+ * persistent launch.  cells[b] is bucket b's cell count; q_dev[b], f_dev[b] are its
+ * [N_Q x K x cells[b]] device arrays.  forms[b] (NULL: all CF_FORM_AF) is the FP64 form of bucket b:
+ * buckets in CF_FORM_AF or CF_FORM_AF_SYM with K <= 8 share the fused launch, any other bucket runs
+ * its own plan's kernels in the same step.  tail_split (0, 4 or 16) is how many q1-pair bins each of
+ * the last half-tiles of the fused work table is cut into, so that the launch ends evenly.
+ * cf_ragged_q enqueues pack, fused launch, the separate buckets and unpack on the stream;
+ * cf_ragged_graph_launch records that sequence into a CUDA graph on first use (per set of buffers)
+ * and replays it.  No counterpart in the reference (it contracts one f at a time).
+ * ------------------------------------------------------------------------------------------ */
+typedef struct cf_ragged cf_ragged;
+int cf_ragged_create(cf_ragged** ragged, cf_plan* const* plans, const int64_t* cells, const int32_t* forms,
+                     int32_t n_buckets, int32_t tail_split);
+int cf_ragged_destroy(cf_ragged* ragged);
+int cf_ragged_q(cf_ragged* ragged, double* const* q_dev, const double* const* f_dev, void* stream);
+int cf_ragged_graph_launch(cf_ragged* ragged, double* const* q_dev, const double* const* f_dev, void* stream);
+/* The contraction alone on the handle's resident tiled buffers, as the last cf_ragged_q or
+ * cf_ragged_graph_launch left them (Q_tiled += Q(f_tiled)): the step without its layout passes. */
+int cf_ragged_q_resident(cf_ragged* ragged, void* stream);
+/* Work units of the fused table, CTAs of the fused launch, its dynamic shared memory and the number
+ * of buckets it contracts (the others run their own kernels). */
+int cf_ragged_info(const cf_ragged* ragged, int32_t* n_units, int32_t* ctas, int64_t* smem_bytes, int32_t* n_fused);
+
+/* ------------------------------------------------------------------------------------------
+ * Explicit time stepping df/dt = Q(f) for a batch of cells, Heun's method (RK2):
+ * f <- f + dt/2 (Q(f) + Q(f + dt Q(f))), n_steps times, in the tiled layout (cf_pack_cells), with
+ * the contraction in `form` (any FP64 form).  The reference steps one cell with its dense tensor
+ * (tutorial_stress_relaxation.m:77-91, tutorial_collisions_bwu_solution.m:77-92).  The workspace
+ * (cf_rk2_workspace_size bytes) holds the two stage values and the intermediate state; a step
+ * allocates nothing and never synchronises, so n steps can be recorded into a CUDA graph.
+ * ------------------------------------------------------------------------------------------ */
+int cf_rk2_workspace_size(const cf_plan* plan, int64_t b, size_t* bytes);
+int cf_rk2_steps_tiled(cf_plan* plan, double* f_tiled, int64_t b, double dt, int32_t n_steps, int32_t form,
+                       void* workspace, size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------------------------------
  * Implicit solves: (I - dt J(f)) x = b per cell with restarted GMRES, FP64.  No counterpart in

@@ -90,7 +90,7 @@ def test_fast_forms_vs_oracle(L, K, cuda_available, oracle_lib):
     args = (geo.labels, geo.vals, geo.ic_map, R, NQ, K)
     Qo = np.zeros_like(f, order="F")
     oracle_lib.af_batch(Qo, f, *args)
-    for form in ("af", "rf"):
+    for form in ("af", "rf", "af_sym"):
         Qg = np.zeros_like(f, order="F")
         cf_b200.contract_batched(Qg, f, *args, form=form)
         err = per_cell_err(Qg.transpose(2, 1, 0), Qo.transpose(2, 1, 0))
@@ -116,6 +116,9 @@ def test_jacobian_apply_vs_oracle(L, K, cuda_available, oracle_lib):
     out = np.zeros_like(f, order="F")
     cf_b200.collision_jacobian_apply_mex(out, f, v, *args)
     assert per_cell_err(out.transpose(2, 1, 0), ref.transpose(2, 1, 0)) <= TOL_FP64
+    out3 = np.zeros_like(f, order="F")
+    cf_b200.collision_jacobian_apply_mex(out3, f, v, *args, exact=2)  # folded operator
+    assert per_cell_err(out3.transpose(2, 1, 0), ref.transpose(2, 1, 0)) <= TOL_FP64
     if K <= 8:
         out2 = np.zeros_like(f, order="F")
         cf_b200.collision_jacobian_apply_mex(out2, f, v, *args, exact=True)
@@ -260,10 +263,12 @@ def test_kernel_paths_agree(L, K, B, cuda_available, oracle_lib):
     oracle_lib.af_batch(Qo, _cells_cm(cells), geo.labels, geo.vals, geo.ic_map, R, NQ, K)
     ref = Qo.transpose(2, 1, 0)
     outs = {}
-    for path in ("pair", "pair_l1", "tile", "gather"):
+    for path in ("pair_split", "pair", "pair_l1", "tile", "gather"):
         op.set_kernel_path(path)
         Qf = op.q(f).cpu().numpy()
         assert per_cell_err(Qf, ref) <= TOL_FP64, f"{path}: {per_cell_err(Qf, ref):.3e}"
+        Qs = op.q(f, form="af_sym").cpu().numpy()
+        assert per_cell_err(Qs, ref) <= TOL_FP64, f"{path} folded: {per_cell_err(Qs, ref):.3e}"
         outs[path] = op.q(f, form="af_exact").cpu().numpy()
         assert np.array_equal(outs[path], ref), f"{path}: exact form not bitwise equal to the oracle"
     op.close()
@@ -295,6 +300,24 @@ def test_tile_path_jacobian(L, K, B, cuda_available, oracle_lib):
     op.close()
 
 
+def test_folded_form_rejects_an_asymmetric_list(cuda_available):
+    """A COO list that is not symmetric in (q2, q3) cannot be folded: CF_EUNSUPPORTED, not a wrong answer."""
+    import cf_b200
+    from cf_b200 import CFError
+
+    d = load_op("cfg1_k3_l4_g0")
+    NQ, K = d["NQ"], d["K"]
+    keep = np.ones(d["labels"].shape[0], dtype=bool)
+    lab = d["labels"]
+    off = np.flatnonzero(lab[:, 1] != lab[:, 2])[0]
+    keep[off] = False  # drop one entry: its mirror is left without a partner
+    Q = np.zeros((NQ, K), order="F")
+    with pytest.raises(CFError) as e:
+        cf_b200.contract_batched(Q, d["f"], np.asfortranarray(lab[keep]), d["vals"][keep], d["ic_map"][keep], d["R"],
+                                 NQ, K, form="af_sym")
+    assert e.value.status == 8
+
+
 def test_pair_path_with_unpaired_rows(cuda_available, oracle_lib):
     """A shuffled COO list breaks the mirrored-row structure: rows fall back to single items and the
     result is unchanged (exact form bitwise, in the caller's run order)."""
@@ -316,4 +339,93 @@ def test_pair_path_with_unpaired_rows(cuda_available, oracle_lib):
     op.set_kernel_path("pair")
     out = op.q(torch.from_numpy(cells).cuda(), form="af_exact").cpu().numpy()
     assert np.array_equal(out, ref.transpose(2, 1, 0))
+    op.set_kernel_path("pair_split")  # single rows use all 32 lanes, k3 split over the half-warps
+    out = op.q(torch.from_numpy(cells).cuda()).cpu().numpy()
+    assert per_cell_err(out, ref.transpose(2, 1, 0)) <= TOL_FP64
+    op.close()
+
+
+@pytest.mark.parametrize("L,K,B", [(8, 8, 50), (10, 8, 40), (16, 12, 13)])
+def test_fp32_forms_error_and_invariants(L, K, B, cuda_available, oracle_lib):
+    """FP32 forms: relative error at FP32 level (<= 1e-5 per cell), invariant rows exactly zero."""
+    import cf_b200
+    from cf_b200 import geometry, workloads
+    from oracle import rtensor
+
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=2)
+    NQ = geo.n_q
+    f = _cells_cm(workloads.maxwellian_cells(K, L, B, seed=6, amplitude=0.05))
+    args = (geo.labels, geo.vals, geo.ic_map, R, NQ, K)
+    Qo = np.zeros_like(f, order="F")
+    oracle_lib.af_batch(Qo, f, *args)
+    for form in ("af_f32", "af_sym_f32"):
+        Qg = np.zeros_like(f, order="F")
+        cf_b200.contract_batched(Qg, f, *args, form=form)
+        err = per_cell_err(Qg.transpose(2, 1, 0), Qo.transpose(2, 1, 0))
+        assert 1e-12 < err <= 1e-5, f"{form}: {err:.3e}"
+        inv = Qg.transpose(2, 1, 0).reshape(B, -1)[:, [0, 1, 2, 3, NQ]]
+        assert np.all(inv == 0.0)
+
+
+def test_host_entry_chunked_matches_oracle(cuda_available, oracle_lib):
+    """Batches of >= 1024 cells go through the host entry points in chunks on three streams; the
+    result is the same as the oracle's (fast and folded Q, J.v), cells split at ragged chunk ends."""
+    import cf_b200
+    from cf_b200 import geometry, workloads
+    from oracle import rtensor
+
+    L, K, B = 4, 4, 1500
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=21)
+    NQ = geo.n_q
+    f = _cells_cm(workloads.maxwellian_cells(K, L, B, seed=8))
+    args = (geo.labels, geo.vals, geo.ic_map, R, NQ, K)
+    Qo = np.zeros_like(f, order="F")
+    oracle_lib.af_batch(Qo, f, *args)
+    for form in ("af", "af_sym", "af_exact"):
+        Qg = np.asfortranarray(np.full_like(f, 0.5))
+        cf_b200.contract_batched(Qg, f, *args, form=form)
+        Qg -= 0.5
+        assert per_cell_err(Qg.transpose(2, 1, 0), Qo.transpose(2, 1, 0)) <= TOL_FP64, form
+    rng = np.random.default_rng(2)
+    v = np.asfortranarray(rng.standard_normal(f.shape))
+    Jo = np.zeros_like(f, order="F")
+    oracle_lib.jv_batch(Jo, f, v, *args)
+    Jg = np.zeros_like(f, order="F")
+    cf_b200.collision_jacobian_apply_mex(Jg, f, v, *args)
+    assert per_cell_err(Jg.transpose(2, 1, 0), Jo.transpose(2, 1, 0)) <= TOL_FP64
+    Je = np.zeros_like(f, order="F")
+    cf_b200.collision_jacobian_apply_mex(Je, f, v, *args, exact=1)
+    assert np.array_equal(Je, Jo)
+
+
+def test_two_streams_share_a_plan(cuda_available):
+    """Persistent launches of one plan on two streams at once each get their own work counter."""
+    import torch
+
+    import cf_b200
+    from cf_b200 import geometry, workloads
+    from oracle import rtensor
+
+    L, K = 8, 8
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=5)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+    op.set_kernel_path("pair_split")
+    f1 = torch.from_numpy(workloads.maxwellian_cells(K, L, 600, seed=1)).cuda()
+    f2 = torch.from_numpy(workloads.maxwellian_cells(K, L, 700, seed=2)).cuda()
+    ref1, ref2 = op.q(f1), op.q(f2)
+    torch.cuda.synchronize()
+    s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    ws1 = torch.empty(op.workspace_bytes(600) // 8 + 8, dtype=torch.float64, device="cuda")
+    ws2 = torch.empty(op.workspace_bytes(700) // 8 + 8, dtype=torch.float64, device="cuda")
+    outs1 = [torch.zeros_like(f1) for _ in range(4)]
+    outs2 = [torch.zeros_like(f2) for _ in range(4)]
+    for o1, o2 in zip(outs1, outs2):
+        op.q(f1, out=o1, stream=s1, workspace=ws1)
+        op.q(f2, out=o2, stream=s2, workspace=ws2)
+    torch.cuda.synchronize()
+    assert all(torch.equal(o, ref1) for o in outs1)
+    assert all(torch.equal(o, ref2) for o in outs2)
     op.close()

@@ -131,3 +131,19 @@ def test_batched_oracle_equals_per_cell(oracle_lib, reference_lib):
         Q1 = np.zeros((NQ, K), order="F")
         oracle_lib.af(Q1, np.asfortranarray(fb[:, :, b]), *args)
         assert np.array_equal(Q1, Qb[:, :, b])
+
+
+@pytest.mark.parametrize("name", ["cfg1_k3_l4_g0", "hs_k4_l4_g1"])
+def test_q2q3_folded_operator_is_the_same_quadratic_form(name, oracle_lib):
+    """The folded list (half the entries, R_t + R_t'^T) gives the reference's Q to rounding."""
+    from cf_b200 import geometry
+
+    d = load_op(name)
+    NQ, K = d["NQ"], d["K"]
+    geo = geometry.sort_for_contraction(
+        geometry.Geometry(d["L"], d["labels"], d["vals"], d["ic_map"], d["l_triplets"]))
+    lab, vals, ic, Rs = geometry.fold_q2q3(geo, d["R"], K)
+    assert lab.shape[0] < 0.6 * geo.n_g
+    Q = np.zeros((NQ, K), order="F")
+    oracle_lib.af(Q, d["f"], lab, vals, ic, Rs, NQ, K)
+    assert normwise_err(Q, d["Q_af"]) < 1e-14
