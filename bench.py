@@ -335,13 +335,15 @@ def run_ours(args):
     err_sym = float((num / den).max())
     sym_ms = timed(lambda: step("af_sym"), args.steps)
     sym_kern_ms = timed(lambda: kernel_only("af_sym"), max(2, args.steps // 2))
-    path_ms = {}
+    path_ms, sym_path_ms = {}, {}
     for path in ("pair_split", "pair", "pair_l1", "tile", "gather"):
         try:
             op.set_kernel_path(path)
             path_ms[path] = timed(step, max(2, args.steps // 4))
+            sym_path_ms[path] = timed(lambda: step("af_sym"), max(2, args.steps // 4))
         except Exception:
             path_ms[path] = None
+            sym_path_ms[path] = None
     op.set_kernel_path(args.path)
     exact_ms = timed(lambda: step("af_exact"), max(2, args.steps // 4)) if K <= 8 else None
     # reduced-precision forms (FP32 contraction, FP64 accumulation of Q): error and throughput
@@ -429,6 +431,7 @@ def run_ours(args):
                                     "af": "the plain FP64 form (the exact order is built for K <= 8)"}[ref_form],
                 "rf": {"cells_per_s": rf_rate},
                 "af_by_kernel": {p: (B / (sum(v) / len(v) / 1e3) if v else None) for p, v in path_ms.items()},
+                "af_sym_by_kernel": {p: (B / (sum(v) / len(v) / 1e3) if v else None) for p, v in sym_path_ms.items()},
                 **f32,
                 "chosen": chosen,
                 "plain_cells_per_s": plain_rate,
@@ -700,9 +703,10 @@ def run_ragged(args):
         ops.append(cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K, device=local))
         fs_np.append(make_cells(L, K, counts[b], seed=args.seed + rank * 101 + b))
     t0 = time.perf_counter()
-    forms, tail, tune = autotune(ops, counts, candidates=("af_sym", "af", "rf"), tail_splits=(0, 4, 16), reps=5)
+    forms, tail, family, tune = autotune(ops, counts, candidates=("af_sym", "af", "rf"), tail_splits=(0, 4, 16),
+                                         families=("pair", "tile"), reps=5)
     tune_s = time.perf_counter() - t0
-    rb = RaggedBatch(ops, counts, forms, tail_split=tail)
+    rb = RaggedBatch(ops, counts, forms, tail_split=tail, family=family)
     fs = [torch.from_numpy(c).to(dev) for c in fs_np]
     qs = [torch.zeros_like(f) for f in fs]
 
@@ -815,7 +819,7 @@ def run_ragged(args):
             "config": {"workload": args.workload, "cells_per_gpu": B, "gamma": 1.0,
                        "buckets": [{"L": L, "K": K, "cells": c, "form": fm, "max_rel_err_vs_fp64": e}
                                    for (L, K), c, fm, e in zip(RAGGED_BUCKETS, counts, forms, errs)],
-                       "tail_split": tail, "fused_units": rb.n_units, "ctas": rb.ctas, "smem_bytes": rb.smem_bytes,
+                       "tail_split": tail, "family": family, "fused_units": rb.n_units, "ctas": rb.ctas, "smem_bytes": rb.smem_bytes,
                        "R": sources, "l2": "flushed (256 MB write) before every timed step",
                        "parallelism": f"cells sharded, {B} per GPU, no collective"},
             "variants": {"graph_step_cells_per_s": value,
@@ -823,7 +827,8 @@ def run_ragged(args):
                          "separate_calls_cells_per_s": B * len(sep_ms) / (sum(sep_ms) / 1e3),
                          "contraction_only_cells_per_s": B / kern_s},
             "autotune": dict(tune, seconds=tune_s),
-            "roofline": {"bound": "fp64", "kernel": "af_pair_ragged_kernel (one persistent launch over the buckets)",
+            "roofline": {"bound": "fp64", "kernel": f"af_ragged_kernel<{family} routine> (one persistent launch over "
+                                                    "the buckets)",
                          "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
                          "traffic": None, "algorithmic_flop_per_launch": rb.flops_q, "kernel_ms": kern_s * 1e3,
                          "peak_source": "DFMA probe measured on this GPU in this run"},

@@ -90,7 +90,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_fp64_fma_peak.argtypes = [_I32, C.POINTER(C.c_double)]
     lib.cf_plan_set_kernel_path.argtypes = [C.c_void_p, _I32]
     V = C.c_void_p
-    lib.cf_ragged_create.argtypes = [C.POINTER(V), V, V, V, _I32, _I32]
+    lib.cf_ragged_create.argtypes = [C.POINTER(V), V, V, V, _I32, _I32, _I32]
     lib.cf_ragged_destroy.argtypes = [V]
     lib.cf_ragged_q.argtypes = [V, V, V, V]
     lib.cf_ragged_graph_launch.argtypes = [V, V, V, V]

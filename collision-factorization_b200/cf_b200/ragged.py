@@ -8,8 +8,8 @@ step from a CUDA graph recorded on first use (cf_ragged_graph_launch), which is 
 calls it once per step.
 
 ``autotune`` picks each bucket's form (radial-first against angular-first, plain or q2 <-> q3
-folded) and the fused table's tail split by timing them on the device, and keeps the choice in a
-small JSON cache keyed by the device and the buckets' shapes.
+folded), the fused launch's routine (pair or tile) and its tail split by timing them on the device,
+and keeps the choice in a small JSON cache keyed by the device and the buckets' operators.
 """
 from __future__ import annotations
 
@@ -23,9 +23,11 @@ import numpy as np
 
 from . import _lib
 
+FAMILIES = {"pair": 0, "tile": 1}  # routine of the fused launch: mirrored row pairs, or split Phi rows
+
 
 class RaggedBatch:
-    def __init__(self, operators, cells_per_bucket, forms=None, tail_split: int = 4):
+    def __init__(self, operators, cells_per_bucket, forms=None, tail_split: int = 4, family: str = "pair"):
         self.ops = list(operators)
         self.cells = [int(c) for c in cells_per_bucket]
         n = len(self.ops)
@@ -34,11 +36,15 @@ class RaggedBatch:
         self.forms = list(forms) if forms is not None else ["af"] * n
         codes = [_lib.FORMS[f] for f in self.forms]
         self.tail_split = int(tail_split)
+        if family not in FAMILIES:
+            raise _lib.CFError(_lib.CF_EINVAL, f"family must be one of {sorted(FAMILIES)}")
+        self.family = family
         plans = (C.c_void_p * n)(*[op._h.value for op in self.ops])
         counts = (C.c_int64 * n)(*self.cells)
         fc = (C.c_int32 * n)(*codes)
         h = C.c_void_p()
-        _lib.check(_lib.load().cf_ragged_create(C.byref(h), plans, counts, fc, n, self.tail_split))
+        _lib.check(_lib.load().cf_ragged_create(C.byref(h), plans, counts, fc, n, self.tail_split,
+                                                FAMILIES[family]))
         self._h = h
         nu, ct, sm, nf = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int32()
         _lib.check(_lib.load().cf_ragged_info(h, C.byref(nu), C.byref(ct), C.byref(sm), C.byref(nf)))
@@ -86,8 +92,11 @@ class RaggedBatch:
         launch, and one contraction kernel per bucket outside it."""
         nb = sum(1 for c in self.cells if c > 0)
         sep = sum(1 for op, c, f in zip(self.ops, self.cells, self.forms)
-                  if c > 0 and not (f in ("af", "af_sym") and op.K <= 8))
+                  if c > 0 and not self._fused(op, f))
         return 3 * nb + (1 if self.n_fused else 0) + sep
+
+    def _fused(self, op, form) -> bool:
+        return form in ("af", "af_sym") and op.K <= 8 and (self.family == "pair" or op.K % 2 == 0)
 
     def q_resident(self, stream=None):
         """The contraction alone on the resident tiled buffers left by the last step."""
@@ -138,57 +147,66 @@ def _time_step(rb: RaggedBatch, fs, qs, reps: int) -> float:
     return best
 
 
-def autotune(ops, cells, candidates=("af_sym", "af", "rf"), tail_splits=(0, 4, 16), reps: int = 5,
-             use_cache: bool = True, seed: int = 0):
-    """Choose each bucket's form and the fused table's tail split by timing them.
+def autotune(ops, cells, candidates=("af_sym", "af", "rf"), tail_splits=(0, 4, 16), families=("pair", "tile"),
+             reps: int = 5, use_cache: bool = True, seed: int = 0):
+    """Choose each bucket's form, the fused launch's routine and its tail split by timing them.
 
-    Returns (forms, tail_split, report).  Each bucket's candidates are timed alone (a one-bucket ragged
-    step on that bucket's cells); a candidate the operator does not support (an unfoldable Gaunt list
-    for af_sym) is skipped.  Then the whole step is timed for each tail split with the chosen forms.
+    Returns (forms, tail_split, family, report).  For each routine family, each bucket's candidate
+    forms are timed alone (a one-bucket ragged step on that bucket's cells) and the fastest kept; a
+    candidate the operator does not support (an unfoldable Gaunt list for af_sym) is skipped.  Then
+    the whole step is timed for every (family, tail split) with those forms, and the fastest wins.
     """
     import torch
 
     cells = [int(c) for c in cells]
-    key = _key(ops, cells, candidates, tail_splits)
+    key = _key(ops, cells, list(candidates) + list(families), tail_splits)
     path = _cache_path()
     if use_cache and path.exists():
         try:
             hit = json.loads(path.read_text()).get(key)
             if hit:
-                return hit["forms"], hit["tail_split"], dict(hit["report"], cached=True)
+                return hit["forms"], hit["tail_split"], hit["family"], dict(hit["report"], cached=True)
         except (OSError, ValueError):
             pass
     rng = np.random.default_rng(seed)
     fs = [torch.from_numpy(1e-2 * rng.standard_normal((c, op.K, op.N_Q))).cuda(op.device) for op, c in zip(ops, cells)]
     qs = [torch.zeros_like(f) for f in fs]
-    forms, per_bucket = [], []
+    per_bucket = []
+    forms_by_family = {fam: [] for fam in families}
     for op, c, f, q in zip(ops, cells, fs, qs):
-        times = {}
-        for form in candidates:
-            try:
-                rb = RaggedBatch([op], [c], [form], tail_split=4)
-            except _lib.CFError:
-                continue
-            times[form] = _time_step(rb, [f], [q], reps)
+        entry = {"N_Q": op.N_Q, "K": op.K, "cells": c, "seconds": {}, "chosen": {}}
+        for fam in families:
+            times = {}
+            for form in candidates:
+                try:
+                    rb = RaggedBatch([op], [c], [form], tail_split=4, family=fam)
+                except _lib.CFError:
+                    continue
+                times[form] = _time_step(rb, [f], [q], reps)
+                rb.close()
+            if not times:
+                raise _lib.CFError(_lib.CF_EUNSUPPORTED, f"no candidate form runs for bucket N_Q={op.N_Q} K={op.K}")
+            best = min(times, key=times.get)
+            forms_by_family[fam].append(best)
+            entry["seconds"][fam] = times
+            entry["chosen"][fam] = best
+        per_bucket.append(entry)
+    step_times = {}
+    for fam in families:
+        for ts in tail_splits:
+            rb = RaggedBatch(ops, cells, forms_by_family[fam], tail_split=ts, family=fam)
+            step_times[f"{fam}/{int(ts)}"] = _time_step(rb, fs, qs, reps)
             rb.close()
-        if not times:
-            raise _lib.CFError(_lib.CF_EUNSUPPORTED, f"no candidate form runs for bucket N_Q={op.N_Q} K={op.K}")
-        best = min(times, key=times.get)
-        forms.append(best)
-        per_bucket.append({"N_Q": op.N_Q, "K": op.K, "cells": c, "seconds": times, "chosen": best})
-    split_times = {}
-    for ts in tail_splits:
-        rb = RaggedBatch(ops, cells, forms, tail_split=ts)
-        split_times[int(ts)] = _time_step(rb, fs, qs, reps)
-        rb.close()
-    tail = min(split_times, key=split_times.get)
-    report = {"buckets": per_bucket, "tail_split_seconds": split_times, "cached": False}
+    best = min(step_times, key=step_times.get)
+    family, tail = best.split("/")[0], int(best.split("/")[1])
+    forms = forms_by_family[family]
+    report = {"buckets": per_bucket, "step_seconds": step_times, "cached": False}
     if use_cache:
         try:
             path.parent.mkdir(parents=True, exist_ok=True)
             data = json.loads(path.read_text()) if path.exists() else {}
-            data[key] = {"forms": forms, "tail_split": tail, "report": report}
+            data[key] = {"forms": forms, "tail_split": tail, "family": family, "report": report}
             path.write_text(json.dumps(data, indent=1))
         except (OSError, ValueError):
             pass
-    return forms, tail, report
+    return forms, tail, family, report

@@ -46,9 +46,11 @@ class RK2Stepper:
         key = (float(dt), int(n))
         g = self._graphs.get(key)
         if g is None:
-            # one eager step first builds what the library creates lazily (kernel attributes, the
-            # folded operator); recording itself executes nothing
+            # one eager step on a saved state builds what the library creates lazily (kernel
+            # attributes, the folded operator) outside the recording; the state is then restored
+            saved = self.state.clone()
             self.step(dt, 1)
+            self.state.copy_(saved)
             torch.cuda.synchronize()
             g = torch.cuda.CUDAGraph()
             s = torch.cuda.Stream()

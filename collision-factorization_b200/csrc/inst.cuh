@@ -175,6 +175,12 @@ static LaunchResult launch_for_k(const LaunchArgs& a) {
     }
     if (a.what == OP_RF) return a.exact ? launch_rf<K, true>(a) : launch_rf<K, false>(a);
     const bool jv = a.what == OP_JV;
+    if constexpr (K % 2 == 0 && K <= 8) {
+        if (a.path == PATH_AUTO && a.tile_first && !jv && !a.exact) {
+            const LaunchResult r = launch_tile<K, tile_W(K, false), false, false>(a);
+            if (r.status != -1) return r;
+        }
+    }
     if constexpr (K <= 8 && K % 2 == 0) {
         if (a.path == PATH_PAIR_SPLIT && !jv && !a.exact) {
             const LaunchResult r = launch_pair<K, 8, false, false, false, double, true>(a);

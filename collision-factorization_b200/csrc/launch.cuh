@@ -37,6 +37,8 @@ struct LaunchArgs {
     // FP32 form: tiled FP32 copies of f (and v) in place of fT / vT
     bool f32;
     const float* fT32;
+    // automatic order for the fast Q form: false = pair kernel first, true = tile kernel first
+    bool tile_first;
 };
 
 // Status codes mirror cf_status: 0 ok, 5 CUDA error, 8 unsupported, 2 shape.

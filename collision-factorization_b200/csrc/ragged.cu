@@ -2,11 +2,12 @@
 //
 // A ragged batch is a set of buckets, each a plan (one (L, K) operator) with its own cells and its
 // own form.  Buckets in the angular-first forms CF_FORM_AF / CF_FORM_AF_SYM with K <= 8 are "fused":
-// one kernel runs the pair routine of pair_kernels.cuh for all of them in a single launch.  The work
+// one kernel runs the pair or tile routine of the plans for all of them in a single launch.  The work
 // units of the fused buckets -- whole 16-cell half-tiles first, heaviest buckets first, then the last
 // half-tiles split into 4 or 16 q1-pair bins (or not split) -- sit in one table that persistent CTAs
 // drain through a device counter; a unit names its bucket, and the CTA stages that bucket's tile and
-// switches to the pair routine compiled for the bucket's K.  Shared memory and registers are sized
+// switches to the routine compiled for the bucket's K: the pair routine (8 warps per CTA) or the
+// tile routine (16 warps, even K only), chosen per batch.  Shared memory and registers are sized
 // for the largest fused bucket.  Any other bucket (radial-first, the exact forms, K > 8) runs its
 // own plan's kernels on its tiled buffers in the same step.
 //
@@ -28,20 +29,25 @@
 
 void cf_set_last_error(const char* msg);
 int cf_plan_internal_view(const cf_plan* plan, DevOp* op, const int** pbin_begin, const int** pbin_item,
-                          const int2** pitems, int* n_sms, size_t* max_smem);
+                          const int2** pitems, const int** bin_begin, const int** bin_q1, int* n_sms,
+                          size_t* max_smem);
 int cf_plan_folded(cf_plan* plan, cf_plan** folded);
 
 namespace {
 
-constexpr int kRW = 8;                  // warps per CTA
-constexpr int kMaxK = 8;                // buckets of K <= 8 (FP64 pair routine)
-constexpr int kRBuf = kMaxK * kMaxK * kMaxK;
+constexpr int kRW = 8;                  // warps per CTA, pair routine
+constexpr int kTW = 16;                 // warps per CTA, tile routine
+constexpr int kMaxK = 8;                // fused buckets have K <= 8 (FP64 pair / tile routines)
+constexpr int kRBufPair = kMaxK * kMaxK * kMaxK;
+constexpr int kRBufTile = cf::RBuf<kMaxK>::SIZE;
 
 struct Bucket {
     DevOp op;
-    const int* pbin_begin;
+    const int* pbin_begin;  // pair routine: bins over mirrored-row items
     const int* pbin_item;
     const int2* pitems;
+    const int* bin_begin;   // tile routine: bins over q1 rows
+    const int* bin_q1;
     const double* fT;
     double* QT;
     int K, M;
@@ -51,16 +57,22 @@ struct Unit {
     int bucket, ht, bin, pad;
 };
 
-__global__ void __launch_bounds__(kRW * 32, 1)
-    af_pair_ragged_kernel(const Bucket* __restrict__ buckets, const Unit* __restrict__ units, int n_units,
-                          int* __restrict__ counter) {
+// TILE = false: the pair routine (8 warps, one mirrored row pair per warp, whole Phi per lane);
+// TILE = true: the tile routine (16 warps, one q1 row per warp, Phi split over two lanes per cell;
+// even K only).  Both are the routines the buckets' own plans run, so a bucket's result is the same
+// bit for bit as its plan's pair or tile kernel.
+template <bool TILE>
+__global__ void __launch_bounds__((TILE ? kTW : kRW) * 32, 1)
+    af_ragged_kernel(const Bucket* __restrict__ buckets, const Unit* __restrict__ units, int n_units,
+                     int* __restrict__ counter) {
+    constexpr int W = TILE ? kTW : kRW;
+    constexpr int RBS = TILE ? kRBufTile : kRBufPair;
     extern __shared__ __align__(16) double smem[];
     __shared__ int s_unit, s_next;
-    __shared__ Bucket s_bk;  // the current unit's bucket (uniform shared loads inside the pair routine)
+    __shared__ Bucket s_bk;  // the current unit's bucket (uniform shared loads inside the routines)
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    double* rb_all = smem;  // kRW x kRBuf
-    double* fs = smem + kRW * kRBuf;
-    double* rb = rb_all + warp * kRBuf;
+    double* fs = smem + W * RBS;
+    double* rb = smem + warp * RBS;
     int staged_b = -1, staged_ht = -1;
     for (;;) {
         if (tid == 0) {
@@ -77,7 +89,7 @@ __global__ void __launch_bounds__(kRW * 32, 1)
         const size_t tile_base = (size_t)(un.ht >> 1) * M * CF_TILE + (size_t)(un.ht & 1) * cf::kTileCells;
         if (un.bucket != staged_b || un.ht != staged_ht) {
             const double* srcf = bk.fT + tile_base;
-            for (int i = tid; i < M * 8; i += kRW * 32) {
+            for (int i = tid; i < M * 8; i += W * 32) {
                 const int r = i >> 3, w = (i & 7) * 2;
                 cf::cp_async16(fs + r * cf::kTileCells + w, srcf + (size_t)r * CF_TILE + w);
             }
@@ -88,24 +100,36 @@ __global__ void __launch_bounds__(kRW * 32, 1)
         }
         if (tid == 0) s_next = 0;
         __syncthreads();
-        const int b0 = bk.pbin_begin[un.bin], nb = bk.pbin_begin[un.bin + 1] - b0;
+        const int* bb = TILE ? bk.bin_begin : bk.pbin_begin;
+        const int b0 = bb[un.bin], nb = bb[un.bin + 1] - b0;
         double* qtc = bk.QT + tile_base + (lane & 15);
         for (;;) {
             int i = 0;
             if (lane == 0) i = atomicAdd(&s_next, 1);
             i = __shfl_sync(0xffffffffu, i, 0);
             if (i >= nb) break;
-            const int2 item = bk.pitems[bk.pbin_item[b0 + i]];
-            switch (bk.K) {
-                case 1: cf::pair_item<1, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
-                case 2: cf::pair_item<2, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
-                case 3: cf::pair_item<3, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
-                case 4: cf::pair_item<4, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
-                case 5: cf::pair_item<5, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
-                case 6: cf::pair_item<6, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
-                case 7: cf::pair_item<7, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
-                case 8: cf::pair_item<8, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
-                default: break;
+            if constexpr (TILE) {
+                const int q1 = bk.bin_q1[b0 + i];
+                switch (bk.K) {
+                    case 2: cf::tile_q1<2, false, false>(bk.op, q1, fs, nullptr, rb, qtc, lane); break;
+                    case 4: cf::tile_q1<4, false, false>(bk.op, q1, fs, nullptr, rb, qtc, lane); break;
+                    case 6: cf::tile_q1<6, false, false>(bk.op, q1, fs, nullptr, rb, qtc, lane); break;
+                    case 8: cf::tile_q1<8, false, false>(bk.op, q1, fs, nullptr, rb, qtc, lane); break;
+                    default: break;
+                }
+            } else {
+                const int2 item = bk.pitems[bk.pbin_item[b0 + i]];
+                switch (bk.K) {
+                    case 1: cf::pair_item<1, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                    case 2: cf::pair_item<2, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                    case 3: cf::pair_item<3, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                    case 4: cf::pair_item<4, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                    case 5: cf::pair_item<5, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                    case 6: cf::pair_item<6, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                    case 7: cf::pair_item<7, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                    case 8: cf::pair_item<8, false, false, false, double>(bk.op, item, fs, nullptr, rb, qtc, lane); break;
+                    default: break;
+                }
             }
         }
         __syncthreads();
@@ -135,6 +159,7 @@ struct cf_ragged {
     std::vector<char> fused;   // per bucket: part of the fused launch
     std::vector<double> cost;  // relative cost of one half-tile of each bucket
     int tail_split = 4;
+    int family = 0;  // 0: pair routine, 1: tile routine
     Bucket* d_buckets = nullptr;
     Unit* d_units = nullptr;
     int* d_counter = nullptr;
@@ -173,7 +198,10 @@ int enqueue_contract(cf_ragged* r, cudaStream_t s) {
     if (r->n_units > 0) {
         RCHECK(cudaMemsetAsync(r->d_counter, 0, sizeof(int), s));
         const unsigned grid = (unsigned)std::min(r->n_units, r->ctas);
-        af_pair_ragged_kernel<<<grid, kRW * 32, r->smem, s>>>(r->d_buckets, r->d_units, r->n_units, r->d_counter);
+        if (r->family == 1)
+            af_ragged_kernel<true><<<grid, kTW * 32, r->smem, s>>>(r->d_buckets, r->d_units, r->n_units, r->d_counter);
+        else
+            af_ragged_kernel<false><<<grid, kRW * 32, r->smem, s>>>(r->d_buckets, r->d_units, r->n_units, r->d_counter);
         RCHECK(cudaGetLastError());
     }
     for (int b = 0; b < r->n_buckets; ++b) {
@@ -211,7 +239,7 @@ int enqueue_step(cf_ragged* r, double* const* q, const double* const* f, cudaStr
 extern "C" {
 
 int cf_ragged_create(cf_ragged** out, cf_plan* const* plans, const int64_t* cells, const int32_t* forms,
-                     int32_t n_buckets, int32_t tail_split) {
+                     int32_t n_buckets, int32_t tail_split, int32_t family) {
     if (!out || !plans || !cells || n_buckets < 1 || n_buckets > 64) {
         cf_set_last_error("cf_ragged_create: need 1..64 buckets");
         return CF_EINVAL;
@@ -220,10 +248,15 @@ int cf_ragged_create(cf_ragged** out, cf_plan* const* plans, const int64_t* cell
         cf_set_last_error("cf_ragged_create: tail_split must be 0, 4 or 16");
         return CF_EINVAL;
     }
+    if (family != 0 && family != 1) {
+        cf_set_last_error("cf_ragged_create: family must be 0 (pair routine) or 1 (tile routine)");
+        return CF_EINVAL;
+    }
     *out = nullptr;
     cf_ragged* r = new cf_ragged();
     r->n_buckets = n_buckets;
     r->tail_split = tail_split;
+    r->family = family;
     std::vector<Bucket> hb(n_buckets);
     int dev = -1;
     size_t max_smem = 0;
@@ -250,11 +283,14 @@ int cf_ragged_create(cf_ragged** out, cf_plan* const* plans, const int64_t* cell
             cf_set_last_error("cf_ragged_create: all plans must live on one device");
             return CF_EINVAL;
         }
-        const bool fused = (form == CF_FORM_AF || form == CF_FORM_AF_SYM) && info.k <= kMaxK;
+        const bool fused = (form == CF_FORM_AF || form == CF_FORM_AF_SYM) && info.k <= kMaxK && info.k >= 1 &&
+                           (family == 0 || info.k % 2 == 0);
         DevOp op{};
         const int* pbb = nullptr;
         const int* pbi = nullptr;
         const int2* pit = nullptr;
+        const int* tbb = nullptr;
+        const int* tbq = nullptr;
         cf_plan* view = plans[b];
         if (form == CF_FORM_AF_SYM) {
             // built here, never inside a graph recording (the build copies from the host)
@@ -266,8 +302,8 @@ int cf_ragged_create(cf_ragged** out, cf_plan* const* plans, const int64_t* cell
             }
             if (fused) view = folded;
         }
-        cf_plan_internal_view(view, &op, &pbb, &pbi, &pit, &n_sms, &max_smem);
-        hb[b] = Bucket{op, pbb, pbi, pit, nullptr, nullptr, info.k, info.n_q * info.k};
+        cf_plan_internal_view(view, &op, &pbb, &pbi, &pit, &tbb, &tbq, &n_sms, &max_smem);
+        hb[b] = Bucket{op, pbb, pbi, pit, tbb, tbq, nullptr, nullptr, info.k, info.n_q * info.k};
         r->form.push_back(form);
         r->fused.push_back(fused ? 1 : 0);
         r->plans.push_back(plans[b]);
@@ -285,18 +321,18 @@ int cf_ragged_create(cf_ragged** out, cf_plan* const* plans, const int64_t* cell
     cudaGetDevice(&cur);
     if (cur != dev) cudaSetDevice(dev);
     int st = CF_OK;
-    r->smem = sizeof(double) * ((size_t)kRW * kRBuf + max_M * cf::kTileCells);
+    const int W = family == 1 ? kTW : kRW;
+    r->smem = sizeof(double) * ((size_t)W * (family == 1 ? kRBufTile : kRBufPair) + max_M * cf::kTileCells);
+    const void* kern = family == 1 ? (const void*)af_ragged_kernel<true> : (const void*)af_ragged_kernel<false>;
     do {
         if (max_M > 0 && r->smem + 256 > max_smem) {
             cf_set_last_error("cf_ragged_create: the largest bucket's 16-cell tile does not fit in shared memory");
             st = CF_EUNSUPPORTED;
             break;
         }
-        cudaError_t e = cudaFuncSetAttribute(af_pair_ragged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)r->smem);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)r->smem);
         int per_sm = 0;
-        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, af_pair_ragged_kernel,
-                                                                                kRW * 32, r->smem);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, W * 32, r->smem);
         if (e != cudaSuccess || per_sm < 1) {
             cf_set_last_error("cf_ragged_create: fused kernel does not fit on this device");
             st = CF_EUNSUPPORTED;

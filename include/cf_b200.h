@@ -153,7 +153,8 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
                 int32_t exact, void* stream);
 
 /* Kernel family of a plan's angular-first and Jacobian contractions: 0 = automatic (the first of
- * split pair, pair, tile, gather that fits), 1 = the gather kernel (warp per row and 32-cell tile,
+ * pair, tile, gather that fits; tile before pair for the fast Q form of the folded operator, whose
+ * lighter Phi step favours the tile kernel's higher occupancy), 1 = the gather kernel (warp per row and 32-cell tile,
  * f read through L1/L2), 2 = the tile-resident kernel (16 cells in shared memory, Phi split over
  * two lanes per cell), 3 = the pair kernel (16 cells in shared memory, the mirrored rows (l,+m) and
  * (l,-m) on the two half-warps), 4 = the pair kernel reading R through L1 instead of shared
@@ -188,15 +189,17 @@ int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f_dev, int64
  * persistent launch.  cells[b] is bucket b's cell count; q_dev[b], f_dev[b] are its
  * [N_Q x K x cells[b]] device arrays.  forms[b] (NULL: all CF_FORM_AF) is the FP64 form of bucket b:
  * buckets in CF_FORM_AF or CF_FORM_AF_SYM with K <= 8 share the fused launch, any other bucket runs
- * its own plan's kernels in the same step.  tail_split (0, 4 or 16) is how many q1-pair bins each of
- * the last half-tiles of the fused work table is cut into, so that the launch ends evenly.
+ * its own plan's kernels in the same step.  family picks the routine of the fused launch: 0 the
+ * pair routine (8 warps per CTA), 1 the tile routine (16 warps per CTA; buckets of odd K then run
+ * on their own).  tail_split (0, 4 or 16) is how many bins each of the last half-tiles of the fused
+ * work table is cut into, so that the launch ends evenly.
  * cf_ragged_q enqueues pack, fused launch, the separate buckets and unpack on the stream;
  * cf_ragged_graph_launch records that sequence into a CUDA graph on first use (per set of buffers)
  * and replays it.  No counterpart in the reference (it contracts one f at a time).
  * ------------------------------------------------------------------------------------------ */
 typedef struct cf_ragged cf_ragged;
 int cf_ragged_create(cf_ragged** ragged, cf_plan* const* plans, const int64_t* cells, const int32_t* forms,
-                     int32_t n_buckets, int32_t tail_split);
+                     int32_t n_buckets, int32_t tail_split, int32_t family);
 int cf_ragged_destroy(cf_ragged* ragged);
 int cf_ragged_q(cf_ragged* ragged, double* const* q_dev, const double* const* f_dev, void* stream);
 int cf_ragged_graph_launch(cf_ragged* ragged, double* const* q_dev, const double* const* f_dev, void* stream);

@@ -41,20 +41,20 @@ def _oracle_q(oracle_lib, geo, R, K, f):
     return Qo.transpose(2, 1, 0)
 
 
-@pytest.mark.parametrize("tail_split", [0, 4, 16])
-def test_ragged_fused_equals_per_bucket_and_oracle(tail_split, cuda_available, oracle_lib):
+@pytest.mark.parametrize("tail_split,family", [(0, "pair"), (4, "pair"), (16, "pair"), (4, "tile"), (16, "tile")])
+def test_ragged_fused_equals_per_bucket_and_oracle(tail_split, family, cuda_available, oracle_lib):
     import torch
 
     from cf_b200.ragged import RaggedBatch
 
     ops = _bucket_ops(BUCKETS)
     fs = _cells(BUCKETS, CELLS)
-    rb = RaggedBatch([o for _, _, o in ops], CELLS, tail_split=tail_split)
+    rb = RaggedBatch([o for _, _, o in ops], CELLS, tail_split=tail_split, family=family)
     qs = [torch.zeros_like(f) for f in fs]
     rb.q(fs, qs)
     for (geo, R, op), f, q, (L, K) in zip(ops, fs, qs, BUCKETS):
-        op.set_kernel_path("pair")
-        assert torch.equal(q, op.q(f)), "the fused launch must equal the bucket's own pair kernel bit for bit"
+        op.set_kernel_path(family)
+        assert torch.equal(q, op.q(f)), f"the fused launch must equal the bucket's own {family} kernel bit for bit"
         assert per_cell_err(q.cpu().numpy(), _oracle_q(oracle_lib, geo, R, K, f)) <= 1e-12
     for _ in range(2):  # graph replay: same result, twice
         qg = [torch.zeros_like(f) for f in fs]
@@ -73,7 +73,7 @@ def test_ragged_mixed_forms(cuda_available, oracle_lib):
     forms = ["rf", "af_sym", "af", "af_sym"]
     ops = _bucket_ops(BUCKETS, seed=7)
     fs = _cells(BUCKETS, CELLS)
-    rb = RaggedBatch([o for _, _, o in ops], CELLS, forms=forms, tail_split=4)
+    rb = RaggedBatch([o for _, _, o in ops], CELLS, forms=forms, tail_split=4, family="pair")
     qs = [torch.full_like(f, 0.25) for f in fs]  # += semantics
     rb.q_graph(fs, qs)
     torch.cuda.synchronize()
@@ -96,6 +96,8 @@ def test_ragged_rejects_bad_input(cuda_available):
         RaggedBatch([o for _, _, o in ops], [3, 4], tail_split=5)
     with pytest.raises(CFError):
         RaggedBatch([o for _, _, o in ops], [3, 4], forms=["af", "af_f32"])
+    with pytest.raises(CFError):
+        RaggedBatch([o for _, _, o in ops], [3, 4], family="gather")
     rb = RaggedBatch([o for _, _, o in ops], [3, 4])
     fs = _cells(BUCKETS[:2], [3, 4])
     with pytest.raises(CFError):
@@ -107,9 +109,11 @@ def test_autotune_chooses_and_caches(cuda_available, tmp_path, monkeypatch):
 
     monkeypatch.setenv("CF_B200_CACHE", str(tmp_path))
     ops = [o for _, _, o in _bucket_ops(BUCKETS[:2])]
-    forms, tail, rep = ragged.autotune(ops, [64, 48], reps=2)
-    assert len(forms) == 2 and tail in (0, 4, 16) and not rep["cached"]
+    forms, tail, family, rep = ragged.autotune(ops, [64, 48], reps=2)
+    assert len(forms) == 2 and tail in (0, 4, 16) and family in ("pair", "tile") and not rep["cached"]
     for b in rep["buckets"]:
-        assert b["chosen"] == min(b["seconds"], key=b["seconds"].get)
-    forms2, tail2, rep2 = ragged.autotune(ops, [64, 48], reps=2)
-    assert rep2["cached"] and forms2 == forms and tail2 == tail
+        for fam, times in b["seconds"].items():
+            assert b["chosen"][fam] == min(times, key=times.get)
+    assert rep["step_seconds"][f"{family}/{tail}"] == min(rep["step_seconds"].values())
+    forms2, tail2, family2, rep2 = ragged.autotune(ops, [64, 48], reps=2)
+    assert rep2["cached"] and forms2 == forms and tail2 == tail and family2 == family
