@@ -44,6 +44,7 @@ WORKLOADS = {
     "hs_l16_k12_b1024": (16, 12, 1024, 1.0),
     "implicit_hs_l8_k8_b2048": (8, 8, 2048, 1.0),
     "ragged_hs_b16384": (10, 8, 16384, 1.0),  # largest bucket's (L, K); buckets in RAGGED_BUCKETS
+    "rtensor_hs_k7_l10": (10, 8, 0, 1.0),  # the R-tensor quadrature itself (pad 20)
 }
 RAGGED_BUCKETS = [(4, 4), (6, 6), (8, 6), (10, 8)]  # (L, K), drawn with RAGGED_WEIGHTS per cell
 R_FILES = {(10, 8): "R_hs_k7_l10_pad20.npy", (8, 8): "R_hs_k7_l8_pad20.npy"}
@@ -63,7 +64,7 @@ def parse_args(argv=None):
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--form", default="af", choices=["af", "af_sym", "af_exact", "rf"],
                     help="form launched by --profile")
-    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split"],
+    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split", "tile_quad"],
                     help="kernel family of the angular-first contraction")
     ap.add_argument("--profile", action="store_true",
                     help="only build the workload and launch the contraction (steps+1 times); for ncu captures")
@@ -336,7 +337,7 @@ def run_ours(args):
     sym_ms = timed(lambda: step("af_sym"), args.steps)
     sym_kern_ms = timed(lambda: kernel_only("af_sym"), max(2, args.steps // 2))
     path_ms, sym_path_ms = {}, {}
-    for path in ("pair_split", "pair", "pair_l1", "tile", "gather"):
+    for path in ("tile_quad", "pair_split", "pair", "pair_l1", "tile", "gather"):
         try:
             op.set_kernel_path(path)
             path_ms[path] = timed(step, max(2, args.steps // 4))
@@ -374,7 +375,8 @@ def run_ours(args):
     kern_name = {"pair": "af_pair_kernel (persistent, tile-resident, mirrored row pairs)",
                  "pair_split": "af_pair_kernel, split variant (both mirrored rows per lane, k3 halves)",
                  "pair_l1": "af_pair_kernel (R_t through L1)", "tile": "af_tile_kernel (persistent, tile-resident)",
-                 "gather": "af_kernel (gathers through L1/L2)"}.get(_lib.PATH_NAMES[op.info()["last_path"]], "?")
+                 "gather": "af_kernel (gathers through L1/L2)",
+                 "tile_quad": "af_tile_kernel, quad variant (cell pairs over k3 quarters)"}.get(_lib.PATH_NAMES[op.info()["last_path"]], "?")
     kern_s = sum(kern_list) / len(kern_list) / 1e3
     flops_launch = op.flops_q * B
     achieved_tf = flops_launch / kern_s / 1e12
@@ -850,9 +852,85 @@ def run_ragged(args):
     return out
 
 
+def run_rtensor(args):
+    """The reduced radial tensor R of hard spheres (K_max = 7, L = 10, pad 20) by the GPU quadrature
+    (cf_rtensor_sumfac), against the reference's compute_rtensor_sumfac_mex on the host cores."""
+    import torch
+
+    from cf_b200 import geometry, rtensor
+
+    L, K_max, pad = 10, 7, 20
+    geo = geometry.generate_geometry(L)
+    t0 = time.perf_counter()
+    in_args = rtensor.sumfac_inputs(geo, K_max, 1.0, pad, pad)
+    prep_s = time.perf_counter() - t0
+    steps = max(1, min(args.steps, 5))
+    rtensor.compute_R(in_args)  # warm-up (module load, first allocations)
+    times, dev_times = [], []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        tm = {}
+        R = rtensor.compute_R(in_args, timing=tm)
+        times.append(time.perf_counter() - t)
+        dev_times.append(tm["device_seconds"])
+    fix = ROOT / "tests" / "golden" / "R_hs_k7_l10_pad20.npy"
+    err = float(np.max(np.abs(R - np.load(fix))) / np.max(np.abs(R))) if fix.exists() else None
+    s = rtensor.grid_sizes(K_max, L, pad, pad)
+    points = s["N_x"] * (s["N_u1"] * s["N_t1"] + s["N_y2"] * s["N_t2"]) * s["N_chi"] * s["N_eps"]
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            from oracle.reference import Reference
+
+            ref = Reference("fast")
+            thr = ref.num_threads()
+            # The reference parallelises over the radial nodes x (OpenMP), and every node, every u of
+            # patch 1 and every y of patch 2 carries the same work.  Sample: one node per thread
+            # (all cores busy, one round) and the first n_u of the u and y nodes; scale the wall
+            # time by the rounds over all nodes and by the u / y fraction.
+            nx = min(thr, s["N_x"])
+            n_u = 2
+            smp = list(in_args)
+            smp[4], smp[5] = in_args[4][:nx], in_args[5][:nx]
+            smp[6], smp[7] = in_args[6][:n_u], in_args[7][:n_u]
+            smp[10], smp[11] = in_args[10][:n_u], in_args[11][:n_u]
+            smp[22] = np.asfortranarray(in_args[22][:, :n_u, :])
+            smp[23] = np.asfortranarray(in_args[23][:, :n_u, :, :])
+            smp[24] = np.asfortranarray(in_args[24][:n_u, :])
+            smp[25] = np.asfortranarray(in_args[25][:n_u, :, :])
+            t = time.perf_counter()
+            ref.call("ref_sumfac_mexFunction", smp, nlhs=1)
+            dt = time.perf_counter() - t
+            rounds = math.ceil(s["N_x"] / thr)
+            est = dt * rounds * (s["N_u1"] / n_u)
+            cpu = {"value": est, "unit": "s", "cores": thr, "kind": "reference",
+                   "sample": f"compute_rtensor_sumfac_mex compiled unmodified (-O3 -mavx2 -mfma, OpenMP over x) on "
+                             f"{nx} of {s['N_x']} radial nodes (one per thread) and {n_u} of the {s['N_u1']} u and "
+                             f"{s['N_y2']} y nodes: {dt:.1f} s wall, scaled by {rounds} node rounds and "
+                             f"{s['N_u1']}/{n_u}"}
+        except Exception as e:
+            cpu = {"value": None, "unit": "s", "cores": None, "kind": "reference", "sample": f"unavailable: {e}"}
+    gpu_s = sum(times) / len(times)
+    dev_s = sum(dev_times) / len(dev_times)
+    out = {"metric": "R-tensor quadrature time (hard spheres, K_max=7, L=10, pad 20)", "value": gpu_s, "unit": "s",
+           "n_gpus": 1, "steps": steps, "warmup": 1, "higher_is_better": False, "dtype": "f64",
+           "data": "the reference's quadrature inputs (restated driver)",
+           "config": {"workload": args.workload, "K_max": K_max, "L": L, "pad": pad, "N_L": int(in_args[1]),
+                      "quadrature_points": points, "input_preparation_s_host": prep_s},
+           "device_kernels_s": dev_s,
+           "host_side_s": gpu_s - dev_s,
+           "max_rel_err_vs_committed_reference_R": err, "cpu_baseline": cpu,
+           "speedup_vs_cpu_baseline": (cpu["value"] / gpu_s) if cpu and cpu.get("value") else None}
+    print(json.dumps(out), flush=True)
+    return out
+
+
 def main(argv=None):
     args = parse_args(argv)
-    if args.workload == "implicit_hs_l8_k8_b2048":
+    if args.workload == "rtensor_hs_k7_l10":
+        run_rtensor(args)
+    elif args.workload == "implicit_hs_l8_k8_b2048":
         run_implicit(args)
     elif args.workload == "ragged_hs_b16384" and args.impl == "ours" and not args.profile:
         run_ragged(args)

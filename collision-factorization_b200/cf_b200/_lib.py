@@ -32,7 +32,7 @@ EXPORTS = [
     "cf_plan_create", "cf_plan_destroy", "cf_plan_get_info", "cf_plan_workspace_size",
     "cf_q_device", "cf_q_device_ws", "cf_jv_device", "cf_q_device_noalloc",
     "cf_ragged_create", "cf_ragged_destroy", "cf_ragged_q", "cf_ragged_graph_launch", "cf_ragged_q_resident",
-    "cf_ragged_info", "cf_rk2_workspace_size", "cf_rk2_steps_tiled",
+    "cf_ragged_info", "cf_rk2_workspace_size", "cf_rk2_steps_tiled", "cf_rtensor_sumfac",
     "cf_gmres_workspace_size", "cf_gmres_solve_tiled",
     "cf_mlp_create", "cf_mlp_destroy", "cf_mlp_num_params", "cf_mlp_copy", "cf_mlp_forward", "cf_mlp_backward",
     "cf_mlp_adam_step", "cf_precond_probe_loss", "cf_precond_assemble",
@@ -54,7 +54,25 @@ class PlanInfo(C.Structure):
         ("device_bytes", C.c_int64), ("last_path", C.c_int32), ("reserved", C.c_int32),
     ]
 
-PATH_NAMES = {0: "none", 1: "gather", 2: "tile", 3: "pair", 4: "pair_l1", 5: "pair_split"}
+PATH_NAMES = {0: "none", 1: "gather", 2: "tile", 3: "pair", 4: "pair_l1", 5: "pair_split", 6: "tile_quad"}
+
+_DP = C.POINTER(C.c_double)
+
+
+class SumfacInputs(C.Structure):
+    """cf_sumfac_inputs: the 26 inputs of compute_rtensor_sumfac_mex."""
+    _fields_ = [
+        ("k_max", C.c_int32), ("n_l", C.c_int32), ("n_q", C.c_int32), ("alpha", C.c_double),
+        ("x_nodes", _DP), ("w_x", _DP), ("n_x", C.c_int32),
+        ("u1_nodes", _DP), ("w_u1", _DP), ("n_u1", C.c_int32),
+        ("t1_nodes", _DP), ("w_t1", _DP), ("n_t1", C.c_int32),
+        ("y2_nodes", _DP), ("w_y2", _DP), ("n_y2", C.c_int32),
+        ("t2_nodes", _DP), ("w_t2", _DP), ("n_t2", C.c_int32),
+        ("mu_chi", _DP), ("w_chi", _DP), ("n_chi", C.c_int32),
+        ("eps", _DP), ("w_eps", _DP), ("n_eps", C.c_int32),
+        ("radial_norm", _DP), ("sh_norm", _DP), ("l_triplets", _DP), ("qi_valid", _DP),
+        ("p_loss_p1", _DP), ("p_gain_p1", _DP), ("p_loss_p2", _DP), ("p_gain_p2", _DP),
+    ]
 
 
 _lib = None
@@ -96,6 +114,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_ragged_graph_launch.argtypes = [V, V, V, V]
     lib.cf_ragged_q_resident.argtypes = [V, V]
     lib.cf_rk2_workspace_size.argtypes = [V, _I64, C.POINTER(C.c_size_t)]
+    lib.cf_rtensor_sumfac.argtypes = [_D, C.POINTER(SumfacInputs), _I32, C.POINTER(C.c_double)]
     lib.cf_rk2_steps_tiled.argtypes = [V, V, _I64, C.c_double, _I32, _I32, V, C.c_size_t, V]
     lib.cf_ragged_info.argtypes = [V, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(C.c_int64), C.POINTER(_I32)]
     lib.cf_mlp_create.argtypes = [C.POINTER(V), _I32, _I32, _I32, _I32, C.c_uint64, _I32]

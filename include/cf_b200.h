@@ -211,6 +211,36 @@ int cf_ragged_q_resident(cf_ragged* ragged, void* stream);
 int cf_ragged_info(const cf_ragged* ragged, int32_t* n_units, int32_t* ctas, int64_t* smem_bytes, int32_t* n_fused);
 
 /* ------------------------------------------------------------------------------------------
+ * The reduced radial tensor R on the GPU: replaces compute_rtensor_sumfac_mex
+ * (src/mex/compute_rtensor_sumfac_mex.cpp:80-397), whose 26 inputs GeneralCollisionTensor.m:177-181
+ * prepares; the fields below are those inputs in order (arrays column-major doubles as MATLAB
+ * passes them, sizes taken from their lengths).  R_out (host, N_K^3 x N_L doubles with
+ * N_K = k_max + 1) receives the quadrature, before the conservation rows are zeroed (the driver
+ * does that, GeneralCollisionTensor.m:184-191).  k_max + 1 <= 12, N_Q = (L+1)^2 with L <= 31.
+ * ------------------------------------------------------------------------------------------ */
+typedef struct cf_sumfac_inputs {
+    int32_t k_max, n_l, n_q;
+    double alpha;                                   /* gamma: B = |u|^gamma                       */
+    const double *x_nodes, *w_x;   int32_t n_x;     /* generalised Laguerre nodes and weights     */
+    const double *u1_nodes, *w_u1; int32_t n_u1;    /* patch 1: u outer                           */
+    const double *t1_nodes, *w_t1; int32_t n_t1;    /* patch 1: t inner                           */
+    const double *y2_nodes, *w_y2; int32_t n_y2;    /* patch 2: y outer                           */
+    const double *t2_nodes, *w_t2; int32_t n_t2;    /* patch 2: t inner                           */
+    const double *mu_chi, *w_chi;  int32_t n_chi;   /* scattering angle cosines                   */
+    const double *eps, *w_eps;     int32_t n_eps;   /* azimuths                                   */
+    const double *radial_norm;                      /* [N_K x (L+1)]                               */
+    const double *sh_norm;                          /* [N_Q]                                       */
+    const double *l_triplets;                       /* [N_L x 3]                                   */
+    const double *qi_valid;                         /* [N_Q x N_L], 1-based, -1 terminated         */
+    const double *p_loss_p1;                        /* [n_t1 x n_u1 x N_L]                         */
+    const double *p_gain_p1;                        /* [n_t1 x n_u1 x N_Q x N_L]                   */
+    const double *p_loss_p2;                        /* [n_y2 x N_L]                                */
+    const double *p_gain_p2;                        /* [n_y2 x N_Q x N_L]                          */
+} cf_sumfac_inputs;
+/* device_seconds (may be NULL) receives the device time of the quadrature kernels. */
+int cf_rtensor_sumfac(double* R_out, const cf_sumfac_inputs* inputs, int32_t device, double* device_seconds);
+
+/* ------------------------------------------------------------------------------------------
  * Explicit time stepping df/dt = Q(f) for a batch of cells, Heun's method (RK2):
  * f <- f + dt/2 (Q(f) + Q(f + dt Q(f))), n_steps times, in the tiled layout (cf_pack_cells), with
  * the contraction in `form` (any FP64 form).  The reference steps one cell with its dense tensor
