@@ -64,7 +64,7 @@ def parse_args(argv=None):
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--form", default="af", choices=["af", "af_sym", "af_exact", "rf"],
                     help="form launched by --profile")
-    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split", "tile_quad"],
+    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split"],
                     help="kernel family of the angular-first contraction")
     ap.add_argument("--profile", action="store_true",
                     help="only build the workload and launch the contraction (steps+1 times); for ncu captures")
@@ -337,7 +337,7 @@ def run_ours(args):
     sym_ms = timed(lambda: step("af_sym"), args.steps)
     sym_kern_ms = timed(lambda: kernel_only("af_sym"), max(2, args.steps // 2))
     path_ms, sym_path_ms = {}, {}
-    for path in ("tile_quad", "pair_split", "pair", "pair_l1", "tile", "gather"):
+    for path in ("pair_split", "pair", "pair_l1", "tile", "gather"):
         try:
             op.set_kernel_path(path)
             path_ms[path] = timed(step, max(2, args.steps // 4))
@@ -375,8 +375,7 @@ def run_ours(args):
     kern_name = {"pair": "af_pair_kernel (persistent, tile-resident, mirrored row pairs)",
                  "pair_split": "af_pair_kernel, split variant (both mirrored rows per lane, k3 halves)",
                  "pair_l1": "af_pair_kernel (R_t through L1)", "tile": "af_tile_kernel (persistent, tile-resident)",
-                 "gather": "af_kernel (gathers through L1/L2)",
-                 "tile_quad": "af_tile_kernel, quad variant (cell pairs over k3 quarters)"}.get(_lib.PATH_NAMES[op.info()["last_path"]], "?")
+                 "gather": "af_kernel (gathers through L1/L2)"}.get(_lib.PATH_NAMES[op.info()["last_path"]], "?")
     kern_s = sum(kern_list) / len(kern_list) / 1e3
     flops_launch = op.flops_q * B
     achieved_tf = flops_launch / kern_s / 1e12
@@ -549,6 +548,8 @@ def run_reference(args):
     if not reference_available("fast"):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_fast.so not built"}), flush=True)
         return None
+    if args.workload == "ragged_hs_b16384":
+        return run_reference_ragged(args, world)
     geo, R, r_source = make_operator(L, K, gamma, args.seed)
     ref = Reference("fast")
     nthreads = ref.num_threads()
@@ -585,6 +586,55 @@ def run_reference(args):
         "data": "synthetic (same seeded cells as the GPU arm)",
         "config": {"workload": args.workload, "L": L, "K": K, "M": geo.n_q * K, "gamma": gamma, "R": r_source,
                    "cells_per_step": n},
+        "cpu_baseline": {"value": value, "unit": "cell-evals/s", "cores": nthreads, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "cell-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return out
+
+
+def run_reference_ragged(args, world):
+    """Reference arm of the ragged workload: every step contracts a sample of each bucket's cells, in
+    the batch's bucket proportions, with the reference kernel on all host cores."""
+    from cf_b200 import workloads
+    from oracle.reference import Reference
+
+    ref = Reference("fast")
+    nthreads = ref.num_threads()
+    B = WORKLOADS[args.workload][2]
+    assign = workloads.ragged_assignment(B, seed=rank_seed(args.seed, 0))
+    counts = [int(np.sum(assign == b)) for b in range(len(RAGGED_BUCKETS))]
+    frac = 1024.0 / B  # about 1024 cells per step, mixed as in the batch
+    per = [max(1, int(round(c * frac))) for c in counts]
+    ops = []
+    for b, (L, K) in enumerate(RAGGED_BUCKETS):
+        geo, R, _ = make_operator(L, K, 1.0, args.seed + 17 * b)
+        cells = make_cells(L, K, per[b], seed=args.seed + 101 * b)
+        ops.append((geo, R, K, np.asfortranarray(cells.transpose(2, 1, 0))))
+
+    def one():
+        for geo, R, K, f in ops:
+            Q = np.zeros_like(f, order="F")
+            ref.batch("af", Q, f, geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K, nthreads=nthreads)
+
+    for _ in range(args.warmup):
+        one()
+    times = []
+    for _ in range(args.steps):
+        t = time.perf_counter()
+        one()
+        times.append(time.perf_counter() - t)
+    n = sum(per)
+    value = n * args.steps / sum(times)
+    sample = (f"{n} cells per step ({', '.join(f'{p} of L={L} K={K}' for p, (L, K) in zip(per, RAGGED_BUCKETS))}) "
+              f"through angular_first_collision_kernel_mex compiled unmodified, one call per cell, OpenMP over cells")
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-evals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded cells in the batch's bucket proportions)",
+        "config": {"workload": args.workload, "buckets": RAGGED_BUCKETS, "cells_per_step": n},
         "cpu_baseline": {"value": value, "unit": "cell-evals/s", "cores": nthreads, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "cell-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -852,6 +902,61 @@ def run_ragged(args):
     return out
 
 
+def cpu_sumfac_estimate(in_args, s) -> dict:
+    """The reference's compute_rtensor_sumfac_mex on the host cores, on a bounded sample.
+
+    The reference parallelises over the radial nodes x (OpenMP), and every node, every u of patch 1
+    and every y of patch 2 carries the same work.  Sample: one node per thread (all cores busy, one
+    round) and the first 2 of the u and y nodes; the wall time is scaled by the rounds over all
+    nodes and by the u / y fraction (N_u1 = N_y2 for these grids)."""
+    try:
+        from oracle.reference import Reference
+
+        ref = Reference("fast")
+        thr = ref.num_threads()
+        nx = min(thr, s["N_x"])
+        n_u = 2
+        smp = list(in_args)
+        smp[4], smp[5] = in_args[4][:nx], in_args[5][:nx]
+        smp[6], smp[7] = in_args[6][:n_u], in_args[7][:n_u]
+        smp[10], smp[11] = in_args[10][:n_u], in_args[11][:n_u]
+        smp[22] = np.asfortranarray(in_args[22][:, :n_u, :])
+        smp[23] = np.asfortranarray(in_args[23][:, :n_u, :, :])
+        smp[24] = np.asfortranarray(in_args[24][:n_u, :])
+        smp[25] = np.asfortranarray(in_args[25][:n_u, :, :])
+        t = time.perf_counter()
+        ref.call("ref_sumfac_mexFunction", smp, nlhs=1)
+        dt = time.perf_counter() - t
+        rounds = math.ceil(s["N_x"] / thr)
+        return {"value": dt * rounds * (s["N_u1"] / n_u), "unit": "s", "cores": thr, "kind": "reference",
+                "sample": f"compute_rtensor_sumfac_mex compiled unmodified (-O3 -mavx2 -mfma, OpenMP over x) on "
+                          f"{nx} of {s['N_x']} radial nodes (one per thread) and {n_u} of the {s['N_u1']} u and "
+                          f"{s['N_y2']} y nodes: {dt:.1f} s wall, scaled by {rounds} node rounds and "
+                          f"{s['N_u1']}/{n_u}"}
+    except Exception as e:
+        return {"value": None, "unit": "s", "cores": None, "kind": "reference", "sample": f"unavailable: {e}"}
+
+
+def run_reference_rtensor(args):
+    """Reference arm of the R-tensor workload: the compiled sumfac MEX on the host cores."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return None
+    from cf_b200 import geometry, rtensor
+
+    L, K_max, pad = 10, 7, 20
+    in_args = rtensor.sumfac_inputs(geometry.generate_geometry(L), K_max, 1.0, pad, pad)
+    s = rtensor.grid_sizes(K_max, L, pad, pad)
+    cpu = cpu_sumfac_estimate(in_args, s)
+    out = {"impl": "reference", "metric": "R-tensor quadrature time (hard spheres, K_max=7, L=10, pad 20)",
+           "value": cpu["value"], "unit": "s", "n_gpus": 1, "steps": 1, "warmup": 0, "higher_is_better": False,
+           "dtype": "f64", "data": "the reference's quadrature inputs (restated driver)",
+           "config": {"workload": args.workload, "K_max": K_max, "L": L, "pad": pad},
+           "cpu_baseline": cpu, "e2e": {"value": cpu["value"], "unit": "s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return out
+
+
 def run_rtensor(args):
     """The reduced radial tensor R of hard spheres (K_max = 7, L = 10, pad 20) by the GPU quadrature
     (cf_rtensor_sumfac), against the reference's compute_rtensor_sumfac_mex on the host cores."""
@@ -878,39 +983,7 @@ def run_rtensor(args):
     err = float(np.max(np.abs(R - np.load(fix))) / np.max(np.abs(R))) if fix.exists() else None
     s = rtensor.grid_sizes(K_max, L, pad, pad)
     points = s["N_x"] * (s["N_u1"] * s["N_t1"] + s["N_y2"] * s["N_t2"]) * s["N_chi"] * s["N_eps"]
-    cpu = None
-    if not args.no_cpu_baseline:
-        try:
-            from oracle.reference import Reference
-
-            ref = Reference("fast")
-            thr = ref.num_threads()
-            # The reference parallelises over the radial nodes x (OpenMP), and every node, every u of
-            # patch 1 and every y of patch 2 carries the same work.  Sample: one node per thread
-            # (all cores busy, one round) and the first n_u of the u and y nodes; scale the wall
-            # time by the rounds over all nodes and by the u / y fraction.
-            nx = min(thr, s["N_x"])
-            n_u = 2
-            smp = list(in_args)
-            smp[4], smp[5] = in_args[4][:nx], in_args[5][:nx]
-            smp[6], smp[7] = in_args[6][:n_u], in_args[7][:n_u]
-            smp[10], smp[11] = in_args[10][:n_u], in_args[11][:n_u]
-            smp[22] = np.asfortranarray(in_args[22][:, :n_u, :])
-            smp[23] = np.asfortranarray(in_args[23][:, :n_u, :, :])
-            smp[24] = np.asfortranarray(in_args[24][:n_u, :])
-            smp[25] = np.asfortranarray(in_args[25][:n_u, :, :])
-            t = time.perf_counter()
-            ref.call("ref_sumfac_mexFunction", smp, nlhs=1)
-            dt = time.perf_counter() - t
-            rounds = math.ceil(s["N_x"] / thr)
-            est = dt * rounds * (s["N_u1"] / n_u)
-            cpu = {"value": est, "unit": "s", "cores": thr, "kind": "reference",
-                   "sample": f"compute_rtensor_sumfac_mex compiled unmodified (-O3 -mavx2 -mfma, OpenMP over x) on "
-                             f"{nx} of {s['N_x']} radial nodes (one per thread) and {n_u} of the {s['N_u1']} u and "
-                             f"{s['N_y2']} y nodes: {dt:.1f} s wall, scaled by {rounds} node rounds and "
-                             f"{s['N_u1']}/{n_u}"}
-        except Exception as e:
-            cpu = {"value": None, "unit": "s", "cores": None, "kind": "reference", "sample": f"unavailable: {e}"}
+    cpu = None if args.no_cpu_baseline else cpu_sumfac_estimate(in_args, s)
     gpu_s = sum(times) / len(times)
     dev_s = sum(dev_times) / len(dev_times)
     out = {"metric": "R-tensor quadrature time (hard spheres, K_max=7, L=10, pad 20)", "value": gpu_s, "unit": "s",
@@ -928,16 +1001,30 @@ def run_rtensor(args):
 
 def main(argv=None):
     args = parse_args(argv)
-    if args.workload == "rtensor_hs_k7_l10":
+    if args.impl == "reference":
+        if args.workload == "implicit_hs_l8_k8_b2048":
+            if int(os.environ.get("RANK", "0")) == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no implicit solver, "
+                                  "Jacobian apply or preconditioner (it steps explicitly with a dense tensor)"}),
+                      flush=True)
+        elif args.workload == "rtensor_hs_k7_l10":
+            run_reference_rtensor(args)
+        else:
+            run_reference(args)
+    elif args.workload == "rtensor_hs_k7_l10" and args.profile:
+        # for ncu: one quadrature of a small operator (hard spheres K_max = 4, L = 4, pad 20)
+        from cf_b200 import geometry, rtensor
+
+        R = rtensor.compute_R(rtensor.sumfac_inputs(geometry.generate_geometry(4), 4, 1.0, 20, 20))
+        print(json.dumps({"profile": "rtensor hs K_max=4 L=4 pad 20", "R_abs_max": float(np.abs(R).max())}))
+    elif args.workload == "rtensor_hs_k7_l10":
         run_rtensor(args)
     elif args.workload == "implicit_hs_l8_k8_b2048":
         run_implicit(args)
-    elif args.workload == "ragged_hs_b16384" and args.impl == "ours" and not args.profile:
-        run_ragged(args)
     elif args.profile:
         run_profile(args)
-    elif args.impl == "reference":
-        run_reference(args)
+    elif args.workload == "ragged_hs_b16384":
+        run_ragged(args)
     else:
         run_ours(args)
     return 0

@@ -64,13 +64,12 @@ static LaunchResult launch_af(const LaunchArgs& a) {
 
 // Tile-resident persistent kernel.  Returns status -1 when it does not fit (shared memory or
 // occupancy), in which case the caller uses the gather kernel.
-template <int K, int W, bool EXACT, bool JV, bool QUAD = false>
+template <int K, int W, bool EXACT, bool JV>
 static LaunchResult launch_tile(const LaunchArgs& a) {
-    static_assert(!QUAD || (!EXACT && !JV && K % 4 == 0), "the quad variant is the fast Q form");
     const int M = a.op.n_q * K;
     const size_t smem = tile_smem_bytes<K>(M, W, JV);
     if (smem + 256 > a.max_smem || a.counter == nullptr) return {-1, 0, cudaSuccess, PATH_TILE};
-    auto kern = af_tile_kernel<K, W, EXACT, JV, QUAD>;
+    auto kern = af_tile_kernel<K, W, EXACT, JV>;
     int per_sm = 0;
     cudaError_t e = resident_ctas((const void*)kern, W * 32, smem, &per_sm);
     if (e != cudaSuccess) return {5, 0, e, PATH_TILE};
@@ -94,7 +93,7 @@ static LaunchResult launch_tile(const LaunchArgs& a) {
     const unsigned grid = (unsigned)(n_units < ctas ? n_units : ctas);
     kern<<<grid, W * 32, smem, a.stream>>>(a.op, sc, a.fT, a.vT, a.QT);
     e = cudaGetLastError();
-    return {e == cudaSuccess ? 0 : 5, 1, e, QUAD ? PATH_TILE_QUAD : PATH_TILE};
+    return {e == cudaSuccess ? 0 : 5, 1, e, PATH_TILE};
 }
 
 // Work-unit schedule shared by the persistent kernels: whole half-tiles while there are more
@@ -176,14 +175,8 @@ static LaunchResult launch_for_k(const LaunchArgs& a) {
     }
     if (a.what == OP_RF) return a.exact ? launch_rf<K, true>(a) : launch_rf<K, false>(a);
     const bool jv = a.what == OP_JV;
-    if constexpr (K % 4 == 0 && K <= 8) {
-        if (a.path == PATH_TILE_QUAD && !jv && !a.exact) {
-            const LaunchResult r = launch_tile<K, 12, false, false, true>(a);
-            if (r.status != -1) return r;
-        }
-    }
     if constexpr (K % 2 == 0 && K <= 8) {
-        if ((a.path == PATH_AUTO && a.tile_first && !jv && !a.exact) || a.path == PATH_TILE_QUAD) {
+        if (a.path == PATH_AUTO && a.tile_first && !jv && !a.exact) {
             const LaunchResult r = launch_tile<K, tile_W(K, false), false, false>(a);
             if (r.status != -1) return r;
         }

@@ -1025,10 +1025,10 @@ extern "C" {
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    if (path < 0 || path > 6)
+    if (path < 0 || path > 5)
         return fail(CF_EINVAL,
-                    "kernel path %d is not 0 (auto), 1 (gather), 2 (tile), 3 (pair), 4 (pair, R via L1), 5 (pair, "
-                    "split rows) or 6 (tile, cell pairs over k3 quarters)",
+                    "kernel path %d is not 0 (auto), 1 (gather), 2 (tile), 3 (pair), 4 (pair, R via L1) or 5 (pair, "
+                    "split rows)",
                     path);
     std::lock_guard<std::mutex> lk(plan->mu);
     plan->path = path;

@@ -526,8 +526,9 @@ int cf_rtensor_sumfac(double* R_out, const cf_sumfac_inputs* in, int32_t device,
     RT_CHECK(upload(&d.pgain1, pg1.data(), pg1.size(), owned));
     RT_CHECK(upload(&d.ploss2, in->p_loss_p2, (size_t)in->n_y2 * NL, owned));
     RT_CHECK(upload(&d.pgain2, pg2.data(), pg2.size(), owned));
-    // chunk of items: the net vectors of a chunk take at most ~1 GiB
-    chunk = std::max<int64_t>(1, std::min<int64_t>(n_items, ((int64_t)1 << 30) / ((int64_t)NL * 2 * NK * 8)));
+    // chunk of items: the net vectors of a chunk (written by k_items, read once by k_contract) stay
+    // within 48 MB, so they live in the 126 MB L2 between the two kernels instead of crossing HBM
+    chunk = std::max<int64_t>(1, std::min<int64_t>(n_items, ((int64_t)48 << 20) / ((int64_t)NL * 2 * NK * 8)));
     chunk = std::min<int64_t>(chunk, 65535);  // grid x of k_items
     RT_CHECK(cudaMalloc((void**)&net, (size_t)chunk * NL * 2 * NK * sizeof(double)));
     owned.push_back(net);

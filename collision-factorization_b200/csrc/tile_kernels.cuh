@@ -199,116 +199,7 @@ __device__ __forceinline__ void tile_q1(const DevOp& op, int q1, const double* _
     }
 }
 
-// Quad variant (fast Q form, K a multiple of 4): lane = (cell pair p = lane & 7, k3 quarter
-// qt = lane >> 3).  A lane holds Phi over all k2, its quarter of k3, for TWO cells, so every R_t
-// value it reads in the K^3 step feeds two FMAs and the K^3 step reads half the shared-memory
-// wavefronts of tile_q1 (the Phi step reads the same bytes: f2 rows as 16-byte cell pairs, f3 rows
-// split over the quarters).  The four quarters' partial row sums meet with two shuffles per k1.
-template <int K>
-__device__ __forceinline__ void tile_q1_quad(const DevOp& op, int q1, const double* __restrict__ fs, double* rb,
-                                             double* qtc_lane, int lane) {
-    static_assert(K % 4 == 0, "the quad variant splits k3 into four quarters");
-    constexpr int KQ = K / 4;
-    constexpr int SL = RBuf<K>::SL;
-    const int p = lane & 7, qt = lane >> 3;
-    const int k3b = qt * KQ;
-    double* qtc = qtc_lane - (lane & 15) + 2 * p;  // this lane's two cells: 2p, 2p + 1
-
-    double acc[K][2];
-#pragma unroll
-    for (int k1 = 0; k1 < K; ++k1) {
-        acc[k1][0] = qt == 0 ? qtc[(size_t)(q1 * K + k1) * CF_TILE] : 0.0;
-        acc[k1][1] = qt == 0 ? qtc[(size_t)(q1 * K + k1) * CF_TILE + 1] : 0.0;
-    }
-
-    const int s0 = op.q1_begin[q1], s1 = op.q1_begin[q1 + 1];
-    for (int s = s0; s < s1; ++s) {
-        const int t = op.slice_t[s];
-        const int e0 = op.slice_e[s], e1 = op.slice_e[s + 1];
-        __syncwarp();
-        const double* __restrict__ Rt = op.R + (size_t)t * K * K * K;
-        for (int i = lane; i < K * K * K / 2; i += 32) {
-            const int j = (2 * i) / (K * K), w = (2 * i) % (K * K);
-            cp_async16(rb + j * SL + w, Rt + 2 * i);
-        }
-        cp_async_commit();
-
-        double phi[K][KQ][2];
-#pragma unroll
-        for (int a = 0; a < K; ++a)
-#pragma unroll
-            for (int b = 0; b < KQ; ++b) {
-                phi[a][b][0] = 0.0;
-                phi[a][b][1] = 0.0;
-            }
-
-        for (int eb = e0; eb < e1; eb += 32) {
-            const int n = min(32, e1 - eb);
-            uint32_t my_q23 = 0;
-            double my_g = 0.0;
-            if (lane < n) {
-                my_q23 = __ldg(op.e_q23 + eb + lane);
-                my_g = __ldg(op.e_g + eb + lane);
-            }
-            for (int j = 0; j < n; ++j) {
-                const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, j);
-                const double g = __shfl_sync(0xffffffffu, my_g, j);
-                const int r2 = (int)(q23 & 0xffffu) * K, r3 = (int)(q23 >> 16) * K + k3b;
-                double gf3[KQ][2];
-#pragma unroll
-                for (int b = 0; b < KQ; ++b) {
-                    const double2 f3 = *reinterpret_cast<const double2*>(fs + (r3 + b) * kTileCells + 2 * p);
-                    gf3[b][0] = g * f3.x;
-                    gf3[b][1] = g * f3.y;
-                }
-#pragma unroll
-                for (int k2 = 0; k2 < K; ++k2) {
-                    const double2 f2 = *reinterpret_cast<const double2*>(fs + (r2 + k2) * kTileCells + 2 * p);
-#pragma unroll
-                    for (int b = 0; b < KQ; ++b) {
-                        phi[k2][b][0] = fma(f2.x, gf3[b][0], phi[k2][b][0]);
-                        phi[k2][b][1] = fma(f2.y, gf3[b][1], phi[k2][b][1]);
-                    }
-                }
-            }
-        }
-        cp_async_wait_all();
-        __syncwarp();
-
-        // K^3 step: element (k1,k2,k3) at rb[k3*SL + k2*K + k1], this lane's k3 quarter
-        const double* __restrict__ rk = rb + k3b * SL;
-#pragma unroll
-        for (int b = 0; b < KQ; ++b)
-#pragma unroll
-            for (int k2 = 0; k2 < K; ++k2) {
-                const double2* r2v = reinterpret_cast<const double2*>(rk + b * SL + k2 * K);
-#pragma unroll
-                for (int h = 0; h < K / 2; ++h) {
-                    const double2 r = r2v[h];
-                    acc[2 * h][0] = fma(r.x, phi[k2][b][0], acc[2 * h][0]);
-                    acc[2 * h][1] = fma(r.x, phi[k2][b][1], acc[2 * h][1]);
-                    acc[2 * h + 1][0] = fma(r.y, phi[k2][b][0], acc[2 * h + 1][0]);
-                    acc[2 * h + 1][1] = fma(r.y, phi[k2][b][1], acc[2 * h + 1][1]);
-                }
-            }
-    }
-#pragma unroll
-    for (int k1 = 0; k1 < K; ++k1)
-#pragma unroll
-        for (int cl = 0; cl < 2; ++cl) {
-            acc[k1][cl] += __shfl_xor_sync(0xffffffffu, acc[k1][cl], 8);
-            acc[k1][cl] += __shfl_xor_sync(0xffffffffu, acc[k1][cl], 16);
-        }
-    if (qt == 0) {
-#pragma unroll
-        for (int k1 = 0; k1 < K; ++k1) {
-            double2* out = reinterpret_cast<double2*>(qtc + (size_t)(q1 * K + k1) * CF_TILE);
-            *out = make_double2(acc[k1][0], acc[k1][1]);
-        }
-    }
-}
-
-template <int K, int W, bool EXACT, bool JV, bool QUAD = false>
+template <int K, int W, bool EXACT, bool JV>
 __global__ void __launch_bounds__(W * 32, 1)
     af_tile_kernel(DevOp op, TileSched sc, const double* __restrict__ fT, const double* __restrict__ vT,
                    double* __restrict__ QT) {
@@ -364,10 +255,7 @@ __global__ void __launch_bounds__(W * 32, 1)
             if (lane == 0) i = atomicAdd(&s_next, 1);
             i = __shfl_sync(0xffffffffu, i, 0);
             if (i >= nb) break;
-            if constexpr (QUAD)
-                tile_q1_quad<K>(op, sc.bin_q1[b0 + i], fs, rb, qtc, lane);
-            else
-                tile_q1<K, EXACT, JV>(op, sc.bin_q1[b0 + i], fs, vs, rb, qtc, lane);
+            tile_q1<K, EXACT, JV>(op, sc.bin_q1[b0 + i], fs, vs, rb, qtc, lane);
         }
         __syncthreads();
     }
