@@ -64,7 +64,7 @@ def parse_args(argv=None):
     ap.add_argument("--epochs", type=int, default=12)
     ap.add_argument("--form", default="af", choices=["af", "af_sym", "af_exact", "rf"],
                     help="form launched by --profile")
-    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split"],
+    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split", "tile_mma"],
                     help="kernel family of the angular-first contraction")
     ap.add_argument("--profile", action="store_true",
                     help="only build the workload and launch the contraction (steps+1 times); for ncu captures")
@@ -337,7 +337,7 @@ def run_ours(args):
     sym_ms = timed(lambda: step("af_sym"), args.steps)
     sym_kern_ms = timed(lambda: kernel_only("af_sym"), max(2, args.steps // 2))
     path_ms, sym_path_ms = {}, {}
-    for path in ("pair_split", "pair", "pair_l1", "tile", "gather"):
+    for path in ("tile_mma", "pair_split", "pair", "pair_l1", "tile", "gather"):
         try:
             op.set_kernel_path(path)
             path_ms[path] = timed(step, max(2, args.steps // 4))
@@ -375,7 +375,8 @@ def run_ours(args):
     kern_name = {"pair": "af_pair_kernel (persistent, tile-resident, mirrored row pairs)",
                  "pair_split": "af_pair_kernel, split variant (both mirrored rows per lane, k3 halves)",
                  "pair_l1": "af_pair_kernel (R_t through L1)", "tile": "af_tile_kernel (persistent, tile-resident)",
-                 "gather": "af_kernel (gathers through L1/L2)"}.get(_lib.PATH_NAMES[op.info()["last_path"]], "?")
+                 "gather": "af_kernel (gathers through L1/L2)",
+                 "tile_mma": "af_mma_kernel (tile-resident, K^3 step on the FP64 MMA)"}.get(_lib.PATH_NAMES[op.info()["last_path"]], "?")
     kern_s = sum(kern_list) / len(kern_list) / 1e3
     flops_launch = op.flops_q * B
     achieved_tf = flops_launch / kern_s / 1e12

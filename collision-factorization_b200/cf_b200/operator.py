@@ -118,7 +118,7 @@ class CollisionOperator:
 
     def set_kernel_path(self, path: str) -> None:
         """'auto' (default), 'gather', 'tile', 'pair' or 'pair_l1': the kernel family of the AF and J.v forms."""
-        code = {"auto": 0, "gather": 1, "tile": 2, "pair": 3, "pair_l1": 4, "pair_split": 5}[path]
+        code = {"auto": 0, "gather": 1, "tile": 2, "pair": 3, "pair_l1": 4, "pair_split": 5, "tile_mma": 6}[path]
         _lib.check(_lib.load().cf_plan_set_kernel_path(self._h, code))
 
     def workspace_bytes(self, B: int, jacobian: bool = False) -> int:

@@ -7,6 +7,7 @@
 #include "launch.cuh"
 #include "tile_kernels.cuh"
 #include "pair_kernels.cuh"
+#include "mma_kernels.cuh"
 
 namespace cf {
 
@@ -141,6 +142,28 @@ static LaunchResult launch_pair(const LaunchArgs& a) {
     return {e == cudaSuccess ? 0 : 5, 1, e, SPLIT ? PATH_PAIR_SPLIT : (RG ? PATH_PAIR_L1 : PATH_PAIR)};
 }
 
+// Tile-resident kernel with the K^3 step on the FP64 MMA (K = 8, fast Q form).
+template <int W>
+static LaunchResult launch_mma(const LaunchArgs& a) {
+    const int M = a.op.n_q * kMmaK;
+    const size_t smem = mma_smem_bytes(M, W);
+    if (smem + 256 > a.max_smem || a.counter == nullptr || a.op.RT == nullptr) return {-1, 0, cudaSuccess, PATH_TILE_MMA};
+    auto kern = af_mma_kernel<W>;
+    int per_sm = 0;
+    cudaError_t e = resident_ctas((const void*)kern, W * 32, smem, &per_sm);
+    if (e != cudaSuccess) return {5, 0, e, PATH_TILE_MMA};
+    if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_TILE_MMA};
+    const int64_t ctas = (int64_t)per_sm * a.n_sms;
+    const UnitPlan up = plan_units(a.n_cells, ctas);
+    TileSched sc{a.bin_begin, a.bin_q1, up.n_ht, up.n_whole, up.split, up.n_units, a.counter};
+    e = cudaMemsetAsync(a.counter, 0, sizeof(int), a.stream);
+    if (e != cudaSuccess) return {5, 0, e, PATH_TILE_MMA};
+    const unsigned grid = (unsigned)(up.n_units < ctas ? up.n_units : ctas);
+    kern<<<grid, W * 32, smem, a.stream>>>(a.op, sc, a.fT, a.QT);
+    e = cudaGetLastError();
+    return {e == cudaSuccess ? 0 : 5, 1, e, PATH_TILE_MMA};
+}
+
 template <int K, bool EXACT>
 static LaunchResult launch_rf(const LaunchArgs& a) {
     const int64_t warps = (int64_t)a.op.n_items * a.n_tiles;
@@ -175,6 +198,18 @@ static LaunchResult launch_for_k(const LaunchArgs& a) {
     }
     if (a.what == OP_RF) return a.exact ? launch_rf<K, true>(a) : launch_rf<K, false>(a);
     const bool jv = a.what == OP_JV;
+    if (a.path == PATH_TILE_MMA) {
+        if constexpr (K == kMmaK) {
+            if (!jv && !a.exact) {
+                const LaunchResult r = launch_mma<16>(a);
+                if (r.status != -1) return r;
+            }
+        }
+        // the MMA kernel is the fast Q form at K = 8: anything else runs as PATH_TILE
+        LaunchArgs b = a;
+        b.path = PATH_TILE;
+        return launch_for_k<K>(b);
+    }
     if constexpr (K % 2 == 0 && K <= 8) {
         if (a.path == PATH_AUTO && a.tile_first && !jv && !a.exact) {
             const LaunchResult r = launch_tile<K, tile_W(K, false), false, false>(a);

@@ -11,7 +11,7 @@ namespace cf {
 enum Op { OP_AF = 0, OP_RF = 1, OP_JV = 2 };
 
 // Kernel families for the angular-first / Jacobian forms.
-enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3, PATH_PAIR_L1 = 4, PATH_PAIR_SPLIT = 5 };
+enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3, PATH_PAIR_L1 = 4, PATH_PAIR_SPLIT = 5, PATH_TILE_MMA = 6 };
 
 struct LaunchArgs {
     DevOp op;

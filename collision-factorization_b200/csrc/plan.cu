@@ -82,6 +82,7 @@ struct cf_plan {
     double* d_e_g = nullptr;
     double* d_R = nullptr;
     float* d_R32 = nullptr;  // FP32 copy of R for CF_FORM_AF_F32
+    double* d_RT = nullptr;  // K = 8: R_t as [k1][8 k2 + k3] for the MMA kernel
     int* d_item_q1 = nullptr;
     int* d_bin_begin = nullptr;  // q1 bins of the tile kernel's work units (bin 0 = all, 1..4, 5..20)
     int* d_bin_q1 = nullptr;
@@ -124,6 +125,7 @@ struct cf_plan {
         o.e_g = d_e_g;
         o.R = d_R;
         o.R32 = d_R32;
+        o.RT = d_RT;
         o.item_q1 = d_item_q1;
         o.n_items = n_items;
         o.n_q = n_q;
@@ -211,6 +213,7 @@ void free_plan_memory(cf_plan* p) {
     cudaFree(p->d_e_g);
     cudaFree(p->d_R);
     cudaFree(p->d_R32);
+    cudaFree(p->d_RT);
     cudaFree(p->d_item_q1);
     cudaFree(p->d_bin_begin);
     cudaFree(p->d_bin_q1);
@@ -354,6 +357,15 @@ int build_plan(cf_plan* p, const double* labels, const double* vals, const doubl
     CF_TRY(upload(&p->d_R, Rv, bytes));
     std::vector<float> R32(Rv.begin(), Rv.end());
     CF_TRY(upload(&p->d_R32, R32, bytes));
+    if (K == 8) {
+        std::vector<double> RT(Rv.size());
+        for (int t = 0; t < p->n_l; ++t)
+            for (int k1 = 0; k1 < 8; ++k1)
+                for (int k2 = 0; k2 < 8; ++k2)
+                    for (int k3 = 0; k3 < 8; ++k3)
+                        RT[(size_t)t * 512 + k1 * 64 + 8 * k2 + k3] = Rv[(size_t)t * 512 + k1 + 8 * k2 + 64 * k3];
+        CF_TRY(upload(&p->d_RT, RT, bytes));
+    }
     CF_TRY(upload(&p->d_item_q1, items, bytes));
     CF_TRY(upload(&p->d_bin_begin, bin_begin, bytes));
     CF_TRY(upload(&p->d_bin_q1, bin_q1, bytes));
@@ -1025,10 +1037,10 @@ extern "C" {
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    if (path < 0 || path > 5)
+    if (path < 0 || path > 6)
         return fail(CF_EINVAL,
-                    "kernel path %d is not 0 (auto), 1 (gather), 2 (tile), 3 (pair), 4 (pair, R via L1) or 5 (pair, "
-                    "split rows)",
+                    "kernel path %d is not 0 (auto), 1 (gather), 2 (tile), 3 (pair), 4 (pair, R via L1), 5 (pair, "
+                    "split rows) or 6 (tile, K^3 step on the FP64 MMA)",
                     path);
     std::lock_guard<std::mutex> lk(plan->mu);
     plan->path = path;

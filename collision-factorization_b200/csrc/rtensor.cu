@@ -41,6 +41,7 @@ namespace {
 constexpr int kItemWarps = 16;          // warps per k_items CTA
 constexpr int kPointsPerRound = kItemWarps / 2;  // each point has two post-collision velocities
 constexpr int kMaxL = 31;               // one lane per m (harmonics) and per l (radial functions)
+constexpr int kMaxNK = 12;              // radial functions per l (k_contract's per-thread entries too)
 constexpr double kEpsSafe = 1e-15;      // the reference's floor under square roots
 constexpr double kPi = 3.14159265358979323846;
 
@@ -146,9 +147,10 @@ __global__ void __launch_bounds__(kItemWarps * 32, 1)
     const int c0 = blockIdx.y * G, c1 = min(d.NL, c0 + G);
     const int j0 = d.vq_begin[c0], j1 = d.vq_begin[c1];
     // shared layout
-    double* gG1 = sm;                          // [G][NK] gains
+    // accumulators [NK][G]: consecutive channels (consecutive threads) in consecutive words
+    double* gG1 = sm;                          // [NK][G] gains
     double* gG2 = gG1 + (size_t)G * NK;
-    double* gL1 = gG2 + (size_t)G * NK;        // [G][NK] losses
+    double* gL1 = gG2 + (size_t)G * NK;        // [NK][G] losses
     double* gL2 = gL1 + (size_t)G * NK;
     double* Y = gL2 + (size_t)G * NK;          // [kItemWarps][NQ]: harmonics of the round's velocities
     double* RV = Y + (size_t)kItemWarps * NQ;  // [kItemWarps][NR]: radial values at |vp|
@@ -229,11 +231,11 @@ __global__ void __launch_bounds__(kItemWarps * 32, 1)
                                          : d.ploss2[o + (size_t)d.Ny2 * ch];
             const double li = lw * pl;
             const int l1 = d.l1[ch];
-            double* a1 = gL1 + (size_t)(ch - c0) * NK;
-            double* a2 = gL2 + (size_t)(ch - c0) * NK;
+            double* a1 = gL1 + (ch - c0);
+            double* a2 = gL2 + (ch - c0);
             for (int k = 0; k < NK; ++k) {
-                a1[k] += RVL[l1 * NK + k] * li;
-                a2[k] += RVS[l1 * NK + k] * li;
+                a1[(size_t)k * G] += RVL[l1 * NK + k] * li;
+                a2[(size_t)k * G] += RVS[l1 * NK + k] * li;
             }
         }
         __syncthreads();
@@ -271,8 +273,15 @@ __global__ void __launch_bounds__(kItemWarps * 32, 1)
             const int np = min(kPointsPerRound, n_pts - p0);
             for (int ch = c0 + tid; ch < c1; ch += blockDim.x) {
                 const int l1 = d.l1[ch], jb = d.vq_begin[ch], je = d.vq_begin[ch + 1];
-                double* a1 = gG1 + (size_t)(ch - c0) * NK;
-                double* a2 = gG2 + (size_t)(ch - c0) * NK;
+                double* a1 = gG1 + (ch - c0);
+                double* a2 = gG2 + (ch - c0);
+                // the round's points summed in registers, then added to the item's accumulators
+                double s1[kMaxNK], s2[kMaxNK];
+#pragma unroll
+                for (int k = 0; k < kMaxNK; ++k) {
+                    s1[k] = 0.0;
+                    s2[k] = 0.0;
+                }
                 for (int pp = 0; pp < np; ++pp) {
                     const double* Y1 = Y + (size_t)(2 * pp) * NQ;
                     const double* Y2 = Y1 + NQ;
@@ -286,11 +295,19 @@ __global__ void __launch_bounds__(kItemWarps * 32, 1)
                     const double w1 = g1 * wgt[pp], w2 = g2 * wgt[pp];
                     const double* r1 = RV + (size_t)(2 * pp) * NR + l1 * NK;
                     const double* r2 = r1 + NR;
-                    for (int k = 0; k < NK; ++k) {
-                        a1[k] += w1 * r1[k];
-                        a2[k] += w2 * r2[k];
-                    }
+#pragma unroll
+                    for (int k = 0; k < kMaxNK; ++k)
+                        if (k < NK) {
+                            s1[k] += w1 * r1[k];
+                            s2[k] += w2 * r2[k];
+                        }
                 }
+#pragma unroll
+                for (int k = 0; k < kMaxNK; ++k)
+                    if (k < NK) {
+                        a1[(size_t)k * G] += s1[k];
+                        a2[(size_t)k * G] += s2[k];
+                    }
             }
             __syncthreads();
         }
@@ -298,10 +315,10 @@ __global__ void __launch_bounds__(kItemWarps * 32, 1)
     // net vectors J (gain - loss), [channel][item][2][NK]
     for (int ch = c0 + tid; ch < c1; ch += blockDim.x) {
         double* dst = net + ((size_t)ch * n_items_chunk + itl) * 2 * NK;
-        const size_t b = (size_t)(ch - c0) * NK;
+        const size_t b = (size_t)(ch - c0);
         for (int k = 0; k < NK; ++k) {
-            dst[k] = Jo * (gG1[b + k] - gL1[b + k]);
-            dst[NK + k] = Jo * (gG2[b + k] - gL2[b + k]);
+            dst[k] = Jo * (gG1[b + (size_t)k * G] - gL1[b + (size_t)k * G]);
+            dst[NK + k] = Jo * (gG2[b + (size_t)k * G] - gL2[b + (size_t)k * G]);
         }
     }
     if (blockIdx.y == 0)

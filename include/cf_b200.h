@@ -159,8 +159,9 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
  * two lanes per cell), 3 = the pair kernel (16 cells in shared memory, the mirrored rows (l,+m) and
  * (l,-m) on the two half-warps), 4 = the pair kernel reading R through L1 instead of shared
  * memory, 5 = the split pair kernel (both mirrored rows in every lane, the k3 range split over the
- * half-warps; fast Q forms with even K <= 8, the pair kernel otherwise).  2-5 return
- * CF_EUNSUPPORTED where they do not fit.  All families agree to rounding, and bit for bit in the
+ * half-warps; fast Q forms with even K <= 8, the pair kernel otherwise), 6 = the tile kernel with
+ * its K^3 step on the FP64 tensor cores (warp-level MMA; fast Q form at K = 8, the tile kernel
+ * otherwise).  2-6 return CF_EUNSUPPORTED where they do not fit.  All families agree to rounding, and bit for bit in the
  * exact forms. */
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path);
 

@@ -263,7 +263,7 @@ def test_kernel_paths_agree(L, K, B, cuda_available, oracle_lib):
     oracle_lib.af_batch(Qo, _cells_cm(cells), geo.labels, geo.vals, geo.ic_map, R, NQ, K)
     ref = Qo.transpose(2, 1, 0)
     outs = {}
-    for path in ("pair_split", "pair", "pair_l1", "tile", "gather"):
+    for path in ("tile_mma", "pair_split", "pair", "pair_l1", "tile", "gather"):
         op.set_kernel_path(path)
         Qf = op.q(f).cpu().numpy()
         assert per_cell_err(Qf, ref) <= TOL_FP64, f"{path}: {per_cell_err(Qf, ref):.3e}"
