@@ -347,6 +347,19 @@ def run_ours(args):
             sym_path_ms[path] = None
     op.set_kernel_path(args.path)
     exact_ms = timed(lambda: step("af_exact"), max(2, args.steps // 4)) if K <= 8 else None
+    # J(f).v (the Jacobian apply of the implicit solves) on the same cells: fast, folded, exact order
+    v_dev = torch.from_numpy(np.random.default_rng(args.seed + 5).standard_normal(cells.shape)).to(dev)
+    Jout = torch.zeros_like(f)
+    jv_ms = {}
+    for name, kw in (("jv", {}), ("jv_folded", {"folded": True}), ("jv_exact", {"exact": True})):
+        if name == "jv_exact" and K > 8:
+            continue
+
+        def jstep(kw=kw):
+            Jout.zero_()
+            op.jv(f, v_dev, out=Jout, **kw)
+
+        jv_ms[name] = timed(jstep, max(2, args.steps // 4))
     # reduced-precision forms (FP32 contraction, FP64 accumulation of Q): error and throughput
     f32 = {}
     for form in ("af_f32", "af_sym_f32"):
@@ -434,6 +447,7 @@ def run_ours(args):
                 "rf": {"cells_per_s": rf_rate},
                 "af_by_kernel": {p: (B / (sum(v) / len(v) / 1e3) if v else None) for p, v in path_ms.items()},
                 "af_sym_by_kernel": {p: (B / (sum(v) / len(v) / 1e3) if v else None) for p, v in sym_path_ms.items()},
+                "jacobian_apply_cells_per_s": {k: B / (sum(v) / len(v) / 1e3) for k, v in jv_ms.items()},
                 **f32,
                 "chosen": chosen,
                 "plain_cells_per_s": plain_rate,

@@ -51,8 +51,18 @@ int fail(int status, const char* fmt, ...) {
 
 constexpr int kMaxK = 16;
 constexpr int kCounterSlots = 64;  // work-queue heads per plan (one per stream in use)
-constexpr int kHostStreams = 3;    // streams of the chunked host entry points
-constexpr int64_t kHostChunkMin = 512;
+#ifndef CF_HOST_STREAMS
+#define CF_HOST_STREAMS 3
+#endif
+#ifndef CF_HOST_CHUNK_MIN
+#define CF_HOST_CHUNK_MIN 256
+#endif
+#ifndef CF_HOST_MAX_CHUNKS
+#define CF_HOST_MAX_CHUNKS 16
+#endif
+constexpr int kHostStreams = CF_HOST_STREAMS;        // streams of the chunked host entry points
+constexpr int64_t kHostChunkMin = CF_HOST_CHUNK_MIN;  // cells per chunk at least
+constexpr int64_t kHostMaxChunks = CF_HOST_MAX_CHUNKS;
 
 }  // namespace
 
@@ -790,7 +800,7 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
     // makes the copies asynchronous; pageable memory still gives the right answer, serialised).
     for (cudaStream_t& hs : p->host_streams)
         if (!hs) CF_CUDA(cudaStreamCreateWithFlags(&hs, cudaStreamNonBlocking));
-    int64_t n_chunks = std::min<int64_t>(8, B / kHostChunkMin);
+    int64_t n_chunks = std::min<int64_t>(kHostMaxChunks, B / kHostChunkMin);
     const int64_t per = (B + n_chunks - 1) / n_chunks;
     const int64_t chunk = (per + CF_TILE - 1) / CF_TILE * CF_TILE;  // whole 32-cell tiles per chunk
     n_chunks = (B + chunk - 1) / chunk;
