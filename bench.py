@@ -362,7 +362,7 @@ def run_ours(args):
         jv_ms[name] = timed(jstep, max(2, args.steps // 4))
     # reduced-precision forms (FP32 contraction, FP64 accumulation of Q): error and throughput
     f32 = {}
-    for form in ("af_f32", "af_sym_f32"):
+    for form in ("af_f32", "af_sym_f32", "af_bf16", "af_sym_bf16"):
         try:
             step(form)
             num = (Q - Q_exact).abs().reshape(B, -1).amax(dim=1)

@@ -32,6 +32,7 @@ struct DevOp {
     const double* R;
     const float* R32;  // FP32 copy of R for the FP32 form
     const double* RT;  // K = 8 only: R_t transposed to [k1][kk = K k2 + k3] (A operands of the MMA kernel)
+    const unsigned short* RTbf;  // K = 8 only: R_t^T split in BF16, [t][hi, lo][k1][kk] (BF16-split form)
     const int* item_q1;
     int n_items;  // number of q1 with at least one slice
     int n_q;

@@ -8,6 +8,7 @@
 #include "tile_kernels.cuh"
 #include "pair_kernels.cuh"
 #include "mma_kernels.cuh"
+#include "bf16_kernels.cuh"
 
 namespace cf {
 
@@ -164,6 +165,29 @@ static LaunchResult launch_mma(const LaunchArgs& a) {
     return {e == cudaSuccess ? 0 : 5, 1, e, PATH_TILE_MMA};
 }
 
+// BF16-split form: the K^3 step on the BF16 tensor cores (K = 8).
+template <int W>
+static LaunchResult launch_bf16(const LaunchArgs& a) {
+    const int M = a.op.n_q * kBfK;
+    const size_t smem = bf16_smem_bytes(M, W);
+    if (smem + 256 > a.max_smem || a.counter == nullptr || a.op.RTbf == nullptr || a.fT32 == nullptr)
+        return {-1, 0, cudaSuccess, PATH_BF16_MMA};
+    auto kern = af_bf16_kernel<W>;
+    int per_sm = 0;
+    cudaError_t e = resident_ctas((const void*)kern, W * 32, smem, &per_sm);
+    if (e != cudaSuccess) return {5, 0, e, PATH_BF16_MMA};
+    if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_BF16_MMA};
+    const int64_t ctas = (int64_t)per_sm * a.n_sms;
+    const UnitPlan up = plan_units(a.n_cells, ctas);
+    TileSched sc{a.bin_begin, a.bin_q1, up.n_ht, up.n_whole, up.split, up.n_units, a.counter};
+    e = cudaMemsetAsync(a.counter, 0, sizeof(int), a.stream);
+    if (e != cudaSuccess) return {5, 0, e, PATH_BF16_MMA};
+    const unsigned grid = (unsigned)(up.n_units < ctas ? up.n_units : ctas);
+    kern<<<grid, W * 32, smem, a.stream>>>(a.op, sc, a.fT32, a.QT);
+    e = cudaGetLastError();
+    return {e == cudaSuccess ? 0 : 5, 1, e, PATH_BF16_MMA};
+}
+
 template <int K, bool EXACT>
 static LaunchResult launch_rf(const LaunchArgs& a) {
     const int64_t warps = (int64_t)a.op.n_items * a.n_tiles;
@@ -180,6 +204,16 @@ constexpr int tile_W(int K, bool jv) { return jv ? (K >= 8 ? 12 : 16) : 16; }
 
 template <int K>
 static LaunchResult launch_for_k(const LaunchArgs& a) {
+    if (a.bf16) {
+        if (a.what != OP_AF || a.exact) return {8, 0, cudaSuccess, PATH_BF16_MMA};
+        if constexpr (K == kBfK) {
+            const LaunchResult r = launch_bf16<16>(a);
+            if (r.status == -1) return {8, 0, cudaSuccess, PATH_BF16_MMA};
+            return r;
+        } else {
+            return {8, 0, cudaSuccess, PATH_BF16_MMA};
+        }
+    }
     if (a.f32) {
         // FP32 form: the pair kernel in FP32 (angular first only), R staged in shared memory when the
         // FP32 tile leaves room for it, else read through L1

@@ -11,7 +11,8 @@ namespace cf {
 enum Op { OP_AF = 0, OP_RF = 1, OP_JV = 2 };
 
 // Kernel families for the angular-first / Jacobian forms.
-enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3, PATH_PAIR_L1 = 4, PATH_PAIR_SPLIT = 5, PATH_TILE_MMA = 6 };
+enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3, PATH_PAIR_L1 = 4, PATH_PAIR_SPLIT = 5, PATH_TILE_MMA = 6,
+           PATH_BF16_MMA = 7 /* reported only: the BF16-split form's kernel */ };
 
 struct LaunchArgs {
     DevOp op;
@@ -39,6 +40,8 @@ struct LaunchArgs {
     const float* fT32;
     // automatic order for the fast Q form: false = pair kernel first, true = tile kernel first
     bool tile_first;
+    // BF16-split form (f32 is set too: FP32 tiles of f)
+    bool bf16;
 };
 
 // Status codes mirror cf_status: 0 ok, 5 CUDA error, 8 unsupported, 2 shape.

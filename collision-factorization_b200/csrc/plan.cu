@@ -50,6 +50,20 @@ int fail(int status, const char* fmt, ...) {
     } while (0)
 
 constexpr int kMaxK = 16;
+
+// BF16 bits of a finite float, rounded to nearest even; and back
+static unsigned short bf16_bits(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (unsigned short)(u >> 16);
+}
+static float bf16_value(unsigned short b) {
+    const uint32_t u = (uint32_t)b << 16;
+    float x;
+    std::memcpy(&x, &u, 4);
+    return x;
+}
 constexpr int kCounterSlots = 64;  // work-queue heads per plan (one per stream in use)
 #ifndef CF_HOST_STREAMS
 #define CF_HOST_STREAMS 3
@@ -93,6 +107,7 @@ struct cf_plan {
     double* d_R = nullptr;
     float* d_R32 = nullptr;  // FP32 copy of R for CF_FORM_AF_F32
     double* d_RT = nullptr;  // K = 8: R_t as [k1][8 k2 + k3] for the MMA kernel
+    unsigned short* d_RTbf = nullptr;  // K = 8: the same split into BF16 hi and lo parts
     int* d_item_q1 = nullptr;
     int* d_bin_begin = nullptr;  // q1 bins of the tile kernel's work units (bin 0 = all, 1..4, 5..20)
     int* d_bin_q1 = nullptr;
@@ -136,6 +151,7 @@ struct cf_plan {
         o.R = d_R;
         o.R32 = d_R32;
         o.RT = d_RT;
+        o.RTbf = d_RTbf;
         o.item_q1 = d_item_q1;
         o.n_items = n_items;
         o.n_q = n_q;
@@ -224,6 +240,7 @@ void free_plan_memory(cf_plan* p) {
     cudaFree(p->d_R);
     cudaFree(p->d_R32);
     cudaFree(p->d_RT);
+    cudaFree(p->d_RTbf);
     cudaFree(p->d_item_q1);
     cudaFree(p->d_bin_begin);
     cudaFree(p->d_bin_q1);
@@ -375,6 +392,17 @@ int build_plan(cf_plan* p, const double* labels, const double* vals, const doubl
                     for (int k3 = 0; k3 < 8; ++k3)
                         RT[(size_t)t * 512 + k1 * 64 + 8 * k2 + k3] = Rv[(size_t)t * 512 + k1 + 8 * k2 + 64 * k3];
         CF_TRY(upload(&p->d_RT, RT, bytes));
+        // R_t^T = hi + lo in BF16 (round to nearest even), [t][hi, lo][k1][kk]
+        std::vector<unsigned short> RTbf(2 * RT.size());
+        for (int t = 0; t < p->n_l; ++t)
+            for (int e = 0; e < 512; ++e) {
+                const double r = RT[(size_t)t * 512 + e];
+                const unsigned short hi = bf16_bits((float)r);
+                const unsigned short lo = bf16_bits((float)(r - (double)bf16_value(hi)));
+                RTbf[(size_t)t * 1024 + e] = hi;
+                RTbf[(size_t)t * 1024 + 512 + e] = lo;
+            }
+        CF_TRY(upload(&p->d_RTbf, RTbf, bytes));
     }
     CF_TRY(upload(&p->d_item_q1, items, bytes));
     CF_TRY(upload(&p->d_bin_begin, bin_begin, bytes));
@@ -420,7 +448,7 @@ int* counter_for(const cf_plan* pc, cudaStream_t st) {
 }
 
 int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const double* vT, double* QT, int64_t B,
-             cudaStream_t st, const float* fT32 = nullptr) {
+             cudaStream_t st, const float* fT32 = nullptr, bool bf16 = false) {
     const int64_t nt = n_tiles_for(B);
     // The folded operator has about half the COO entries per slice of the plain one, so its Phi step
     // is light next to the K^3 step; there the tile kernel (16 warps per SM) runs ahead of the pair
@@ -428,7 +456,7 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
     const bool tile_first = p->parent != nullptr && what == cf::OP_AF && !exact;
     cf::LaunchArgs a{p->op(), fT, vT, QT, nt, B, st, what, exact, p->path, p->d_bin_begin, p->d_bin_q1,
                      counter_for(p, st), p->n_sms, p->max_smem, p->d_pbin_begin, p->d_pbin_item, p->d_pitems,
-                     fT32 != nullptr, fT32, tile_first};
+                     fT32 != nullptr, fT32, tile_first, bf16};
     cf::LaunchResult r{8, 0, cudaSuccess};
     switch (p->k) {
 #define CF_K(KK) \
@@ -491,7 +519,8 @@ int launch_unpack(const cf_plan* p, const double* src, double* dst, int64_t B, c
 int get_sym(cf_plan* p, cf_plan** out);
 
 int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_dev, const double* v_dev,
-               int64_t B, void* ws, size_t ws_bytes, cudaStream_t st, bool sym = false, bool f32 = false) {
+               int64_t B, void* ws, size_t ws_bytes, cudaStream_t st, bool sym = false, int f32 = 0) {
+    // f32: 0 the FP64 forms, 1 the FP32 forms, 2 the BF16-split forms (both read FP32 tiles of f)
     if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
     if (B == 0 || p->n_g == 0) return CF_OK;
     if (!q_dev || !f_dev || (what == 2 && !v_dev)) return fail(CF_EINVAL, "null device buffer");
@@ -510,7 +539,7 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
     CF_TRY(launch_pack(p, q_dev, QT, B, st));
     cf_plan* target = p;
     if (sym) CF_TRY(get_sym(p, &target));
-    CF_TRY(dispatch(target, what, exact, fT, vT, QT, B, st, fT32));
+    CF_TRY(dispatch(target, what, exact, fT, vT, QT, B, st, fT32, f32 == 2));
     CF_TRY(launch_unpack(p, QT, q_dev, B, st));
     return CF_OK;
 }
@@ -769,7 +798,7 @@ int cached_plan(cf_plan** out, const double* labels, const double* vals, const d
 // Host-pointer contraction: upload, run, download.  what: 0 AF, 1 RF, 2 JV.
 int run_host(int what, bool exact, double* Q, const double* f, const double* v, int64_t B, const double* labels,
              const double* vals, const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
-             int32_t k, bool sym = false, bool f32 = false) {
+             int32_t k, bool sym = false, int f32 = 0) {
     if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
     if (!Q || !f || (what == 2 && !v)) return fail(CF_EINVAL, "null host buffer");
     cf_plan* p = nullptr;
@@ -832,12 +861,14 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
     return st;
 }
 
-int form_what(int form, bool& exact, bool& sym, bool& f32) {
+int form_what(int form, bool& exact, bool& sym, int& f32) {
     sym = false;
-    f32 = false;
+    f32 = 0;
     switch (form) {
-        case CF_FORM_AF_F32: exact = false; f32 = true; return 0;
-        case CF_FORM_AF_SYM_F32: exact = false; f32 = true; sym = true; return 0;
+        case CF_FORM_AF_F32: exact = false; f32 = 1; return 0;
+        case CF_FORM_AF_SYM_F32: exact = false; f32 = 1; sym = true; return 0;
+        case CF_FORM_AF_BF16: exact = false; f32 = 2; return 0;
+        case CF_FORM_AF_SYM_BF16: exact = false; f32 = 2; sym = true; return 0;
         case CF_FORM_AF: exact = false; return 0;
         case CF_FORM_RF: exact = false; return 1;
         case CF_FORM_AF_EXACT: exact = true; return 0;
@@ -877,7 +908,8 @@ int cf_contract_host(double* Q, const double* f, int64_t b, const double* labels
                      const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k,
                      int32_t form) {
     g_last_error.clear();
-    bool exact = false, sym = false, f32 = false;
+    bool exact = false, sym = false;
+    int f32 = 0;
     const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
     return run_host(what, exact, Q, f, nullptr, b, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym, f32);
@@ -937,7 +969,8 @@ int cf_q_device_ws(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b,
                    size_t workspace_bytes, void* stream) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    bool exact = false, sym = false, f32 = false;
+    bool exact = false, sym = false;
+    int f32 = 0;
     const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
     DeviceGuard guard(plan->device);
@@ -948,7 +981,8 @@ int cf_q_device_ws(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b,
 int cf_q_device(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form, void* stream) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    bool exact = false, sym = false, f32 = false;
+    bool exact = false, sym = false;
+    int f32 = 0;
     const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
     std::lock_guard<std::mutex> lk(plan->mu);
@@ -991,7 +1025,8 @@ int cf_unpack_cells(const cf_plan* plan, double* dst_cells, const double* src_ti
 int cf_q_tiled(cf_plan* plan, double* q_tiled, const double* f_tiled, int64_t b, int32_t form, void* stream) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    bool exact = false, sym = false, f32 = false;
+    bool exact = false, sym = false;
+    int f32 = 0;
     const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
     if (f32) return fail(CF_EUNSUPPORTED, "the FP32 forms read FP64 cells through cf_q_device / cf_contract_host");

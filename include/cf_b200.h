@@ -59,7 +59,11 @@ typedef enum cf_form {
     CF_FORM_AF_F32 = 5,    /* angular first in FP32 (f, R, Phi and the row sums rounded to FP32; result
                               added to the FP64 Q): ~1e-7 relative error, the invariant rows stay exactly
                               zero because R's conservation rows are exactly zero in FP32 too          */
-    CF_FORM_AF_SYM_F32 = 6 /* the FP32 form on the folded operator                                       */
+    CF_FORM_AF_SYM_F32 = 6, /* the FP32 form on the folded operator                                      */
+    CF_FORM_AF_BF16 = 7,   /* angular first with the K^3 step on the BF16 tensor cores as a two-term
+                              split: R_t = R_hi + R_lo and Phi = Phi_hi + Phi_lo in BF16, products
+                              accumulated in FP32 (the Phi step in FP32); ~1e-5 relative error; K = 8 */
+    CF_FORM_AF_SYM_BF16 = 8 /* the BF16-split form on the folded operator                             */
 } cf_form;
 
 typedef struct cf_plan cf_plan;

@@ -368,6 +368,38 @@ def test_fp32_forms_error_and_invariants(L, K, B, cuda_available, oracle_lib):
         assert np.all(inv == 0.0)
 
 
+@pytest.mark.parametrize("L,K,B", [(4, 8, 33), (8, 8, 50), (10, 8, 300)])
+def test_bf16_split_forms_error_and_invariants(L, K, B, cuda_available, oracle_lib):
+    """BF16-split forms (K^3 step on the BF16 tensor cores, R and Phi as hi + lo): relative error
+    near FP32's (<= 1e-4 per cell), invariant rows exactly zero, other K refused."""
+    import cf_b200
+    from cf_b200 import CFError, geometry, workloads
+    from oracle import rtensor
+
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=4)
+    NQ = geo.n_q
+    f = _cells_cm(workloads.maxwellian_cells(K, L, B, seed=9, amplitude=0.05))
+    args = (geo.labels, geo.vals, geo.ic_map, R, NQ, K)
+    Qo = np.zeros_like(f, order="F")
+    oracle_lib.af_batch(Qo, f, *args)
+    for form in ("af_bf16", "af_sym_bf16"):
+        Qg = np.asfortranarray(np.full_like(f, 0.125))  # += semantics
+        cf_b200.contract_batched(Qg, f, *args, form=form)
+        Qg -= 0.125
+        err = per_cell_err(Qg.transpose(2, 1, 0), Qo.transpose(2, 1, 0))
+        assert 1e-12 < err <= 1e-4, f"{form}: {err:.3e}"
+        inv = Qg.transpose(2, 1, 0).reshape(B, -1)[:, [0, 1, 2, 3, NQ]]
+        assert np.all(inv == 0.0)
+    geo6 = geometry.sort_for_contraction(geometry.generate_geometry(4))
+    R6 = workloads.synthetic_R(rtensor.l_triplets_of(geo6), 6, seed=1)
+    f6 = _cells_cm(workloads.maxwellian_cells(6, 4, 3, seed=1))
+    with pytest.raises(CFError) as e:
+        cf_b200.contract_batched(np.zeros_like(f6, order="F"), f6, geo6.labels, geo6.vals, geo6.ic_map, R6,
+                                 geo6.n_q, 6, form="af_bf16")
+    assert e.value.status == 8
+
+
 def test_host_entry_chunked_matches_oracle(cuda_available, oracle_lib):
     """Batches of >= 1024 cells go through the host entry points in chunks on three streams; the
     result is the same as the oracle's (fast and folded Q, J.v), cells split at ragged chunk ends."""
