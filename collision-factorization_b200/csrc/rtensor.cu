@@ -16,7 +16,8 @@
 //
 // On the device this is two kernels over chunks of items:
 //   k_items     one CTA per (item, channel group): the warps evaluate the harmonics and radial
-//               functions of 8 inner points at a time into shared memory, then each thread owns
+//               functions of 16 inner points at a time (8 when L > 15: one velocity per half-warp
+//               or per warp) into shared memory, then each thread owns
 //               channels and accumulates their gain/loss vectors; the CTA writes the item's
 //               "net" vectors J (gain - loss) and its radial values at vL and vS;
 //   k_contract  one CTA per channel: every thread owns entries of R_t and sums the rank-2 updates
@@ -39,7 +40,10 @@ void cf_set_last_error(const char* msg);
 namespace {
 
 constexpr int kItemWarps = 16;          // warps per k_items CTA
-constexpr int kPointsPerRound = kItemWarps / 2;  // each point has two post-collision velocities
+// velocity slots per round: one per warp, or one per half-warp when L <= 15 (a lane per m or l
+// fits in 16 lanes); each point has two post-collision velocities
+constexpr int kMaxSlots = 2 * kItemWarps;
+constexpr int kMaxPointsPerRound = kMaxSlots / 2;
 constexpr int kMaxL = 31;               // one lane per m (harmonics) and per l (radial functions)
 constexpr int kMaxNK = 12;              // radial functions per l (k_contract's per-thread entries too)
 constexpr double kEpsSafe = 1e-15;      // the reference's floor under square roots
@@ -152,12 +156,16 @@ __global__ void __launch_bounds__(kItemWarps * 32, 1)
     double* gG2 = gG1 + (size_t)G * NK;
     double* gL1 = gG2 + (size_t)G * NK;        // [NK][G] losses
     double* gL2 = gL1 + (size_t)G * NK;
-    double* Y = gL2 + (size_t)G * NK;          // [kItemWarps][NQ]: harmonics of the round's velocities
-    double* RV = Y + (size_t)kItemWarps * NQ;  // [kItemWarps][NR]: radial values at |vp|
-    double* RVL = RV + (size_t)kItemWarps * NR;  // [NR] at vL
+    double* Y = gL2 + (size_t)G * NK;          // [kMaxSlots][NQ]: harmonics of the round's velocities
+    double* RV = Y + (size_t)kMaxSlots * NQ;   // [kMaxSlots][NR]: radial values at |vp|
+    double* RVL = RV + (size_t)kMaxSlots * NR;   // [NR] at vL
     double* RVS = RVL + NR;                      // [NR] at vS
-    double* wgt = RVS + NR;                      // [kPointsPerRound]
-    double* pg = wgt + kPointsPerRound;          // [j1 - j0] this (t, u) or y slice of P_gain
+    double* wgt = RVS + NR;                      // [kMaxPointsPerRound]
+    double* pg = wgt + kMaxPointsPerRound;       // [j1 - j0] this (t, u) or y slice of P_gain
+    const int sub = L <= 15 ? 2 : 1;             // velocity slots per warp
+    const int slot = sub == 2 ? 2 * warp + (lane >> 4) : warp;
+    const int m_lane = sub == 2 ? (lane & 15) : lane;
+    const int ppr = kItemWarps * sub / 2;        // points per round
 
     // decode the item
     const int64_t n1 = (int64_t)d.Nx * d.Nu1;
@@ -240,9 +248,9 @@ __global__ void __launch_bounds__(kItemWarps * 32, 1)
         }
         __syncthreads();
 
-        for (int p0 = 0; p0 < n_pts; p0 += kPointsPerRound) {
-            // warp w evaluates velocity (w & 1) of point p0 + (w >> 1)
-            const int p = p0 + (warp >> 1), side = warp & 1;
+        for (int p0 = 0; p0 < n_pts; p0 += ppr) {
+            // slot s (a warp, or a half-warp) evaluates velocity (s & 1) of point p0 + (s >> 1)
+            const int p = p0 + (slot >> 1), side = slot & 1;
             if (p < n_pts) {
                 const int n = p / d.Neps, e = p % d.Neps;
                 const double cc = d.chi[n];
@@ -263,14 +271,14 @@ __global__ void __launch_bounds__(kItemWarps * 32, 1)
                 const double vm = sqrt(fmax(vpx * vpx + vpy * vpy + vpz * vpz, kEpsSafe));
                 const double xc = fmax(fmin(vpz / vm, 1.0), -1.0);
                 const double phi = atan2(vpy, vpx);
-                if (lane <= L) {
-                    harmonics_lane(L, lane, xc, phi, d.shnorm, Y + (size_t)warp * NQ);
-                    radial_all(NK, lane, vm, d.rnorm, RV + (size_t)warp * NR + lane * NK);
+                if (m_lane <= L) {
+                    harmonics_lane(L, m_lane, xc, phi, d.shnorm, Y + (size_t)slot * NQ);
+                    radial_all(NK, m_lane, vm, d.rnorm, RV + (size_t)slot * NR + m_lane * NK);
                 }
-                if (lane == 0 && side == 0) wgt[warp >> 1] = d.Wchi[n] * B * Jt * d.Weps[e];
+                if (m_lane == 0 && side == 0) wgt[slot >> 1] = d.Wchi[n] * B * Jt * d.Weps[e];
             }
             __syncthreads();
-            const int np = min(kPointsPerRound, n_pts - p0);
+            const int np = min(ppr, n_pts - p0);
             for (int ch = c0 + tid; ch < c1; ch += blockDim.x) {
                 const int l1 = d.l1[ch], jb = d.vq_begin[ch], je = d.vq_begin[ch + 1];
                 double* a1 = gG1 + (ch - c0);
@@ -507,7 +515,7 @@ int cf_rtensor_sumfac(double* R_out, const cf_sumfac_inputs* in, int32_t device,
         max_nnz_g = 0;
         for (int g = 0; g < n_groups; ++g)
             max_nnz_g = std::max(max_nnz_g, vq_begin[std::min(NL, (g + 1) * G)] - vq_begin[g * G]);
-        smem = sizeof(double) * ((size_t)4 * G * NK + (size_t)kItemWarps * (NQ + NR) + 2 * NR + kPointsPerRound +
+        smem = sizeof(double) * ((size_t)4 * G * NK + (size_t)kMaxSlots * (NQ + NR) + 2 * NR + kMaxPointsPerRound +
                                  max_nnz_g);
         if (smem + 1024 <= (size_t)max_smem || G == 1) break;
         G = (G + 1) / 2;
