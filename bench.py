@@ -48,6 +48,13 @@ WORKLOADS = {
 }
 RAGGED_BUCKETS = [(4, 4), (6, 6), (8, 6), (10, 8)]  # (L, K), drawn with RAGGED_WEIGHTS per cell
 R_FILES = {(10, 8): "R_hs_k7_l10_pad20.npy", (8, 8): "R_hs_k7_l8_pad20.npy"}
+# DRAM bytes (read + write) of one contraction launch, from the ncu captures summarised in profiles/
+NCU_TRAFFIC = {
+    ("hs_l10_k8_b4096", "tile", "af_sym"): (64.769024e6 + 1.074688e6,
+                                            "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                            "profiles/af_tile_kernel_folded_hs_l10_k8_b4096.md"),
+    ("hs_l10_k8_b4096", "pair", "af"): (65.9e6 + 1.8e6, "ncu, profiles/af_pair_kernel_hs_l10_k8_b4096.md"),
+}
 
 
 def parse_args(argv=None):
@@ -385,11 +392,13 @@ def run_ours(args):
     kern_list = sym_kern_ms if chosen == "af_sym" else kern_ms
     kernel_only(chosen)
     torch.cuda.synchronize(dev)
+    last_path = _lib.PATH_NAMES[op.info()["last_path"]]
+    traffic = NCU_TRAFFIC.get((args.workload, last_path, chosen))
     kern_name = {"pair": "af_pair_kernel (persistent, tile-resident, mirrored row pairs)",
                  "pair_split": "af_pair_kernel, split variant (both mirrored rows per lane, k3 halves)",
                  "pair_l1": "af_pair_kernel (R_t through L1)", "tile": "af_tile_kernel (persistent, tile-resident)",
                  "gather": "af_kernel (gathers through L1/L2)",
-                 "tile_mma": "af_mma_kernel (tile-resident, K^3 step on the FP64 MMA)"}.get(_lib.PATH_NAMES[op.info()["last_path"]], "?")
+                 "tile_mma": "af_mma_kernel (tile-resident, K^3 step on the FP64 MMA)"}.get(last_path, "?")
     kern_s = sum(kern_list) / len(kern_list) / 1e3
     flops_launch = op.flops_q * B
     achieved_tf = flops_launch / kern_s / 1e12
@@ -457,7 +466,8 @@ def run_ours(args):
             "roofline": {
                 "bound": "fp64", "kernel": f"{kern_name}, K={K}" + (" on the folded operator" if chosen == "af_sym" else ""),
                 "achieved": achieved_tf, "peak": peak_tf,
-                "unit": "TFLOP/s", "frac": achieved_tf / peak_tf, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved_tf / peak_tf, "traffic": traffic[0] if traffic else None,
+                "traffic_source": traffic[1] if traffic else "no ncu capture of this kernel and form on this workload",
                 "algorithmic_flop_per_launch": flops_launch, "kernel_ms": kern_s * 1e3,
                 "executed_flop_per_launch": exec_flops, "executed_tflops": exec_tf, "executed_frac": exec_tf / peak_tf,
                 "peak_source": f"measured on this GPU in this run: DFMA probe {dfma_tf:.2f}, cuBLAS DGEMM "
