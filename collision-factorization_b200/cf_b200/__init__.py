@@ -5,6 +5,7 @@
 * ``operator`` -- ``CollisionOperator``: a device-resident operator for batches of cells.
 * ``geometry`` -- the COO Gaunt routing lists (labels, vals, ic_map) in the reference's order.
 * ``basis``, ``quadrature`` -- basis conventions, Gauss rules and projections of distributions.
+* ``matfile``  -- the reference's precomputed operators (MATLAB v7.3 ``.mat``) read into ``CollisionOperator``.
 
 The contraction itself is hand-written CUDA for sm_100a in ``libcf_b200.so`` (C ABI in
 ``include/cf_b200.h``); there is no CPU fallback.
