@@ -32,7 +32,7 @@ FORMS = {"af": FORM_AF, "rf": FORM_RF, "af_exact": FORM_AF_EXACT, "rf_exact": FO
 EXPORTS = [
     "cf_angular_first", "cf_radial_first", "cf_contract_host", "cf_jacobian_apply_host",
     "cf_plan_create", "cf_plan_destroy", "cf_plan_get_info", "cf_plan_workspace_size",
-    "cf_q_device", "cf_q_device_ws", "cf_jv_device", "cf_q_device_noalloc",
+    "cf_q_device", "cf_q_device_ws", "cf_jv_device", "cf_q_device_noalloc", "cf_plan_stream_selftest",
     "cf_ragged_create", "cf_ragged_destroy", "cf_ragged_q", "cf_ragged_graph_launch", "cf_ragged_q_resident",
     "cf_ragged_info", "cf_rk2_workspace_size", "cf_rk2_steps_tiled", "cf_rtensor_sumfac",
     "cf_gmres_workspace_size", "cf_gmres_solve_tiled",
@@ -109,6 +109,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_jv_tiled.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, _I64, _I32, C.c_void_p]
     lib.cf_fp64_fma_peak.argtypes = [_I32, C.POINTER(C.c_double)]
     lib.cf_plan_set_kernel_path.argtypes = [C.c_void_p, _I32]
+    lib.cf_plan_stream_selftest.argtypes = [C.c_void_p, C.c_double]
     V = C.c_void_p
     lib.cf_ragged_create.argtypes = [C.POINTER(V), V, V, V, _I32, _I32, _I32]
     lib.cf_ragged_destroy.argtypes = [V]

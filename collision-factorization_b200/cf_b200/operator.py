@@ -121,6 +121,11 @@ class CollisionOperator:
         code = {"auto": 0, "gather": 1, "tile": 2, "pair": 3, "pair_l1": 4, "pair_split": 5, "tile_mma": 6}[path]
         _lib.check(_lib.load().cf_plan_set_kernel_path(self._h, code))
 
+    def stream_selftest(self, wait_seconds: float = 1e-3) -> int:
+        """Run the streamed host path's bounded-wait self-test; returns the status (CF_ETIMEOUT = 9
+        when the kernel's waits ran out and it returned, which is the expected outcome)."""
+        return int(_lib.load().cf_plan_stream_selftest(self._h, float(wait_seconds)))
+
     def workspace_bytes(self, B: int, jacobian: bool = False) -> int:
         n = C.c_size_t()
         _lib.check(_lib.load().cf_plan_workspace_size(self._h, int(B), int(jacobian), C.byref(n)))

@@ -40,6 +40,18 @@ struct DevOp {
     int n_l;
 };
 
+// Synchronisation words of the streamed tile kernel (tile_kernels.cuh, af_tile_stream_kernel).
+struct StreamSync {
+    const int* ready;  // [n_chunks] device; == epoch once chunk c's f and Q are in
+    int* done;         // [n_chunks] device; units finished (zeroed before the launch)
+    int* host_done;    // [n_chunks] mapped host memory; set to epoch once chunk c is final
+    int* err;          // mapped host memory; set to 1 if a wait gave up
+    int* abort;        // device; == epoch once a wait gave up (the other CTAs then stop waiting)
+    int epoch;
+    int ht_per_chunk;
+    long long wait_cycles;
+};
+
 // Lanes per cell used by the angular-first kernels: the K x K Phi accumulator of one cell
 // is split over P lanes (by k3 column) once it no longer fits one lane's registers.
 __host__ __device__ constexpr int af_lanes_per_cell(int K) { return K <= 8 ? 1 : (K <= 12 ? 2 : 4); }

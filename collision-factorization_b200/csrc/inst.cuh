@@ -98,6 +98,38 @@ static LaunchResult launch_tile(const LaunchArgs& a) {
     return {e == cudaSuccess ? 0 : 5, 1, e, PATH_TILE};
 }
 
+// Streamed tile kernel over the whole batch (host entry points): every half-tile split into 4 q1
+// bins, cell-major f and Q, chunk flags in a.ss.  Status -1 when the tile does not fit.
+template <int K, int W>
+static LaunchResult launch_tile_stream(const LaunchArgs& a) {
+    const int M = a.op.n_q * K;
+    const size_t smem = tile_smem_bytes<K>(M, W, false);
+    if (smem + 256 > a.max_smem || a.counter == nullptr) return {-1, 0, cudaSuccess, PATH_TILE};
+    auto kern = af_tile_stream_kernel<K, W>;
+    int per_sm = 0;
+    cudaError_t e = resident_ctas((const void*)kern, W * 32, smem, &per_sm);
+    if (e != cudaSuccess) return {5, 0, e, PATH_TILE};
+    if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_TILE};
+    const int64_t ctas = (int64_t)per_sm * a.n_sms;
+    const int64_t n_ht = (a.n_cells + kTileCells - 1) / kTileCells;
+    TileSched sc;
+    sc.bin_begin = a.bin_begin;
+    sc.bin_q1 = a.bin_q1;
+    sc.n_ht = (int)n_ht;
+    sc.n_whole = 0;
+    sc.split = 4;
+    const int64_t n_units = n_ht * sc.split;
+    if (n_units > INT32_MAX) return {2, 0, cudaSuccess, PATH_TILE};
+    sc.n_units = (int)n_units;
+    sc.counter = a.counter;
+    e = cudaMemsetAsync(a.counter, 0, sizeof(int), a.stream);
+    if (e != cudaSuccess) return {5, 0, e, PATH_TILE};
+    const unsigned grid = (unsigned)(n_units < ctas ? n_units : ctas);
+    kern<<<grid, W * 32, smem, a.stream>>>(a.op, sc, *a.ss, a.f_cm, a.q_cm, (long long)a.n_cells);
+    e = cudaGetLastError();
+    return {e == cudaSuccess ? 0 : 5, 1, e, PATH_TILE};
+}
+
 // Work-unit schedule shared by the persistent kernels: whole half-tiles while there are more
 // half-tiles than CTAs, then the last `ctas` half-tiles split into 4 (or 16) bins each.
 struct UnitPlan {
@@ -204,6 +236,16 @@ constexpr int tile_W(int K, bool jv) { return jv ? (K >= 8 ? 12 : 16) : 16; }
 
 template <int K>
 static LaunchResult launch_for_k(const LaunchArgs& a) {
+    if (a.ss) {
+        if (a.what != OP_AF || a.exact || a.f32) return {8, 0, cudaSuccess, PATH_TILE};
+        if constexpr (K % 2 == 0 && K <= 8) {
+            const LaunchResult r = launch_tile_stream<K, tile_W(K, false)>(a);
+            if (r.status == -1) return {8, 0, cudaSuccess, PATH_TILE};
+            return r;
+        } else {
+            return {8, 0, cudaSuccess, PATH_TILE};
+        }
+    }
     if (a.bf16) {
         if (a.what != OP_AF || a.exact) return {8, 0, cudaSuccess, PATH_BF16_MMA};
         if constexpr (K == kBfK) {

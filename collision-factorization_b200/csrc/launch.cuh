@@ -42,6 +42,10 @@ struct LaunchArgs {
     bool tile_first;
     // BF16-split form (f32 is set too: FP32 tiles of f)
     bool bf16;
+    // streamed host path: the tile kernel on cell-major f and Q while they are copied in and out
+    const StreamSync* ss = nullptr;
+    const double* f_cm = nullptr;
+    double* q_cm = nullptr;
 };
 
 // Status codes mirror cf_status: 0 ok, 5 CUDA error, 8 unsupported, 2 shape.

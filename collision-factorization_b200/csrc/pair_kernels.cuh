@@ -44,11 +44,6 @@ __device__ __forceinline__ const double* r_tensor<double>(const DevOp& op) { ret
 template <>
 __device__ __forceinline__ const float* r_tensor<float>(const DevOp& op) { return op.R32; }
 
-__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-
 // RG = false: R_t is staged into the warp's shared buffer with cp.async.  RG = true: R_t is read
 // straight from global memory with warp-uniform loads through L1 (prefetched into L1 at the start
 // of the slice), which keeps the K^3 step off the shared-memory wavefront budget.

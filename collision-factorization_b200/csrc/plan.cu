@@ -3,6 +3,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
+#include <thread>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -74,6 +76,8 @@ constexpr int kCounterSlots = 64;  // work-queue heads per plan (one per stream 
 #ifndef CF_HOST_MAX_CHUNKS
 #define CF_HOST_MAX_CHUNKS 16
 #endif
+constexpr int kStreamChunks = 16;  // chunks of the streamed host path (at most)
+constexpr double kStreamWaitSeconds = 5.0;  // a streamed-kernel CTA gives up on a chunk flag after this
 constexpr int kHostStreams = CF_HOST_STREAMS;        // streams of the chunked host entry points
 constexpr int64_t kHostChunkMin = CF_HOST_CHUNK_MIN;  // cells per chunk at least
 constexpr int64_t kHostMaxChunks = CF_HOST_MAX_CHUNKS;
@@ -133,6 +137,16 @@ struct cf_plan {
     size_t io_bytes = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t host_streams[kHostStreams] = {};  // chunked host path: copies overlap the contraction
+    // streamed host path: copy-in, kernel and copy-out streams; per chunk a ready flag (device) and
+    // a completion word (mapped pinned host memory); the epoch values the flag copies read (pinned)
+    cudaStream_t xs[3] = {};
+    int* d_xready = nullptr;
+    int* d_xdone = nullptr;
+    int* h_xepoch = nullptr;
+    int* h_xsync = nullptr;      // [kStreamChunks] completion words, then the error word
+    int* h_xsync_dev = nullptr;  // device alias of h_xsync
+    int xepoch = 0;
+    long long xwait_cycles = 0;
     std::mutex mu;
     // q2 <-> q3 folded operator (built on first use of CF_FORM_AF_SYM); fold_status != 0 if the
     // COO list is not symmetric in its last two indices
@@ -250,8 +264,13 @@ void free_plan_memory(cf_plan* p) {
     cudaFree(p->d_pitems);
     cudaFree(p->d_ws);
     cudaFree(p->d_io);
+    cudaFree(p->d_xready);
+    if (p->h_xepoch) cudaFreeHost(p->h_xepoch);
+    if (p->h_xsync) cudaFreeHost(p->h_xsync);
     if (p->stream) cudaStreamDestroy(p->stream);
     for (cudaStream_t& hs : p->host_streams)
+        if (hs) cudaStreamDestroy(hs);
+    for (cudaStream_t& hs : p->xs)
         if (hs) cudaStreamDestroy(hs);
 }
 
@@ -448,7 +467,8 @@ int* counter_for(const cf_plan* pc, cudaStream_t st) {
 }
 
 int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const double* vT, double* QT, int64_t B,
-             cudaStream_t st, const float* fT32 = nullptr, bool bf16 = false) {
+             cudaStream_t st, const float* fT32 = nullptr, bool bf16 = false, const StreamSync* ss = nullptr,
+             const double* f_cm = nullptr, double* q_cm = nullptr) {
     const int64_t nt = n_tiles_for(B);
     // The folded operator has about half the COO entries per slice of the plain one, so its Phi step
     // is light next to the K^3 step; there the tile kernel (16 warps per SM) runs ahead of the pair
@@ -457,6 +477,9 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
     cf::LaunchArgs a{p->op(), fT, vT, QT, nt, B, st, what, exact, p->path, p->d_bin_begin, p->d_bin_q1,
                      counter_for(p, st), p->n_sms, p->max_smem, p->d_pbin_begin, p->d_pbin_item, p->d_pitems,
                      fT32 != nullptr, fT32, tile_first, bf16};
+    a.ss = ss;
+    a.f_cm = f_cm;
+    a.q_cm = q_cm;
     cf::LaunchResult r{8, 0, cudaSuccess};
     switch (p->k) {
 #define CF_K(KK) \
@@ -795,6 +818,109 @@ int cached_plan(cf_plan** out, const double* labels, const double* vals, const d
     return CF_OK;
 }
 
+// Streamed host path: whether the fast angular-first form on `target` runs on the tile kernel (so the
+// streamed kernel reproduces the device path bit for bit) and the tile fits in shared memory.
+bool streamable(const cf_plan* p, const cf_plan* target, int what, bool exact, int f32) {
+    if (what != 0 || exact || f32 != 0 || p->k % 2 != 0 || p->k > 8) return false;
+    const bool tile = target->parent != nullptr ? (p->path == 0 || p->path == cf::PATH_TILE) : p->path == cf::PATH_TILE;
+    if (!tile) return false;
+    const size_t smem = sizeof(double) * ((size_t)p->n_q * p->k * 16 + (size_t)16 * p->k * (p->k * p->k + 2));
+    return smem + 256 <= p->max_smem;
+}
+
+int ensure_stream_sync(cf_plan* p) {
+    if (p->d_xready) return CF_OK;
+    for (cudaStream_t& s : p->xs)
+        if (!s) CF_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int khz = 0;
+    CF_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, p->device));
+    p->xwait_cycles = (long long)((double)std::max(khz, 1000000) * 1e3 * kStreamWaitSeconds);
+    CF_CUDA(cudaHostAlloc((void**)&p->h_xepoch, kStreamChunks * sizeof(int), cudaHostAllocDefault));
+    CF_CUDA(cudaHostAlloc((void**)&p->h_xsync, (kStreamChunks + 1) * sizeof(int), cudaHostAllocMapped));
+    CF_CUDA(cudaHostGetDevicePointer((void**)&p->h_xsync_dev, p->h_xsync, 0));
+    int* d = nullptr;
+    CF_CUDA(cudaMalloc((void**)&d, (2 * kStreamChunks + 1) * sizeof(int)));
+    CF_CUDA(cudaMemset(d, 0, (2 * kStreamChunks + 1) * sizeof(int)));
+    p->d_xready = d;
+    p->d_xdone = d + kStreamChunks;
+    return CF_OK;
+}
+
+// Q += op(f) for B cells in host memory with one launch of the streamed tile kernel: every chunk's
+// uploads and ready flag are queued first (copy-in stream), then the kernel (kernel stream), then
+// each chunk's download as soon as the kernel marks it final (copy-out stream).  Queueing every
+// upload before the launch keeps the copies ahead of the kernel even where the two streams share a
+// hardware queue.  The host waits for a chunk's completion word only while the kernel is still
+// running, and the kernel's own waits are bounded, so the call always ends.
+//
+// send = false (the self-test) queues no uploads and no flags, so the kernel's waits run out after
+// wait_cycles; the call then returns CF_ETIMEOUT with Q untouched on the host.
+int run_host_streamed(cf_plan* p, cf_plan* target, double* Q, const double* f, int64_t B, double* dQ, double* df,
+                      bool send = true, long long wait_cycles = 0) {
+    CF_TRY(ensure_stream_sync(p));
+    const int64_t M = (int64_t)p->n_q * p->k;
+    const int64_t n_ht = (B + 15) / 16;
+    const int64_t hpc = (n_ht + kStreamChunks - 1) / kStreamChunks;
+    const int n_chunks = (int)((n_ht + hpc - 1) / hpc);
+    p->xepoch = p->xepoch % 0x3fffffff + 1;
+    const int epoch = p->xepoch;
+    volatile int* hs = p->h_xsync;
+    for (int c = 0; c < n_chunks; ++c) {
+        p->h_xepoch[c] = epoch;
+        hs[c] = 0;
+    }
+    hs[kStreamChunks] = 0;
+    cudaStream_t s_in = p->xs[0], s_k = p->xs[1], s_out = p->xs[2];
+    CF_CUDA(cudaMemsetAsync(p->d_xdone, 0, n_chunks * sizeof(int), s_k));
+    auto span = [&](int c, int64_t& off, size_t& nb) {
+        const int64_t b0 = (int64_t)c * hpc * 16, b1 = std::min<int64_t>(B, (int64_t)(c + 1) * hpc * 16);
+        off = b0 * M;
+        nb = (size_t)(b1 - b0) * M * sizeof(double);
+    };
+    for (int c = 0; c < n_chunks && send; ++c) {
+        int64_t off;
+        size_t nb;
+        span(c, off, nb);
+        CF_CUDA(cudaMemcpyAsync(df + off, f + off, nb, cudaMemcpyHostToDevice, s_in));
+        CF_CUDA(cudaMemcpyAsync(dQ + off, Q + off, nb, cudaMemcpyHostToDevice, s_in));
+        CF_CUDA(cudaMemcpyAsync(p->d_xready + c, p->h_xepoch + c, sizeof(int), cudaMemcpyHostToDevice, s_in));
+    }
+    StreamSync ss{p->d_xready, p->d_xdone, p->h_xsync_dev, p->h_xsync_dev + kStreamChunks,
+                  p->d_xdone + kStreamChunks, epoch, (int)hpc, wait_cycles > 0 ? wait_cycles : p->xwait_cycles};
+    int st = dispatch(target, 0, false, nullptr, nullptr, nullptr, B, s_k, nullptr, false, &ss, df, dQ);
+    int next = 0;
+    while (st == CF_OK && next < n_chunks) {
+        bool all = false;
+        if (hs[next] != epoch) {
+            const cudaError_t q = cudaStreamQuery(s_k);
+            if (q == cudaErrorNotReady) {
+                std::this_thread::yield();
+                continue;
+            }
+            if (q != cudaSuccess) {
+                st = fail(CF_ECUDA, "streamed contraction: %s", cudaGetErrorString(q));
+                break;
+            }
+            all = true;  // the kernel has ended: every chunk is final
+        }
+        for (int c = next; c < (all ? n_chunks : next + 1) && send; ++c) {
+            int64_t off;
+            size_t nb;
+            span(c, off, nb);
+            const cudaError_t e = cudaMemcpyAsync(Q + off, dQ + off, nb, cudaMemcpyDeviceToHost, s_out);
+            if (e != cudaSuccess) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+        }
+        next = all ? n_chunks : next + 1;
+    }
+    for (cudaStream_t s : p->xs) {
+        const cudaError_t e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess && st == CF_OK) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+    }
+    if (st == CF_OK && hs[kStreamChunks] != 0)
+        st = fail(CF_ETIMEOUT, "streamed contraction: a chunk's data did not arrive within the wait limit");
+    return st;
+}
+
 // Host-pointer contraction: upload, run, download.  what: 0 AF, 1 RF, 2 JV.
 int run_host(int what, bool exact, double* Q, const double* f, const double* v, int64_t B, const double* labels,
              const double* vals, const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
@@ -823,6 +949,11 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
         CF_CUDA(cudaMemcpyAsync(Q, dQ, cell_bytes, cudaMemcpyDeviceToHost, p->stream));
         CF_CUDA(cudaStreamSynchronize(p->stream));
         return CF_OK;
+    }
+    if (B >= 2 * kHostChunkMin) {
+        cf_plan* target = p;
+        if (sym) CF_TRY(get_sym(p, &target));
+        if (streamable(p, target, what, exact, f32)) return run_host_streamed(p, target, Q, f, B, dQ, df);
     }
     // Chunked: chunk c goes up, is contracted and comes back on stream c mod kHostStreams, so the
     // host<->device copies of one chunk overlap the contraction of the others (pinned host memory
@@ -1091,6 +1222,27 @@ int cf_plan_set_kernel_path(cf_plan* plan, int32_t path) {
     plan->path = path;
     if (plan->sym) plan->sym->path = path;
     return CF_OK;
+}
+
+int cf_plan_stream_selftest(cf_plan* plan, double wait_seconds) {
+    g_last_error.clear();
+    if (!plan) return fail(CF_EINVAL, "null plan");
+    if (!(wait_seconds > 0.0 && wait_seconds <= 10.0)) return fail(CF_EINVAL, "wait_seconds must be in (0, 10]");
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard guard(plan->device);
+    if (!guard.ok) return fail(CF_ENODEVICE, "cannot select device %d", plan->device);
+    if (plan->n_g == 0 || plan->k % 2 != 0 || plan->k > 8)
+        return fail(CF_EUNSUPPORTED, "the streamed tile kernel needs an even K <= 8 and a non-empty operator");
+    const int64_t B = 64;
+    const size_t cell_bytes = (size_t)B * plan->n_q * plan->k * sizeof(double);
+    CF_TRY(ensure_io(plan, 2 * cell_bytes));
+    CF_TRY(ensure_stream_sync(plan));
+    int khz = 0;
+    CF_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, plan->device));
+    const long long cycles = std::max(1LL, (long long)((double)std::max(khz, 1000000) * 1e3 * wait_seconds));
+    double* dQ = plan->d_io;
+    double* df = (double*)((char*)plan->d_io + cell_bytes);
+    return run_host_streamed(plan, plan, nullptr, nullptr, B, dQ, df, false, cycles);
 }
 
 int cf_fp64_fma_peak(int32_t device, double* tflops) {

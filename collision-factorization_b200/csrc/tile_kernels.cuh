@@ -13,7 +13,8 @@
 //     half-tiles split into q1 bins, so the last wave is made of small units.  Inside a unit the
 //     warps pull q1 values (heaviest first) from a shared counter.
 //
-// The counter is the only inter-CTA interaction; nothing waits on another CTA.
+// The counter is the only inter-CTA interaction; nothing waits on another CTA.  The streamed
+// variant at the end also waits, with a bound, on flags that the host's copies set.
 #pragma once
 #include "common.cuh"
 
@@ -46,11 +47,20 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+// Offset of Q[q1][k1] from a lane's cell: tiled rows (stride CF_TILE) or, with CELL_MAJOR, the
+// caller's [N_Q x K x B] layout (qtc then points at the cell's first element).
+template <int K, bool CELL_MAJOR>
+__device__ __forceinline__ size_t q_off(int q1, int k1, int n_q) {
+    return CELL_MAJOR ? (size_t)q1 + (size_t)k1 * n_q : (size_t)(q1 * K + k1) * CF_TILE;
+}
+
 // Contract every slice of one q1 for the resident half-tile.  qtc points at this lane's cell of
-// the tiled output; the result is accumulated into it (out += ...).
-template <int K, bool EXACT, bool JV>
+// the output; the result is accumulated into it (out += ...).  live = false: the lane's cell is
+// past the end of the batch (cell-major output only), and Q is neither read nor written.
+template <int K, bool EXACT, bool JV, bool CELL_MAJOR = false>
 __device__ __forceinline__ void tile_q1(const DevOp& op, int q1, const double* __restrict__ fs,
-                                        const double* __restrict__ vs, double* rb, double* qtc, int lane) {
+                                        const double* __restrict__ vs, double* rb, double* qtc, int lane,
+                                        bool live = true) {
     constexpr int KC = K / 2;
     constexpr int SL = RBuf<K>::SL;
     const int c = lane & 15;
@@ -60,7 +70,8 @@ __device__ __forceinline__ void tile_q1(const DevOp& op, int q1, const double* _
 
     double acc[K];
 #pragma unroll
-    for (int k1 = 0; k1 < K; ++k1) acc[k1] = (part == owner) ? qtc[(size_t)(q1 * K + k1) * CF_TILE] : 0.0;
+    for (int k1 = 0; k1 < K; ++k1)
+        acc[k1] = (part == owner && live) ? qtc[q_off<K, CELL_MAJOR>(q1, k1, op.n_q)] : 0.0;
 
     const int s0 = op.q1_begin[q1], s1 = op.q1_begin[q1 + 1];
     for (int s = s0; s < s1; ++s) {
@@ -193,9 +204,9 @@ __device__ __forceinline__ void tile_q1(const DevOp& op, int q1, const double* _
 #pragma unroll
         for (int k1 = 0; k1 < K; ++k1) acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], 16);
     }
-    if (part == owner) {
+    if (part == owner && live) {
 #pragma unroll
-        for (int k1 = 0; k1 < K; ++k1) qtc[(size_t)(q1 * K + k1) * CF_TILE] = acc[k1];
+        for (int k1 = 0; k1 < K; ++k1) qtc[q_off<K, CELL_MAJOR>(q1, k1, op.n_q)] = acc[k1];
     }
 }
 
@@ -264,6 +275,109 @@ __global__ void __launch_bounds__(W * 32, 1)
 template <int K>
 constexpr size_t tile_smem_bytes(int M, int W, bool jv) {
     return sizeof(double) * ((size_t)(jv ? 2 : 1) * M * kTileCells + (size_t)W * RBuf<K>::SIZE);
+}
+
+// ------------------------------------------------------------------------------------------
+// Streamed tile kernel (host entry points): one launch over the whole batch while the batch is
+// still being copied in and the results are being copied out.
+//
+// f and Q stay in the caller's cell-major layout [N_Q x K x B] in device memory.  The host cuts
+// the batch into chunks of whole half-tiles and queues, on a copy stream, each chunk's f and Q
+// uploads followed by a 4-byte copy that sets ready[c] = epoch.  Every half-tile is split into
+// `split` q1 bins, so the first chunk already gives work to every CTA.  A CTA waits for its
+// chunk's flag (bounded by wait_cycles of the SM clock; past that it records err and abort, and
+// every later wait returns at once),
+// stages the 16 cells from the cell-major rows, and contracts its bin with the same per-row code
+// as the tile kernel, reading Q_in and writing Q_out in place: the same operations in the same
+// order as the tiled kernel, hence the same bits.  After a unit every thread fences and the CTA
+// counts the unit in done[c]; the CTA that completes chunk c fences at system scope and writes
+// epoch into host_done[c], a word of mapped pinned host memory the host polls before queueing the
+// chunk's download.
+// ------------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template <int K, int W>
+__global__ void __launch_bounds__(W * 32, 1)
+    af_tile_stream_kernel(DevOp op, TileSched sc, StreamSync ss, const double* __restrict__ f, double* q,
+                          long long n_cells) {
+    static_assert(K % 2 == 0, "the tile kernel splits Phi into two column halves");
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_unit, s_next;
+    const int M = op.n_q * K;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    double* fs = smem;
+    double* rb = smem + (size_t)M * kTileCells + (size_t)warp * RBuf<K>::SIZE;
+    int staged = -1;
+
+    for (;;) {
+        if (tid == 0) s_unit = atomicAdd(sc.counter, 1);
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= sc.n_units) break;
+        const int ht = u / sc.split;
+        const int bin = bin_base(sc.split) + u % sc.split;
+        const int chunk = ht / ss.ht_per_chunk;
+        const long long cell0 = (long long)ht * kTileCells;
+        if (ht != staged) {
+            if (tid == 0) {
+                const long long t0 = clock64();
+                while (ld_acquire(ss.ready + chunk) != ss.epoch) {
+                    if (*reinterpret_cast<volatile int*>(ss.abort) == ss.epoch) break;
+                    if (clock64() - t0 > ss.wait_cycles) {
+                        *reinterpret_cast<volatile int*>(ss.abort) = ss.epoch;
+                        *reinterpret_cast<volatile int*>(ss.err) = 1;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+            }
+            __syncthreads();
+            // element j = q + N_Q k of cell c (cell-major) goes to row q K + k of the tile; a warp
+            // reads two consecutive j of 16 cells and writes two 16-cell rows of shared memory
+            for (int i = tid; i < M * kTileCells; i += W * 32) {
+                const int c = i & 15, j = i >> 4;
+                const int r = (j % op.n_q) * K + j / op.n_q;
+                if (cell0 + c < n_cells)
+                    cp_async8(fs + r * kTileCells + c, f + (size_t)(cell0 + c) * M + j);
+                else
+                    fs[r * kTileCells + c] = 0.0;
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            staged = ht;
+        }
+        if (tid == 0) s_next = 0;
+        __syncthreads();
+        const int b0 = sc.bin_begin[bin], nb = sc.bin_begin[bin + 1] - b0;
+        const long long cell = cell0 + (lane & 15);
+        const bool live = cell < n_cells;
+        double* qc = q + (size_t)(live ? cell : 0) * M;
+        for (;;) {
+            int i = 0;
+            if (lane == 0) i = atomicAdd(&s_next, 1);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= nb) break;
+            tile_q1<K, false, false, true>(op, sc.bin_q1[b0 + i], fs, nullptr, rb, qc, lane, live);
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) {
+            const int c_ht = min(ss.ht_per_chunk, sc.n_ht - chunk * ss.ht_per_chunk);
+            if (atomicAdd(ss.done + chunk, 1) == c_ht * sc.split - 1) {
+                __threadfence_system();
+                *reinterpret_cast<volatile int*>(ss.host_done + chunk) = ss.epoch;
+            }
+        }
+    }
 }
 
 }  // namespace cf

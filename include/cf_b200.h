@@ -102,7 +102,12 @@ int cf_radial_first(double* Q, const double* f, const double* labels, const doub
                     int32_t k);
 
 /* Batched host-pointer form of both (Q, f: [N_Q x K x B]); form is a cf_form.  The host-side
- * counterpart of calling the reference MEX once per cell (benchmark_collision_contraction_scaling.m:96-108). */
+ * counterpart of calling the reference MEX once per cell (benchmark_collision_contraction_scaling.m:96-108).
+ * From 512 cells up, the fast FP64 forms that run on the tile kernel (CF_FORM_AF_SYM with the
+ * automatic kernel order; either fast form with kernel path 2) are streamed: one launch over the
+ * whole batch starts as soon as the first chunk of cells is on the device and hands each chunk back
+ * as soon as it is final, with the same result bits as the device entry points.  Other forms cut
+ * the batch into chunks that go up, are contracted and come back on three streams. */
 int cf_contract_host(double* Q, const double* f, int64_t b, const double* labels, const double* vals,
                      const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
                      int32_t k, int32_t form);
@@ -188,6 +193,13 @@ int cf_fp64_fma_peak(int32_t device, double* tflops);
 #define CF_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form,
                         void* stream);
+
+/* Self-test of the streamed host path's bounded wait (no counterpart in the reference): launches
+ * the streamed tile kernel of `plan` (even K <= 8) over 64 cells whose data and ready flags are
+ * never sent, so every CTA's wait runs out after wait_seconds (0 < wait_seconds <= 10) and the
+ * kernel returns.  Returns CF_ETIMEOUT when the wait gave up and reported it, as it should; the
+ * plan's device scratch then holds garbage, nothing else is touched. */
+int cf_plan_stream_selftest(cf_plan* plan, double wait_seconds);
 
 /* ------------------------------------------------------------------------------------------
  * Ragged batches: cells of several resolutions (one plan per (L, K) bucket) contracted in ONE
