@@ -72,7 +72,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = True) ->
                 fut.result()
     objs = [str(u[1]) for u in units]
     if force or todo or not LIB.exists():
-        cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(LIB), *objs, "-lcudart"]
+        cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(LIB), *objs, "-lcudart", "-lpthread"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")

@@ -744,24 +744,58 @@ int get_sym(cf_plan* p, cf_plan** out) {
 // Content-keyed cache of plans for the MEX-style host entry points
 // ------------------------------------------------------------------------------------------
 uint64_t hash_words(const double* a, int64_t n, uint64_t h) {
-    // four independent multiply-xorshift lanes (the dependency chain of one lane bounds the speed)
+    // eight independent multiply-xorshift lanes, so the multiplier's throughput rather than one
+    // lane's dependency chain bounds the speed
+    constexpr int NL = 8;
     const uint64_t* w = reinterpret_cast<const uint64_t*>(a);
-    uint64_t l[4] = {h, h ^ 0x9e3779b97f4a7c15ULL, h ^ 0xbf58476d1ce4e5b9ULL, h ^ 0x94d049bb133111ebULL};
+    uint64_t l[NL];
+    for (int j = 0; j < NL; ++j) l[j] = h ^ (0x9e3779b97f4a7c15ULL * (uint64_t)(j + 1));
     int64_t i = 0;
-    for (; i + 4 <= n; i += 4)
-        for (int j = 0; j < 4; ++j) {
+    for (; i + NL <= n; i += NL)
+        for (int j = 0; j < NL; ++j) {
             l[j] ^= w[i + j];
             l[j] *= 0x100000001b3ULL;
             l[j] ^= l[j] >> 29;
         }
+    uint64_t r = (uint64_t)n ^ h;
     for (; i < n; ++i) {
-        l[0] ^= w[i];
-        l[0] *= 0x100000001b3ULL;
-        l[0] ^= l[0] >> 29;
+        r ^= w[i];
+        r *= 0x100000001b3ULL;
+        r ^= r >> 29;
     }
-    uint64_t r = (uint64_t)n;
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < NL; ++j) {
         r ^= l[j];
+        r *= 0x100000001b3ULL;
+        r ^= r >> 31;
+    }
+    return r;
+}
+
+// Content key of an operator: the four arrays hashed separately and combined in a fixed order.
+// Above 1 MB a helper thread hashes labels and vals while the caller hashes ic_map and R (the
+// key does not depend on which thread hashed what).
+uint64_t hash_operator(const double* labels, const double* vals, const double* ic_map, const double* R, int64_t n_g,
+                       int64_t n_r) {
+    uint64_t hl = 0, hv = 0;
+    auto first = [&] {
+        hl = hash_words(labels, 3 * n_g, 0x11);
+        hv = hash_words(vals, n_g, 0x22);
+    };
+    bool threaded = (5 * n_g + n_r) * (int64_t)sizeof(double) > ((int64_t)1 << 20);
+    std::thread helper;
+    if (threaded) {
+        try {
+            helper = std::thread(first);
+        } catch (...) {
+            threaded = false;
+        }
+    }
+    if (!threaded) first();
+    const uint64_t hi = hash_words(ic_map, n_g, 0x33), hr = hash_words(R, n_r, 0x44);
+    if (threaded) helper.join();
+    uint64_t r = 0xcbf29ce484222325ULL;
+    for (uint64_t x : {hl, hv, hi, hr}) {
+        r ^= x;
         r *= 0x100000001b3ULL;
         r ^= r >> 31;
     }
@@ -773,6 +807,7 @@ struct CacheEntry {
     int64_t n_g;
     int n_l, n_q, k, device;
     cf_plan* plan;
+    const void* ptrs[4];  // labels, vals, ic_map, R of the last call that found this entry by content
 };
 
 std::mutex g_cache_mu;
@@ -786,23 +821,22 @@ int cached_plan(cf_plan** out, const double* labels, const double* vals, const d
     CF_CUDA(cudaGetDevice(&device));
     if (n_g < 0 || k < 1 || k > kMaxK || n_l < 0) return validate(labels, vals, ic_map, R, n_g, n_l, n_q, k);
     uint64_t h = 0xcbf29ce484222325ULL;
-    if (n_g > 0 && labels && vals && ic_map && R) {
-        h = hash_words(labels, 3 * n_g, h);
-        h = hash_words(vals, n_g, h);
-        h = hash_words(ic_map, n_g, h);
-        h = hash_words(R, (int64_t)k * k * k * n_l, h);
-    }
+    if (n_g > 0 && labels && vals && ic_map && R) h = hash_operator(labels, vals, ic_map, R, n_g, (int64_t)k * k * k * n_l);
+    const void* ptrs[4] = {labels, vals, ic_map, R};
     std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (CacheEntry& e : g_cache)  // these pointers now belong to the entry found or made below
+        if (std::equal(e.ptrs, e.ptrs + 4, ptrs)) std::fill(e.ptrs, e.ptrs + 4, nullptr);
     for (auto it = g_cache.begin(); it != g_cache.end(); ++it) {
         if (it->key == h && it->n_g == n_g && it->n_l == n_l && it->n_q == n_q && it->k == k && it->device == device) {
             g_cache.splice(g_cache.begin(), g_cache, it);
+            std::copy(ptrs, ptrs + 4, g_cache.front().ptrs);
             *out = g_cache.front().plan;
             return CF_OK;
         }
     }
     cf_plan* p = nullptr;
     CF_TRY(plan_create(&p, labels, vals, ic_map, R, n_g, n_l, n_q, k, device));
-    g_cache.push_front({h, n_g, n_l, n_q, k, device, p});
+    g_cache.push_front({h, n_g, n_l, n_q, k, device, p, {labels, vals, ic_map, R}});
     while (g_cache.size() > kCacheMax) {
         cf_plan* old = g_cache.back().plan;
         g_cache.pop_back();
@@ -816,6 +850,26 @@ int cached_plan(cf_plan** out, const double* labels, const double* vals, const d
     }
     *out = p;
     return CF_OK;
+}
+
+// The plan that the last content lookup with these very pointers (and sizes, on the current device)
+// found, with its content key: a guess that the arrays did not change since, which the streamed
+// host path verifies while the GPU already works on it.
+bool plan_by_pointers(cf_plan** out, uint64_t* key, const double* labels, const double* vals, const double* ic_map,
+                      const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k) {
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return false;
+    const void* ptrs[4] = {labels, vals, ic_map, R};
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (auto it = g_cache.begin(); it != g_cache.end(); ++it)
+        if (std::equal(it->ptrs, it->ptrs + 4, ptrs) && it->n_g == n_g && it->n_l == n_l && it->n_q == n_q &&
+            it->k == k && it->device == device) {
+            g_cache.splice(g_cache.begin(), g_cache, it);
+            *out = g_cache.front().plan;
+            *key = g_cache.front().key;
+            return true;
+        }
+    return false;
 }
 
 // Streamed host path: whether the fast angular-first form on `target` runs on the tile kernel (so the
@@ -855,8 +909,13 @@ int ensure_stream_sync(cf_plan* p) {
 //
 // send = false (the self-test) queues no uploads and no flags, so the kernel's waits run out after
 // wait_cycles; the call then returns CF_ETIMEOUT with Q untouched on the host.
+//
+// gate (speculative calls): no chunk goes back to Q before *gate is 1 (the operator's content was
+// verified); 2 means it changed: the call copies nothing back, waits for the kernel and returns
+// kRetry, and the caller contracts again with the right plan.
+constexpr int kRetry = -1;
 int run_host_streamed(cf_plan* p, cf_plan* target, double* Q, const double* f, int64_t B, double* dQ, double* df,
-                      bool send = true, long long wait_cycles = 0) {
+                      bool send = true, long long wait_cycles = 0, const std::atomic<int>* gate = nullptr) {
     CF_TRY(ensure_stream_sync(p));
     const int64_t M = (int64_t)p->n_q * p->k;
     const int64_t n_ht = (B + 15) / 16;
@@ -890,6 +949,17 @@ int run_host_streamed(cf_plan* p, cf_plan* target, double* Q, const double* f, i
     int st = dispatch(target, 0, false, nullptr, nullptr, nullptr, B, s_k, nullptr, false, &ss, df, dQ);
     int next = 0;
     while (st == CF_OK && next < n_chunks) {
+        if (gate) {
+            const int g = gate->load(std::memory_order_acquire);
+            if (g == 2) {
+                st = kRetry;
+                break;
+            }
+            if (g == 0) {
+                std::this_thread::yield();
+                continue;
+            }
+        }
         bool all = false;
         if (hs[next] != epoch) {
             const cudaError_t q = cudaStreamQuery(s_k);
@@ -914,10 +984,46 @@ int run_host_streamed(cf_plan* p, cf_plan* target, double* Q, const double* f, i
     }
     for (cudaStream_t s : p->xs) {
         const cudaError_t e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess && st == CF_OK) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+        if (e != cudaSuccess && (st == CF_OK || st == kRetry)) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
     }
     if (st == CF_OK && hs[kStreamChunks] != 0)
         st = fail(CF_ETIMEOUT, "streamed contraction: a chunk's data did not arrive within the wait limit");
+    return st;
+}
+
+// The streamed contraction with the plan these pointers had last time, while a helper thread checks
+// the operator's content hash; nothing reaches Q before the check passes.  kRetry: no guess, the
+// guess does not stream, or the content changed (Q untouched) -- contract the ordinary way.
+int run_host_speculative(double* Q, const double* f, int64_t B, const double* labels, const double* vals,
+                         const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k,
+                         bool sym) {
+    cf_plan* p = nullptr;
+    uint64_t key = 0;
+    if (n_g <= 0 || !labels || !vals || !ic_map || !R) return kRetry;
+    if (!plan_by_pointers(&p, &key, labels, vals, ic_map, R, n_g, n_l, n_q, k)) return kRetry;
+    std::lock_guard<std::mutex> lk(p->mu);
+    DeviceGuard guard(p->device);
+    if (!guard.ok) return kRetry;
+    cf_plan* target = p;
+    if (sym && get_sym(p, &target) != CF_OK) return kRetry;
+    if (!streamable(p, target, 0, false, 0)) return kRetry;
+    const size_t cell_bytes = (size_t)B * p->n_q * p->k * sizeof(double);
+    if (ensure_io(p, 2 * cell_bytes) != CF_OK) return kRetry;
+    std::atomic<int> gate{0};
+    std::thread check;
+    try {
+        check = std::thread([&] {
+            const uint64_t h = hash_operator(labels, vals, ic_map, R, n_g, (int64_t)k * k * k * n_l);
+            gate.store(h == key ? 1 : 2, std::memory_order_release);
+        });
+    } catch (...) {
+        return kRetry;
+    }
+    double* dQ = p->d_io;
+    double* df = (double*)((char*)p->d_io + cell_bytes);
+    const int st = run_host_streamed(p, target, Q, f, B, dQ, df, true, 0, &gate);
+    check.join();
+    if (gate.load() == 2) return kRetry;  // nothing was copied back: Q is as the caller passed it
     return st;
 }
 
@@ -927,6 +1033,10 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
              int32_t k, bool sym = false, int f32 = 0) {
     if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
     if (!Q || !f || (what == 2 && !v)) return fail(CF_EINVAL, "null host buffer");
+    if (what == 0 && !exact && f32 == 0 && B >= 2 * kHostChunkMin) {
+        const int r = run_host_speculative(Q, f, B, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym);
+        if (r != kRetry) return r;
+    }
     cf_plan* p = nullptr;
     CF_TRY(cached_plan(&p, labels, vals, ic_map, R, n_g, n_l, n_q, k));
     if (B == 0 || n_g == 0) return CF_OK;

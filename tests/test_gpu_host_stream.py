@@ -114,3 +114,40 @@ def test_stream_wait_gives_up_and_reports(cuda_available):
     assert op.stream_selftest(1e-3) == 9
     assert np.array_equal(op.q(f, form="af").cpu().numpy(), ref)
     op.close()
+
+
+def test_operator_changed_in_place_between_calls(cuda_available):
+    """The host call guesses the plan from the operator arrays' addresses and checks their content
+    while the GPU works; arrays changed in place (same addresses) must still give the new operator's
+    result, and Q is written only once the check passed."""
+    import torch
+
+    import cf_b200
+
+    L, K, B = 8, 8, 1500
+    geo, R, cells, q0 = _setup(L, K, B, seed=6)
+    labels = np.asfortranarray(geo.labels)
+    vals = np.array(geo.vals)
+    ic = np.array(geo.ic_map)
+    Rf = np.asfortranarray(R)
+    f_cm = np.asfortranarray(cells.transpose(2, 1, 0))
+
+    def host(Rx):
+        Q = np.array(q0.transpose(2, 1, 0), order="F")
+        cf_b200.contract_batched(Q, f_cm, labels, vals, ic, Rx, geo.n_q, K, form="af_sym")
+        return Q
+
+    def device(vx, Rx):
+        op = cf_b200.CollisionOperator(labels, vx, ic, Rx, geo.n_q, K)
+        Qd = torch.from_numpy(q0.copy()).cuda()
+        op.q(torch.from_numpy(cells).cuda(), out=Qd, form="af_sym")
+        op.close()
+        return Qd.cpu().numpy()
+
+    first = host(Rf)
+    assert np.array_equal(host(Rf).transpose(2, 1, 0), device(vals, Rf))  # same arrays: the guess holds
+    Rf *= 1.5  # same addresses, new content (kept symmetric in q2 <-> q3, as the folded form needs)
+    vals *= 0.75
+    changed = host(Rf)
+    assert np.array_equal(changed.transpose(2, 1, 0), device(vals, Rf))
+    assert not np.array_equal(changed, first)
