@@ -238,8 +238,9 @@ def fold_q2q3(geo: Geometry, R: np.ndarray, K: int):
     t' = (l1,l3,l2) contribute G R_t.(f2 (x) f3) + G' R_t'.(f3 (x) f2); with G = G' (real Gaunt
     symmetry) this is G (R_t + R_t'^T23).(f2 (x) f3).  The folded list keeps entries with l2 < l3, or
     l2 = l3 and q2 <= q3 (q2 = q3 at G/2), against R^S_t = R_t + R_t'^T23, renumbering the kept
-    triplets in order.  This is the host-side statement of what the library builds for
-    CF_FORM_AF_SYM (csrc/plan.cu, build_folded).
+    triplets in order.  Inside each run of equal (triplet, q1) the entries are then ordered by
+    (q2, q3).  This is the host-side statement of what the library builds for CF_FORM_AF_SYM
+    (csrc/plan.cu, build_folded).
     """
     lab = geo.labels.astype(np.int64)
     ic = geo.ic_map.astype(np.int64) - 1
@@ -268,4 +269,10 @@ def fold_q2q3(geo: Geometry, R: np.ndarray, K: int):
         rows.append((q1, q2, q3))
         vals.append(g)
         ics.append(tnew[ic[z]] + 1)
-    return (np.asfortranarray(np.array(rows, dtype=np.float64)), np.array(vals), np.array(ics, dtype=np.float64), Rs)
+    rows = np.array(rows, dtype=np.float64).reshape(-1, 3)
+    vals = np.array(vals)
+    ics = np.array(ics, dtype=np.float64)
+    # order by (q2, q3) inside each run of equal (triplet, q1)
+    run = np.cumsum(np.r_[True, (np.diff(ics) != 0) | (np.diff(rows[:, 0]) != 0)]) if len(ics) else np.zeros(0)
+    o = np.lexsort((rows[:, 2], rows[:, 1], run))
+    return np.asfortranarray(rows[o]), vals[o], ics[o], Rs

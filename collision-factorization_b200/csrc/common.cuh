@@ -34,6 +34,8 @@ struct DevOp {
     const double* RT;  // K = 8 only: R_t transposed to [k1][kk = K k2 + k3] (A operands of the MMA kernel)
     const unsigned short* RTbf;  // K = 8 only: R_t^T split in BF16, [t][hi, lo][k1][kk] (BF16-split form)
     const int* item_q1;
+    int grouped;  // 1: each slice's entries are sorted by q2 (the folded operator), so the fast tile
+                  // routine sums G f(q3) over each run of equal q2 before the outer product with f(q2)
     int n_items;  // number of q1 with at least one slice
     int n_q;
     int k;

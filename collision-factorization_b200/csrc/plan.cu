@@ -127,6 +127,7 @@ struct cf_plan {
     int n_pairs = 0, n_pair_items = 0;
     int n_sms = 0;
     size_t max_smem = 0;
+    bool grouped = false;  // entries of each slice sorted by (q2, q3): the folded plan
     int path = 0;  // cf::Path requested: 0 automatic, 1 gather, 2 tile, 3 pair, 4 pair (R via L1), 5 split pair
     int last_path = 0;  // family of the last angular-first / J.v launch (of this plan or its folded twin)
     cf_plan* parent = nullptr;  // for a folded twin: the plan it folds
@@ -167,6 +168,7 @@ struct cf_plan {
         o.RT = d_RT;
         o.RTbf = d_RTbf;
         o.item_q1 = d_item_q1;
+        o.grouped = grouped ? 1 : 0;
         o.n_items = n_items;
         o.n_q = n_q;
         o.k = k;
@@ -704,7 +706,32 @@ int build_folded(const cf_plan* p, std::vector<double>& lab2, std::vector<double
         val2.push_back(q2 == q3 ? 0.5 * val[z] : 0.5 * (val[z] + gp));
         ic2.push_back((double)(tnew[t] + 1));
     }
+    // inside each run of equal (l-triplet, q1) the entries are ordered by (q2, q3), so that runs of
+    // equal q2 are as long as they can be (the tile routine's grouped Phi step); the folded operator
+    // has no exact form, so the order is free
     ng2 = (int64_t)q1v.size();
+    {
+        std::vector<int64_t> perm(ng2);
+        for (int64_t i = 0; i < ng2; ++i) perm[i] = i;
+        for (int64_t a = 0; a < ng2;) {
+            int64_t b = a + 1;
+            while (b < ng2 && ic2[b] == ic2[a] && q1v[b] == q1v[a]) ++b;
+            std::stable_sort(perm.begin() + a, perm.begin() + b, [&](int64_t x, int64_t y) {
+                return q2v[x] != q2v[y] ? q2v[x] < q2v[y] : q3v[x] < q3v[y];
+            });
+            a = b;
+        }
+        auto apply = [&](std::vector<double>& v) {
+            std::vector<double> w(v.size());
+            for (int64_t i = 0; i < ng2; ++i) w[i] = v[perm[i]];
+            v.swap(w);
+        };
+        apply(q1v);
+        apply(q2v);
+        apply(q3v);
+        apply(val2);
+        apply(ic2);
+    }
     lab2.clear();
     lab2.insert(lab2.end(), q1v.begin(), q1v.end());
     lab2.insert(lab2.end(), q2v.begin(), q2v.end());
@@ -733,6 +760,7 @@ int get_sym(cf_plan* p, cf_plan** out) {
     if (st != CF_OK) return st;
     s->path = p->path;
     s->parent = p;
+    s->grouped = true;
     s->h_labels.clear();  // the folded plan is never folded again
     p->sym = s;
     p->fold_status = 0;

@@ -92,7 +92,59 @@ __device__ __forceinline__ void tile_q1(const DevOp& op, int q1, const double* _
 #pragma unroll
             for (int b = 0; b < KC; ++b) phi[a][b] = 0.0;
 
-        for (int eb = e0; eb < e1; eb += 32) {
+        bool phi_done = false;
+        if constexpr (!EXACT && !JV) {
+            if (op.grouped) {
+                // entries sorted by q2: h = sum over a run of equal q2 of G f(q3), then
+                // Phi += f(q2) (x) h once per run -- the f(q2) loads and the K x K/2 FMAs once per
+                // run instead of once per entry (the run index is warp-uniform)
+                double h[KC];
+#pragma unroll
+                for (int b = 0; b < KC; ++b) h[b] = 0.0;
+                int cur = -1;
+                for (int eb = e0; eb < e1; eb += 32) {
+                    const int n = min(32, e1 - eb);
+                    uint32_t my_q23 = 0;
+                    double my_g = 0.0;
+                    if (lane < n) {
+                        my_q23 = __ldg(op.e_q23 + eb + lane);
+                        my_g = __ldg(op.e_g + eb + lane);
+                    }
+                    for (int j = 0; j < n; ++j) {
+                        const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, j);
+                        const double g = __shfl_sync(0xffffffffu, my_g, j);
+                        const int q2 = (int)(q23 & 0xffffu), r3 = (int)(q23 >> 16) * K + k3b;
+                        if (q2 != cur) {
+                            if (cur >= 0) {
+                                const int r2 = cur * K;
+#pragma unroll
+                                for (int k2 = 0; k2 < K; ++k2) {
+                                    const double f2 = fs[(r2 + k2) * kTileCells + c];
+#pragma unroll
+                                    for (int b = 0; b < KC; ++b) phi[k2][b] = fma(f2, h[b], phi[k2][b]);
+                                }
+#pragma unroll
+                                for (int b = 0; b < KC; ++b) h[b] = 0.0;
+                            }
+                            cur = q2;
+                        }
+#pragma unroll
+                        for (int b = 0; b < KC; ++b) h[b] = fma(g, fs[(r3 + b) * kTileCells + c], h[b]);
+                    }
+                }
+                if (cur >= 0) {
+                    const int r2 = cur * K;
+#pragma unroll
+                    for (int k2 = 0; k2 < K; ++k2) {
+                        const double f2 = fs[(r2 + k2) * kTileCells + c];
+#pragma unroll
+                        for (int b = 0; b < KC; ++b) phi[k2][b] = fma(f2, h[b], phi[k2][b]);
+                    }
+                }
+                phi_done = true;
+            }
+        }
+        for (int eb = e0; eb < e1 && !phi_done; eb += 32) {
             const int n = min(32, e1 - eb);
             uint32_t my_q23 = 0;
             double my_g = 0.0;
