@@ -335,10 +335,18 @@ extern "C" int cf_gmres_solve_tiled(cf_plan* plan, const double* f_t, double dt,
     const int gc = (int)((C + 255) / 256);
     KCHECK(cudaMemsetAsync(iters, 0, C * sizeof(int), s));
 
-    // A u = u - dt * J(f) u, preconditioned operand z = P^-1 u
+    // A u = u - dt * J(f) u, preconditioned operand z = P^-1 u.  J(f) u runs on the q2 <-> q3 folded
+    // operator (the same bilinear form on half the entries) when the operator folds, else on the
+    // plain one.
+    int jv_mode = 2;
     auto apply_A = [&](double* out, const double* u) -> int {
         KCHECK(cudaMemsetAsync(out, 0, vec * sizeof(double), s));
-        int rc = cf_jv_tiled(plan, out, f_t, u, b, 0, s);
+        int rc = cf_jv_tiled(plan, out, f_t, u, b, jv_mode, s);
+        if (rc == CF_EUNSUPPORTED && jv_mode == 2) {
+            jv_mode = 0;
+            cf_set_last_error("");
+            rc = cf_jv_tiled(plan, out, f_t, u, b, jv_mode, s);
+        }
         if (rc != CF_OK) return rc;
         k_axpby<<<gv, 256, 0, s>>>(out, u, 1.0, -dt, vec);
         KLAUNCH();

@@ -93,15 +93,33 @@ __device__ __forceinline__ void tile_q1(const DevOp& op, int q1, const double* _
             for (int b = 0; b < KC; ++b) phi[a][b] = 0.0;
 
         bool phi_done = false;
-        if constexpr (!EXACT && !JV) {
+        if constexpr (!EXACT) {
             if (op.grouped) {
-                // entries sorted by q2: h = sum over a run of equal q2 of G f(q3), then
-                // Phi += f(q2) (x) h once per run -- the f(q2) loads and the K x K/2 FMAs once per
-                // run instead of once per entry (the run index is warp-uniform)
-                double h[KC];
+                // entries sorted by q2: over a run of equal q2, hf = sum G f(q3) (and, for J.v,
+                // hv = sum G v(q3)); then Phi += f(q2) (x) hf (J.v: v(q2) (x) hf + f(q2) (x) hv) once
+                // per run -- the q2 loads and the K x K/2 FMAs once per run instead of once per
+                // entry (the run index is warp-uniform)
+                double hf[KC], hv[KC];
 #pragma unroll
-                for (int b = 0; b < KC; ++b) h[b] = 0.0;
+                for (int b = 0; b < KC; ++b) hf[b] = hv[b] = 0.0;
                 int cur = -1;
+                auto flush = [&]() {
+                    const int r2 = cur * K;
+#pragma unroll
+                    for (int k2 = 0; k2 < K; ++k2) {
+                        const double f2 = fs[(r2 + k2) * kTileCells + c];
+                        if constexpr (JV) {
+                            const double v2 = vs[(r2 + k2) * kTileCells + c];
+#pragma unroll
+                            for (int b = 0; b < KC; ++b) phi[k2][b] = fma(v2, hf[b], fma(f2, hv[b], phi[k2][b]));
+                        } else {
+#pragma unroll
+                            for (int b = 0; b < KC; ++b) phi[k2][b] = fma(f2, hf[b], phi[k2][b]);
+                        }
+                    }
+#pragma unroll
+                    for (int b = 0; b < KC; ++b) hf[b] = hv[b] = 0.0;
+                };
                 for (int eb = e0; eb < e1; eb += 32) {
                     const int n = min(32, e1 - eb);
                     uint32_t my_q23 = 0;
@@ -115,32 +133,17 @@ __device__ __forceinline__ void tile_q1(const DevOp& op, int q1, const double* _
                         const double g = __shfl_sync(0xffffffffu, my_g, j);
                         const int q2 = (int)(q23 & 0xffffu), r3 = (int)(q23 >> 16) * K + k3b;
                         if (q2 != cur) {
-                            if (cur >= 0) {
-                                const int r2 = cur * K;
-#pragma unroll
-                                for (int k2 = 0; k2 < K; ++k2) {
-                                    const double f2 = fs[(r2 + k2) * kTileCells + c];
-#pragma unroll
-                                    for (int b = 0; b < KC; ++b) phi[k2][b] = fma(f2, h[b], phi[k2][b]);
-                                }
-#pragma unroll
-                                for (int b = 0; b < KC; ++b) h[b] = 0.0;
-                            }
+                            if (cur >= 0) flush();
                             cur = q2;
                         }
 #pragma unroll
-                        for (int b = 0; b < KC; ++b) h[b] = fma(g, fs[(r3 + b) * kTileCells + c], h[b]);
+                        for (int b = 0; b < KC; ++b) {
+                            hf[b] = fma(g, fs[(r3 + b) * kTileCells + c], hf[b]);
+                            if constexpr (JV) hv[b] = fma(g, vs[(r3 + b) * kTileCells + c], hv[b]);
+                        }
                     }
                 }
-                if (cur >= 0) {
-                    const int r2 = cur * K;
-#pragma unroll
-                    for (int k2 = 0; k2 < K; ++k2) {
-                        const double f2 = fs[(r2 + k2) * kTileCells + c];
-#pragma unroll
-                        for (int b = 0; b < KC; ++b) phi[k2][b] = fma(f2, h[b], phi[k2][b]);
-                    }
-                }
+                if (cur >= 0) flush();
                 phi_done = true;
             }
         }

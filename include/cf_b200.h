@@ -276,7 +276,9 @@ int cf_rk2_steps_tiled(cf_plan* plan, double* f_tiled, int64_t b, double dt, int
  * entry.  Preconditioning is on the right with block-Jacobi over the angular modes: `precond` is
  * NULL (none), N_Q blocks of K x K shared by all cells (precond_per_cell = 0), or B sets of N_Q
  * blocks (precond_per_cell = 1); block q maps rows q*K..q*K+K-1 (row-major, [out][in]).  A cell
- * is done when |b - A x| <= tol |b| in FP64.  iters_out[B] (host, may be NULL) receives the
+ * is done when |b - A x| <= tol |b| in FP64.  J(f) u runs on the q2 <-> q3 folded operator when
+ * the operator folds (the same bilinear form on half the entries), else on the plain one.
+ * iters_out[B] (host, may be NULL) receives the
  * Arnoldi steps each cell used, relres_out[B] (host, may be NULL) the final relative residuals.
  * Returns CF_ETIMEOUT if some cell is still above tol after max_iters steps.
  * ------------------------------------------------------------------------------------------ */
