@@ -287,8 +287,9 @@ static LaunchResult launch_for_k(const LaunchArgs& a) {
         return launch_for_k<K>(b);
     }
     if constexpr (K % 2 == 0 && K <= 8) {
-        if (a.path == PATH_AUTO && a.tile_first && !jv && !a.exact) {
-            const LaunchResult r = launch_tile<K, tile_W(K, false), false, false>(a);
+        if (a.path == PATH_AUTO && a.tile_first && !a.exact) {
+            const LaunchResult r = jv ? launch_tile<K, tile_W(K, true), false, true>(a)
+                                      : launch_tile<K, tile_W(K, false), false, false>(a);
             if (r.status != -1) return r;
         }
     }

@@ -472,10 +472,11 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
              cudaStream_t st, const float* fT32 = nullptr, bool bf16 = false, const StreamSync* ss = nullptr,
              const double* f_cm = nullptr, double* q_cm = nullptr) {
     const int64_t nt = n_tiles_for(B);
-    // The folded operator has about half the COO entries per slice of the plain one, so its Phi step
-    // is light next to the K^3 step; there the tile kernel (16 warps per SM) runs ahead of the pair
-    // kernel (8 warps per SM): 2.41 M against 1.86 M cells/s at L=10, K=8 on B200.
-    const bool tile_first = p->parent != nullptr && what == cf::OP_AF && !exact;
+    // The folded operator has about half the COO entries per slice of the plain one, and its tile
+    // routine groups them by q2, so its Phi step is light next to the K^3 step; there the tile kernel
+    // (16 warps per SM) runs ahead of the pair kernel (8 warps per SM): Q 2.50 M against 1.92 M
+    // cells/s at L=10, K=8 on B200, J.v 0.59 against 0.75 ms for 2048 cells at L=8, K=8.
+    const bool tile_first = p->parent != nullptr && (what == cf::OP_AF || what == cf::OP_JV) && !exact;
     cf::LaunchArgs a{p->op(), fT, vT, QT, nt, B, st, what, exact, p->path, p->d_bin_begin, p->d_bin_q1,
                      counter_for(p, st), p->n_sms, p->max_smem, p->d_pbin_begin, p->d_pbin_item, p->d_pitems,
                      fT32 != nullptr, fT32, tile_first, bf16};
