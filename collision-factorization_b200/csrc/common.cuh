@@ -34,8 +34,9 @@ struct DevOp {
     const double* RT;  // K = 8 only: R_t transposed to [k1][kk = K k2 + k3] (A operands of the MMA kernel)
     const unsigned short* RTbf;  // K = 8 only: R_t^T split in BF16, [t][hi, lo][k1][kk] (BF16-split form)
     const int* item_q1;
-    int grouped;  // 1: each slice's entries are sorted by q2 (the folded operator), so the fast tile
-                  // routine sums G f(q3) over each run of equal q2 before the outer product with f(q2)
+    int grouped;  // each slice's entries sorted by q2 (the folded operator); bit 0: the fast Q tile
+                  // routine sums G f(q3) over each run of equal q2 before one outer product with
+                  // f(q2), bit 1: the fast J.v tile routine does the same with f and v
     int n_items;  // number of q1 with at least one slice
     int n_q;
     int k;

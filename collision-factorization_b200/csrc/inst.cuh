@@ -98,8 +98,9 @@ static LaunchResult launch_tile(const LaunchArgs& a) {
     return {e == cudaSuccess ? 0 : 5, 1, e, PATH_TILE};
 }
 
-// Streamed tile kernel over the whole batch (host entry points): every half-tile split into 4 q1
-// bins, cell-major f and Q, chunk flags in a.ss.  Status -1 when the tile does not fit.
+// Tile kernel on cell-major f and Q (a.f_cm, a.q_cm).  Streamed (a.ss->ready set): every half-tile
+// split into 4 q1 bins, chunk flags in a.ss.  Resident (a.ss->ready null): the tile kernel's own
+// schedule, no waits.  Status -1 when the tile does not fit.
 template <int K, int W>
 static LaunchResult launch_tile_stream(const LaunchArgs& a) {
     const int M = a.op.n_q * K;
@@ -116,9 +117,15 @@ static LaunchResult launch_tile_stream(const LaunchArgs& a) {
     sc.bin_begin = a.bin_begin;
     sc.bin_q1 = a.bin_q1;
     sc.n_ht = (int)n_ht;
-    sc.n_whole = 0;
-    sc.split = 4;
-    const int64_t n_units = n_ht * sc.split;
+    if (a.ss->ready) {
+        sc.n_whole = 0;
+        sc.split = 4;
+    } else {
+        const int64_t n_whole = n_ht > ctas ? n_ht - ctas : 0;
+        sc.n_whole = (int)n_whole;
+        sc.split = (n_ht - n_whole) * 4 >= ctas ? 4 : 16;
+    }
+    const int64_t n_units = sc.n_whole + (n_ht - sc.n_whole) * sc.split;
     if (n_units > INT32_MAX) return {2, 0, cudaSuccess, PATH_TILE};
     sc.n_units = (int)n_units;
     sc.counter = a.counter;

@@ -127,7 +127,7 @@ struct cf_plan {
     int n_pairs = 0, n_pair_items = 0;
     int n_sms = 0;
     size_t max_smem = 0;
-    bool grouped = false;  // entries of each slice sorted by (q2, q3): the folded plan
+    int grouped = 0;  // folded plan, entries of each slice sorted by (q2, q3): bit 0 Q, bit 1 J.v (DevOp::grouped)
     int path = 0;  // cf::Path requested: 0 automatic, 1 gather, 2 tile, 3 pair, 4 pair (R via L1), 5 split pair
     int last_path = 0;  // family of the last angular-first / J.v launch (of this plan or its folded twin)
     cf_plan* parent = nullptr;  // for a folded twin: the plan it folds
@@ -168,7 +168,7 @@ struct cf_plan {
         o.RT = d_RT;
         o.RTbf = d_RTbf;
         o.item_q1 = d_item_q1;
-        o.grouped = grouped ? 1 : 0;
+        o.grouped = grouped;
         o.n_items = n_items;
         o.n_q = n_q;
         o.k = k;
@@ -542,7 +542,10 @@ int launch_unpack(const cf_plan* p, const double* src, double* dst, int64_t B, c
 }
 
 // Q_dev (cell-major) += op(f_dev[, v_dev]) using the tiled workspace ws (>= 2 or 3 tiled buffers).
+// The forms that run on the tile kernel skip the layout passes: the kernel reads f and updates Q in
+// the caller's cell-major arrays (the same per-row operations, so the same bits).
 int get_sym(cf_plan* p, cf_plan** out);
+bool streamable(const cf_plan* p, const cf_plan* target, int what, bool exact, int f32);
 
 int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_dev, const double* v_dev,
                int64_t B, void* ws, size_t ws_bytes, cudaStream_t st, bool sym = false, int f32 = 0) {
@@ -557,6 +560,15 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
     double* QT = (double*)((char*)ws + tb);
     double* vT = what == 2 ? (double*)((char*)ws + 2 * tb) : nullptr;
     float* fT32 = f32 ? reinterpret_cast<float*>(fT) : nullptr;  // FP32 tiles use half of the f slot
+    if (what == 0) {
+        cf_plan* target = p;
+        if (sym) CF_TRY(get_sym(p, &target));
+        if (streamable(p, target, what, exact, f32)) {
+            const StreamSync resident{nullptr, nullptr, nullptr, nullptr, nullptr, 0, 1, 0};
+            return dispatch(target, 0, false, nullptr, nullptr, nullptr, B, st, nullptr, false, &resident, f_dev,
+                            q_dev);
+        }
+    }
     if (f32)
         CF_TRY(launch_pack32(p, f_dev, fT32, B, st));
     else
@@ -761,7 +773,12 @@ int get_sym(cf_plan* p, cf_plan** out) {
     if (st != CF_OK) return st;
     s->path = p->path;
     s->parent = p;
-    s->grouped = true;
+    // Grouping the Phi step by q2 pays where it was measured to (B200, folded hard-sphere operators):
+    // for Q at K = 8 with long slices (L = 10: 12.8 entries per slice, 1.654 against 1.699 ms for
+    // 4096 cells), not with short ones (L = 8: 9.8 per slice, 0.483 against 0.471 ms) or at K = 4
+    // (0.373 against 0.324 ms at L = 8); for J.v from K = 6 on (L = 8, K = 8: 0.619 against 0.655 ms).
+    const double per_slice = s->n_slices > 0 ? (double)s->n_g / (double)s->n_slices : 0.0;
+    s->grouped = ((s->k == 8 && per_slice >= 12.0) ? 1 : 0) | (s->k >= 6 ? 2 : 0);
     s->h_labels.clear();  // the folded plan is never folded again
     p->sym = s;
     p->fold_status = 0;

@@ -94,7 +94,7 @@ __device__ __forceinline__ void tile_q1(const DevOp& op, int q1, const double* _
 
         bool phi_done = false;
         if constexpr (!EXACT) {
-            if (op.grouped) {
+            if (op.grouped & (JV ? 2 : 1)) {
                 // entries sorted by q2: over a run of equal q2, hf = sum G f(q3) (and, for J.v,
                 // hv = sum G v(q3)); then Phi += f(q2) (x) hf (J.v: v(q2) (x) hf + f(q2) (x) hv) once
                 // per run -- the q2 loads and the K x K/2 FMAs once per run instead of once per
@@ -333,8 +333,9 @@ constexpr size_t tile_smem_bytes(int M, int W, bool jv) {
 }
 
 // ------------------------------------------------------------------------------------------
-// Streamed tile kernel (host entry points): one launch over the whole batch while the batch is
-// still being copied in and the results are being copied out.
+// Tile kernel on the caller's cell-major f and Q.  Resident (ss.ready == null): the device entry
+// points, no layout passes, the tile kernel's schedule.  Streamed (host entry points): one launch
+// over the whole batch while the batch is still being copied in and the results copied out.
 //
 // f and Q stay in the caller's cell-major layout [N_Q x K x B] in device memory.  The host cuts
 // the batch into chunks of whole half-tiles and queues, on a copy stream, each chunk's f and Q
@@ -378,12 +379,19 @@ __global__ void __launch_bounds__(W * 32, 1)
         __syncthreads();
         const int u = s_unit;
         if (u >= sc.n_units) break;
-        const int ht = u / sc.split;
-        const int bin = bin_base(sc.split) + u % sc.split;
+        int ht, bin;
+        if (u < sc.n_whole) {
+            ht = u;
+            bin = 0;
+        } else {
+            const int v = u - sc.n_whole;
+            ht = sc.n_whole + v / sc.split;
+            bin = bin_base(sc.split) + v % sc.split;
+        }
         const int chunk = ht / ss.ht_per_chunk;
         const long long cell0 = (long long)ht * kTileCells;
         if (ht != staged) {
-            if (tid == 0) {
+            if (tid == 0 && ss.ready) {
                 const long long t0 = clock64();
                 while (ld_acquire(ss.ready + chunk) != ss.epoch) {
                     if (*reinterpret_cast<volatile int*>(ss.abort) == ss.epoch) break;
@@ -423,11 +431,12 @@ __global__ void __launch_bounds__(W * 32, 1)
             if (i >= nb) break;
             tile_q1<K, false, false, true>(op, sc.bin_q1[b0 + i], fs, nullptr, rb, qc, lane, live);
         }
-        __threadfence();
+        if (ss.done) __threadfence();
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && ss.done) {
             const int c_ht = min(ss.ht_per_chunk, sc.n_ht - chunk * ss.ht_per_chunk);
-            if (atomicAdd(ss.done + chunk, 1) == c_ht * sc.split - 1) {
+            const int c_units = c_ht * sc.split;  // the streamed schedule splits every half-tile
+            if (atomicAdd(ss.done + chunk, 1) == c_units - 1) {
                 __threadfence_system();
                 *reinterpret_cast<volatile int*>(ss.host_done + chunk) = ss.epoch;
             }
