@@ -20,6 +20,7 @@
 
 // Sets the message cf_last_error() returns (plan.cu; not part of the C ABI).
 void cf_set_last_error(const char* msg);
+bool cf_plan_folded_built(cf_plan* plan);
 
 namespace {
 
@@ -62,6 +63,13 @@ extern "C" int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f
     cf_plan_info info;
     int st = cf_plan_get_info(plan, &info);
     if (st != CF_OK) return st;
+    // The folded forms run on the plan's folded twin, which its first use builds, with allocations.
+    const bool folded = form == CF_FORM_AF_SYM || form == CF_FORM_AF_SYM_F32 || form == CF_FORM_AF_SYM_BF16;
+    if (folded && !cf_plan_folded_built(plan)) {
+        cf_set_last_error("cf_q_device_noalloc: this plan's folded operator is not built yet, and building it "
+                          "allocates; make one cf_q_device or cf_q_tiled call in a folded form first");
+        return CF_EINVAL;
+    }
     size_t need = 0;
     st = cf_plan_workspace_size(plan, b, 0, &need);
     if (st != CF_OK) return st;

@@ -1364,6 +1364,12 @@ __attribute__((visibility("hidden"))) int cf_plan_folded(cf_plan* plan, cf_plan*
     return get_sym(plan, folded);
 }
 
+// Whether the folded twin exists already (building it allocates device memory).
+__attribute__((visibility("hidden"))) bool cf_plan_folded_built(cf_plan* plan) {
+    std::lock_guard<std::mutex> lk(plan->sym_mu);
+    return plan->sym != nullptr;
+}
+
 extern "C" {
 
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path) {

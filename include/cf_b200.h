@@ -189,7 +189,9 @@ int cf_fp64_fma_peak(int32_t device, double* tflops);
  * cells at N_Q*K = 968).  The first call on a device looks up the array's device address with
  * that device current; make that first call before any stream capture.  All calls share the one
  * array, so calls that overlap on the GPU (other streams, other host threads) race on it.  The
- * plan itself is created beforehand with cf_plan_create, which does allocate. */
+ * plan itself is created beforehand with cf_plan_create, which does allocate, and so is its folded
+ * operator: the folded forms (CF_FORM_AF_SYM and its FP32 / BF16 variants) return CF_EINVAL until
+ * one cf_q_device or cf_q_tiled call in a folded form has built it. */
 #define CF_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form,
                         void* stream);

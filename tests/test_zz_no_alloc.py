@@ -80,3 +80,39 @@ def test_noalloc_matches_cf_q_device_on_two_calls(cuda_available):
     torch.cuda.synchronize()
     assert float(out_big.abs().max()) == 0.0
     op.close()
+
+
+def test_noalloc_folded_form_needs_its_operator_built_first(cuda_available):
+    """The folded form runs on the plan's folded operator, whose first use builds it with
+    allocations; the allocation-free call refuses it until then, and afterwards matches cf_q_device
+    on two calls in a row, allocating nothing."""
+    import torch
+
+    import cf_b200
+    from cf_b200 import _lib, geometry, workloads
+
+    L, K, B = 8, 8, 700
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = np.load(GOLDEN / "R_hs_k7_l8_pad20.npy")
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+    f = torch.from_numpy(workloads.maxwellian_cells(K, L, B, seed=78)).cuda()
+    lib = _lib.load()
+    stream = torch.cuda.current_stream()
+    out = torch.zeros_like(f)
+    st = lib.cf_q_device_noalloc(op._h, out.data_ptr(), f.data_ptr(), B, _lib.FORM_AF_SYM, stream.cuda_stream)
+    assert st == 1 and b"folded operator is not built" in lib.cf_last_error()
+    ref = op.q(f, form="af_sym").cpu().numpy()  # builds the folded operator
+    free_after_first = None
+    for call in range(2):
+        out = torch.zeros_like(f)
+        torch.cuda.synchronize()
+        st = lib.cf_q_device_noalloc(op._h, out.data_ptr(), f.data_ptr(), B, _lib.FORM_AF_SYM, stream.cuda_stream)
+        assert st == 0, lib.cf_last_error().decode()
+        torch.cuda.synchronize()
+        assert per_cell_err(out.cpu().numpy(), ref) <= TOL_FP64, f"call {call}"
+        free_now = torch.cuda.mem_get_info()[0]
+        if call == 0:
+            free_after_first = free_now
+        else:
+            assert free_now == free_after_first
+    op.close()
