@@ -54,6 +54,9 @@ NCU_TRAFFIC = {
                                             "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
                                             "profiles/af_tile_kernel_folded_hs_l10_k8_b4096.md"),
     ("hs_l10_k8_b4096", "pair", "af"): (65.9e6 + 1.8e6, "ncu, profiles/af_pair_kernel_hs_l10_k8_b4096.md"),
+    ("hs_l10_k8_b4096", "tile_cell_major", "af_sym"): (64.777728e6 + 2.003456e6,
+                                                       "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                                       "profiles/af_tile_stream_kernel_folded_hs_l10_k8_b4096.md"),
 }
 
 
@@ -73,6 +76,8 @@ def parse_args(argv=None):
                     help="form launched by --profile")
     ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split", "tile_mma"],
                     help="kernel family of the angular-first contraction")
+    ap.add_argument("--entry", choices=("tiled", "device"), default="tiled",
+                    help="--profile: launch the tiled kernel (cf_q_tiled) or the device entry point (cf_q_device)")
     ap.add_argument("--profile", action="store_true",
                     help="only build the workload and launch the contraction (steps+1 times); for ncu captures")
     return ap.parse_args(argv)
@@ -343,6 +348,14 @@ def run_ours(args):
     err_sym = float((num / den).max())
     sym_ms = timed(lambda: step("af_sym"), args.steps)
     sym_kern_ms = timed(lambda: kernel_only("af_sym"), max(2, args.steps // 2))
+    # the folded form's device step is one launch of the tile kernel on the cell-major arrays (no
+    # layout passes) when it runs on the tile kernel: then that launch is the roofline kernel
+    n0 = _lib.launch_count()
+    op.q(f, out=Q, form="af_sym", workspace=ws)
+    torch.cuda.synchronize(dev)
+    sym_single = _lib.launch_count() - n0 == 1 and _lib.PATH_NAMES[op.info()["last_path"]] == "tile"
+    if sym_single:
+        sym_kern_ms = timed(lambda: op.q(f, out=Q, form="af_sym", workspace=ws), max(2, args.steps // 2))
     path_ms, sym_path_ms = {}, {}
     for path in ("tile_mma", "pair_split", "pair", "pair_l1", "tile", "gather"):
         try:
@@ -393,10 +406,14 @@ def run_ours(args):
     kernel_only(chosen)
     torch.cuda.synchronize(dev)
     last_path = _lib.PATH_NAMES[op.info()["last_path"]]
+    if chosen == "af_sym" and sym_single:
+        last_path = "tile_cell_major"
     traffic = NCU_TRAFFIC.get((args.workload, last_path, chosen))
     kern_name = {"pair": "af_pair_kernel (persistent, tile-resident, mirrored row pairs)",
                  "pair_split": "af_pair_kernel, split variant (both mirrored rows per lane, k3 halves)",
                  "pair_l1": "af_pair_kernel (R_t through L1)", "tile": "af_tile_kernel (persistent, tile-resident)",
+                 "tile_cell_major": "af_tile_stream_kernel, resident (the tile kernel on the cell-major arrays, "
+                                    "no layout passes; the whole device step)",
                  "gather": "af_kernel (gathers through L1/L2)",
                  "tile_mma": "af_mma_kernel (tile-resident, K^3 step on the FP64 MMA)"}.get(last_path, "?")
     kern_s = sum(kern_list) / len(kern_list) / 1e3
@@ -690,10 +707,14 @@ def run_profile(args):
     QT = torch.zeros_like(fT)
     sh = int(torch.cuda.current_stream().cuda_stream)
     _lib.check(lib.cf_pack_cells(op._h, int(fT.data_ptr()), int(f.data_ptr()), B, sh))
+    Q = torch.zeros_like(f)
     for _ in range(args.steps + 1):
-        _lib.check(lib.cf_q_tiled(op._h, int(QT.data_ptr()), int(fT.data_ptr()), B, _lib.FORMS[args.form], sh))
+        if args.entry == "device":
+            op.q(f, out=Q, form=args.form)
+        else:
+            _lib.check(lib.cf_q_tiled(op._h, int(QT.data_ptr()), int(fT.data_ptr()), B, _lib.FORMS[args.form], sh))
     torch.cuda.synchronize()
-    print(json.dumps({"profile": args.workload, "launches": args.steps + 1, "B": B}))
+    print(json.dumps({"profile": args.workload, "entry": args.entry, "launches": args.steps + 1, "B": B}))
 
 
 def run_implicit(args):
