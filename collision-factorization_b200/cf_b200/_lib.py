@@ -34,6 +34,7 @@ EXPORTS = [
     "cf_plan_create", "cf_plan_destroy", "cf_plan_get_info", "cf_plan_workspace_size",
     "cf_q_device", "cf_q_device_ws", "cf_jv_device", "cf_q_device_noalloc", "cf_plan_stream_selftest",
     "cf_ragged_create", "cf_ragged_destroy", "cf_ragged_q", "cf_ragged_graph_launch", "cf_ragged_q_resident",
+    "cf_ragged_q_host",
     "cf_ragged_info", "cf_rk2_workspace_size", "cf_rk2_steps_tiled", "cf_rtensor_sumfac",
     "cf_gmres_workspace_size", "cf_gmres_solve_tiled",
     "cf_mlp_create", "cf_mlp_destroy", "cf_mlp_num_params", "cf_mlp_copy", "cf_mlp_forward", "cf_mlp_backward",
@@ -116,6 +117,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_ragged_q.argtypes = [V, V, V, V]
     lib.cf_ragged_graph_launch.argtypes = [V, V, V, V]
     lib.cf_ragged_q_resident.argtypes = [V, V]
+    lib.cf_ragged_q_host.argtypes = [V, V, V]
     lib.cf_rk2_workspace_size.argtypes = [V, _I64, C.POINTER(C.c_size_t)]
     lib.cf_rtensor_sumfac.argtypes = [_D, C.POINTER(SumfacInputs), _I32, C.POINTER(C.c_double)]
     lib.cf_rk2_steps_tiled.argtypes = [V, V, _I64, C.c_double, _I32, _I32, V, C.c_size_t, V]

@@ -105,6 +105,31 @@ class RaggedBatch:
         s = int((stream or torch.cuda.current_stream()).cuda_stream)
         _lib.check(_lib.load().cf_ragged_q_resident(self._h, s))
 
+    def q_host(self, fs, qs):
+        """qs[b] += Q(fs[b]) for every bucket, with host arrays (numpy arrays or CPU tensors of shape
+        (cells, K, N_Q), C-contiguous float64; pinned memory makes the copies asynchronous).  With the
+        tile routine and every bucket fused, one launch runs while the buckets are copied in and out
+        (cf_ragged_q_host)."""
+        import numpy as np
+
+        n = len(self.ops)
+        if len(fs) != n or len(qs) != n:
+            raise _lib.CFError(_lib.CF_EINVAL, "one f and one q array per bucket")
+        fps, qps = [], []
+        for op, f, q, c in zip(self.ops, fs, qs, self.cells):
+            shape = (c, op.K, op.N_Q)
+            for a in (f, q):
+                arr = a.numpy() if hasattr(a, "numpy") else a
+                if not isinstance(arr, np.ndarray) or arr.dtype != np.float64 or tuple(arr.shape) != shape \
+                        or not arr.flags.c_contiguous:
+                    raise _lib.CFError(_lib.CF_ESHAPE, f"bucket arrays must be C-contiguous {shape} float64 host arrays")
+            fps.append((f.numpy() if hasattr(f, "numpy") else f).ctypes.data)
+            qps.append((q.numpy() if hasattr(q, "numpy") else q).ctypes.data)
+        fp = (C.c_void_p * n)(*fps)
+        qp = (C.c_void_p * n)(*qps)
+        _lib.check(_lib.load().cf_ragged_q_host(self._h, qp, fp))
+        return qs
+
     def q_graph(self, fs, qs, stream=None):
         """The same step replayed from a CUDA graph (recorded on first use for these buffers)."""
         import torch

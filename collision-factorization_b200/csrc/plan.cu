@@ -1364,6 +1364,9 @@ __attribute__((visibility("hidden"))) int cf_plan_folded(cf_plan* plan, cf_plan*
     return get_sym(plan, folded);
 }
 
+// Kernels launched by the other translation units (ragged.cu), for cf_launch_count().
+__attribute__((visibility("hidden"))) void cf_add_launches(int64_t n) { g_launches += n; }
+
 // Whether the folded twin exists already (building it allocates device memory).
 __attribute__((visibility("hidden"))) bool cf_plan_folded_built(cf_plan* plan) {
     std::lock_guard<std::mutex> lk(plan->sym_mu);

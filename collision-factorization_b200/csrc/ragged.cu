@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "../../include/cf_b200.h"
@@ -32,6 +33,7 @@ int cf_plan_internal_view(const cf_plan* plan, DevOp* op, const int** pbin_begin
                           const int2** pitems, const int** bin_begin, const int** bin_q1, int* n_sms,
                           size_t* max_smem);
 int cf_plan_folded(cf_plan* plan, cf_plan** folded);
+void cf_add_launches(int64_t n);
 
 namespace {
 
@@ -51,6 +53,12 @@ struct Bucket {
     const double* fT;
     double* QT;
     int K, M;
+    // host entry point (cf_ragged_q_host): the bucket's cell-major device copies and its chunks
+    const double* f_cm;
+    double* q_cm;
+    long long cells;
+    int chunk_base;  // index of the bucket's first upload chunk
+    int hpc;         // half-tiles per chunk
 };
 
 struct Unit {
@@ -136,6 +144,109 @@ __global__ void __launch_bounds__((TILE ? kTW : kRW) * 32, 1)
     }
 }
 
+// Words of the streamed launch of cf_ragged_q_host (per upload chunk; see af_ragged_stream_kernel).
+struct RaggedSync {
+    const int* ready;        // [n_chunks] device; == epoch once the chunk's f and Q are in
+    int* done;               // [n_chunks] device; units finished (zeroed before the launch)
+    const int* chunk_units;  // [n_chunks] device; units of the work table that read the chunk
+    int* host_done;          // [n_chunks] mapped host memory; set to epoch once the chunk is final
+    int* err;                // mapped host memory; set to 1 if a wait gave up
+    int* abort;              // device; == epoch once a wait gave up
+    int epoch;
+    long long wait_cycles;
+};
+
+// The tile routine of af_ragged_kernel over the buckets' cell-major arrays while they are being
+// copied in and out (cf_ragged_q_host).  Its work table holds the buckets' half-tiles heaviest
+// bucket first, each cut into 4 q1 bins, and the host uploads every bucket in chunks of whole
+// half-tiles in that order, each chunk followed by a 4-byte copy that sets its ready word.  A CTA waits (bounded by wait_cycles of the SM clock; past that it records err and
+// abort, and later waits return at once) for the chunk of its unit, stages the half-tile from the
+// cell-major rows and contracts its rows with the same per-row code as af_ragged_kernel, reading Q_in
+// at each row's start and writing Q in place, so a bucket's result equals the resident step's bit
+// for bit.  The CTA that finishes a chunk's last unit fences at system scope and writes the epoch
+// into the chunk's mapped host word; the host then queues that chunk's download.
+__global__ void __launch_bounds__(kTW * 32, 1)
+    af_ragged_stream_kernel(const Bucket* __restrict__ buckets, const Unit* __restrict__ units, int n_units,
+                            int* __restrict__ counter, RaggedSync rs) {
+    constexpr int W = kTW;
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_unit, s_next;
+    __shared__ Bucket s_bk;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    double* fs = smem + W * kRBufTile;
+    double* rb = smem + warp * kRBufTile;
+    int staged_b = -1, staged_ht = -1;
+    for (;;) {
+        if (tid == 0) {
+            const int uu = atomicAdd(counter, 1);
+            s_unit = uu;
+            if (uu < n_units) s_bk = buckets[units[uu].bucket];
+        }
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= n_units) break;
+        const Unit un = units[u];
+        const Bucket& bk = s_bk;
+        const int M = bk.M, NQ = bk.op.n_q, K = bk.K;
+        const int chunk = bk.chunk_base + un.ht / bk.hpc;
+        const long long cell0 = (long long)un.ht * cf::kTileCells;
+        if (un.bucket != staged_b || un.ht != staged_ht) {
+            if (tid == 0) {
+                const long long t0 = clock64();
+                while (cf::ld_acquire(rs.ready + chunk) != rs.epoch) {
+                    if (*reinterpret_cast<volatile int*>(rs.abort) == rs.epoch) break;
+                    if (clock64() - t0 > rs.wait_cycles) {
+                        *reinterpret_cast<volatile int*>(rs.abort) = rs.epoch;
+                        *reinterpret_cast<volatile int*>(rs.err) = 1;
+                        break;
+                    }
+                    __nanosleep(256);
+                }
+            }
+            __syncthreads();
+            // element j = q + N_Q k of cell c goes to row q K + k of the tile
+            for (int i = tid; i < M * cf::kTileCells; i += W * 32) {
+                const int c = i & 15, j = i >> 4;
+                const int r = (j % NQ) * K + j / NQ;
+                if (cell0 + c < bk.cells)
+                    cf::cp_async8(fs + r * cf::kTileCells + c, bk.f_cm + (size_t)(cell0 + c) * M + j);
+                else
+                    fs[r * cf::kTileCells + c] = 0.0;
+            }
+            cf::cp_async_commit();
+            cf::cp_async_wait_all();
+            staged_b = un.bucket;
+            staged_ht = un.ht;
+        }
+        if (tid == 0) s_next = 0;
+        __syncthreads();
+        const int b0 = bk.bin_begin[un.bin], nb = bk.bin_begin[un.bin + 1] - b0;
+        const long long cell = cell0 + (lane & 15);
+        const bool live = cell < bk.cells;
+        double* qc = bk.q_cm + (size_t)(live ? cell : 0) * M;
+        for (;;) {
+            int i = 0;
+            if (lane == 0) i = atomicAdd(&s_next, 1);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= nb) break;
+            const int q1 = bk.bin_q1[b0 + i];
+            switch (K) {
+                case 2: cf::tile_q1<2, false, false, true>(bk.op, q1, fs, nullptr, rb, qc, lane, live); break;
+                case 4: cf::tile_q1<4, false, false, true>(bk.op, q1, fs, nullptr, rb, qc, lane, live); break;
+                case 6: cf::tile_q1<6, false, false, true>(bk.op, q1, fs, nullptr, rb, qc, lane, live); break;
+                case 8: cf::tile_q1<8, false, false, true>(bk.op, q1, fs, nullptr, rb, qc, lane, live); break;
+                default: break;
+            }
+        }
+        __threadfence();
+        __syncthreads();
+        if (tid == 0 && atomicAdd(rs.done + chunk, 1) == rs.chunk_units[chunk] - 1) {
+            __threadfence_system();
+            *reinterpret_cast<volatile int*>(rs.host_done + chunk) = rs.epoch;
+        }
+    }
+}
+
 #define RCHECK(expr)                                                                                    \
     do {                                                                                                \
         cudaError_t e_ = (expr);                                                                        \
@@ -169,15 +280,37 @@ struct cf_ragged {
     size_t smem = 0;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
+    int64_t step_kernels = 0;  // layout passes and fused launch of the last step enqueued
     std::vector<const double*> graph_f;
     std::vector<double*> graph_q;
     cudaStream_t graph_stream = nullptr;
+    // host entry point (cf_ragged_q_host), set up on its first call: cell-major device copies of
+    // every bucket's f and Q; for the streamed launch, the upload chunks and their words
+    std::vector<Unit> h_units;
+    std::vector<Bucket> h_buckets;
+    bool host_ready = false, host_stream = false;
+    double* d_io = nullptr;
+    std::vector<size_t> io_off;
+    std::vector<int> chunk_bucket, chunk_ht0, chunk_ht1;  // upload order = the work table's order
+    Unit* d_xunits = nullptr;  // the streamed launch's work table: every half-tile in 4 q1 bins
+    int n_xunits = 0;
+    cudaStream_t xs[3] = {};
+    int* d_xsync = nullptr;   // ready[kHostChunks], done[kHostChunks], chunk_units[kHostChunks], abort
+    int* h_xepoch = nullptr;  // pinned: the epoch values the ready copies read
+    int* h_xsync = nullptr;   // mapped: chunk completion words [kHostChunks], then the error word
+    int* h_xsync_dev = nullptr;
+    int xepoch = 0;
+    long long xwait = 0;
     std::mutex mu;
 };
 
 namespace {
 
 int64_t ntiles(int64_t B) { return (B + CF_TILE - 1) / CF_TILE; }
+
+constexpr int kHostChunks = 128;            // upload chunks of the streamed host call, at most
+constexpr int kTargetChunks = 24;           // upload chunks aimed at
+constexpr double kHostWaitSeconds = 5.0;     // a CTA gives up on a chunk's ready word after this
 
 void free_ragged(cf_ragged* r) {
     if (r->graph_exec) cudaGraphExecDestroy(r->graph_exec);
@@ -186,6 +319,13 @@ void free_ragged(cf_ragged* r) {
     cudaFree(r->d_units);
     cudaFree(r->d_counter);
     cudaFree(r->d_tiles);
+    cudaFree(r->d_io);
+    cudaFree(r->d_xunits);
+    cudaFree(r->d_xsync);
+    if (r->h_xepoch) cudaFreeHost(r->h_xepoch);
+    if (r->h_xsync) cudaFreeHost(r->h_xsync);
+    for (cudaStream_t& s : r->xs)
+        if (s) cudaStreamDestroy(s);
 }
 
 double* tiled_f(cf_ragged* r, int b) { return r->d_tiles + r->tile_off[b]; }
@@ -193,9 +333,11 @@ double* tiled_q(cf_ragged* r, int b) {
     return r->d_tiles + r->tile_off[b] + (size_t)ntiles(r->cells[b]) * CF_TILE * r->NQ[b] * r->K[b];
 }
 
-// the contraction on the handle's tiled buffers: the fused launch, then the separate buckets
-int enqueue_contract(cf_ragged* r, cudaStream_t s) {
+// the contraction on the handle's tiled buffers: the fused launch, then the separate buckets (whose
+// plans count their own kernels)
+int enqueue_contract(cf_ragged* r, cudaStream_t s, bool count = true) {
     if (r->n_units > 0) {
+        if (count) cf_add_launches(1);
         RCHECK(cudaMemsetAsync(r->d_counter, 0, sizeof(int), s));
         const unsigned grid = (unsigned)std::min(r->n_units, r->ctas);
         if (r->family == 1)
@@ -212,8 +354,13 @@ int enqueue_contract(cf_ragged* r, cudaStream_t s) {
     return CF_OK;
 }
 
-// pack every bucket, the contraction, unpack (q += Q(f) per bucket), all on stream s
-int enqueue_step(cf_ragged* r, double* const* q, const double* const* f, cudaStream_t s) {
+// pack every bucket, the contraction, unpack (q += Q(f) per bucket), all on stream s; count: add the
+// step's kernels to the launch counter now (false while recording a graph: each replay adds them)
+int enqueue_step(cf_ragged* r, double* const* q, const double* const* f, cudaStream_t s, bool count = true) {
+    int64_t nk = r->n_units > 0 ? 1 : 0;
+    for (int b = 0; b < r->n_buckets; ++b) nk += r->cells[b] > 0 ? 3 : 0;
+    r->step_kernels = nk;
+    if (count) cf_add_launches(nk - (r->n_units > 0 ? 1 : 0));
     for (int b = 0; b < r->n_buckets; ++b) {
         if (r->cells[b] == 0) continue;
         const int M = r->NQ[b] * r->K[b];
@@ -222,7 +369,7 @@ int enqueue_step(cf_ragged* r, double* const* q, const double* const* f, cudaStr
         cf::pack_tiles_kernel<double><<<grid, block, 0, s>>>(q[b], tiled_q(r, b), r->cells[b], r->NQ[b], r->K[b]);
     }
     RCHECK(cudaGetLastError());
-    const int st = enqueue_contract(r, s);
+    const int st = enqueue_contract(r, s, count);
     if (st != CF_OK) return st;
     for (int b = 0; b < r->n_buckets; ++b) {
         if (r->cells[b] == 0) continue;
@@ -231,6 +378,226 @@ int enqueue_step(cf_ragged* r, double* const* q, const double* const* f, cudaStr
         cf::unpack_tiles_kernel<<<grid, block, 0, s>>>(tiled_q(r, b), q[b], r->cells[b], r->NQ[b], r->K[b]);
     }
     RCHECK(cudaGetLastError());
+    return CF_OK;
+}
+
+// First host call: cell-major device copies of every bucket's f and Q; and, when every non-empty
+// bucket runs in the fused launch on the tile routine, the streamed launch's work table, its upload
+// chunks (whole half-tiles, about kTargetChunks, in the table's order) and their words.
+int host_setup(cf_ragged* r) {
+    if (r->host_ready) return CF_OK;
+    size_t total = 0;
+    r->io_off.clear();
+    for (int b = 0; b < r->n_buckets; ++b) {
+        r->io_off.push_back(total);
+        total += 2 * (size_t)r->cells[b] * r->NQ[b] * r->K[b];
+    }
+    RCHECK(cudaMalloc(&r->d_io, std::max<size_t>(total, 1) * sizeof(double)));
+    for (cudaStream_t& s : r->xs)
+        if (!s) RCHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    bool stream = r->family == 1 && r->n_units > 0;
+    for (int b = 0; b < r->n_buckets; ++b)
+        if (r->cells[b] > 0 && !r->fused[b]) stream = false;
+    if (stream) {
+        // buckets in the order the work table first names them; the table runs over each bucket's
+        // half-tiles in ascending order, so chunks uploaded in this order arrive in the order the
+        // CTAs take them
+        std::vector<int> order;
+        std::vector<char> seen(r->n_buckets, 0);
+        for (const Unit& u : r->h_units)
+            if (!seen[u.bucket]) {
+                seen[u.bucket] = 1;
+                order.push_back(u.bucket);
+            }
+        // about kTargetChunks chunks in all: every chunk costs three copy calls before the launch
+        int total_ht = 0;
+        for (int b : order) total_ht += (int)((r->cells[b] + 15) / 16);
+        int hpc = std::max(4, (total_ht + kTargetChunks - 1) / kTargetChunks);
+        for (;;) {
+            int n = 0;
+            for (int b : order) n += (int)(((r->cells[b] + 15) / 16 + hpc - 1) / hpc);
+            if (n <= kHostChunks) break;
+            hpc *= 2;
+        }
+        r->chunk_bucket.clear();
+        r->chunk_ht0.clear();
+        r->chunk_ht1.clear();
+        for (int b : order) {
+            const int n_ht = (int)((r->cells[b] + 15) / 16);
+            r->h_buckets[b].chunk_base = (int)r->chunk_bucket.size();
+            r->h_buckets[b].hpc = hpc;
+            for (int h = 0; h < n_ht; h += hpc) {
+                r->chunk_bucket.push_back(b);
+                r->chunk_ht0.push_back(h);
+                r->chunk_ht1.push_back(std::min(n_ht, h + hpc));
+            }
+        }
+        const int n_chunks = (int)r->chunk_bucket.size();
+        // the streamed work table: the buckets' half-tiles in the upload order, each in 4 q1 bins, so
+        // that the first chunk already feeds every SM and results complete (and go back) steadily
+        std::vector<Unit> xunits;
+        for (int b : order)
+            for (int h = 0; h < (int)((r->cells[b] + 15) / 16); ++h)
+                for (int k = 0; k < 4; ++k) xunits.push_back({b, h, 1 + k, 0});
+        r->n_xunits = (int)xunits.size();
+        RCHECK(cudaMalloc(&r->d_xunits, std::max<size_t>(xunits.size(), 1) * sizeof(Unit)));
+        RCHECK(cudaMemcpy(r->d_xunits, xunits.data(), xunits.size() * sizeof(Unit), cudaMemcpyHostToDevice));
+        std::vector<int> chunk_units(kHostChunks, 0);
+        for (const Unit& u : xunits)
+            chunk_units[r->h_buckets[u.bucket].chunk_base + u.ht / hpc]++;
+        RCHECK(cudaMalloc(&r->d_xsync, (3 * kHostChunks + 1) * sizeof(int)));
+        RCHECK(cudaMemset(r->d_xsync, 0, (3 * kHostChunks + 1) * sizeof(int)));
+        RCHECK(cudaMemcpy(r->d_xsync + 2 * kHostChunks, chunk_units.data(), kHostChunks * sizeof(int),
+                          cudaMemcpyHostToDevice));
+        RCHECK(cudaHostAlloc((void**)&r->h_xepoch, kHostChunks * sizeof(int), cudaHostAllocDefault));
+        RCHECK(cudaHostAlloc((void**)&r->h_xsync, (kHostChunks + 1) * sizeof(int), cudaHostAllocMapped));
+        RCHECK(cudaHostGetDevicePointer((void**)&r->h_xsync_dev, r->h_xsync, 0));
+        int khz = 0;
+        RCHECK(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, r->device));
+        r->xwait = (long long)((double)std::max(khz, 1000000) * 1e3 * kHostWaitSeconds);
+        RCHECK(cudaFuncSetAttribute(af_ragged_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)r->smem));
+        (void)n_chunks;
+    }
+    for (int b = 0; b < r->n_buckets; ++b) {
+        r->h_buckets[b].f_cm = r->d_io + r->io_off[b];
+        r->h_buckets[b].q_cm = r->d_io + r->io_off[b] + (size_t)r->cells[b] * r->NQ[b] * r->K[b];
+    }
+    RCHECK(cudaMemcpy(r->d_buckets, r->h_buckets.data(), r->n_buckets * sizeof(Bucket), cudaMemcpyHostToDevice));
+    r->host_stream = stream;
+    r->host_ready = true;
+    return CF_OK;
+}
+
+// q_host[b] += Q(f_host[b]) through the streamed launch (see af_ragged_stream_kernel).  Every upload
+// is queued before the launch, so the copies stay ahead of the kernel even where the copy and kernel
+// streams share a hardware queue; the host polls the chunks' completion words only while the kernel
+// runs, and the kernel's own waits are bounded, so the call always ends.
+int host_streamed(cf_ragged* r, double* const* q_host, const double* const* f_host) {
+    const int n_chunks = (int)r->chunk_bucket.size();
+    r->xepoch = r->xepoch % 0x3fffffff + 1;
+    const int epoch = r->xepoch;
+    volatile int* hs = r->h_xsync;
+    for (int c = 0; c < n_chunks; ++c) {
+        r->h_xepoch[c] = epoch;
+        hs[c] = 0;
+    }
+    hs[kHostChunks] = 0;
+    cudaStream_t s_in = r->xs[0], s_k = r->xs[1], s_out = r->xs[2];
+    int* d_ready = r->d_xsync;
+    int* d_done = r->d_xsync + kHostChunks;
+    const int* d_units = r->d_xsync + 2 * kHostChunks;
+    int* d_abort = r->d_xsync + 3 * kHostChunks;
+    RCHECK(cudaMemsetAsync(d_done, 0, n_chunks * sizeof(int), s_k));
+    auto span = [&](int c, size_t& off, size_t& nb) {
+        const int b = r->chunk_bucket[c];
+        const int64_t c0 = (int64_t)r->chunk_ht0[c] * 16, c1 = std::min<int64_t>(r->cells[b], (int64_t)r->chunk_ht1[c] * 16);
+        const size_t M = (size_t)r->NQ[b] * r->K[b];
+        off = (size_t)c0 * M;
+        nb = (size_t)(c1 - c0) * M * sizeof(double);
+    };
+    for (int c = 0; c < n_chunks; ++c) {
+        const int b = r->chunk_bucket[c];
+        size_t off, nb;
+        span(c, off, nb);
+        const Bucket& bk = r->h_buckets[b];
+        RCHECK(cudaMemcpyAsync(const_cast<double*>(bk.f_cm) + off, f_host[b] + off, nb, cudaMemcpyHostToDevice, s_in));
+        RCHECK(cudaMemcpyAsync(bk.q_cm + off, q_host[b] + off, nb, cudaMemcpyHostToDevice, s_in));
+        RCHECK(cudaMemcpyAsync(d_ready + c, r->h_xepoch + c, sizeof(int), cudaMemcpyHostToDevice, s_in));
+    }
+    RCHECK(cudaMemsetAsync(r->d_counter, 0, sizeof(int), s_k));
+    const RaggedSync rs{d_ready, d_done, d_units, r->h_xsync_dev, r->h_xsync_dev + kHostChunks, d_abort, epoch,
+                        r->xwait};
+    const unsigned grid = (unsigned)std::min(r->n_xunits, r->ctas);
+    af_ragged_stream_kernel<<<grid, kTW * 32, r->smem, s_k>>>(r->d_buckets, r->d_xunits, r->n_xunits, r->d_counter,
+                                                              rs);
+    cf_add_launches(1);
+    int st = CF_OK;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        cf_set_last_error(cudaGetErrorString(e));
+        st = CF_ECUDA;
+    }
+    std::vector<char> sent(n_chunks, 0);
+    int left = st == CF_OK ? n_chunks : 0;
+    while (left > 0) {
+        bool progress = false;
+        for (int c = 0; c < n_chunks; ++c) {
+            if (sent[c] || hs[c] != epoch) continue;
+            size_t off, nb;
+            span(c, off, nb);
+            const int b = r->chunk_bucket[c];
+            e = cudaMemcpyAsync(q_host[b] + off, r->h_buckets[b].q_cm + off, nb, cudaMemcpyDeviceToHost, s_out);
+            if (e != cudaSuccess) break;
+            sent[c] = 1;
+            --left;
+            progress = true;
+        }
+        if (e != cudaSuccess) {
+            cf_set_last_error(cudaGetErrorString(e));
+            st = CF_ECUDA;
+            break;
+        }
+        if (progress || left == 0) continue;
+        const cudaError_t q = cudaStreamQuery(s_k);
+        if (q == cudaErrorNotReady) {
+            std::this_thread::yield();
+            continue;
+        }
+        if (q != cudaSuccess) {
+            cf_set_last_error(cudaGetErrorString(q));
+            st = CF_ECUDA;
+            break;
+        }
+        // the kernel has ended: every chunk is final
+        for (int c = 0; c < n_chunks && st == CF_OK; ++c) {
+            if (sent[c]) continue;
+            size_t off, nb;
+            span(c, off, nb);
+            const int b = r->chunk_bucket[c];
+            e = cudaMemcpyAsync(q_host[b] + off, r->h_buckets[b].q_cm + off, nb, cudaMemcpyDeviceToHost, s_out);
+            if (e != cudaSuccess) {
+                cf_set_last_error(cudaGetErrorString(e));
+                st = CF_ECUDA;
+            }
+            sent[c] = 1;
+        }
+        left = 0;
+    }
+    for (cudaStream_t x : r->xs) {
+        const cudaError_t ex = cudaStreamSynchronize(x);
+        if (ex != cudaSuccess && st == CF_OK) {
+            cf_set_last_error(cudaGetErrorString(ex));
+            st = CF_ECUDA;
+        }
+    }
+    if (st == CF_OK && hs[kHostChunks] != 0) {
+        cf_set_last_error("cf_ragged_q_host: a chunk's data did not arrive within the wait limit");
+        st = CF_ETIMEOUT;
+    }
+    return st;
+}
+
+// Any other handle: every bucket up, the ordinary step on the device copies, every bucket back.
+int host_plain(cf_ragged* r, double* const* q_host, const double* const* f_host) {
+    cudaStream_t s = r->xs[0];
+    std::vector<double*> qd(r->n_buckets);
+    std::vector<const double*> fd(r->n_buckets);
+    for (int b = 0; b < r->n_buckets; ++b) {
+        fd[b] = r->h_buckets[b].f_cm;
+        qd[b] = r->h_buckets[b].q_cm;
+        const size_t nb = (size_t)r->cells[b] * r->NQ[b] * r->K[b] * sizeof(double);
+        if (nb == 0) continue;
+        RCHECK(cudaMemcpyAsync(const_cast<double*>(fd[b]), f_host[b], nb, cudaMemcpyHostToDevice, s));
+        RCHECK(cudaMemcpyAsync(qd[b], q_host[b], nb, cudaMemcpyHostToDevice, s));
+    }
+    const int st = enqueue_step(r, qd.data(), fd.data(), s);
+    if (st != CF_OK) return st;
+    for (int b = 0; b < r->n_buckets; ++b) {
+        const size_t nb = (size_t)r->cells[b] * r->NQ[b] * r->K[b] * sizeof(double);
+        if (nb) RCHECK(cudaMemcpyAsync(q_host[b], qd[b], nb, cudaMemcpyDeviceToHost, s));
+    }
+    RCHECK(cudaStreamSynchronize(s));
     return CF_OK;
 }
 
@@ -361,6 +728,7 @@ int cf_ragged_create(cf_ragged** out, cf_plan* const* plans, const int64_t* cell
             }
         }
         r->n_units = (int)units.size();
+        r->h_units = units;
         e = cudaMalloc(&r->d_tiles, std::max<size_t>(tiles_total, 1) * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&r->d_buckets, n_buckets * sizeof(Bucket));
         if (e == cudaSuccess) e = cudaMalloc(&r->d_units, std::max<size_t>(units.size(), 1) * sizeof(Unit));
@@ -373,7 +741,10 @@ int cf_ragged_create(cf_ragged** out, cf_plan* const* plans, const int64_t* cell
         for (int b = 0; b < n_buckets; ++b) {
             hb[b].fT = r->d_tiles + r->tile_off[b];
             hb[b].QT = r->d_tiles + r->tile_off[b] + (size_t)ntiles(r->cells[b]) * CF_TILE * r->NQ[b] * r->K[b];
+            hb[b].cells = r->cells[b];
+            hb[b].hpc = 1;
         }
+        r->h_buckets = hb;
         e = cudaMemcpy(r->d_buckets, hb.data(), n_buckets * sizeof(Bucket), cudaMemcpyHostToDevice);
         if (e == cudaSuccess && !units.empty())
             e = cudaMemcpy(r->d_units, units.data(), units.size() * sizeof(Unit), cudaMemcpyHostToDevice);
@@ -422,7 +793,7 @@ int cf_ragged_graph_launch(cf_ragged* r, double* const* q_dev, const double* con
         r->graph = nullptr;
         if (!r->graph_stream) RCHECK(cudaStreamCreateWithFlags(&r->graph_stream, cudaStreamNonBlocking));
         RCHECK(cudaStreamBeginCapture(r->graph_stream, cudaStreamCaptureModeThreadLocal));
-        const int st = enqueue_step(r, q_dev, f_dev, r->graph_stream);
+        const int st = enqueue_step(r, q_dev, f_dev, r->graph_stream, false);
         cudaGraph_t g = nullptr;
         const cudaError_t e = cudaStreamEndCapture(r->graph_stream, &g);
         if (st != CF_OK) {
@@ -436,6 +807,7 @@ int cf_ragged_graph_launch(cf_ragged* r, double* const* q_dev, const double* con
         r->graph_q.assign(q_dev, q_dev + r->n_buckets);
     }
     RCHECK(cudaGraphLaunch(r->graph_exec, (cudaStream_t)stream));
+    cf_add_launches(r->step_kernels);
     return CF_OK;
 }
 
@@ -445,6 +817,24 @@ int cf_ragged_q_resident(cf_ragged* r, void* stream) {
     if (!r) return CF_EINVAL;
     std::lock_guard<std::mutex> lk(r->mu);
     return enqueue_contract(r, (cudaStream_t)stream);
+}
+
+// q_host[b] += Q(f_host[b]) for every bucket, host arrays; synchronous.
+int cf_ragged_q_host(cf_ragged* r, double* const* q_host, const double* const* f_host) {
+    if (!r || !q_host || !f_host) return CF_EINVAL;
+    for (int b = 0; b < r->n_buckets; ++b)
+        if (r->cells[b] > 0 && (!q_host[b] || !f_host[b])) {
+            cf_set_last_error("cf_ragged_q_host: null host array");
+            return CF_EINVAL;
+        }
+    std::lock_guard<std::mutex> lk(r->mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != r->device) cudaSetDevice(r->device);
+    int st = host_setup(r);
+    if (st == CF_OK) st = r->host_stream ? host_streamed(r, q_host, f_host) : host_plain(r, q_host, f_host);
+    if (cur != r->device) cudaSetDevice(cur);
+    return st;
 }
 
 int cf_ragged_info(const cf_ragged* r, int32_t* n_units, int32_t* ctas, int64_t* smem_bytes, int32_t* n_fused) {

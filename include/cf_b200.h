@@ -225,6 +225,14 @@ int cf_ragged_graph_launch(cf_ragged* ragged, double* const* q_dev, const double
 /* The contraction alone on the handle's resident tiled buffers, as the last cf_ragged_q or
  * cf_ragged_graph_launch left them (Q_tiled += Q(f_tiled)): the step without its layout passes. */
 int cf_ragged_q_resident(cf_ragged* ragged, void* stream);
+/* q_host[b] += Q(f_host[b]) for every bucket, with host arrays [N_Q x K x cells[b]]; synchronous.
+ * No counterpart in the reference.  When every non-empty bucket runs in the fused launch on the tile
+ * routine (family 1), the batch is streamed: each bucket goes up in chunks of whole half-tiles in the
+ * order the fused launch takes them, one launch starts on the first chunk, and each chunk comes back
+ * as soon as it is final, with the same result bits as cf_ragged_q.  Any other handle copies every
+ * bucket up, runs the cf_ragged_q step and copies back.  The first call allocates the handle's
+ * device copies of the buckets; pinned host memory makes the copies asynchronous. */
+int cf_ragged_q_host(cf_ragged* ragged, double* const* q_host, const double* const* f_host);
 /* Work units of the fused table, CTAs of the fused launch, its dynamic shared memory and the number
  * of buckets it contracts (the others run their own kernels). */
 int cf_ragged_info(const cf_ragged* ragged, int32_t* n_units, int32_t* ctas, int64_t* smem_bytes, int32_t* n_fused);
