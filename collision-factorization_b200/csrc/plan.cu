@@ -935,12 +935,18 @@ int ensure_stream_sync(cf_plan* p) {
     int khz = 0;
     CF_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, p->device));
     p->xwait_cycles = (long long)((double)std::max(khz, 1000000) * 1e3 * kStreamWaitSeconds);
-    CF_CUDA(cudaHostAlloc((void**)&p->h_xepoch, kStreamChunks * sizeof(int), cudaHostAllocDefault));
-    CF_CUDA(cudaHostAlloc((void**)&p->h_xsync, (kStreamChunks + 1) * sizeof(int), cudaHostAllocMapped));
+    // each allocation is kept once made, so a call after a failed set-up does not allocate it twice
+    if (!p->h_xepoch) CF_CUDA(cudaHostAlloc((void**)&p->h_xepoch, kStreamChunks * sizeof(int), cudaHostAllocDefault));
+    if (!p->h_xsync)
+        CF_CUDA(cudaHostAlloc((void**)&p->h_xsync, (kStreamChunks + 1) * sizeof(int), cudaHostAllocMapped));
     CF_CUDA(cudaHostGetDevicePointer((void**)&p->h_xsync_dev, p->h_xsync, 0));
     int* d = nullptr;
     CF_CUDA(cudaMalloc((void**)&d, (2 * kStreamChunks + 1) * sizeof(int)));
-    CF_CUDA(cudaMemset(d, 0, (2 * kStreamChunks + 1) * sizeof(int)));
+    const cudaError_t e = cudaMemset(d, 0, (2 * kStreamChunks + 1) * sizeof(int));
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return fail(CF_ECUDA, "cudaMemset: %s", cudaGetErrorString(e));
+    }
     p->d_xready = d;
     p->d_xdone = d + kStreamChunks;
     return CF_OK;

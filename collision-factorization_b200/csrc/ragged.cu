@@ -392,7 +392,7 @@ int host_setup(cf_ragged* r) {
         r->io_off.push_back(total);
         total += 2 * (size_t)r->cells[b] * r->NQ[b] * r->K[b];
     }
-    RCHECK(cudaMalloc(&r->d_io, std::max<size_t>(total, 1) * sizeof(double)));
+    if (!r->d_io) RCHECK(cudaMalloc(&r->d_io, std::max<size_t>(total, 1) * sizeof(double)));
     for (cudaStream_t& s : r->xs)
         if (!s) RCHECK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     bool stream = r->family == 1 && r->n_units > 0;
@@ -440,17 +440,17 @@ int host_setup(cf_ragged* r) {
             for (int h = 0; h < (int)((r->cells[b] + 15) / 16); ++h)
                 for (int k = 0; k < 4; ++k) xunits.push_back({b, h, 1 + k, 0});
         r->n_xunits = (int)xunits.size();
-        RCHECK(cudaMalloc(&r->d_xunits, std::max<size_t>(xunits.size(), 1) * sizeof(Unit)));
+        if (!r->d_xunits) RCHECK(cudaMalloc(&r->d_xunits, std::max<size_t>(xunits.size(), 1) * sizeof(Unit)));
         RCHECK(cudaMemcpy(r->d_xunits, xunits.data(), xunits.size() * sizeof(Unit), cudaMemcpyHostToDevice));
         std::vector<int> chunk_units(kHostChunks, 0);
         for (const Unit& u : xunits)
             chunk_units[r->h_buckets[u.bucket].chunk_base + u.ht / hpc]++;
-        RCHECK(cudaMalloc(&r->d_xsync, (3 * kHostChunks + 1) * sizeof(int)));
+        if (!r->d_xsync) RCHECK(cudaMalloc(&r->d_xsync, (3 * kHostChunks + 1) * sizeof(int)));
         RCHECK(cudaMemset(r->d_xsync, 0, (3 * kHostChunks + 1) * sizeof(int)));
         RCHECK(cudaMemcpy(r->d_xsync + 2 * kHostChunks, chunk_units.data(), kHostChunks * sizeof(int),
                           cudaMemcpyHostToDevice));
-        RCHECK(cudaHostAlloc((void**)&r->h_xepoch, kHostChunks * sizeof(int), cudaHostAllocDefault));
-        RCHECK(cudaHostAlloc((void**)&r->h_xsync, (kHostChunks + 1) * sizeof(int), cudaHostAllocMapped));
+        if (!r->h_xepoch) RCHECK(cudaHostAlloc((void**)&r->h_xepoch, kHostChunks * sizeof(int), cudaHostAllocDefault));
+        if (!r->h_xsync) RCHECK(cudaHostAlloc((void**)&r->h_xsync, (kHostChunks + 1) * sizeof(int), cudaHostAllocMapped));
         RCHECK(cudaHostGetDevicePointer((void**)&r->h_xsync_dev, r->h_xsync, 0));
         int khz = 0;
         RCHECK(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, r->device));
