@@ -54,6 +54,9 @@ NCU_TRAFFIC = {
                                             "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
                                             "profiles/af_tile_kernel_folded_hs_l10_k8_b4096.md"),
     ("hs_l10_k8_b4096", "pair", "af"): (65.9e6 + 1.8e6, "ncu, profiles/af_pair_kernel_hs_l10_k8_b4096.md"),
+    ("ragged_hs_b16384", "ragged_tile_0", "af_sym"): (86.450176e6 + 4.645632e6,
+                                                     "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                                     "profiles/af_ragged_kernel_tile_hs_b16384.md"),
     ("hs_l10_k8_b4096", "tile_cell_major", "af_sym"): (64.777728e6 + 2.003456e6,
                                                        "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
                                                        "profiles/af_tile_stream_kernel_folded_hs_l10_k8_b4096.md"),
@@ -689,6 +692,31 @@ def run_reference_ragged(args, world):
     return out
 
 
+def run_profile_ragged(args):
+    """Minimal launch sequence for ncu on the ragged mix: the tile routine, no tail split, the folded
+    form in every bucket (the autotuner's choice on B200), then steps+1 device steps."""
+    import torch
+
+    import cf_b200
+    from cf_b200 import workloads
+    from cf_b200.ragged import RaggedBatch
+
+    B = WORKLOADS[args.workload][2]
+    assign = workloads.ragged_assignment(B, seed=rank_seed(args.seed, 0))
+    counts = [int(np.sum(assign == b)) for b in range(len(RAGGED_BUCKETS))]
+    ops, fs = [], []
+    for b, (L, K) in enumerate(RAGGED_BUCKETS):
+        geo, R, _ = make_operator(L, K, 1.0, args.seed + 17 * b)
+        ops.append(cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K, device=0))
+        fs.append(torch.from_numpy(make_cells(L, K, counts[b], seed=args.seed + b)).cuda())
+    rb = RaggedBatch(ops, counts, ["af_sym"] * len(ops), tail_split=0, family="tile")
+    qs = [torch.zeros_like(f) for f in fs]
+    for _ in range(args.steps + 1):
+        rb.q(fs, qs)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": args.workload, "launches": args.steps + 1, "B": B}))
+
+
 def run_profile(args):
     """Minimal launch sequence for ncu: pack once, then steps+1 launches of the plain contraction."""
     import torch
@@ -892,6 +920,9 @@ def run_ragged(args):
     e2e_s = dist_max(sum(e2e_times), world)
     nbytes = sum(int(x.numel()) * 8 for x in f_h)
 
+    # DRAM bytes of one fused launch from its ncu capture, for the configuration captured there
+    ragged_traffic = NCU_TRAFFIC.get((args.workload, f"ragged_{family}_{tail}", "af_sym")) \
+        if all(fm == "af_sym" for fm in forms) else None
     out = None
     if rank == 0:
         cpu = None
@@ -929,7 +960,9 @@ def run_ragged(args):
             "roofline": {"bound": "fp64", "kernel": f"af_ragged_kernel<{family} routine> (one persistent launch over "
                                                     "the buckets)",
                          "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
-                         "traffic": None, "algorithmic_flop_per_launch": rb.flops_q, "kernel_ms": kern_s * 1e3,
+                         "traffic": ragged_traffic[0] if ragged_traffic else None,
+                         "traffic_source": ragged_traffic[1] if ragged_traffic else None,
+                         "algorithmic_flop_per_launch": rb.flops_q, "kernel_ms": kern_s * 1e3,
                          "peak_source": "DFMA probe measured on this GPU in this run"},
             "cpu_baseline": cpu,
             "e2e": {"value": world * B * n_e2e / e2e_s, "unit": "cell-evals/s", "h2d_bytes_per_step": 2 * nbytes,
@@ -1069,6 +1102,8 @@ def main(argv=None):
         run_rtensor(args)
     elif args.workload == "implicit_hs_l8_k8_b2048":
         run_implicit(args)
+    elif args.profile and args.workload == "ragged_hs_b16384":
+        run_profile_ragged(args)
     elif args.profile:
         run_profile(args)
     elif args.workload == "ragged_hs_b16384":
