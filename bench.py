@@ -54,6 +54,9 @@ NCU_TRAFFIC = {
                                             "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
                                             "profiles/af_tile_kernel_folded_hs_l10_k8_b4096.md"),
     ("hs_l10_k8_b4096", "pair", "af"): (65.9e6 + 1.8e6, "ncu, profiles/af_pair_kernel_hs_l10_k8_b4096.md"),
+    ("ragged_hs_b16384", "ragged_cm_0", "af_sym"): (86.157056e6 + 4.121856e6,
+                                                   "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
+                                                   "profiles/af_ragged_stream_kernel_resident_hs_b16384.md"),
     ("ragged_hs_b16384", "ragged_tile_0", "af_sym"): (86.450176e6 + 4.645632e6,
                                                      "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
                                                      "profiles/af_ragged_kernel_tile_hs_b16384.md"),
@@ -921,7 +924,8 @@ def run_ragged(args):
     nbytes = sum(int(x.numel()) * 8 for x in f_h)
 
     # DRAM bytes of one fused launch from its ncu capture, for the configuration captured there
-    ragged_traffic = NCU_TRAFFIC.get((args.workload, f"ragged_{family}_{tail}", "af_sym")) \
+    ragged_key = "ragged_cm" if rb.launches_per_step() == 1 else f"ragged_{family}"
+    ragged_traffic = NCU_TRAFFIC.get((args.workload, f"{ragged_key}_{tail}", "af_sym")) \
         if all(fm == "af_sym" for fm in forms) else None
     out = None
     if rank == 0:
@@ -957,8 +961,11 @@ def run_ragged(args):
                          "separate_calls_cells_per_s": B * len(sep_ms) / (sum(sep_ms) / 1e3),
                          "contraction_only_cells_per_s": B / kern_s},
             "autotune": dict(tune, seconds=tune_s),
-            "roofline": {"bound": "fp64", "kernel": f"af_ragged_kernel<{family} routine> (one persistent launch over "
-                                                    "the buckets)",
+            "roofline": {"bound": "fp64", "kernel": ("af_ragged_stream_kernel, resident (the tile routine on the buckets' "
+                                                    "cell-major arrays: the whole step in one persistent launch)"
+                                                    if rb.launches_per_step() == 1 else
+                                                    f"af_ragged_kernel<{family} routine> (one persistent launch over "
+                                                    "the buckets)"),
                          "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s", "frac": achieved / peak_tf,
                          "traffic": ragged_traffic[0] if ragged_traffic else None,
                          "traffic_source": ragged_traffic[1] if ragged_traffic else None,

@@ -88,8 +88,12 @@ class RaggedBatch:
         return qs
 
     def launches_per_step(self) -> int:
-        """Kernels one step launches: two layout passes in and one out per non-empty bucket, the fused
-        launch, and one contraction kernel per bucket outside it."""
+        """Kernels one step launches: with the tile routine and every non-empty bucket fused, the one
+        launch on the cell-major arrays; otherwise two layout passes in and one out per non-empty bucket,
+        the fused launch, and one contraction kernel per bucket outside it."""
+        if self.family == "tile" and self.n_fused and all(
+                self._fused(op, f) for op, c, f in zip(self.ops, self.cells, self.forms) if c > 0):
+            return 1
         nb = sum(1 for c in self.cells if c > 0)
         sep = sum(1 for op, c, f in zip(self.ops, self.cells, self.forms)
                   if c > 0 and not self._fused(op, f))

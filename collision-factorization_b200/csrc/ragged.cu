@@ -144,6 +144,12 @@ __global__ void __launch_bounds__((TILE ? kTW : kRW) * 32, 1)
     }
 }
 
+// The callers' cell-major arrays of a resident launch (cf_ragged_q / cf_ragged_graph_launch), by bucket.
+struct CmPtrs {
+    const double* f[64];
+    double* q[64];
+};
+
 // Words of the streamed launch of cf_ragged_q_host (per upload chunk; see af_ragged_stream_kernel).
 struct RaggedSync {
     const int* ready;        // [n_chunks] device; == epoch once the chunk's f and Q are in
@@ -165,9 +171,13 @@ struct RaggedSync {
 // at each row's start and writing Q in place, so a bucket's result equals the resident step's bit
 // for bit.  The CTA that finishes a chunk's last unit fences at system scope and writes the epoch
 // into the chunk's mapped host word; the host then queues that chunk's download.
+//
+// Resident (rs.ready null; the device steps): the same routine on the callers' cell-major arrays in
+// `ptrs`, with the handle's own work table, no waits and no chunk words -- the whole step in one
+// launch, without layout passes.
 __global__ void __launch_bounds__(kTW * 32, 1)
     af_ragged_stream_kernel(const Bucket* __restrict__ buckets, const Unit* __restrict__ units, int n_units,
-                            int* __restrict__ counter, RaggedSync rs) {
+                            int* __restrict__ counter, RaggedSync rs, CmPtrs ptrs) {
     constexpr int W = kTW;
     extern __shared__ __align__(16) double smem[];
     __shared__ int s_unit, s_next;
@@ -190,8 +200,10 @@ __global__ void __launch_bounds__(kTW * 32, 1)
         const int M = bk.M, NQ = bk.op.n_q, K = bk.K;
         const int chunk = bk.chunk_base + un.ht / bk.hpc;
         const long long cell0 = (long long)un.ht * cf::kTileCells;
+        const double* fb = rs.ready ? bk.f_cm : ptrs.f[un.bucket];
+        double* qb = rs.ready ? bk.q_cm : ptrs.q[un.bucket];
         if (un.bucket != staged_b || un.ht != staged_ht) {
-            if (tid == 0) {
+            if (tid == 0 && rs.ready) {
                 const long long t0 = clock64();
                 while (cf::ld_acquire(rs.ready + chunk) != rs.epoch) {
                     if (*reinterpret_cast<volatile int*>(rs.abort) == rs.epoch) break;
@@ -209,7 +221,7 @@ __global__ void __launch_bounds__(kTW * 32, 1)
                 const int c = i & 15, j = i >> 4;
                 const int r = (j % NQ) * K + j / NQ;
                 if (cell0 + c < bk.cells)
-                    cf::cp_async8(fs + r * cf::kTileCells + c, bk.f_cm + (size_t)(cell0 + c) * M + j);
+                    cf::cp_async8(fs + r * cf::kTileCells + c, fb + (size_t)(cell0 + c) * M + j);
                 else
                     fs[r * cf::kTileCells + c] = 0.0;
             }
@@ -223,7 +235,7 @@ __global__ void __launch_bounds__(kTW * 32, 1)
         const int b0 = bk.bin_begin[un.bin], nb = bk.bin_begin[un.bin + 1] - b0;
         const long long cell = cell0 + (lane & 15);
         const bool live = cell < bk.cells;
-        double* qc = bk.q_cm + (size_t)(live ? cell : 0) * M;
+        double* qc = qb + (size_t)(live ? cell : 0) * M;
         for (;;) {
             int i = 0;
             if (lane == 0) i = atomicAdd(&s_next, 1);
@@ -238,9 +250,9 @@ __global__ void __launch_bounds__(kTW * 32, 1)
                 default: break;
             }
         }
-        __threadfence();
+        if (rs.done) __threadfence();
         __syncthreads();
-        if (tid == 0 && atomicAdd(rs.done + chunk, 1) == rs.chunk_units[chunk] - 1) {
+        if (tid == 0 && rs.done && atomicAdd(rs.done + chunk, 1) == rs.chunk_units[chunk] - 1) {
             __threadfence_system();
             *reinterpret_cast<volatile int*>(rs.host_done + chunk) = rs.epoch;
         }
@@ -281,6 +293,12 @@ struct cf_ragged {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int64_t step_kernels = 0;  // layout passes and fused launch of the last step enqueued
+    // every non-empty bucket fused on the tile routine: a device step is one resident launch of
+    // af_ragged_stream_kernel on the callers' cell-major arrays (the last ones kept for
+    // cf_ragged_q_resident)
+    bool cell_major = false;
+    CmPtrs last_ptrs{};
+    bool have_last = false;
     std::vector<const double*> graph_f;
     std::vector<double*> graph_q;
     cudaStream_t graph_stream = nullptr;
@@ -356,7 +374,27 @@ int enqueue_contract(cf_ragged* r, cudaStream_t s, bool count = true) {
 
 // pack every bucket, the contraction, unpack (q += Q(f) per bucket), all on stream s; count: add the
 // step's kernels to the launch counter now (false while recording a graph: each replay adds them)
+int enqueue_resident_cm(cf_ragged* r, cudaStream_t s, bool count) {
+    RCHECK(cudaMemsetAsync(r->d_counter, 0, sizeof(int), s));
+    const RaggedSync none{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, 0};
+    const unsigned grid = (unsigned)std::min(r->n_units, r->ctas);
+    af_ragged_stream_kernel<<<grid, kTW * 32, r->smem, s>>>(r->d_buckets, r->d_units, r->n_units, r->d_counter,
+                                                            none, r->last_ptrs);
+    RCHECK(cudaGetLastError());
+    if (count) cf_add_launches(1);
+    return CF_OK;
+}
+
 int enqueue_step(cf_ragged* r, double* const* q, const double* const* f, cudaStream_t s, bool count = true) {
+    if (r->cell_major) {
+        for (int b = 0; b < r->n_buckets; ++b) {
+            r->last_ptrs.f[b] = f[b];
+            r->last_ptrs.q[b] = q[b];
+        }
+        r->have_last = true;
+        r->step_kernels = 1;
+        return enqueue_resident_cm(r, s, count);
+    }
     int64_t nk = r->n_units > 0 ? 1 : 0;
     for (int b = 0; b < r->n_buckets; ++b) nk += r->cells[b] > 0 ? 3 : 0;
     r->step_kernels = nk;
@@ -510,7 +548,7 @@ int host_streamed(cf_ragged* r, double* const* q_host, const double* const* f_ho
                         r->xwait};
     const unsigned grid = (unsigned)std::min(r->n_xunits, r->ctas);
     af_ragged_stream_kernel<<<grid, kTW * 32, r->smem, s_k>>>(r->d_buckets, r->d_xunits, r->n_xunits, r->d_counter,
-                                                              rs);
+                                                              rs, CmPtrs{});
     cf_add_launches(1);
     int st = CF_OK;
     cudaError_t e = cudaGetLastError();
@@ -729,6 +767,19 @@ int cf_ragged_create(cf_ragged** out, cf_plan* const* plans, const int64_t* cell
         }
         r->n_units = (int)units.size();
         r->h_units = units;
+        bool cm = family == 1 && r->n_units > 0;
+        for (int b = 0; b < n_buckets; ++b)
+            if (r->cells[b] > 0 && !r->fused[b]) cm = false;
+        if (cm) {
+            e = cudaFuncSetAttribute(af_ragged_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)r->smem);
+            if (e != cudaSuccess) {
+                cf_set_last_error(cudaGetErrorString(e));
+                st = CF_ECUDA;
+                break;
+            }
+        }
+        r->cell_major = cm;
         e = cudaMalloc(&r->d_tiles, std::max<size_t>(tiles_total, 1) * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&r->d_buckets, n_buckets * sizeof(Bucket));
         if (e == cudaSuccess) e = cudaMalloc(&r->d_units, std::max<size_t>(units.size(), 1) * sizeof(Unit));
@@ -816,6 +867,13 @@ int cf_ragged_graph_launch(cf_ragged* r, double* const* q_dev, const double* con
 int cf_ragged_q_resident(cf_ragged* r, void* stream) {
     if (!r) return CF_EINVAL;
     std::lock_guard<std::mutex> lk(r->mu);
+    if (r->cell_major) {
+        if (!r->have_last) {
+            cf_set_last_error("cf_ragged_q_resident: no step has run on this handle yet");
+            return CF_EINVAL;
+        }
+        return enqueue_resident_cm(r, (cudaStream_t)stream, true);
+    }
     return enqueue_contract(r, (cudaStream_t)stream);
 }
 

@@ -212,7 +212,8 @@ int cf_plan_stream_selftest(cf_plan* plan, double wait_seconds);
  * pair routine (8 warps per CTA), 1 the tile routine (16 warps per CTA; buckets of odd K then run
  * on their own).  tail_split (0, 4 or 16) is how many bins each of the last half-tiles of the fused
  * work table is cut into, so that the launch ends evenly.
- * cf_ragged_q enqueues pack, fused launch, the separate buckets and unpack on the stream;
+ * cf_ragged_q enqueues pack, fused launch, the separate buckets and unpack on the stream (when every
+ * non-empty bucket is fused on the tile routine: one launch on the cell-major arrays instead);
  * cf_ragged_graph_launch records that sequence into a CUDA graph on first use (per set of buffers)
  * and replays it.  No counterpart in the reference (it contracts one f at a time).
  * ------------------------------------------------------------------------------------------ */
