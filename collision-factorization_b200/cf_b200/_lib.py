@@ -57,7 +57,7 @@ class PlanInfo(C.Structure):
         ("device_bytes", C.c_int64), ("last_path", C.c_int32), ("reserved", C.c_int32),
     ]
 
-PATH_NAMES = {0: "none", 1: "gather", 2: "tile", 3: "pair", 4: "pair_l1", 5: "pair_split", 6: "tile_mma", 7: "bf16_mma"}
+PATH_NAMES = {0: "none", 1: "gather", 2: "tile", 3: "pair", 4: "pair_l1", 5: "pair_split", 6: "tile_mma", 7: "bf16_mma", 8: "tile_quarter"}
 
 _DP = C.POINTER(C.c_double)
 

@@ -137,6 +137,39 @@ static LaunchResult launch_tile_stream(const LaunchArgs& a) {
     return {e == cudaSuccess ? 0 : 5, 1, e, PATH_TILE};
 }
 
+// Quarter-tile kernel (8 cells per CTA, fast forms, K % 4 == 0).  Status -1 when it does not fit.
+template <int K, int W, bool JV>
+static LaunchResult launch_tile4(const LaunchArgs& a) {
+    const int M = a.op.n_q * K;
+    const size_t smem = tile4_smem_bytes<K>(M, W, JV);
+    if (smem + 256 > a.max_smem || a.counter == nullptr) return {-1, 0, cudaSuccess, PATH_TILE4};
+    auto kern = af_tile4_kernel<K, W, JV>;
+    int per_sm = 0;
+    cudaError_t e = resident_ctas((const void*)kern, W * 32, smem, &per_sm);
+    if (e != cudaSuccess) return {5, 0, e, PATH_TILE4};
+    if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_TILE4};
+    const int64_t ctas = (int64_t)per_sm * a.n_sms;
+    const int64_t n_qt = (a.n_cells + kQuarterCells - 1) / kQuarterCells;
+    TileSched sc;
+    sc.bin_begin = a.bin_begin;
+    sc.bin_q1 = a.bin_q1;
+    sc.n_ht = (int)n_qt;
+    const int64_t n_whole = n_qt > ctas ? n_qt - ctas : 0;
+    const int64_t rem = n_qt - n_whole;
+    sc.split = rem * 4 >= ctas ? 4 : 16;
+    sc.n_whole = (int)n_whole;
+    const int64_t n_units = n_whole + rem * sc.split;
+    if (n_units > INT32_MAX) return {2, 0, cudaSuccess, PATH_TILE4};
+    sc.n_units = (int)n_units;
+    sc.counter = a.counter;
+    e = cudaMemsetAsync(a.counter, 0, sizeof(int), a.stream);
+    if (e != cudaSuccess) return {5, 0, e, PATH_TILE4};
+    const unsigned grid = (unsigned)(n_units < ctas ? n_units : ctas);
+    kern<<<grid, W * 32, smem, a.stream>>>(a.op, sc, a.fT, a.vT, a.QT);
+    e = cudaGetLastError();
+    return {e == cudaSuccess ? 0 : 5, 1, e, PATH_TILE4};
+}
+
 // Work-unit schedule shared by the persistent kernels: whole half-tiles while there are more
 // half-tiles than CTAs, then the last `ctas` half-tiles split into 4 (or 16) bins each.
 struct UnitPlan {
@@ -341,6 +374,13 @@ static LaunchResult launch_for_k(const LaunchArgs& a) {
         }
     } else {
         if (a.path == PATH_TILE) return {8, 0, cudaSuccess, PATH_TILE};
+    }
+    // the 16-cell tile (and the pair kernel) did not fit: 8-cell quarter tiles before the gather kernel
+    if constexpr (K % 4 == 0 && K <= 8) {
+        if (a.path == PATH_AUTO && !a.exact && !a.f32) {
+            const LaunchResult r = jv ? launch_tile4<K, 16, true>(a) : launch_tile4<K, 16, false>(a);
+            if (r.status != -1) return r;
+        }
     }
     if constexpr (K <= 8) {
         if (a.exact)

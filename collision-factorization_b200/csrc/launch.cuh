@@ -12,7 +12,8 @@ enum Op { OP_AF = 0, OP_RF = 1, OP_JV = 2 };
 
 // Kernel families for the angular-first / Jacobian forms.
 enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3, PATH_PAIR_L1 = 4, PATH_PAIR_SPLIT = 5, PATH_TILE_MMA = 6,
-           PATH_BF16_MMA = 7 /* reported only: the BF16-split form's kernel */ };
+           PATH_BF16_MMA = 7 /* reported only: the BF16-split form's kernel */,
+           PATH_TILE4 = 8 /* reported only: the quarter-tile kernel, where the 16-cell tile does not fit */ };
 
 struct LaunchArgs {
     DevOp op;

@@ -333,6 +333,209 @@ constexpr size_t tile_smem_bytes(int M, int W, bool jv) {
 }
 
 // ------------------------------------------------------------------------------------------
+// Quarter-tile kernels: 8 cells of f (and, for J.v, of v) resident per CTA, 4 lanes per cell that
+// split the K x K Phi accumulator by k3 quarter -- for the shapes whose 16-cell tile does not fit in
+// shared memory (at K = 8: Q from L = 12 on, J.v from L = 10 on).  The routine is the tile routine's
+// with 4 lane groups instead of 2; fast forms only.  An 8-cell row is 64 bytes, half of the banks,
+// so rows are stored pairwise swapped (row r at r ^ ((r >> 1) & 1)): the four lane groups' f(q3)
+// rows r, r + 2, r + 4, r + 6 then fall into both halves and cost 2 wavefronts, not 4.
+// ------------------------------------------------------------------------------------------
+constexpr int kQuarterCells = 8;
+
+__device__ __forceinline__ int qrow(int r) { return r ^ ((r >> 1) & 1); }
+
+template <int K, bool JV>
+__device__ __forceinline__ void tile4_q1(const DevOp& op, int q1, const double* __restrict__ fs,
+                                         const double* __restrict__ vs, double* rb, double* qtc, int lane) {
+    static_assert(K % 4 == 0, "the quarter-tile routine splits Phi into four column quarters");
+    constexpr int KC = K / 4;
+    constexpr int SL = RBuf<K>::SL;
+    constexpr int QC = kQuarterCells;
+    const int c = lane & 7;
+    const int part = lane >> 3;
+    const int k3b = part * KC;
+
+    double acc[K];
+#pragma unroll
+    for (int k1 = 0; k1 < K; ++k1) acc[k1] = part == 0 ? qtc[(size_t)(q1 * K + k1) * CF_TILE] : 0.0;
+
+    const int s0 = op.q1_begin[q1], s1 = op.q1_begin[q1 + 1];
+    for (int s = s0; s < s1; ++s) {
+        const int t = op.slice_t[s];
+        const int e0 = op.slice_e[s], e1 = op.slice_e[s + 1];
+        __syncwarp();
+        const double* __restrict__ Rt = op.R + (size_t)t * K * K * K;
+        for (int i = lane; i < K * K * K / 2; i += 32) {
+            const int j = (2 * i) / (K * K), w = (2 * i) % (K * K);
+            cp_async16(rb + j * SL + w, Rt + 2 * i);
+        }
+        cp_async_commit();
+
+        double phi[K][KC];
+#pragma unroll
+        for (int a = 0; a < K; ++a)
+#pragma unroll
+            for (int b = 0; b < KC; ++b) phi[a][b] = 0.0;
+
+        const bool grouped = op.grouped & (JV ? 2 : 1);
+        double hf[KC], hv[KC];
+#pragma unroll
+        for (int b = 0; b < KC; ++b) hf[b] = hv[b] = 0.0;
+        int cur = -1;
+        auto flush = [&]() {
+#pragma unroll
+            for (int k2 = 0; k2 < K; ++k2) {
+                const double f2 = fs[qrow(cur * K + k2) * QC + c];
+                if constexpr (JV) {
+                    const double v2 = vs[qrow(cur * K + k2) * QC + c];
+#pragma unroll
+                    for (int b = 0; b < KC; ++b) phi[k2][b] = fma(v2, hf[b], fma(f2, hv[b], phi[k2][b]));
+                } else {
+#pragma unroll
+                    for (int b = 0; b < KC; ++b) phi[k2][b] = fma(f2, hf[b], phi[k2][b]);
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < KC; ++b) hf[b] = hv[b] = 0.0;
+        };
+        for (int eb = e0; eb < e1; eb += 32) {
+            const int n = min(32, e1 - eb);
+            uint32_t my_q23 = 0;
+            double my_g = 0.0;
+            if (lane < n) {
+                my_q23 = __ldg(op.e_q23 + eb + lane);
+                my_g = __ldg(op.e_g + eb + lane);
+            }
+            for (int j = 0; j < n; ++j) {
+                const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, j);
+                const double g = __shfl_sync(0xffffffffu, my_g, j);
+                const int q2 = (int)(q23 & 0xffffu), r3 = (int)(q23 >> 16) * K + k3b;
+                double f3[KC], v3[KC];
+#pragma unroll
+                for (int b = 0; b < KC; ++b) {
+                    f3[b] = fs[qrow(r3 + b) * QC + c];
+                    if constexpr (JV) v3[b] = vs[qrow(r3 + b) * QC + c];
+                }
+                if (grouped) {
+                    // entries sorted by q2: sum G f(q3) (and G v(q3)) over the run, one outer product per run
+                    if (q2 != cur) {
+                        if (cur >= 0) flush();
+                        cur = q2;
+                    }
+#pragma unroll
+                    for (int b = 0; b < KC; ++b) {
+                        hf[b] = fma(g, f3[b], hf[b]);
+                        if constexpr (JV) hv[b] = fma(g, v3[b], hv[b]);
+                    }
+                } else {
+                    const int r2 = q2 * K;
+#pragma unroll
+                    for (int k2 = 0; k2 < K; ++k2) {
+                        const double f2 = fs[qrow(r2 + k2) * QC + c];
+                        if constexpr (JV) {
+                            const double v2 = vs[qrow(r2 + k2) * QC + c];
+#pragma unroll
+                            for (int b = 0; b < KC; ++b) phi[k2][b] = fma(v2, g * f3[b], fma(f2, g * v3[b], phi[k2][b]));
+                        } else {
+#pragma unroll
+                            for (int b = 0; b < KC; ++b) phi[k2][b] = fma(f2, g * f3[b], phi[k2][b]);
+                        }
+                    }
+                }
+            }
+        }
+        if (grouped && cur >= 0) flush();
+        cp_async_wait_all();
+        __syncwarp();
+
+        // K^3 step: this lane's k3 quarter; element (k1,k2,k3) at rb[k3*SL + k2*K + k1]
+        const double* __restrict__ rk = rb + k3b * SL;
+#pragma unroll
+        for (int b = 0; b < KC; ++b) {
+#pragma unroll
+            for (int k2 = 0; k2 < K; ++k2) {
+                const double2* r2v = reinterpret_cast<const double2*>(rk + b * SL + k2 * K);
+#pragma unroll
+                for (int h = 0; h < K / 2; ++h) {
+                    const double2 r = r2v[h];
+                    acc[2 * h] = fma(r.x, phi[k2][b], acc[2 * h]);
+                    acc[2 * h + 1] = fma(r.y, phi[k2][b], acc[2 * h + 1]);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < K; ++k1) {
+        acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], 8);
+        acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], 16);
+    }
+    if (part == 0) {
+#pragma unroll
+        for (int k1 = 0; k1 < K; ++k1) qtc[(size_t)(q1 * K + k1) * CF_TILE] = acc[k1];
+    }
+}
+
+template <int K, int W, bool JV>
+__global__ void __launch_bounds__(W * 32, 1)
+    af_tile4_kernel(DevOp op, TileSched sc, const double* __restrict__ fT, const double* __restrict__ vT,
+                    double* __restrict__ QT) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ int s_unit, s_next;
+    constexpr int QC = kQuarterCells;
+    const int M = op.n_q * K;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    double* fs = smem;
+    double* vs = JV ? smem + (size_t)M * QC : nullptr;
+    double* rb = smem + (size_t)(JV ? 2 : 1) * M * QC + (size_t)warp * RBuf<K>::SIZE;
+    int staged = -1;
+    for (;;) {
+        if (tid == 0) s_unit = atomicAdd(sc.counter, 1);
+        __syncthreads();
+        const int u = s_unit;
+        if (u >= sc.n_units) break;
+        int qt, bin;
+        if (u < sc.n_whole) {
+            qt = u;
+            bin = 0;
+        } else {
+            const int v = u - sc.n_whole;
+            qt = sc.n_whole + v / sc.split;
+            bin = bin_base(sc.split) + v % sc.split;
+        }
+        // quarter qt of the tiled layout: tile qt / 4, cells 8 (qt % 4) .. + 7
+        const size_t tile_base = (size_t)(qt >> 2) * M * CF_TILE + (size_t)(qt & 3) * QC;
+        if (qt != staged) {
+            // rows of 8 cells (64 B), 4 x 16-byte copies per row, to the row's swapped slot
+            for (int i = tid; i < M * 4; i += W * 32) {
+                const int r = i >> 2, w = (i & 3) * 2;
+                cp_async16(fs + qrow(r) * QC + w, fT + tile_base + (size_t)r * CF_TILE + w);
+                if constexpr (JV) cp_async16(vs + qrow(r) * QC + w, vT + tile_base + (size_t)r * CF_TILE + w);
+            }
+            cp_async_commit();
+            cp_async_wait_all();
+            staged = qt;
+        }
+        if (tid == 0) s_next = 0;
+        __syncthreads();
+        const int b0 = sc.bin_begin[bin], nb = sc.bin_begin[bin + 1] - b0;
+        double* qtc = QT + tile_base + (lane & 7);
+        for (;;) {
+            int i = 0;
+            if (lane == 0) i = atomicAdd(&s_next, 1);
+            i = __shfl_sync(0xffffffffu, i, 0);
+            if (i >= nb) break;
+            tile4_q1<K, JV>(op, sc.bin_q1[b0 + i], fs, vs, rb, qtc, lane);
+        }
+        __syncthreads();
+    }
+}
+
+template <int K>
+constexpr size_t tile4_smem_bytes(int M, int W, bool jv) {
+    return sizeof(double) * ((size_t)(jv ? 2 : 1) * M * kQuarterCells + (size_t)W * RBuf<K>::SIZE);
+}
+
+// ------------------------------------------------------------------------------------------
 // Tile kernel on the caller's cell-major f and Q.  Resident (ss.ready == null): the device entry
 // points, no layout passes, the tile kernel's schedule.  Streamed (host entry points): one launch
 // over the whole batch while the batch is still being copied in and the results copied out.

@@ -461,3 +461,57 @@ def test_two_streams_share_a_plan(cuda_available):
     assert all(torch.equal(o, ref1) for o in outs1)
     assert all(torch.equal(o, ref2) for o in outs2)
     op.close()
+
+
+@pytest.mark.parametrize("L,K,B", [(10, 8, 37), (10, 8, 300), (16, 4, 45)])
+def test_quarter_tile_jacobian_vs_oracle(L, K, B, cuda_available, oracle_lib):
+    """Where f and v do not fit as 16-cell tiles (L = 10 at K = 8), J.v runs on the 8-cell quarter-tile
+    kernel (plain and folded operator); it must match the oracle like every other family."""
+    import torch
+
+    import cf_b200
+    from cf_b200 import geometry, workloads
+    from oracle import rtensor
+
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=L + K)
+    NQ = geo.n_q
+    cells = workloads.maxwellian_cells(K, L, B, seed=11)
+    rng = np.random.default_rng(3)
+    vc = rng.standard_normal(cells.shape)
+    args = (geo.labels, geo.vals, geo.ic_map, R, NQ, K)
+    ref = np.zeros((NQ, K, B), order="F")
+    oracle_lib.jv_batch(ref, _cells_cm(cells), _cells_cm(vc), *args)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, NQ, K)
+    f, v = torch.from_numpy(cells).cuda(), torch.from_numpy(vc).cuda()
+    for folded in (False, True):
+        out = op.jv(f, v, folded=folded).cpu().numpy()
+        assert cf_b200._lib.PATH_NAMES[op.info()["last_path"]] == "tile_quarter", folded
+        assert per_cell_err(out, ref.transpose(2, 1, 0)) <= TOL_FP64, folded
+    op.close()
+
+
+def test_quarter_tile_q_vs_oracle(cuda_available, oracle_lib):
+    """Q where neither the 16-cell tile nor the pair kernel fits (L = 16, K = 8): the quarter-tile
+    kernel, plain and folded, against the oracle."""
+    import torch
+
+    import cf_b200
+    from cf_b200 import geometry, workloads
+    from oracle import rtensor
+
+    L, K, B = 16, 8, 21
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=4)
+    NQ = geo.n_q
+    cells = workloads.maxwellian_cells(K, L, B, seed=12)
+    args = (geo.labels, geo.vals, geo.ic_map, R, NQ, K)
+    ref = np.zeros((NQ, K, B), order="F")
+    oracle_lib.af_batch(ref, _cells_cm(cells), *args)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, NQ, K)
+    f = torch.from_numpy(cells).cuda()
+    for form in ("af", "af_sym"):
+        out = op.q(f, form=form).cpu().numpy()
+        assert cf_b200._lib.PATH_NAMES[op.info()["last_path"]] == "tile_quarter", form
+        assert per_cell_err(out, ref.transpose(2, 1, 0)) <= TOL_FP64, form
+    op.close()
