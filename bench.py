@@ -45,7 +45,10 @@ WORKLOADS = {
     "implicit_hs_l8_k8_b2048": (8, 8, 2048, 1.0),
     "ragged_hs_b16384": (10, 8, 16384, 1.0),  # largest bucket's (L, K); buckets in RAGGED_BUCKETS
     "rtensor_hs_k7_l10": (10, 8, 0, 1.0),  # the R-tensor quadrature itself (pad 20)
+    "single_g0_l4_k4": (4, 4, 1, 0.0),  # one f per call, Maxwell molecules; latency in us per call
 }
+# operator of the single-f workload: R from the reference's own quadrature (K_max = 3, pad 20)
+SINGLE_OPERATOR = "op_cfg1_k3_l4_g0.npz"
 RAGGED_BUCKETS = [(4, 4), (6, 6), (8, 6), (10, 8)]  # (L, K), drawn with RAGGED_WEIGHTS per cell
 R_FILES = {(10, 8): "R_hs_k7_l10_pad20.npy", (8, 8): "R_hs_k7_l8_pad20.npy"}
 # DRAM bytes (read + write) of one contraction launch, from the ncu captures summarised in profiles/
@@ -1087,10 +1090,290 @@ def run_rtensor(args):
     return out
 
 
+def load_single_operator():
+    """The single-f workload's operator (Maxwell molecules, L = 4, K = 4): the COO lists in
+    sortrows([ic_map, q1]) order, R from the reference's quadrature, one seeded f and the reference's
+    own angular_first output for it."""
+    d = np.load(ROOT / "tests" / "golden" / SINGLE_OPERATOR)
+    return {k: d[k] for k in d.files}
+
+
+def single_cell(K: int, L: int, seed: int) -> np.ndarray:
+    """One f, [K, N_Q] row-major (= the MEX's column-major [N_Q x K]): the projection of a two-Maxwellian
+    mixture with drifts N(0, 0.5^2)^3 and temperatures U[0.5, 1.5], renormalised to unit density."""
+    from cf_b200 import workloads
+
+    return workloads.two_maxwellian_mixture(K, L, seed)
+
+
+def median_us(xs) -> float:
+    return 1e6 * statistics.median(xs)
+
+
+def run_single(args):
+    """One f per call (Maxwell molecules, L = 4, K = 4, M = 100): the latency of a call.
+
+    The timed step is one contraction of one device-resident f, timed with CUDA events behind a
+    256 MB L2 flush (so the call's launches are queued when the GPU reaches it and the span is the
+    device time of the call).  Beside it: the synchronised round trip of the same call from a host
+    thread, the MEX-compatible host call cf_angular_first on pageable host arrays (the e2e figure),
+    the floors of one empty launch and of the copies, and the reference's compiled kernel on one host
+    core."""
+    import ctypes
+
+    import torch
+
+    import cf_b200
+    from cf_b200 import _lib, mex
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    L, K, _, gamma = WORKLOADS[args.workload]
+    d = load_single_operator()
+    lab, vals, ic, R = d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"], np.asfortranarray(d["R"])
+    NQ = (L + 1) ** 2
+    M = NQ * K
+    op = cf_b200.CollisionOperator(lab, vals, ic, R, NQ, K, device=local)
+    lib = _lib.load()
+
+    # parity on the fixture's f: the MEX entry (fast form) and the exact form against the reference's output
+    Qm = np.zeros((NQ, K), order="F")
+    mex.angular_first_collision_kernel_mex(Qm, d["f"], lab, vals, ic, R, NQ, K)
+    q_ref = d["Q_af"]
+    err_mex = float(np.abs(Qm - q_ref).max() / np.abs(q_ref).max())
+    Qx = np.zeros((NQ, K), order="F")
+    mex.contract_batched(Qx, d["f"], lab, vals, ic, R, NQ, K, form="af_exact")
+    exact_bitwise = bool(np.array_equal(Qx, q_ref))
+
+    f_host = single_cell(K, L, rank_seed(args.seed, rank))  # [K, N_Q]
+    f = torch.from_numpy(f_host.reshape(1, K, NQ).copy()).to(dev)
+    Q = torch.zeros_like(f)
+    ws = torch.empty(op.workspace_bytes(1) // 8 + 64, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    steps = max(args.steps, 50)
+
+    def call(form):
+        op.q(f, out=Q, form=form, workspace=ws)
+
+    def timed_cold(fn, n):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(n)]
+        for i in range(n):
+            flush.fill_(float(i))
+            evs[i][0].record(stream)
+            fn()
+            evs[i][1].record(stream)
+        torch.cuda.synchronize(dev)
+        return [a.elapsed_time(b) * 1e-3 for a, b in evs]
+
+    def round_trip(fn, n):
+        """Host wall time of fn plus a wait for its work, starting from an idle GPU."""
+        out = []
+        for _ in range(n):
+            torch.cuda.synchronize(dev)
+            t = time.perf_counter()
+            fn()
+            stream.synchronize()
+            out.append(time.perf_counter() - t)
+        return out
+
+    forms = ("af", "af_sym", "af_exact", "rf")
+    for form in forms:
+        for _ in range(max(args.warmup, 3)):
+            call(form)
+    torch.cuda.synchronize(dev)
+
+    clocks = ClockSampler(local)
+    dist_barrier(world)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    per_form = {}
+    for form in forms:
+        n0 = _lib.launch_count()
+        dev_s = timed_cold(lambda: call(form), steps)
+        launches = (_lib.launch_count() - n0) / steps
+        op.q(f, out=Q, form=form, workspace=ws)
+        torch.cuda.synchronize(dev)
+        per_form[form] = {"device_us": median_us(dev_s), "device_us_mean": 1e6 * sum(dev_s) / len(dev_s),
+                          "round_trip_us": median_us(round_trip(lambda: call(form), steps)),
+                          "launches_per_call": launches, "path": _lib.PATH_NAMES.get(op.info()["last_path"], "?")}
+    # floors: one empty launch (a 1-element fill) and the copies of one f
+    one = torch.zeros(1, dtype=torch.float64, device=dev)
+    floor_launch = median_us(round_trip(lambda: one.fill_(1.0), steps))
+    fh_pin = torch.from_numpy(f_host.reshape(1, K, NQ).copy()).pin_memory()
+    qh_pin = torch.zeros_like(fh_pin).pin_memory()
+
+    def copies():
+        f.copy_(fh_pin, non_blocking=True)
+        Q.copy_(qh_pin, non_blocking=True)
+        qh_pin.copy_(Q, non_blocking=True)
+
+    floor_copies = median_us(round_trip(copies, steps))
+
+    # e2e: the MEX-compatible host entry points on pageable column-major arrays, as MATLAB passes them
+    Dp = ctypes.POINTER(ctypes.c_double)
+    lab_f, vals_c, ic_c = np.asfortranarray(lab), np.ascontiguousarray(vals), np.ascontiguousarray(ic)
+    n_l = R.size // K ** 3
+    fq = np.asfortranarray(f_host.T)  # [N_Q x K]
+    Qh = np.zeros((NQ, K), order="F")
+    opargs = (lab_f.ctypes.data_as(Dp), vals_c.ctypes.data_as(Dp), ic_c.ctypes.data_as(Dp), R.ctypes.data_as(Dp),
+              lab_f.shape[0], n_l, NQ, K)
+    qp, fp = Qh.ctypes.data_as(Dp), fq.ctypes.data_as(Dp)
+    host_calls = {
+        "cf_angular_first": lambda: lib.cf_angular_first(qp, fp, *opargs),
+        "cf_radial_first": lambda: lib.cf_radial_first(qp, fp, *opargs),
+        "cf_contract_host af_exact": lambda: lib.cf_contract_host(qp, fp, 1, *opargs, _lib.FORMS["af_exact"]),
+        "cf_contract_host af_sym": lambda: lib.cf_contract_host(qp, fp, 1, *opargs, _lib.FORMS["af_sym"]),
+    }
+    host_us = {}
+    for name, fn in host_calls.items():
+        for _ in range(5):
+            _lib.check(fn())
+        ts = []
+        for _ in range(steps):
+            Qh.fill(0.0)
+            t = time.perf_counter()
+            rc = fn()
+            ts.append(time.perf_counter() - t)
+            _lib.check(rc)
+        host_us[name] = {"python_median_us": median_us(ts), "python_mean_us": 1e6 * sum(ts) / len(ts)}
+    # the same calls timed in C (cf_time_contract_host: back-to-back calls, no ctypes cost per call),
+    # as the reference's kernel is timed; form af with one cell is cf_angular_first's route
+    secs = ctypes.c_double()
+    for name, form in (("cf_angular_first", "af"), ("cf_radial_first", "rf"),
+                       ("cf_contract_host af_exact", "af_exact"), ("cf_contract_host af_sym", "af_sym")):
+        _lib.check(lib.cf_time_contract_host(steps, ctypes.byref(secs), qp, fp, 1, *opargs, _lib.FORMS[form]))
+        host_us[name]["c_mean_us"] = 1e6 * secs.value / steps
+        host_us[name]["route"] = _lib.few_route_last()
+    clk = clocks.stop()
+    dist_barrier(world)
+
+    # the chosen form: the fastest device call within 1e-10 of the reference's exact order
+    Qd = {}
+    for form in ("af", "af_sym", "af_exact"):
+        Q.zero_()
+        call(form)
+        Qd[form] = Q.cpu().numpy()
+    den = max(np.abs(Qd["af_exact"]).max(), 1e-300)
+    errs = {form: float(np.abs(Qd[form] - Qd["af_exact"]).max() / den) for form in Qd}
+    ok = [fm for fm in ("af", "af_sym", "af_exact") if errs[fm] <= 1e-10]
+    chosen = min(ok, key=lambda fm: per_form[fm]["device_us"])
+    t_dev = per_form[chosen]["device_us_mean"] * 1e-6
+    value, total_s = weak_rate(world, 1, steps, t_dev * steps)
+    e2e_us = host_us["cf_angular_first"]["c_mean_us"]
+    out = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                us, n, dt = cpu_reference_single_us(d, f_host, NQ, K, min(args.cpu_seconds, 10.0))
+                cpu = {"value": 1e6 / us, "unit": "cell-evals/s", "cores": 1, "kind": "reference",
+                       "us_per_call": us,
+                       "sample": f"{n} calls of angular_first_collision_kernel_mex compiled unmodified (-O3 -mavx2 "
+                                 f"-mfma) on this f, one host thread, {dt:.1f} s"}
+            except Exception as e:
+                cpu = {"value": None, "unit": "cell-evals/s", "cores": None, "kind": "reference",
+                       "sample": f"unavailable: {e}"}
+        flops = op.flops_q
+        out = {
+            "metric": METRIC, "value": value, "unit": "cell-evals/s", "n_gpus": world, "steps": steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": 1e3 * total_s / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (one two-Maxwellian mixture, seeded)",
+            "config": {"workload": args.workload, "L": L, "K": K, "M": M, "cells_per_gpu": 1, "gamma": gamma,
+                       "n_g": op.n_g, "n_l": op.n_l, "n_slices": op.n_slices, "form": chosen,
+                       "R": f"reference quadrature (compute_rtensor_sumfac_mex, K_max = 3, pad 20): {SINGLE_OPERATOR}",
+                       "l2": "flushed (256 MB write) before every timed call",
+                       "parallelism": "one f per call; ranks are independent replicas"},
+            "us_per_call": {"device": per_form[chosen]["device_us"], "e2e_mex_host_call": e2e_us,
+                            "cpu_reference_1_thread": cpu.get("us_per_call") if cpu else None},
+            "forms": {**per_form, "max_rel_err_vs_exact": errs, "chosen": chosen},
+            "host_calls": host_us,
+            "parity": {"mex_fast_vs_reference_max_rel": err_mex, "exact_form_bitwise_equal_to_reference": exact_bitwise},
+            "floors_us": {"empty_launch_round_trip": floor_launch, "copies_of_one_f_round_trip": floor_copies},
+            "roofline": {
+                "bound": "latency", "kernel": f"one call in the {chosen} form ({per_form[chosen]['path']})",
+                "achieved": flops / t_dev / 1e12, "peak": None, "unit": "TFLOP/s", "frac": None, "traffic": None,
+                "note": "one f is 71 kFLOP and 1.6 KB: the call is bound by launch and copy latency, not by FP64 "
+                        "throughput or HBM; floors_us gives the latency floors measured in this run",
+                "algorithmic_flop_per_call": flops,
+            },
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * 1e6 / e2e_us, "unit": "cell-evals/s", "h2d_bytes_per_step": 2 * M * 8,
+                    "d2h_bytes_per_step": M * 8,
+                    "us_per_call": e2e_us,
+                    "path": "cf_angular_first's route (cf_contract_host, form af, one cell) on pageable column-major "
+                            "arrays, mean host wall time of back-to-back calls timed in C (cf_time_contract_host); "
+                            f"f and Q_in travel by {host_us['cf_angular_first']['route']}"},
+            "gpu_launches": int(round(per_form[chosen]["launches_per_call"] * steps)),
+            "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    op.close()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return out
+
+
+def cpu_reference_single_us(d, f_host, NQ, K, target_seconds):
+    """µs per call of the reference's compiled angular_first on one host thread (a C loop of calls)."""
+    from oracle.reference import Reference
+
+    ref = Reference("fast")
+    lab, vals, ic, R = d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"], d["R"]
+    per = 2048  # calls per batch (1.6 MB of f)
+    f = np.asfortranarray(np.repeat(f_host.T[:, :, None], per, axis=2))
+    Qc = np.zeros_like(f, order="F")
+    n, dt = 0, 0.0
+    while dt < target_seconds:
+        t = time.perf_counter()
+        ref.batch("af", Qc, f, lab, vals, ic, R, NQ, K, nthreads=1)
+        dt += time.perf_counter() - t
+        n += per
+    return 1e6 * dt / n, n, dt
+
+
+def run_reference_single(args):
+    """Reference arm of the single-f workload: its compiled angular_first, one call per step, one thread."""
+    if int(os.environ.get("RANK", "0")) != 0:
+        return None
+    from oracle.reference import reference_available
+
+    if not reference_available("fast"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_fast.so not built"}), flush=True)
+        return None
+    L, K, _, gamma = WORKLOADS[args.workload]
+    d = load_single_operator()
+    NQ = (L + 1) ** 2
+    f_host = single_cell(K, L, rank_seed(args.seed, 0))
+    steps = max(args.steps, 50)
+    cpu_reference_single_us(d, f_host, NQ, K, 0.2)  # warm-up
+    us, n, dt = cpu_reference_single_us(d, f_host, NQ, K, min(args.cpu_seconds, 10.0))
+    value = 1e6 / us
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "cell-evals/s", "n_gpus": 1,
+        "steps": steps, "warmup": max(args.warmup, 3), "ms_per_step": us * 1e-3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (same f as the GPU arm)",
+        "config": {"workload": args.workload, "L": L, "K": K, "M": NQ * K, "gamma": gamma, "cells_per_step": 1},
+        "us_per_call": us,
+        "cpu_baseline": {"value": value, "unit": "cell-evals/s", "cores": 1, "kind": "reference",
+                         "sample": f"{n} calls of angular_first_collision_kernel_mex compiled unmodified on one f, "
+                                   f"one host thread, {dt:.1f} s"},
+        "e2e": {"value": value, "unit": "cell-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+    return out
+
+
 def main(argv=None):
     args = parse_args(argv)
     if args.impl == "reference":
-        if args.workload == "implicit_hs_l8_k8_b2048":
+        if args.workload == "single_g0_l4_k4":
+            run_reference_single(args)
+        elif args.workload == "implicit_hs_l8_k8_b2048":
             if int(os.environ.get("RANK", "0")) == 0:
                 print(json.dumps({"impl": "reference", "unavailable": "the reference has no implicit solver, "
                                   "Jacobian apply or preconditioner (it steps explicitly with a dense tensor)"}),
@@ -1115,6 +1398,8 @@ def main(argv=None):
         run_profile(args)
     elif args.workload == "ragged_hs_b16384":
         run_ragged(args)
+    elif args.workload == "single_g0_l4_k4":
+        run_single(args)
     else:
         run_ours(args)
     return 0

@@ -11,7 +11,7 @@ The contraction itself is hand-written CUDA for sm_100a in ``libcf_b200.so`` (C 
 ``include/cf_b200.h``); there is no CPU fallback.
 """
 from . import _lib, basis, geometry, quadrature  # noqa: F401
-from ._lib import CFError, launch_count  # noqa: F401
+from ._lib import CFError, few_route_last, launch_count  # noqa: F401
 from .mex import (  # noqa: F401
     angular_first_collision_kernel_mex,
     collision_jacobian_apply_mex,
@@ -22,5 +22,5 @@ from .operator import CollisionOperator  # noqa: F401
 
 __all__ = [
     "CFError", "CollisionOperator", "angular_first_collision_kernel_mex", "radial_first_collision_kernel_mex",
-    "collision_jacobian_apply_mex", "contract_batched", "geometry", "basis", "quadrature", "launch_count",
+    "collision_jacobian_apply_mex", "contract_batched", "geometry", "basis", "quadrature", "launch_count", "few_route_last",
 ]

@@ -30,7 +30,7 @@ FORMS = {"af": FORM_AF, "rf": FORM_RF, "af_exact": FORM_AF_EXACT, "rf_exact": FO
 
 # Every symbol the header declares; the tests check that the library exports all of them.
 EXPORTS = [
-    "cf_angular_first", "cf_radial_first", "cf_contract_host", "cf_jacobian_apply_host",
+    "cf_angular_first", "cf_radial_first", "cf_contract_host", "cf_time_contract_host", "cf_jacobian_apply_host",
     "cf_plan_create", "cf_plan_destroy", "cf_plan_get_info", "cf_plan_workspace_size",
     "cf_q_device", "cf_q_device_ws", "cf_jv_device", "cf_q_device_noalloc", "cf_plan_stream_selftest",
     "cf_ragged_create", "cf_ragged_destroy", "cf_ragged_q", "cf_ragged_graph_launch", "cf_ragged_q_resident",
@@ -40,7 +40,7 @@ EXPORTS = [
     "cf_mlp_create", "cf_mlp_destroy", "cf_mlp_num_params", "cf_mlp_copy", "cf_mlp_forward", "cf_mlp_backward",
     "cf_mlp_adam_step", "cf_precond_probe_loss", "cf_precond_assemble",
     "cf_pack_cells", "cf_unpack_cells", "cf_q_tiled", "cf_jv_tiled", "cf_plan_set_kernel_path", "cf_fp64_fma_peak",
-    "cf_status_string", "cf_last_error", "cf_launch_count", "cf_version",
+    "cf_status_string", "cf_last_error", "cf_launch_count", "cf_few_route_last", "cf_version",
 ]
 
 
@@ -57,7 +57,8 @@ class PlanInfo(C.Structure):
         ("device_bytes", C.c_int64), ("last_path", C.c_int32), ("reserved", C.c_int32),
     ]
 
-PATH_NAMES = {0: "none", 1: "gather", 2: "tile", 3: "pair", 4: "pair_l1", 5: "pair_split", 6: "tile_mma", 7: "bf16_mma", 8: "tile_quarter"}
+PATH_NAMES = {0: "none", 1: "gather", 2: "tile", 3: "pair", 4: "pair_l1", 5: "pair_split", 6: "tile_mma", 7: "bf16_mma", 8: "tile_quarter",
+              9: "few"}
 
 _DP = C.POINTER(C.c_double)
 
@@ -94,6 +95,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_angular_first.argtypes = [_D] + op
     lib.cf_radial_first.argtypes = [_D] + op
     lib.cf_contract_host.argtypes = [_D, _D, _I64, _D, _D, _D, _D, _I64, _I32, _I32, _I32, _I32]
+    lib.cf_time_contract_host.argtypes = [_I64, _D, _D, _D, _I64, _D, _D, _D, _D, _I64, _I32, _I32, _I32, _I32]
     lib.cf_jacobian_apply_host.argtypes = [_D, _D, _D, _I64, _D, _D, _D, _D, _I64, _I32, _I32, _I32, _I32]
     lib.cf_plan_create.argtypes = [C.POINTER(C.c_void_p), _D, _D, _D, _D, _I64, _I32, _I32, _I32, _I32]
     lib.cf_plan_destroy.argtypes = [C.c_void_p]
@@ -139,6 +141,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_status_string.argtypes = [C.c_int]
     lib.cf_last_error.restype = C.c_char_p
     lib.cf_launch_count.restype = C.c_int64
+    lib.cf_few_route_last.restype = C.c_int
     lib.cf_version.restype = C.c_char_p
     if path is None:
         _lib = lib
@@ -153,6 +156,11 @@ def check(status: int) -> None:
 
 def launch_count() -> int:
     return int(load().cf_launch_count())
+
+
+def few_route_last() -> str:
+    """How the calling thread's last host call of at most 8 cells moved its data."""
+    return {0: "none", 1: "parameter block", 2: "copies"}[int(load().cf_few_route_last())]
 
 
 def version() -> str:

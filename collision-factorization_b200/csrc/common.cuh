@@ -43,6 +43,9 @@ struct DevOp {
     int n_l;
 };
 
+// Batches of at most this many cells take the few-cell kernel (few_kernels.cuh).
+constexpr int kFewCells = 8;
+
 // Synchronisation words of the streamed tile kernel (tile_kernels.cuh, af_tile_stream_kernel).
 struct StreamSync {
     const int* ready;  // [n_chunks] device; == epoch once chunk c's f and Q are in

@@ -1,5 +1,6 @@
 // inst.cuh -- the body of one per-K translation unit (included by inst_k<K>.cu with CF_K defined).
 #pragma once
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -9,6 +10,7 @@
 #include "pair_kernels.cuh"
 #include "mma_kernels.cuh"
 #include "bf16_kernels.cuh"
+#include "few_kernels.cuh"
 
 namespace cf {
 
@@ -271,11 +273,74 @@ static LaunchResult launch_rf(const LaunchArgs& a) {
     return {e == cudaSuccess ? 0 : 5, 1, e, PATH_GATHER};
 }
 
+// The few-cell kernel with f and Q_in (host arrays a.few_host_f, a.few_host_q) copied into its
+// parameter block; Q_out to a.q_cm.  A launch the driver refuses (status -1) leaves the caller to
+// take the copy route; the refusal is not sticky.
+template <int K, bool RF, int CAP>
+static LaunchResult launch_few_param(const LaunchArgs& a, dim3 grid, size_t smem, size_t need) {
+    static_assert(sizeof(FewPayload<CAP>) + sizeof(DevOp) + 16 <= 32764, "parameter block too large");
+    auto kern = af_few_param_kernel<K, RF, CAP>;
+    if (smem > 48 * 1024) {
+        int per_sm = 0;
+        const cudaError_t e = resident_ctas((const void*)kern, kFewWarps * 32, smem, &per_sm);
+        if (e != cudaSuccess) return {5, 0, e, PATH_FEW};
+        if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_FEW};
+    }
+    FewPayload<CAP> pay;
+    const size_t half = need / 2;
+    std::memcpy(pay.v, a.few_host_f, half * sizeof(double));
+    std::memcpy(pay.v + half, a.few_host_q, half * sizeof(double));
+    std::memset(pay.v + need, 0, (CAP - need) * sizeof(double));
+    kern<<<grid, kFewWarps * 32, smem, a.stream>>>(a.op, pay, (int)a.n_cells, a.q_cm);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return {-1, 0, cudaSuccess, PATH_FEW};
+    return {0, 1, cudaSuccess, PATH_FEW};
+}
+
+// Few-cell kernel on the cell-major arrays: one CTA per (q1 row, cell).  Status -1 where
+// it does not apply (more than kFewCells cells, the radial-first form above K = 8, or f of one cell
+// larger than the shared memory).
+template <int K, bool RF>
+static LaunchResult launch_few(const LaunchArgs& a) {
+    if constexpr (RF && K > 8) {
+        return {-1, 0, cudaSuccess, PATH_FEW};
+    } else {
+        if (a.n_cells > kFewCells || a.q_cm == nullptr || (a.f_cm == nullptr && a.few_host_f == nullptr))
+            return {-1, 0, cudaSuccess, PATH_FEW};
+        if (a.op.n_items == 0 || a.n_cells == 0) return {0, 0, cudaSuccess, PATH_FEW};
+        const size_t smem = sizeof(double) * (size_t)a.op.n_q * K;
+        if (smem + 256 + sizeof(double) * kFewWarps * K > a.max_smem) return {-1, 0, cudaSuccess, PATH_FEW};
+        const dim3 grid((unsigned)a.op.n_q, (unsigned)a.n_cells);
+        if (a.few_host_f) {
+            // f and Q_in ride in the parameter block: the smallest block that holds them
+            const size_t need = 2 * (size_t)a.n_cells * a.op.n_q * K;
+            if (need <= 512) return launch_few_param<K, RF, 512>(a, grid, smem, need);
+            if (need <= 2048) return launch_few_param<K, RF, 2048>(a, grid, smem, need);
+            if (need <= (size_t)kFewPayloadMax) return launch_few_param<K, RF, kFewPayloadMax>(a, grid, smem, need);
+            return {-1, 0, cudaSuccess, PATH_FEW};
+        }
+        auto kern = af_few_kernel<K, RF>;
+        if (smem > 48 * 1024) {
+            int per_sm = 0;
+            const cudaError_t e = resident_ctas((const void*)kern, kFewWarps * 32, smem, &per_sm);
+            if (e != cudaSuccess) return {5, 0, e, PATH_FEW};
+            if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_FEW};
+        }
+        kern<<<grid, kFewWarps * 32, smem, a.stream>>>(a.op, a.f_cm, a.q_cm);
+        const cudaError_t e = cudaGetLastError();
+        return {e == cudaSuccess ? 0 : 5, 1, e, PATH_FEW};
+    }
+}
+
 // Warps per CTA of the tile kernel (registers: 16 warps leave 128 per thread).
 constexpr int tile_W(int K, bool jv) { return jv ? (K >= 8 ? 12 : 16) : 16; }
 
 template <int K>
 static LaunchResult launch_for_k(const LaunchArgs& a) {
+    if (a.few) {
+        if (a.exact || a.f32 || a.bf16 || a.what == OP_JV) return {-1, 0, cudaSuccess, PATH_FEW};
+        return a.what == OP_RF ? launch_few<K, true>(a) : launch_few<K, false>(a);
+    }
     if (a.ss) {
         if (a.what != OP_AF || a.exact || a.f32) return {8, 0, cudaSuccess, PATH_TILE};
         if constexpr (K % 2 == 0 && K <= 8) {

@@ -13,7 +13,8 @@ enum Op { OP_AF = 0, OP_RF = 1, OP_JV = 2 };
 // Kernel families for the angular-first / Jacobian forms.
 enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3, PATH_PAIR_L1 = 4, PATH_PAIR_SPLIT = 5, PATH_TILE_MMA = 6,
            PATH_BF16_MMA = 7 /* reported only: the BF16-split form's kernel */,
-           PATH_TILE4 = 8 /* reported only: the quarter-tile kernel, where the 16-cell tile does not fit */ };
+           PATH_TILE4 = 8 /* reported only: the quarter-tile kernel, where the 16-cell tile does not fit */,
+           PATH_FEW = 9 /* reported only: the few-cell kernel (a handful of cells per call) */ };
 
 struct LaunchArgs {
     DevOp op;
@@ -47,6 +48,12 @@ struct LaunchArgs {
     const StreamSync* ss = nullptr;
     const double* f_cm = nullptr;
     double* q_cm = nullptr;
+    // a handful of cells: the few-cell kernel on cell-major f_cm and q_cm (status -1 where it does not apply);
+    // with few_host_f / few_host_q set, f and Q_in are those host arrays, passed in the launch's
+    // parameter block, and q_cm receives Q_out
+    bool few = false;
+    const double* few_host_f = nullptr;
+    const double* few_host_q = nullptr;
 };
 
 // Status codes mirror cf_status: 0 ok, 5 CUDA error, 8 unsupported, 2 shape.

@@ -26,6 +26,7 @@ namespace {
 
 thread_local std::string g_last_error;
 std::atomic<int64_t> g_launches{0};
+thread_local int g_few_route = 0;  // cf_few_route_last()
 
 int fail(int status, const char* fmt, ...) {
     char buf[1024];
@@ -148,6 +149,10 @@ struct cf_plan {
     int* h_xsync_dev = nullptr;  // device alias of h_xsync
     int xepoch = 0;
     long long xwait_cycles = 0;
+    // few-cell host path: Q then f of up to kFewCells cells in mapped pinned memory, which the
+    // few-cell kernel reads and writes in place (no copy operations); h_few_dev is its device alias
+    double* h_few = nullptr;
+    double* h_few_dev = nullptr;
     std::mutex mu;
     // q2 <-> q3 folded operator (built on first use of CF_FORM_AF_SYM); fold_status != 0 if the
     // COO list is not symmetric in its last two indices
@@ -269,6 +274,7 @@ void free_plan_memory(cf_plan* p) {
     cudaFree(p->d_xready);
     if (p->h_xepoch) cudaFreeHost(p->h_xepoch);
     if (p->h_xsync) cudaFreeHost(p->h_xsync);
+    if (p->h_few) cudaFreeHost(p->h_few);
     if (p->stream) cudaStreamDestroy(p->stream);
     for (cudaStream_t& hs : p->host_streams)
         if (hs) cudaStreamDestroy(hs);
@@ -468,9 +474,13 @@ int* counter_for(const cf_plan* pc, cudaStream_t st) {
     return p->d_counter + slot;
 }
 
+// dispatch() with `few` set: the few-cell kernel does not apply (the caller takes another route)
+constexpr int kNoFew = -2;
+
 int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const double* vT, double* QT, int64_t B,
              cudaStream_t st, const float* fT32 = nullptr, bool bf16 = false, const StreamSync* ss = nullptr,
-             const double* f_cm = nullptr, double* q_cm = nullptr) {
+             const double* f_cm = nullptr, double* q_cm = nullptr, bool few = false,
+             const double* few_host_f = nullptr, const double* few_host_q = nullptr) {
     const int64_t nt = n_tiles_for(B);
     // The folded operator has about half the COO entries per slice of the plain one, and its tile
     // routine groups them by q2, so its Phi step is light next to the K^3 step; there the tile kernel
@@ -483,6 +493,9 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
     a.ss = ss;
     a.f_cm = f_cm;
     a.q_cm = q_cm;
+    a.few = few;
+    a.few_host_f = few_host_f;
+    a.few_host_q = few_host_q;
     cf::LaunchResult r{8, 0, cudaSuccess};
     switch (p->k) {
 #define CF_K(KK) \
@@ -493,6 +506,7 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
         default: return fail(CF_EUNSUPPORTED, "K = %d not built", p->k);
     }
     g_launches += r.launches;
+    if (few && r.status == -1) return kNoFew;
     if (r.status == CF_OK && r.launches > 0 && what != cf::OP_RF) {
         cf_plan* pm = const_cast<cf_plan*>(p);
         pm->last_path = r.path;
@@ -543,9 +557,23 @@ int launch_unpack(const cf_plan* p, const double* src, double* dst, int64_t B, c
 
 // Q_dev (cell-major) += op(f_dev[, v_dev]) using the tiled workspace ws (>= 2 or 3 tiled buffers).
 // The forms that run on the tile kernel skip the layout passes: the kernel reads f and updates Q in
-// the caller's cell-major arrays (the same per-row operations, so the same bits).
+// the caller's cell-major arrays (the same per-row operations, so the same bits).  So do the fast
+// FP64 Q forms on at most kFewCells cells, on the few-cell kernel (one launch).
 int get_sym(cf_plan* p, cf_plan** out);
 bool streamable(const cf_plan* p, const cf_plan* target, int what, bool exact, int f32);
+
+// The fast FP64 angular-first (plain or folded) or radial-first form of at most kFewCells cells on
+// the few-cell kernel; kNoFew where that kernel does not apply.  With host_f and host_q (host
+// arrays), f and Q_in travel in the launch's parameter block and Q_out goes to q; else Q is
+// updated in place in the device arrays f, q.
+int run_few(cf_plan* p, int what, bool exact, double* q, const double* f, int64_t B, cudaStream_t st, bool sym,
+            int f32, const double* host_f = nullptr, const double* host_q = nullptr) {
+    if (what == 2 || exact || f32 != 0 || B > kFewCells) return kNoFew;
+    cf_plan* target = p;
+    if (sym) CF_TRY(get_sym(p, &target));
+    return dispatch(target, what, false, nullptr, nullptr, nullptr, B, st, nullptr, false, nullptr, f, q, true, host_f,
+                    host_q);
+}
 
 int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_dev, const double* v_dev,
                int64_t B, void* ws, size_t ws_bytes, cudaStream_t st, bool sym = false, int f32 = 0) {
@@ -553,6 +581,10 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
     if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
     if (B == 0 || p->n_g == 0) return CF_OK;
     if (!q_dev || !f_dev || (what == 2 && !v_dev)) return fail(CF_EINVAL, "null device buffer");
+    {
+        const int r = run_few(p, what, exact, q_dev, f_dev, B, st, sym, f32);
+        if (r != kNoFew) return r;
+    }
     const size_t tb = tiled_bytes(p, B);
     const size_t need = tb * (what == 2 ? 3 : 2);
     if (ws_bytes < need) return fail(CF_EINVAL, "workspace of %zu bytes is smaller than %zu", ws_bytes, need);
@@ -1079,12 +1111,81 @@ int run_host_speculative(double* Q, const double* f, int64_t B, const double* la
     return st;
 }
 
+// A handful of cells on plan p from host arrays, one launch and one wait.  Where f and Q_in fit in
+// the launch's parameter block they travel there and the kernel writes Q_out to the plan's mapped
+// pinned staging; else they go up through the staging and a device buffer with two copies, and Q
+// comes back the same way.  With key_check set, p is a guess from the pointers of an earlier call,
+// and the operator's content hash is computed here while the kernel runs; on a mismatch Q is left
+// as it was and kRetry returned.
+int few_on_plan(cf_plan* p, int what, double* Q, const double* f, int64_t B, bool sym, const uint64_t* key_check,
+                const double* labels, const double* vals, const double* ic_map, const double* R) {
+    std::lock_guard<std::mutex> lk(p->mu);
+    DeviceGuard guard(p->device);
+    if (!guard.ok) return fail(CF_ENODEVICE, "cannot select device %d", p->device);
+    const size_t M = (size_t)p->n_q * p->k, nb = (size_t)B * M * sizeof(double);
+    if (!p->h_few) {
+        CF_CUDA(cudaHostAlloc((void**)&p->h_few, 2 * kFewCells * M * sizeof(double), cudaHostAllocMapped));
+        const cudaError_t e = cudaHostGetDevicePointer((void**)&p->h_few_dev, p->h_few, 0);
+        if (e != cudaSuccess) {
+            cudaFreeHost(p->h_few);
+            p->h_few = nullptr;
+            return fail(CF_ECUDA, "cudaHostGetDevicePointer: %s", cudaGetErrorString(e));
+        }
+    }
+    int st = run_few(p, what, false, p->h_few_dev, nullptr, B, p->stream, sym, 0, f, Q);
+    int route = 1;
+    if (st == kNoFew) {
+        route = 2;
+        // the copy route: pinned staging [Q | f] -> device buffer [Q | f] -> kernel -> staging
+        CF_TRY(ensure_io(p, 2 * nb));
+        std::memcpy(p->h_few, Q, nb);
+        std::memcpy(p->h_few + kFewCells * M, f, nb);
+        double* dq = p->d_io;
+        double* df = p->d_io + B * M;
+        CF_CUDA(cudaMemcpyAsync(dq, p->h_few, nb, cudaMemcpyHostToDevice, p->stream));
+        CF_CUDA(cudaMemcpyAsync(df, p->h_few + kFewCells * M, nb, cudaMemcpyHostToDevice, p->stream));
+        st = run_few(p, what, false, dq, df, B, p->stream, sym, 0);
+        if (st == CF_OK) CF_CUDA(cudaMemcpyAsync(p->h_few, dq, nb, cudaMemcpyDeviceToHost, p->stream));
+    }
+    if (st != CF_OK) {  // kNoFew included: the caller takes the ordinary route
+        cudaStreamSynchronize(p->stream);
+        return st;
+    }
+    const bool same = !key_check ||
+                      hash_operator(labels, vals, ic_map, R, p->n_g, (int64_t)p->k * p->k * p->k * p->n_l) == *key_check;
+    CF_CUDA(cudaStreamSynchronize(p->stream));
+    if (!same) return kRetry;
+    std::memcpy(Q, p->h_few, nb);
+    g_few_route = route;
+    return CF_OK;
+}
+
+// The fast angular-first (plain or folded) and radial-first forms of at most kFewCells cells from
+// host arrays; kNoFew where the few-cell kernel does not apply.
+int run_host_few(int what, double* Q, const double* f, int64_t B, const double* labels, const double* vals,
+                 const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k, bool sym) {
+    cf_plan* p = nullptr;
+    uint64_t key = 0;
+    if (n_g > 0 && labels && vals && ic_map && R && plan_by_pointers(&p, &key, labels, vals, ic_map, R, n_g, n_l, n_q, k)) {
+        const int st = few_on_plan(p, what, Q, f, B, sym, &key, labels, vals, ic_map, R);
+        if (st != kRetry) return st;
+    }
+    CF_TRY(cached_plan(&p, labels, vals, ic_map, R, n_g, n_l, n_q, k));
+    if (n_g == 0) return CF_OK;
+    return few_on_plan(p, what, Q, f, B, sym, nullptr, labels, vals, ic_map, R);
+}
+
 // Host-pointer contraction: upload, run, download.  what: 0 AF, 1 RF, 2 JV.
 int run_host(int what, bool exact, double* Q, const double* f, const double* v, int64_t B, const double* labels,
              const double* vals, const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
              int32_t k, bool sym = false, int f32 = 0) {
     if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
     if (!Q || !f || (what == 2 && !v)) return fail(CF_EINVAL, "null host buffer");
+    g_few_route = 0;
+    if (B >= 1 && B <= kFewCells && what != 2 && !exact && f32 == 0) {
+        const int r = run_host_few(what, Q, f, B, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym);
+        if (r != kNoFew) return r;
+    }
     if (what == 0 && !exact && f32 == 0 && B >= 2 * kHostChunkMin) {
         const int r = run_host_speculative(Q, f, B, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym);
         if (r != kRetry) return r;
@@ -1206,6 +1307,20 @@ int cf_contract_host(double* Q, const double* f, int64_t b, const double* labels
     const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
     return run_host(what, exact, Q, f, nullptr, b, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym, f32);
+}
+
+int cf_time_contract_host(int64_t n_calls, double* seconds, double* Q, const double* f, int64_t b,
+                          const double* labels, const double* vals, const double* ic_map, const double* R,
+                          int64_t n_g, int32_t n_l, int32_t n_q, int32_t k, int32_t form) {
+    if (!seconds || n_calls < 0) return fail(CF_EINVAL, "null seconds or negative n_calls");
+    *seconds = 0.0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int64_t i = 0; i < n_calls; ++i) {
+        const int st = cf_contract_host(Q, f, b, labels, vals, ic_map, R, n_g, n_l, n_q, k, form);
+        if (st != CF_OK) return st;
+    }
+    *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return CF_OK;
 }
 
 int cf_jacobian_apply_host(double* out, const double* f, const double* v, int64_t b, const double* labels,
@@ -1469,6 +1584,7 @@ const char* cf_status_string(int status) {
 
 const char* cf_last_error(void) { return g_last_error.c_str(); }
 int64_t cf_launch_count(void) { return g_launches.load(); }
+int cf_few_route_last(void) { return g_few_route; }
 const char* cf_version(void) { return "cf_b200 0.1 (sm_100a)"; }
 
 }  // extern "C"

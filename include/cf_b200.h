@@ -112,6 +112,13 @@ int cf_contract_host(double* Q, const double* f, int64_t b, const double* labels
                      const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
                      int32_t k, int32_t form);
 
+/* n_calls back-to-back calls of cf_contract_host with these arguments (each adds into Q), timed on
+ * the host clock in C: *seconds = their total wall time.  A latency benchmark of the host entry point
+ * without a foreign-function caller's own per-call cost; stops at the first failing call. */
+int cf_time_contract_host(int64_t n_calls, double* seconds, double* Q, const double* f, int64_t b,
+                          const double* labels, const double* vals, const double* ic_map, const double* R,
+                          int64_t n_g, int32_t n_l, int32_t n_q, int32_t k, int32_t form);
+
 /* J(f).v = Q(v,f) + Q(f,v), accumulated into out; no counterpart in the reference (the reference
  * linearises only densely at equilibrium, tutorial_collisions_spectral_properties.m:43).  Host pointers,
  * [N_Q x K x B]. */
@@ -338,6 +345,10 @@ const char* cf_status_string(int status);
 const char* cf_last_error(void);
 /* Number of CUDA kernel launches this library has issued in this process. */
 int64_t cf_launch_count(void);
+/* How the last host call of at most 8 cells on this thread moved its data: 0 it did not take the
+ * few-cell kernel, 1 f and Q_in in the launch's parameter block (Q_out written to mapped pinned
+ * memory), 2 copies through pinned staging and a device buffer. */
+int cf_few_route_last(void);
 /* Library version string. */
 const char* cf_version(void);
 
