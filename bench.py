@@ -1258,7 +1258,7 @@ def run_single(args):
     den = max(np.abs(Qd["af_exact"]).max(), 1e-300)
     errs = {form: float(np.abs(Qd[form] - Qd["af_exact"]).max() / den) for form in Qd}
     ok = [fm for fm in ("af", "af_sym", "af_exact") if errs[fm] <= 1e-10]
-    chosen = min(ok, key=lambda fm: per_form[fm]["device_us"])
+    chosen = min(ok, key=lambda fm: per_form[fm]["device_us_mean"])
     t_dev = per_form[chosen]["device_us_mean"] * 1e-6
     value, total_s = weak_rate(world, 1, steps, t_dev * steps)
     e2e_us = host_us["cf_angular_first"]["c_mean_us"]
@@ -1286,7 +1286,8 @@ def run_single(args):
                        "R": f"reference quadrature (compute_rtensor_sumfac_mex, K_max = 3, pad 20): {SINGLE_OPERATOR}",
                        "l2": "flushed (256 MB write) before every timed call",
                        "parallelism": "one f per call; ranks are independent replicas"},
-            "us_per_call": {"device": per_form[chosen]["device_us"], "e2e_mex_host_call": e2e_us,
+            "us_per_call": {"device": per_form[chosen]["device_us_mean"], "device_median": per_form[chosen]["device_us"],
+                            "e2e_mex_host_call": e2e_us,
                             "cpu_reference_1_thread": cpu.get("us_per_call") if cpu else None},
             "forms": {**per_form, "max_rel_err_vs_exact": errs, "chosen": chosen},
             "host_calls": host_us,
@@ -1316,6 +1317,40 @@ def run_single(args):
 
         dist.destroy_process_group()
     return out
+
+
+def run_profile_single(args):
+    """For ncu: the single-f workload's calls only, steps + 1 of each: the MEX-compatible host call
+    (cf_angular_first: af_few_param_kernel) and the device entry point in the folded form
+    (af_few_kernel)."""
+    import ctypes
+
+    import torch
+
+    import cf_b200
+    from cf_b200 import _lib
+
+    L, K, _, _ = WORKLOADS[args.workload]
+    NQ = (L + 1) ** 2
+    d = load_single_operator()
+    lab, vals = np.asfortranarray(d["labels_sorted"]), np.ascontiguousarray(d["vals_sorted"])
+    ic, R = np.ascontiguousarray(d["ic_map_sorted"]), np.asfortranarray(d["R"])
+    f_host = single_cell(K, L, args.seed)
+    fq, Qh = np.asfortranarray(f_host.T), np.zeros((NQ, K), order="F")
+    lib = _lib.load()
+    Dp = ctypes.POINTER(ctypes.c_double)
+    opargs = (lab.ctypes.data_as(Dp), vals.ctypes.data_as(Dp), ic.ctypes.data_as(Dp), R.ctypes.data_as(Dp),
+              lab.shape[0], R.size // K ** 3, NQ, K)
+    for _ in range(args.steps + 1):
+        _lib.check(lib.cf_angular_first(Qh.ctypes.data_as(Dp), fq.ctypes.data_as(Dp), *opargs))
+    op = cf_b200.CollisionOperator(lab, vals, ic, R, NQ, K)
+    f = torch.from_numpy(f_host.reshape(1, K, NQ).copy()).cuda()
+    Q = torch.zeros_like(f)
+    for _ in range(args.steps + 1):
+        op.q(f, out=Q, form="af_sym")
+    torch.cuda.synchronize()
+    print(json.dumps({"profile": args.workload, "route": _lib.few_route_last(), "Q_abs_max": float(np.abs(Qh).max())}))
+    op.close()
 
 
 def cpu_reference_single_us(d, f_host, NQ, K, target_seconds):
@@ -1394,6 +1429,8 @@ def main(argv=None):
         run_implicit(args)
     elif args.profile and args.workload == "ragged_hs_b16384":
         run_profile_ragged(args)
+    elif args.profile and args.workload == "single_g0_l4_k4":
+        run_profile_single(args)
     elif args.profile:
         run_profile(args)
     elif args.workload == "ragged_hs_b16384":
