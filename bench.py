@@ -114,10 +114,23 @@ def make_operator(L: int, K: int, gamma: float, seed: int):
     return geo, R, r_source
 
 
-def make_cells(L: int, K: int, B: int, seed: int):
+# workloads whose cells are anisotropic bi-Maxwellians (T_par / T_perp ~ U[0.5, 2]) rather than
+# perturbed Maxwellians
+BIMAXWELLIAN = {"hs_l16_k12_b1024"}
+
+
+def make_cells(L: int, K: int, B: int, seed: int, workload: str | None = None):
     from cf_b200 import workloads
 
+    if workload in BIMAXWELLIAN:
+        return workloads.bimaxwellian_cells(K, L, B, seed=seed)
     return workloads.maxwellian_cells(K, L, B, seed=seed, amplitude=1e-2, decay=0.6)
+
+
+def cells_description(workload: str) -> str:
+    if workload in BIMAXWELLIAN:
+        return "synthetic (seeded bi-Maxwellians, T_par / T_perp ~ U[0.5, 2], unit density and temperature)"
+    return "synthetic (seeded Maxwellians + N(0,1) exp(-0.6(k+l)) perturbation, amplitude 1e-2)"
 
 
 # --------------------------------------------------------------------------------------------
@@ -242,29 +255,57 @@ def rank_seed(seed: int, rank: int) -> int:
 # --------------------------------------------------------------------------------------------
 # CPU baseline: the reference's own kernel, compiled unmodified, once per cell on host cores
 # --------------------------------------------------------------------------------------------
-def cpu_reference_rate(geo, R, cells, K, target_seconds: float, nthreads: int = 0):
+def cpu_reference_rate(geo, R, cells, K, target_seconds: float, nthreads: int = 0, kernel: str = "af",
+                       reps: int = 5):
+    """Cells per second of the reference's kernel, called once per cell under an OpenMP loop over
+    cells: the median of `reps` repetitions, each about target_seconds / reps long.  Returns
+    (median rate, cells per rep, total seconds, threads)."""
     from oracle.reference import Reference
 
     ref = Reference("fast")
     nthreads = nthreads or ref.num_threads()
     NQ = geo.n_q
-    # calibrate with one cell per thread
+    # calibrate: grow a batch (a multiple of the thread count) until it takes 50 ms or more
     n0 = max(nthreads, 1)
-    f0 = np.asfortranarray(cells[:n0].transpose(2, 1, 0))
-    Q0 = np.zeros_like(f0, order="F")
-    t = time.perf_counter()
-    ref.batch("af", Q0, f0, geo.labels, geo.vals, geo.ic_map, R, NQ, K, nthreads=nthreads)
-    dt = time.perf_counter() - t
-    per_round = max(dt, 1e-6)
-    rounds = max(1, int(target_seconds / per_round))
-    n = n0 * rounds
+    while True:
+        idx = np.arange(n0) % cells.shape[0]
+        f0 = np.asfortranarray(cells[idx].transpose(2, 1, 0))
+        Q0 = np.zeros_like(f0, order="F")
+        t = time.perf_counter()
+        ref.batch(kernel, Q0, f0, geo.labels, geo.vals, geo.ic_map, R, NQ, K, nthreads=nthreads)
+        dt0 = time.perf_counter() - t
+        if dt0 >= 0.05 or n0 >= (1 << 20):
+            break
+        n0 *= 4
+    per_cell = max(dt0, 1e-6) / n0
+    n = max(nthreads, int(target_seconds / reps / per_cell) // max(nthreads, 1) * max(nthreads, 1))
     idx = np.arange(n) % cells.shape[0]
     f = np.asfortranarray(cells[idx].transpose(2, 1, 0))
-    Q = np.zeros_like(f, order="F")
-    t = time.perf_counter()
-    ref.batch("af", Q, f, geo.labels, geo.vals, geo.ic_map, R, NQ, K, nthreads=nthreads)
-    dt = time.perf_counter() - t
-    return n / dt, n, dt, nthreads
+    rates, total = [], 0.0
+    for _ in range(reps):
+        Q = np.zeros_like(f, order="F")
+        t = time.perf_counter()
+        ref.batch(kernel, Q, f, geo.labels, geo.vals, geo.ic_map, R, NQ, K, nthreads=nthreads)
+        dt = time.perf_counter() - t
+        total += dt
+        rates.append(n / dt)
+    return statistics.median(rates), n, total, nthreads
+
+
+def cpu_baseline_block(geo, R, cells, K, target_seconds: float) -> dict:
+    """The reference's angular_first on all host cores (the baseline), on one core, and its
+    radial_first and naive kernels on all cores, each the median of 5 repetitions."""
+    rate, n, dt, thr = cpu_reference_rate(geo, R, cells, K, target_seconds)
+    one, n1, dt1, _ = cpu_reference_rate(geo, R, cells, K, max(target_seconds / 3, 1.0), nthreads=1)
+    out = {"value": rate, "unit": "cell-evals/s", "cores": thr, "kind": "reference",
+           "sample": f"5 x {n} cells of this workload through angular_first_collision_kernel_mex compiled unmodified "
+                     f"(-O3 -mavx2 -mfma), one call per cell under an OpenMP loop over cells, {dt:.1f} s; median",
+           "one_thread": {"value": one, "sample": f"5 x {n1} cells on one thread, {dt1:.1f} s; median"}}
+    for kernel in ("rf", "naive"):
+        r, nk, dk, _ = cpu_reference_rate(geo, R, cells, K, max(target_seconds / 4, 1.0), kernel=kernel)
+        name = {"rf": "radial_first_collision_kernel_mex", "naive": "naive_collision_kernel_mex"}[kernel]
+        out[kernel] = {"value": r, "sample": f"5 x {nk} cells through {name} on {thr} threads, {dk:.1f} s; median"}
+    return out
 
 
 # --------------------------------------------------------------------------------------------
@@ -283,7 +324,7 @@ def run_ours(args):
     geo, R, r_source = make_operator(L, K, gamma, args.seed)
     NQ = geo.n_q
     M = NQ * K
-    cells = make_cells(L, K, B, seed=rank_seed(args.seed, rank))
+    cells = make_cells(L, K, B, seed=rank_seed(args.seed, rank), workload=args.workload)
     op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, NQ, K, device=local)
     op.set_kernel_path(args.path)
     lib = _lib.load()
@@ -377,7 +418,9 @@ def run_ours(args):
     op.set_kernel_path(args.path)
     exact_ms = timed(lambda: step("af_exact"), max(2, args.steps // 4)) if K <= 8 else None
     # J(f).v (the Jacobian apply of the implicit solves) on the same cells: fast, folded, exact order
-    v_dev = torch.from_numpy(np.random.default_rng(args.seed + 5).standard_normal(cells.shape)).to(dev)
+    v_np = np.random.default_rng(args.seed + 5).standard_normal(cells.shape)
+    v_np /= np.linalg.norm(v_np.reshape(B, -1), axis=1)[:, None, None]  # unit norm per cell
+    v_dev = torch.from_numpy(v_np).to(dev)
     Jout = torch.zeros_like(f)
     jv_ms = {}
     for name, kw in (("jv", {}), ("jv_folded", {"folded": True}), ("jv_exact", {"exact": True})):
@@ -440,11 +483,7 @@ def run_ours(args):
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             try:
-                rate, n, dt, thr = cpu_reference_rate(geo, R, cells, K, args.cpu_seconds)
-                cpu = {"value": rate, "unit": "cell-evals/s", "cores": thr, "kind": "reference",
-                       "sample": f"{n} cells of this workload through angular_first_collision_kernel_mex compiled "
-                                 f"unmodified (-O3 -mavx2 -mfma), one call per cell under an OpenMP loop over "
-                                 f"cells, {dt:.1f} s"}
+                cpu = cpu_baseline_block(geo, R, cells, K, args.cpu_seconds)
             except Exception as e:  # the baseline is reported, not required
                 cpu = {"value": None, "unit": "cell-evals/s", "cores": None, "kind": "reference",
                        "sample": f"unavailable: {e}"}
@@ -464,7 +503,7 @@ def run_ours(args):
             "scaling": "weak",
             "vs_baseline": None,
             "dtype": "f64",
-            "data": "synthetic (seeded Maxwellians + N(0,1) exp(-0.6(k+l)) perturbation, amplitude 1e-2)",
+            "data": cells_description(args.workload),
             "config": {
                 "workload": args.workload, "L": L, "K": K, "M": M, "cells_per_gpu": B, "gamma": gamma,
                 "n_g": op.n_g, "n_l": op.n_l, "n_slices": op.n_slices,
@@ -610,7 +649,7 @@ def run_reference(args):
     nthreads = ref.num_threads()
     # size one step so that warmup + steps fit in about two minutes
     budget = 120.0 / max(args.steps + args.warmup, 1)
-    cells_all = make_cells(L, K, min(B, 8 * nthreads), seed=args.seed)
+    cells_all = make_cells(L, K, min(B, 8 * nthreads), seed=args.seed, workload=args.workload)
     f0 = np.asfortranarray(cells_all[:nthreads].transpose(2, 1, 0))
     Q0 = np.zeros_like(f0, order="F")
     t = time.perf_counter()
@@ -940,7 +979,7 @@ def run_ragged(args):
                 for b, (L, K) in enumerate(RAGGED_BUCKETS):
                     rate, n, dt, thr = cpu_reference_rate(geos[b], Rs[b], fs_np[b], K, per)
                     t_mix += counts[b] / rate
-                    desc.append(f"{n} cells of L={L} K={K} in {dt:.1f} s")
+                    desc.append(f"5 x {n} cells of L={L} K={K} in {dt:.1f} s (median)")
                 cpu = {"value": B / t_mix, "unit": "cell-evals/s", "cores": thr, "kind": "reference",
                        "sample": "angular_first_collision_kernel_mex compiled unmodified (-O3 -mavx2 -mfma), one call "
                                  "per cell under an OpenMP loop, per bucket: " + "; ".join(desc)
