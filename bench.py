@@ -774,7 +774,7 @@ def run_profile(args):
     op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K, device=0)
     op.set_kernel_path(args.path)
     lib = _lib.load()
-    f = torch.from_numpy(make_cells(L, K, B, seed=args.seed)).cuda()
+    f = torch.from_numpy(make_cells(L, K, B, seed=args.seed, workload=args.workload)).cuda()
     M = geo.n_q * K
     fT = torch.zeros(((B + 31) // 32) * 32 * M, dtype=torch.float64, device="cuda")
     QT = torch.zeros_like(fT)
