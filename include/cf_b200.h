@@ -107,7 +107,11 @@ int cf_radial_first(double* Q, const double* f, const double* labels, const doub
  * automatic kernel order; either fast form with kernel path 2) are streamed: one launch over the
  * whole batch starts as soon as the first chunk of cells is on the device and hands each chunk back
  * as soon as it is final, with the same result bits as the device entry points.  Other forms cut
- * the batch into chunks that go up, are contracted and come back on three streams. */
+ * the batch into chunks that go up, are contracted and come back on three streams.  Up to 8 cells
+ * (one f per call, as the reference's MEX is called), the fast forms CF_FORM_AF, CF_FORM_AF_SYM and
+ * CF_FORM_RF (K <= 8 for RF) are one launch of the few-cell kernel, with f and Q_in passed in the
+ * launch's parameter block when they fit (2 B N_Q K <= 3968 doubles); cf_angular_first and
+ * cf_radial_first take the same route. */
 int cf_contract_host(double* Q, const double* f, int64_t b, const double* labels, const double* vals,
                      const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q,
                      int32_t k, int32_t form);
