@@ -156,3 +156,27 @@ def test_few_cell_host_call_sees_an_operator_changed_in_place(cuda_available):
     changed = host()
     assert np.array_equal(changed, device())
     assert not np.array_equal(changed, first)
+
+
+def test_time_contract_host_runs_the_calls_it_times(cuda_available):
+    """cf_time_contract_host: n back-to-back cf_contract_host calls, each adding into Q."""
+    import ctypes
+
+    import cf_b200
+    from cf_b200 import _lib
+
+    d = load_op("cfg1_k3_l4_g0")
+    NQ, K = d["NQ"], d["K"]
+    lab = np.asfortranarray(d["labels_sorted"])
+    vals, ic = np.ascontiguousarray(d["vals_sorted"]), np.ascontiguousarray(d["ic_map_sorted"])
+    R, f = np.asfortranarray(d["R"]), np.asfortranarray(d["f"])
+    Q = np.zeros((NQ, K), order="F")
+    Dp = ctypes.POINTER(ctypes.c_double)
+    secs = ctypes.c_double(-1.0)
+    st = _lib.load().cf_time_contract_host(5, ctypes.byref(secs), Q.ctypes.data_as(Dp), f.ctypes.data_as(Dp), 1,
+                                           lab.ctypes.data_as(Dp), vals.ctypes.data_as(Dp), ic.ctypes.data_as(Dp),
+                                           R.ctypes.data_as(Dp), lab.shape[0], R.size // K ** 3, NQ, K,
+                                           _lib.FORMS["af"])
+    assert st == 0 and secs.value > 0.0
+    assert cf_b200.few_route_last() == "parameter block"
+    assert normwise_err(Q, 5 * d["Q_af"]) <= TOL_FP64
