@@ -637,8 +637,11 @@ __global__ void __launch_bounds__(W * 32, 1)
         if (ss.done) __threadfence();
         __syncthreads();
         if (tid == 0 && ss.done) {
-            const int c_ht = min(ss.ht_per_chunk, sc.n_ht - chunk * ss.ht_per_chunk);
-            const int c_units = c_ht * sc.split;  // the streamed schedule splits every half-tile
+            // units of this chunk: its half-tiles below n_whole are one unit each, the rest `split`
+            const int h0 = chunk * ss.ht_per_chunk;
+            const int c_ht = min(ss.ht_per_chunk, sc.n_ht - h0);
+            const int c_whole = max(0, min(c_ht, sc.n_whole - h0));
+            const int c_units = c_whole + (c_ht - c_whole) * sc.split;
             if (atomicAdd(ss.done + chunk, 1) == c_units - 1) {
                 __threadfence_system();
                 *reinterpret_cast<volatile int*>(ss.host_done + chunk) = ss.epoch;
