@@ -180,3 +180,31 @@ def test_time_contract_host_runs_the_calls_it_times(cuda_available):
     assert st == 0 and secs.value > 0.0
     assert cf_b200.few_route_last() == "parameter block"
     assert normwise_err(Q, 5 * d["Q_af"]) <= TOL_FP64
+
+
+def test_rows_without_slices_pass_through(cuda_available, oracle_lib):
+    """One COO entry: every other row of Q has no slice and must come back as it went in, from the
+    host call (f and Q_in in the parameter block, Q_out a separate buffer) and the device call."""
+    import torch
+
+    import cf_b200
+
+    d = load_op("cfg1_k3_l4_g0")
+    NQ, K = d["NQ"], d["K"]
+    lab1 = np.asfortranarray(d["labels_sorted"][7:8])
+    vals1, ic1 = d["vals_sorted"][7:8], d["ic_map_sorted"][7:8]
+    q0 = np.asfortranarray(np.random.default_rng(5).standard_normal((NQ, K)))
+    Qo = q0.copy(order="F")
+    oracle_lib.af(Qo, d["f"], lab1, vals1, ic1, d["R"], NQ, K)
+    Qh = q0.copy(order="F")
+    cf_b200.angular_first_collision_kernel_mex(Qh, d["f"], lab1, vals1, ic1, d["R"], NQ, K)
+    assert cf_b200.few_route_last() == "parameter block"
+    q1 = int(lab1[0, 0]) - 1
+    others = [q for q in range(NQ) if q != q1]
+    assert np.array_equal(Qh[others], q0[others])
+    assert normwise_err(Qh, Qo) <= TOL_FP64
+    op = cf_b200.CollisionOperator(lab1, vals1, ic1, d["R"], NQ, K)
+    Qd = torch.from_numpy(np.ascontiguousarray(q0.T).reshape(1, K, NQ).copy()).cuda()
+    op.q(torch.from_numpy(np.ascontiguousarray(d["f"].T).reshape(1, K, NQ).copy()).cuda(), out=Qd, form="af")
+    assert np.array_equal(Qd.cpu().numpy().reshape(K, NQ).T, Qh)
+    op.close()
