@@ -332,13 +332,66 @@ static LaunchResult launch_few(const LaunchArgs& a) {
     }
 }
 
+// The exact form of the few-cell kernel (one warp per (row, cell)), in place on device arrays or
+// with f and Q_in in the parameter block as launch_few does.  Status -1 where it does not apply.
+template <int K, int CAP>
+static LaunchResult launch_few_exact_param(const LaunchArgs& a, dim3 grid, size_t smem, size_t need) {
+    auto kern = af_few_exact_param_kernel<K, CAP>;
+    if (smem > 48 * 1024) {
+        int per_sm = 0;
+        const cudaError_t e = resident_ctas((const void*)kern, 32, smem, &per_sm);
+        if (e != cudaSuccess) return {5, 0, e, PATH_FEW};
+        if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_FEW};
+    }
+    FewPayload<CAP> pay;
+    const size_t half = need / 2;
+    std::memcpy(pay.v, a.few_host_f, half * sizeof(double));
+    std::memcpy(pay.v + half, a.few_host_q, half * sizeof(double));
+    std::memset(pay.v + need, 0, (CAP - need) * sizeof(double));
+    kern<<<grid, 32, smem, a.stream>>>(a.op, pay, (int)a.n_cells, a.q_cm);
+    if (cudaGetLastError() != cudaSuccess) return {-1, 0, cudaSuccess, PATH_FEW};
+    return {0, 1, cudaSuccess, PATH_FEW};
+}
+
+template <int K>
+static LaunchResult launch_few_exact(const LaunchArgs& a) {
+    if constexpr (K > 8) {
+        return {-1, 0, cudaSuccess, PATH_FEW};
+    } else {
+        if (a.n_cells > kFewCells || a.q_cm == nullptr || (a.f_cm == nullptr && a.few_host_f == nullptr))
+            return {-1, 0, cudaSuccess, PATH_FEW};
+        if (a.op.n_items == 0 || a.n_cells == 0) return {0, 0, cudaSuccess, PATH_FEW};
+        const size_t smem = sizeof(double) * ((size_t)a.op.n_q * K + K * K);
+        if (smem + 256 > a.max_smem) return {-1, 0, cudaSuccess, PATH_FEW};
+        const dim3 grid((unsigned)a.op.n_q, (unsigned)a.n_cells);
+        if (a.few_host_f) {
+            const size_t need = 2 * (size_t)a.n_cells * a.op.n_q * K;
+            if (need <= 512) return launch_few_exact_param<K, 512>(a, grid, smem, need);
+            if (need <= 2048) return launch_few_exact_param<K, 2048>(a, grid, smem, need);
+            if (need <= (size_t)kFewPayloadMax) return launch_few_exact_param<K, kFewPayloadMax>(a, grid, smem, need);
+            return {-1, 0, cudaSuccess, PATH_FEW};
+        }
+        auto kern = af_few_exact_kernel<K>;
+        if (smem > 48 * 1024) {
+            int per_sm = 0;
+            const cudaError_t e = resident_ctas((const void*)kern, 32, smem, &per_sm);
+            if (e != cudaSuccess) return {5, 0, e, PATH_FEW};
+            if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_FEW};
+        }
+        kern<<<grid, 32, smem, a.stream>>>(a.op, a.f_cm, a.q_cm);
+        const cudaError_t e = cudaGetLastError();
+        return {e == cudaSuccess ? 0 : 5, 1, e, PATH_FEW};
+    }
+}
+
 // Warps per CTA of the tile kernel (registers: 16 warps leave 128 per thread).
 constexpr int tile_W(int K, bool jv) { return jv ? (K >= 8 ? 12 : 16) : 16; }
 
 template <int K>
 static LaunchResult launch_for_k(const LaunchArgs& a) {
     if (a.few) {
-        if (a.exact || a.f32 || a.bf16 || a.what == OP_JV) return {-1, 0, cudaSuccess, PATH_FEW};
+        if (a.f32 || a.bf16 || a.what == OP_JV) return {-1, 0, cudaSuccess, PATH_FEW};
+        if (a.exact) return a.what == OP_AF ? launch_few_exact<K>(a) : LaunchResult{-1, 0, cudaSuccess, PATH_FEW};
         return a.what == OP_RF ? launch_few<K, true>(a) : launch_few<K, false>(a);
     }
     if (a.ss) {

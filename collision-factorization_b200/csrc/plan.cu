@@ -562,16 +562,16 @@ int launch_unpack(const cf_plan* p, const double* src, double* dst, int64_t B, c
 int get_sym(cf_plan* p, cf_plan** out);
 bool streamable(const cf_plan* p, const cf_plan* target, int what, bool exact, int f32);
 
-// The fast FP64 angular-first (plain or folded) or radial-first form of at most kFewCells cells on
-// the few-cell kernel; kNoFew where that kernel does not apply.  With host_f and host_q (host
+// The fast FP64 angular-first (plain or folded) or radial-first form, or the exact angular-first
+// form, of at most kFewCells cells on the few-cell kernel; kNoFew where that kernel does not apply.  With host_f and host_q (host
 // arrays), f and Q_in travel in the launch's parameter block and Q_out goes to q; else Q is
 // updated in place in the device arrays f, q.
 int run_few(cf_plan* p, int what, bool exact, double* q, const double* f, int64_t B, cudaStream_t st, bool sym,
             int f32, const double* host_f = nullptr, const double* host_q = nullptr) {
-    if (what == 2 || exact || f32 != 0 || B > kFewCells) return kNoFew;
+    if (what == 2 || (exact && what != 0) || f32 != 0 || B > kFewCells) return kNoFew;
     cf_plan* target = p;
     if (sym) CF_TRY(get_sym(p, &target));
-    return dispatch(target, what, false, nullptr, nullptr, nullptr, B, st, nullptr, false, nullptr, f, q, true, host_f,
+    return dispatch(target, what, exact, nullptr, nullptr, nullptr, B, st, nullptr, false, nullptr, f, q, true, host_f,
                     host_q);
 }
 
@@ -1117,7 +1117,7 @@ int run_host_speculative(double* Q, const double* f, int64_t B, const double* la
 // comes back the same way.  With key_check set, p is a guess from the pointers of an earlier call,
 // and the operator's content hash is computed here while the kernel runs; on a mismatch Q is left
 // as it was and kRetry returned.
-int few_on_plan(cf_plan* p, int what, double* Q, const double* f, int64_t B, bool sym, const uint64_t* key_check,
+int few_on_plan(cf_plan* p, int what, bool exact, double* Q, const double* f, int64_t B, bool sym, const uint64_t* key_check,
                 const double* labels, const double* vals, const double* ic_map, const double* R) {
     std::lock_guard<std::mutex> lk(p->mu);
     DeviceGuard guard(p->device);
@@ -1132,7 +1132,7 @@ int few_on_plan(cf_plan* p, int what, double* Q, const double* f, int64_t B, boo
             return fail(CF_ECUDA, "cudaHostGetDevicePointer: %s", cudaGetErrorString(e));
         }
     }
-    int st = run_few(p, what, false, p->h_few_dev, nullptr, B, p->stream, sym, 0, f, Q);
+    int st = run_few(p, what, exact, p->h_few_dev, nullptr, B, p->stream, sym, 0, f, Q);
     int route = 1;
     if (st == kNoFew) {
         route = 2;
@@ -1144,7 +1144,7 @@ int few_on_plan(cf_plan* p, int what, double* Q, const double* f, int64_t B, boo
         double* df = p->d_io + B * M;
         CF_CUDA(cudaMemcpyAsync(dq, p->h_few, nb, cudaMemcpyHostToDevice, p->stream));
         CF_CUDA(cudaMemcpyAsync(df, p->h_few + kFewCells * M, nb, cudaMemcpyHostToDevice, p->stream));
-        st = run_few(p, what, false, dq, df, B, p->stream, sym, 0);
+        st = run_few(p, what, exact, dq, df, B, p->stream, sym, 0);
         if (st == CF_OK) CF_CUDA(cudaMemcpyAsync(p->h_few, dq, nb, cudaMemcpyDeviceToHost, p->stream));
     }
     if (st != CF_OK) {  // kNoFew included: the caller takes the ordinary route
@@ -1160,19 +1160,19 @@ int few_on_plan(cf_plan* p, int what, double* Q, const double* f, int64_t B, boo
     return CF_OK;
 }
 
-// The fast angular-first (plain or folded) and radial-first forms of at most kFewCells cells from
-// host arrays; kNoFew where the few-cell kernel does not apply.
-int run_host_few(int what, double* Q, const double* f, int64_t B, const double* labels, const double* vals,
+// The fast angular-first (plain or folded) and radial-first forms, and the exact angular-first
+// form, of at most kFewCells cells from host arrays; kNoFew where the few-cell kernel does not apply.
+int run_host_few(int what, bool exact, double* Q, const double* f, int64_t B, const double* labels, const double* vals,
                  const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k, bool sym) {
     cf_plan* p = nullptr;
     uint64_t key = 0;
     if (n_g > 0 && labels && vals && ic_map && R && plan_by_pointers(&p, &key, labels, vals, ic_map, R, n_g, n_l, n_q, k)) {
-        const int st = few_on_plan(p, what, Q, f, B, sym, &key, labels, vals, ic_map, R);
+        const int st = few_on_plan(p, what, exact, Q, f, B, sym, &key, labels, vals, ic_map, R);
         if (st != kRetry) return st;
     }
     CF_TRY(cached_plan(&p, labels, vals, ic_map, R, n_g, n_l, n_q, k));
     if (n_g == 0) return CF_OK;
-    return few_on_plan(p, what, Q, f, B, sym, nullptr, labels, vals, ic_map, R);
+    return few_on_plan(p, what, exact, Q, f, B, sym, nullptr, labels, vals, ic_map, R);
 }
 
 // Host-pointer contraction: upload, run, download.  what: 0 AF, 1 RF, 2 JV.
@@ -1182,8 +1182,8 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
     if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
     if (!Q || !f || (what == 2 && !v)) return fail(CF_EINVAL, "null host buffer");
     g_few_route = 0;
-    if (B >= 1 && B <= kFewCells && what != 2 && !exact && f32 == 0) {
-        const int r = run_host_few(what, Q, f, B, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym);
+    if (B >= 1 && B <= kFewCells && what != 2 && (!exact || what == 0) && f32 == 0) {
+        const int r = run_host_few(what, exact, Q, f, B, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym);
         if (r != kNoFew) return r;
     }
     if (what == 0 && !exact && f32 == 0 && B >= 2 * kHostChunkMin) {

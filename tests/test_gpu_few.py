@@ -95,7 +95,8 @@ def test_single_f_mex_calls_take_one_launch(name, cuda_available):
 
 
 def test_outside_the_few_cell_kernel(cuda_available, oracle_lib):
-    """More than 8 cells, the exact order and J.v keep their kernels (more than one launch here)."""
+    """More than 8 cells and J.v keep their kernels (more than one launch here); the exact order of
+    one cell runs on the few-cell exact kernel, bit for bit the oracle's operation order."""
     import torch
 
     import cf_b200
@@ -105,16 +106,23 @@ def test_outside_the_few_cell_kernel(cuda_available, oracle_lib):
     op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
     f = torch.from_numpy(cells).cuda()
     Qo = _oracle(oracle_lib, geo, R, cells, K, "af")
-    for B, form in ((9, "af"), (1, "af_exact")):
-        Q = torch.zeros_like(f[:B])
-        op.q(f[:B].contiguous(), out=Q, form=form)
+    Q = torch.zeros_like(f)
+    op.q(f, out=Q, form="af")
+    n0 = cf_b200.launch_count()
+    Q.zero_()
+    op.q(f, out=Q, form="af")
+    torch.cuda.synchronize()
+    assert cf_b200.launch_count() - n0 > 1
+    assert cf_b200._lib.PATH_NAMES[op.info()["last_path"]] != "few"
+    assert per_cell_err(Q.cpu().numpy(), Qo) <= TOL_FP64
+    for B in (1, 3):
+        Qe = torch.zeros_like(f[:B])
         n0 = cf_b200.launch_count()
-        Q.zero_()
-        op.q(f[:B].contiguous(), out=Q, form=form)
+        op.q(f[:B].contiguous(), out=Qe, form="af_exact")
         torch.cuda.synchronize()
-        assert cf_b200.launch_count() - n0 > 1, form
-        assert cf_b200._lib.PATH_NAMES[op.info()["last_path"]] != "few", form
-        assert per_cell_err(Q.cpu().numpy(), Qo[:B]) <= TOL_FP64, form
+        assert cf_b200.launch_count() - n0 == 1
+        assert cf_b200._lib.PATH_NAMES[op.info()["last_path"]] == "few"
+        assert np.array_equal(Qe.cpu().numpy(), Qo[:B])
     v = torch.from_numpy(np.random.default_rng(4).standard_normal(cells[:1].shape)).cuda()
     f1 = f[:1].contiguous()
     J = op.jv(f1, v)
@@ -156,6 +164,22 @@ def test_few_cell_host_call_sees_an_operator_changed_in_place(cuda_available):
     changed = host()
     assert np.array_equal(changed, device())
     assert not np.array_equal(changed, first)
+
+
+@pytest.mark.parametrize("name", ["wcu_k2_l2_g0", "cfg1_k3_l4_g0", "hs_k4_l4_g1", "bkw_k5_l1_g0"])
+def test_single_f_exact_host_call_is_the_reference_bit_for_bit(name, cuda_available):
+    import cf_b200
+
+    d = load_op(name)
+    NQ, K = d["NQ"], d["K"]
+    args = (d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"], d["R"], NQ, K)
+    for _ in range(2):  # the second call guesses the plan from the array addresses
+        Q = np.zeros((NQ, K), order="F")
+        n0 = cf_b200.launch_count()
+        cf_b200.contract_batched(Q, d["f"], *args, form="af_exact")
+        assert cf_b200.launch_count() - n0 == 1
+        assert cf_b200.few_route_last() == "parameter block"
+        assert np.array_equal(Q, d["Q_af"])
 
 
 def test_time_contract_host_runs_the_calls_it_times(cuda_available):
