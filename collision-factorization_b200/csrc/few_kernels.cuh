@@ -165,84 +165,94 @@ __device__ __forceinline__ void few_row(const DevOp& op, const double* f, const 
 }
 
 // The exact form of one (q1 row, cell), in the reference's operation order
-// (src/mex/angular_first_collision_kernel_mex.cpp:45-69): one warp walks the row's slices in order;
-// lane p of the warp owns Phi[k2][k3] (p = k2 + K k3) and sums (G f[q2,k2]) f[q3,k3] over the
+// (src/mex/angular_first_collision_kernel_mex.cpp:45-69).  Each warp takes one slice of the row at a
+// time (16 at once): lane p owns Phi[k2][k3] (p = k2 + K k3) and sums (G f[q2,k2]) f[q3,k3] over the
 // slice's entries in order, each product and sum rounded separately; lane k1 then sums
-// R_t[k1,k2,k3] Phi[k2][k3] over k3 (outer) and k2 (inner) and adds the sum to Q[q1,k1].  Bit for
-// bit the reference's result.  Shared memory: f of the cell, then Phi.
+// R_t[k1,k2,k3] Phi[k2][k3] over k3 (outer) and k2 (inner) into the slice's row sum.  Thread k1 of
+// the CTA adds the row sums to Q[q1,k1] in slice order, so the result is the reference's bit for
+// bit.  Shared memory: f of the cell, each warp's Phi, each warp's row sum.
 template <int K>
 __device__ __forceinline__ void few_row_exact(const DevOp& op, const double* f, const double* q_in, double* q_out,
                                               bool pass_through) {
     constexpr int NP = few_pairs_per_lane<K>();
     extern __shared__ double fs[];
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n_q = op.n_q, M = n_q * K;
-    double* phis = fs + M;
+    double* phis = fs + M + warp * K * K;
+    double* sums = fs + M + kFewWarps * K * K;  // [kFewWarps][K]
     const int q1 = blockIdx.x;
     const int s0 = op.q1_begin[q1], s1 = op.q1_begin[q1 + 1];
     double acc = 0.0;
-    if (lane < K) acc = q_in[lane * n_q + q1];
+    if (threadIdx.x < K) acc = q_in[threadIdx.x * n_q + q1];
     if (s0 == s1) {
-        if (pass_through && lane < K) q_out[lane * n_q + q1] = acc;
+        if (pass_through && threadIdx.x < K) q_out[threadIdx.x * n_q + q1] = acc;
         return;
     }
-    for (int i = lane; i < M; i += 32) fs[i] = f[i];
-    __syncwarp();
-    for (int s = s0; s < s1; ++s) {
-        const int t = op.slice_t[s];
-        const int e0 = op.slice_e[s], e1 = op.slice_e[s + 1];
-        double phi[NP];
+    for (int i = threadIdx.x; i < M; i += blockDim.x) fs[i] = f[i];
+    __syncthreads();
+    for (int base = s0; base < s1; base += kFewWarps) {
+        const int s = base + warp;
+        if (s < s1) {
+            const int t = op.slice_t[s];
+            const int e0 = op.slice_e[s], e1 = op.slice_e[s + 1];
+            double phi[NP];
 #pragma unroll
-        for (int j = 0; j < NP; ++j) phi[j] = 0.0;
-        for (int eb = e0; eb < e1; eb += 32) {
-            const int n = min(32, e1 - eb);
-            uint32_t my_q23 = 0;
-            double my_g = 0.0;
-            if (lane < n) {
-                my_q23 = __ldg(op.e_q23 + eb + lane);
-                my_g = __ldg(op.e_g + eb + lane);
-            }
-            for (int z = 0; z < n; ++z) {
-                const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, z);
-                const double g = __shfl_sync(0xffffffffu, my_g, z);
-                const double* f2 = fs + (q23 & 0xffffu);
-                const double* f3 = fs + (q23 >> 16);
+            for (int j = 0; j < NP; ++j) phi[j] = 0.0;
+            for (int eb = e0; eb < e1; eb += 32) {
+                const int n = min(32, e1 - eb);
+                uint32_t my_q23 = 0;
+                double my_g = 0.0;
+                if (lane < n) {
+                    my_q23 = __ldg(op.e_q23 + eb + lane);
+                    my_g = __ldg(op.e_g + eb + lane);
+                }
+                for (int z = 0; z < n; ++z) {
+                    const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, z);
+                    const double g = __shfl_sync(0xffffffffu, my_g, z);
+                    const double* f2 = fs + (q23 & 0xffffu);
+                    const double* f3 = fs + (q23 >> 16);
 #pragma unroll
-                for (int j = 0; j < NP; ++j) {
-                    const int p = lane + 32 * j;
-                    if (p < K * K)
-                        phi[j] = __dadd_rn(phi[j], __dmul_rn(__dmul_rn(g, f2[(p % K) * n_q]), f3[(p / K) * n_q]));
+                    for (int j = 0; j < NP; ++j) {
+                        const int p = lane + 32 * j;
+                        if (p < K * K)
+                            phi[j] = __dadd_rn(phi[j], __dmul_rn(__dmul_rn(g, f2[(p % K) * n_q]), f3[(p / K) * n_q]));
+                    }
                 }
             }
-        }
 #pragma unroll
-        for (int j = 0; j < NP; ++j)
-            if (lane + 32 * j < K * K) phis[lane + 32 * j] = phi[j];
-        __syncwarp();
-        if (lane < K) {
-            const double* __restrict__ Rt = op.R + (size_t)t * K * K * K;
-            double sacc = 0.0;
-            for (int k3 = 0; k3 < K; ++k3)
+            for (int j = 0; j < NP; ++j)
+                if (lane + 32 * j < K * K) phis[lane + 32 * j] = phi[j];
+            __syncwarp();
+            if (lane < K) {
+                const double* __restrict__ Rt = op.R + (size_t)t * K * K * K;
+                double sacc = 0.0;
+                for (int k3 = 0; k3 < K; ++k3)
 #pragma unroll
-                for (int k2 = 0; k2 < K; ++k2)
-                    sacc = __dadd_rn(sacc, __dmul_rn(__ldg(Rt + lane + K * k2 + K * K * k3), phis[k2 + K * k3]));
-            acc = __dadd_rn(acc, sacc);
+                    for (int k2 = 0; k2 < K; ++k2)
+                        sacc = __dadd_rn(sacc, __dmul_rn(__ldg(Rt + lane + K * k2 + K * K * k3), phis[k2 + K * k3]));
+                sums[warp * K + lane] = sacc;
+            }
         }
-        __syncwarp();
+        __syncthreads();
+        if (threadIdx.x < K) {
+            const int n = min(kFewWarps, s1 - base);
+            for (int w = 0; w < n; ++w) acc = __dadd_rn(acc, sums[w * K + threadIdx.x]);
+        }
+        __syncthreads();
     }
-    if (lane < K) q_out[lane * n_q + q1] = acc;
+    if (threadIdx.x < K) q_out[threadIdx.x * n_q + q1] = acc;
 }
 
-// The exact form in place on the caller's cell-major device arrays; grid (N_Q, cells), one warp.
+// The exact form in place on the caller's cell-major device arrays; grid (N_Q, cells).
 template <int K>
-__global__ void __launch_bounds__(32) af_few_exact_kernel(DevOp op, const double* __restrict__ f, double* q) {
+__global__ void __launch_bounds__(kFewWarps * 32) af_few_exact_kernel(DevOp op, const double* __restrict__ f, double* q) {
     const size_t off = (size_t)blockIdx.y * op.n_q * K;
     few_row_exact<K>(op, f + off, q + off, q + off, false);
 }
 
-// The exact form with f and Q_in in the parameter block, Q_out to q_out; grid (N_Q, n_cells), one warp.
+// The exact form with f and Q_in in the parameter block, Q_out to q_out; grid (N_Q, n_cells).
 template <int K, int CAP>
-__global__ void __launch_bounds__(32) af_few_exact_param_kernel(DevOp op, const __grid_constant__ FewPayload<CAP> pay,
+__global__ void __launch_bounds__(kFewWarps * 32) af_few_exact_param_kernel(DevOp op, const __grid_constant__ FewPayload<CAP> pay,
                                                                 int n_cells, double* q_out) {
     const size_t M = (size_t)op.n_q * K, off = (size_t)blockIdx.y * M;
     few_row_exact<K>(op, pay.v + off, pay.v + (size_t)n_cells * M + off, q_out + off, true);

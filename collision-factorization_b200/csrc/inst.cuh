@@ -332,14 +332,14 @@ static LaunchResult launch_few(const LaunchArgs& a) {
     }
 }
 
-// The exact form of the few-cell kernel (one warp per (row, cell)), in place on device arrays or
+// The exact form of the few-cell kernel (one CTA per (row, cell)), in place on device arrays or
 // with f and Q_in in the parameter block as launch_few does.  Status -1 where it does not apply.
 template <int K, int CAP>
 static LaunchResult launch_few_exact_param(const LaunchArgs& a, dim3 grid, size_t smem, size_t need) {
     auto kern = af_few_exact_param_kernel<K, CAP>;
     if (smem > 48 * 1024) {
         int per_sm = 0;
-        const cudaError_t e = resident_ctas((const void*)kern, 32, smem, &per_sm);
+        const cudaError_t e = resident_ctas((const void*)kern, kFewWarps * 32, smem, &per_sm);
         if (e != cudaSuccess) return {5, 0, e, PATH_FEW};
         if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_FEW};
     }
@@ -348,7 +348,7 @@ static LaunchResult launch_few_exact_param(const LaunchArgs& a, dim3 grid, size_
     std::memcpy(pay.v, a.few_host_f, half * sizeof(double));
     std::memcpy(pay.v + half, a.few_host_q, half * sizeof(double));
     std::memset(pay.v + need, 0, (CAP - need) * sizeof(double));
-    kern<<<grid, 32, smem, a.stream>>>(a.op, pay, (int)a.n_cells, a.q_cm);
+    kern<<<grid, kFewWarps * 32, smem, a.stream>>>(a.op, pay, (int)a.n_cells, a.q_cm);
     if (cudaGetLastError() != cudaSuccess) return {-1, 0, cudaSuccess, PATH_FEW};
     return {0, 1, cudaSuccess, PATH_FEW};
 }
@@ -361,7 +361,7 @@ static LaunchResult launch_few_exact(const LaunchArgs& a) {
         if (a.n_cells > kFewCells || a.q_cm == nullptr || (a.f_cm == nullptr && a.few_host_f == nullptr))
             return {-1, 0, cudaSuccess, PATH_FEW};
         if (a.op.n_items == 0 || a.n_cells == 0) return {0, 0, cudaSuccess, PATH_FEW};
-        const size_t smem = sizeof(double) * ((size_t)a.op.n_q * K + K * K);
+        const size_t smem = sizeof(double) * ((size_t)a.op.n_q * K + kFewWarps * (K * K + K));
         if (smem + 256 > a.max_smem) return {-1, 0, cudaSuccess, PATH_FEW};
         const dim3 grid((unsigned)a.op.n_q, (unsigned)a.n_cells);
         if (a.few_host_f) {
@@ -374,11 +374,11 @@ static LaunchResult launch_few_exact(const LaunchArgs& a) {
         auto kern = af_few_exact_kernel<K>;
         if (smem > 48 * 1024) {
             int per_sm = 0;
-            const cudaError_t e = resident_ctas((const void*)kern, 32, smem, &per_sm);
+            const cudaError_t e = resident_ctas((const void*)kern, kFewWarps * 32, smem, &per_sm);
             if (e != cudaSuccess) return {5, 0, e, PATH_FEW};
             if (per_sm < 1) return {-1, 0, cudaSuccess, PATH_FEW};
         }
-        kern<<<grid, 32, smem, a.stream>>>(a.op, a.f_cm, a.q_cm);
+        kern<<<grid, kFewWarps * 32, smem, a.stream>>>(a.op, a.f_cm, a.q_cm);
         const cudaError_t e = cudaGetLastError();
         return {e == cudaSuccess ? 0 : 5, 1, e, PATH_FEW};
     }
