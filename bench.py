@@ -1366,8 +1366,8 @@ def run_single(args):
 
 def run_profile_single(args):
     """For ncu: the single-f workload's calls only, steps + 1 of each: the MEX-compatible host call
-    (cf_angular_first: af_few_param_kernel) and the device entry point in the folded form
-    (af_few_kernel)."""
+    (cf_angular_first: af_few_param_kernel), the exact form from host arrays
+    (af_few_exact_param_kernel) and the device entry point in the folded form (af_few_kernel)."""
     import ctypes
 
     import torch
@@ -1388,6 +1388,9 @@ def run_profile_single(args):
               lab.shape[0], R.size // K ** 3, NQ, K)
     for _ in range(args.steps + 1):
         _lib.check(lib.cf_angular_first(Qh.ctypes.data_as(Dp), fq.ctypes.data_as(Dp), *opargs))
+    for _ in range(args.steps + 1):  # the exact form: af_few_exact_param_kernel
+        _lib.check(lib.cf_contract_host(Qh.ctypes.data_as(Dp), fq.ctypes.data_as(Dp), 1, *opargs,
+                                        _lib.FORMS["af_exact"]))
     op = cf_b200.CollisionOperator(lab, vals, ic, R, NQ, K)
     f = torch.from_numpy(f_host.reshape(1, K, NQ).copy()).cuda()
     Q = torch.zeros_like(f)
