@@ -50,7 +50,13 @@ WORKLOADS = {
 # operator of the single-f workload: R from the reference's own quadrature (K_max = 3, pad 20)
 SINGLE_OPERATOR = "op_cfg1_k3_l4_g0.npz"
 RAGGED_BUCKETS = [(4, 4), (6, 6), (8, 6), (10, 8)]  # (L, K), drawn with RAGGED_WEIGHTS per cell
-R_FILES = {(10, 8): "R_hs_k7_l10_pad20.npy", (8, 8): "R_hs_k7_l8_pad20.npy"}
+# hard-sphere R (pad 20) per (L, K): from the reference's own quadrature (compute_rtensor_sumfac_mex,
+# compiled unmodified) up to L = 10; at L = 16, K = 12 from this library's GPU quadrature
+# (cf_rtensor_sumfac_packed), which equals the reference's to 1e-12 where both can be run
+R_FILES = {(10, 8): "R_hs_k7_l10_pad20.npy", (8, 8): "R_hs_k7_l8_pad20.npy", (4, 4): "R_hs_k3_l4_pad20.npy",
+           (6, 6): "R_hs_k5_l6_pad20.npy", (8, 6): "R_hs_k5_l8_pad20.npy", (16, 12): "R_hs_k11_l16_pad20.npy"}
+R_SOURCES = {(16, 12): "this library's GPU quadrature (cf_rtensor_sumfac_packed, parity-tested against "
+                       "compute_rtensor_sumfac_mex), K_max = 11, pad 20"}
 # DRAM bytes (read + write) of one contraction launch, from the ncu captures summarised in profiles/
 NCU_TRAFFIC = {
     ("hs_l10_k8_b4096", "tile", "af_sym"): (64.769024e6 + 1.074688e6,
@@ -81,9 +87,10 @@ def parse_args(argv=None):
     ap.add_argument("--seed", type=int, default=20260)
     ap.add_argument("--train-states", type=int, default=100000)
     ap.add_argument("--epochs", type=int, default=12)
-    ap.add_argument("--form", default="af", choices=["af", "af_sym", "af_exact", "rf"],
+    ap.add_argument("--form", default="af", choices=["af", "af_sym", "af_exact", "rf", "af_sym_i8"],
                     help="form launched by --profile")
-    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split", "tile_mma"],
+    ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split", "tile_mma",
+                                                       "band"],
                     help="kernel family of the angular-first contraction")
     ap.add_argument("--entry", choices=("tiled", "device"), default="tiled",
                     help="--profile: launch the tiled kernel (cf_q_tiled) or the device entry point (cf_q_device)")
@@ -102,7 +109,8 @@ def make_operator(L: int, K: int, gamma: float, seed: int):
     rfile = ROOT / "tests" / "golden" / R_FILES.get((L, K), "__none__")
     if rfile.exists() and gamma == 1.0:
         R = np.asfortranarray(np.load(rfile))
-        r_source = f"reference quadrature (compute_rtensor_sumfac_mex, pad 20): {rfile.name}"
+        r_source = (f"{R_SOURCES[(L, K)]}: {rfile.name}" if (L, K) in R_SOURCES else
+                    f"reference quadrature (compute_rtensor_sumfac_mex, pad 20): {rfile.name}")
     else:
         from cf_b200.geometry import Geometry  # noqa: F401
 
@@ -292,6 +300,18 @@ def cpu_reference_rate(geo, R, cells, K, target_seconds: float, nthreads: int = 
     return statistics.median(rates), n, total, nthreads
 
 
+def cpu_reference_outputs(geo, R, cells, K) -> np.ndarray:
+    """Q of each given cell ([n, K, N_Q]) from the reference's angular_first kernel, compiled unmodified,
+    on all host cores: the error reference of the forms where the GPU has no exact-order form (K > 8)."""
+    from oracle.reference import Reference
+
+    ref = Reference("fast")
+    f = np.asfortranarray(cells.transpose(2, 1, 0))
+    Qr = np.zeros_like(f, order="F")
+    ref.batch("af", Qr, f, geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K, nthreads=ref.num_threads())
+    return np.ascontiguousarray(Qr.transpose(2, 1, 0))
+
+
 def cpu_baseline_block(geo, R, cells, K, target_seconds: float) -> dict:
     """The reference's angular_first on all host cores (the baseline), on one core, and its
     radial_first and naive kernels on all cores, each the median of 5 repetitions."""
@@ -348,15 +368,29 @@ def run_ours(args):
 
     _lib.check(lib.cf_pack_cells(op._h, int(fT.data_ptr()), int(f.data_ptr()), B, sh))
 
-    # accuracy of the fast form against the reference's exact operation order (bitwise = reference MEX);
-    # the exact order is built for K <= 8, above that the plain FP64 form is the reference
-    ref_form = "af_exact" if K <= 8 else "af"
-    step(ref_form)
-    Q_exact = Q.clone()
+    # accuracy of every form against the reference's exact operation order: for K <= 8 the GPU's
+    # af_exact form on every cell (bitwise equal to the reference MEX); above that the reference's
+    # own compiled kernel on a sample of cells, from the CPU-baseline leg (cpu_reference_outputs)
+    if K <= 8:
+        ref_form, ref_idx = "af_exact", None
+        step(ref_form)
+        Q_exact = Q.clone()
+        den = Q_exact.abs().reshape(B, -1).amax(dim=1).clamp_min(1e-300)
+    else:
+        ref_form, ref_idx = "reference_sample", np.unique(np.linspace(0, B - 1, 24).astype(np.int64))
+        Q_ref = torch.from_numpy(cpu_reference_outputs(geo, R, cells[ref_idx], K)).to(dev)
+        den = Q_ref.abs().reshape(len(ref_idx), -1).amax(dim=1).clamp_min(1e-300)
+
+    def form_err() -> float:
+        # max over the reference cells of max|Q - Q_ref| / max|Q_ref| (Q: the last step's output)
+        if ref_idx is None:
+            num = (Q - Q_exact).abs().reshape(B, -1).amax(dim=1)
+        else:
+            num = (Q[torch.from_numpy(ref_idx).to(dev)] - Q_ref).abs().reshape(len(ref_idx), -1).amax(dim=1)
+        return float((num / den).max())
+
     step("af")
-    num = (Q - Q_exact).abs().reshape(B, -1).amax(dim=1)
-    den = Q_exact.abs().reshape(B, -1).amax(dim=1).clamp_min(1e-300)
-    err_af = float((num / den).max())
+    err_af = form_err()
     inv = Q.reshape(B, -1)[:, [0, 1, 2, 3, NQ]].abs().max().item()
 
     # FP64 peak of this GPU (DFMA probe, cuBLAS DGEMM)
@@ -394,8 +428,7 @@ def run_ours(args):
     rf_ms = timed(lambda: step("rf"), max(2, args.steps // 4))
     # the q2 <-> q3 folded form: accuracy against the exact form, then timing (step and kernel)
     step("af_sym")
-    num = (Q - Q_exact).abs().reshape(B, -1).amax(dim=1)
-    err_sym = float((num / den).max())
+    err_sym = form_err()
     sym_ms = timed(lambda: step("af_sym"), args.steps)
     sym_kern_ms = timed(lambda: kernel_only("af_sym"), max(2, args.steps // 2))
     # the folded form's device step is one launch of the tile kernel on the cell-major arrays (no
@@ -407,7 +440,7 @@ def run_ours(args):
     if sym_single:
         sym_kern_ms = timed(lambda: op.q(f, out=Q, form="af_sym", workspace=ws), max(2, args.steps // 2))
     path_ms, sym_path_ms = {}, {}
-    for path in ("tile_mma", "pair_split", "pair", "pair_l1", "tile", "gather"):
+    for path in ("tile_mma", "pair_split", "pair", "pair_l1", "tile", "gather", "band"):
         try:
             op.set_kernel_path(path)
             path_ms[path] = timed(step, max(2, args.steps // 4))
@@ -432,15 +465,20 @@ def run_ours(args):
             op.jv(f, v_dev, out=Jout, **kw)
 
         jv_ms[name] = timed(jstep, max(2, args.steps // 4))
-    # reduced-precision forms (FP32 contraction, FP64 accumulation of Q): error and throughput
+    # reduced-precision forms (FP32 contraction, FP64 accumulation of Q; BF16 split; the exact int8
+    # split on the tensor cores): error and throughput
     f32 = {}
-    for form in ("af_f32", "af_sym_f32", "af_bf16", "af_sym_bf16"):
+    split_ms = None
+    for form in ("af_f32", "af_sym_f32", "af_bf16", "af_sym_bf16", "af_sym_i8"):
         try:
             step(form)
-            num = (Q - Q_exact).abs().reshape(B, -1).amax(dim=1)
-            ms = timed(lambda: step(form), max(2, args.steps // 4))
-            f32[form] = {"cells_per_s": B * len(ms) / (sum(ms) / 1e3), "max_rel_err_vs_fp64": float((num / den).max()),
-                         "meets_1e-10": bool(float((num / den).max()) <= 1e-10)}
+            err = form_err()
+            inv_f = Q.reshape(B, -1)[:, [0, 1, 2, 3, NQ]].abs().max().item()
+            ms = timed(lambda: step(form), max(2, args.steps // 4) if form != "af_sym_i8" else args.steps)
+            f32[form] = {"cells_per_s": B * len(ms) / (sum(ms) / 1e3), "max_rel_err_vs_fp64": err,
+                         "meets_1e-10": bool(err <= 1e-10), "invariants_abs_max": inv_f}
+            if form == "af_sym_i8":
+                split_ms, err_split = ms, err
         except Exception as e:
             f32[form] = {"unavailable": str(e)[:160]}
     clk = clocks.stop()
@@ -448,18 +486,29 @@ def run_ours(args):
     dist_barrier(world)
 
     # the headline form: the fastest form within 1e-10 of the FP64 (exact-order) result
-    plain_s = sum(step_ms) / 1e3
-    sym_s = sum(sym_ms) / 1e3 * args.steps / len(sym_ms)
-    chosen = "af_sym" if (err_sym <= 1e-10 and sym_s < plain_s) else "af"
-    chosen_ms = sym_ms if chosen == "af_sym" else step_ms
+    cand = {"af": (sum(step_ms) / len(step_ms), err_af, step_ms), "af_sym": (sum(sym_ms) / len(sym_ms), err_sym, sym_ms)}
+    if split_ms:
+        cand["af_sym_i8"] = (sum(split_ms) / len(split_ms), err_split, split_ms)
+    chosen = min((k for k, v in cand.items() if v[1] <= 1e-10), key=lambda k: cand[k][0], default="af")
+    chosen_ms = cand[chosen][2]
     value, total_s = weak_rate(world, B, args.steps, sum(chosen_ms) / 1e3 * args.steps / len(chosen_ms))
     ms_per_step = 1e3 * total_s / args.steps
-    kern_list = sym_kern_ms if chosen == "af_sym" else kern_ms
-    kernel_only(chosen)
+    # the kernel of the device step: one launch on the cell-major arrays for the split form and for the
+    # forms on the band kernel (the step's own events time it); else the tiled launch (cf_q_tiled)
+    n0 = _lib.launch_count()
+    step(chosen)
     torch.cuda.synchronize(dev)
-    last_path = _lib.PATH_NAMES[op.info()["last_path"]]
-    if chosen == "af_sym" and sym_single:
-        last_path = "tile_cell_major"
+    step_path = _lib.PATH_NAMES[op.info()["last_path"]]
+    if step_path in ("split_i8", "band") and _lib.launch_count() - n0 == 1:
+        kern_list = chosen_ms
+        last_path = step_path
+    else:
+        kern_list = sym_kern_ms if chosen == "af_sym" else kern_ms
+        kernel_only(chosen)
+        torch.cuda.synchronize(dev)
+        last_path = _lib.PATH_NAMES[op.info()["last_path"]]
+        if chosen == "af_sym" and sym_single:
+            last_path = "tile_cell_major"
     traffic = NCU_TRAFFIC.get((args.workload, last_path, chosen))
     kern_name = {"pair": "af_pair_kernel (persistent, tile-resident, mirrored row pairs)",
                  "pair_split": "af_pair_kernel, split variant (both mirrored rows per lane, k3 halves)",
@@ -467,12 +516,18 @@ def run_ours(args):
                  "tile_cell_major": "af_tile_stream_kernel, resident (the tile kernel on the cell-major arrays, "
                                     "no layout passes; the whole device step)",
                  "gather": "af_kernel (gathers through L1/L2)",
-                 "tile_mma": "af_mma_kernel (tile-resident, K^3 step on the FP64 MMA)"}.get(last_path, "?")
+                 "tile_mma": "af_mma_kernel (tile-resident, K^3 step on the FP64 MMA)",
+                 "split_i8": "af_split_kernel (Phi in FP64 on the folded operator, K^3 step on the int8 tensor cores "
+                             "(tcgen05.mma kind::i8, exact 6x6-byte split); the whole device step)",
+                 "band": "af_band64_kernel (l1-band units, 4 cells' f resident, R_t staged per t by cp.async.bulk, "
+                         "FP64; the whole device step)"}.get(last_path, "?")
     kern_s = sum(kern_list) / len(kern_list) / 1e3
     flops_launch = op.flops_q * B
     achieved_tf = flops_launch / kern_s / 1e12
-    sym_info = op.sym_info() if chosen == "af_sym" else None
+    sym_info = op.sym_info() if chosen in ("af_sym", "af_sym_i8") else None
     exec_flops = (sym_info["flops_q"] if sym_info else op.flops_q) * B
+    if chosen == "af_sym_i8":  # the K^3 step runs on the tensor cores: the FP64 pipe executes the Phi step
+        exec_flops -= sym_info["n_slices"] * 2.0 * K**3 * B
     exec_tf = exec_flops / kern_s / 1e12
 
     # end to end through the host C-ABI entry point, pinned host buffers, in the headline form
@@ -507,7 +562,9 @@ def run_ours(args):
             "config": {
                 "workload": args.workload, "L": L, "K": K, "M": M, "cells_per_gpu": B, "gamma": gamma,
                 "n_g": op.n_g, "n_l": op.n_l, "n_slices": op.n_slices,
-                "form": {"af_sym": "af_sym (FP64, q2<->q3 folded operator)", "af": "af (plain FP64)"}[chosen],
+                "form": {"af_sym": "af_sym (FP64, q2<->q3 folded operator)", "af": "af (plain FP64)",
+                         "af_sym_i8": "af_sym_i8 (folded operator; Phi in FP64, K^3 step on the int8 tensor cores, "
+                                      "exact byte split, FP64 recombination)"}[chosen],
                 "R": r_source, "l2": "flushed (256 MB write) before every timed step",
                 "parallelism": f"cells sharded, {B} per GPU, no collective",
             },
@@ -516,8 +573,11 @@ def run_ours(args):
                 "af_sym": {"cells_per_s": sym_rate, "max_rel_err_vs_fp64": err_sym},
                 "af_exact": {"cells_per_s": exact_rate, "max_rel_err_vs_fp64": 0.0} if exact_ms else
                 {"unavailable": "the exact operation order is built for K <= 8"},
-                "error_reference": {"af_exact": "the reference's exact operation order (bitwise equal to its MEX)",
-                                    "af": "the plain FP64 form (the exact order is built for K <= 8)"}[ref_form],
+                "error_reference": {"af_exact": "the reference's exact operation order on every cell (the GPU's "
+                                                "af_exact form, bitwise equal to its MEX)",
+                                    "reference_sample": f"the reference's angular_first_collision_kernel_mex, compiled "
+                                                        f"unmodified, on a sample of {0 if ref_idx is None else len(ref_idx)} "
+                                                        f"of the cells (CPU)"}[ref_form],
                 "rf": {"cells_per_s": rf_rate},
                 "af_by_kernel": {p: (B / (sum(v) / len(v) / 1e3) if v else None) for p, v in path_ms.items()},
                 "af_sym_by_kernel": {p: (B / (sum(v) / len(v) / 1e3) if v else None) for p, v in sym_path_ms.items()},
@@ -530,6 +590,8 @@ def run_ours(args):
             "invariants_abs_max": inv,
             "roofline": {
                 "bound": "fp64", "kernel": f"{kern_name}, K={K}" + (" on the folded operator" if chosen == "af_sym" else ""),
+                "note": ("FP64-pipe roofline of the reference operator's FLOP; the form runs its K^3 step on the int8 "
+                         "tensor cores, so executed_frac counts the folded Phi step only") if chosen == "af_sym_i8" else None,
                 "achieved": achieved_tf, "peak": peak_tf,
                 "unit": "TFLOP/s", "frac": achieved_tf / peak_tf, "traffic": traffic[0] if traffic else None,
                 "traffic_source": traffic[1] if traffic else "no ncu capture of this kernel and form on this workload",
@@ -823,14 +885,24 @@ def run_implicit(args):
     f = torch.from_numpy(cells).cuda()
     rhs = op.q(f)
     results = {}
+    n_exact = 256  # states whose exact block-Jacobi preconditioner is assembled (K N_Q J.v probes each)
     for dtnu in (1.0, 10.0, 100.0):
         dt = dtnu / lp.nu
         row = {}
-        for name in ("block", "learned", "none"):
+        for name in ("block", "learned", "none", "block_exact"):
+            fs = f[:n_exact] if name == "block_exact" else f
+            rs = rhs[:n_exact] if name == "block_exact" else rhs
+            if name == "block_exact":
+                torch.cuda.synchronize()
+                ta = time.perf_counter()
+                P_exact = implicit.exact_block_jacobi(op, fs, dt)
+                torch.cuda.synchronize()
+                t_assemble = time.perf_counter() - ta
+
             def solve():
                 P = (implicit.block_preconditioner(op, dt) if name == "block"
-                     else lp.predict(f, dt) if name == "learned" else None)
-                return implicit.gmres_solve(op, f, rhs, dt, restart=30, tol=1e-10, max_iters=3000, precond=P,
+                     else lp.predict(f, dt) if name == "learned" else P_exact if name == "block_exact" else None)
+                return implicit.gmres_solve(op, fs, rs, dt, restart=30, tol=1e-10, max_iters=3000, precond=P,
                                             raise_on_timeout=False)
             solve()  # warm-up
             torch.cuda.synchronize()
@@ -839,7 +911,17 @@ def run_implicit(args):
             torch.cuda.synchronize()
             row[name] = {"seconds": time.perf_counter() - t, "iters_mean": float(it.mean()), "iters_max": int(it.max()),
                          "relres_max": float(rel.max()), "converged": bool(np.all(rel <= 1e-10))}
+            if name == "block_exact":
+                row[name]["cells"] = n_exact
+                row[name]["assembly_seconds"] = t_assemble
+                row[name]["note"] = ("exact diagonal blocks of A(f) = I - dt J(f) per state (K N_Q unit-probe J.v "
+                                     "each), inverted: the ceiling of any block-diagonal preconditioner; solve time "
+                                     "excludes the assembly")
+        row["block_on_exact_sample"] = {"iters_mean": float(np.mean(
+            implicit.gmres_solve(op, f[:n_exact], rhs[:n_exact], dt, restart=30, tol=1e-10, max_iters=3000,
+                                 precond=implicit.block_preconditioner(op, dt), raise_on_timeout=False)[1]))}
         row["speedup_learned_vs_block"] = row["block"]["seconds"] / row["learned"]["seconds"]
+        row["learned_network_used"] = bool(lp._gain(dt) >= lp.min_gain)
         results[f"dt_nu={dtnu:g}"] = row
     out = {"workload": "implicit_hs_l8_k8_b2048", "cells": B, "M": geo.n_q * K, "R": r_source,
            "gmres": "GMRES(30), right block-Jacobi preconditioning, FP64, tol 1e-10 on |b - A x| / |b| per cell",

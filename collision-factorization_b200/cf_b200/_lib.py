@@ -23,10 +23,10 @@ STATUS_NAMES = {
 }
 
 FORM_AF, FORM_RF, FORM_AF_EXACT, FORM_RF_EXACT, FORM_AF_SYM, FORM_AF_F32, FORM_AF_SYM_F32 = 0, 1, 2, 3, 4, 5, 6
-FORM_AF_BF16, FORM_AF_SYM_BF16 = 7, 8
+FORM_AF_BF16, FORM_AF_SYM_BF16, FORM_AF_SYM_I8 = 7, 8, 9
 FORMS = {"af": FORM_AF, "rf": FORM_RF, "af_exact": FORM_AF_EXACT, "rf_exact": FORM_RF_EXACT, "af_sym": FORM_AF_SYM,
          "af_f32": FORM_AF_F32, "af_sym_f32": FORM_AF_SYM_F32, "af_bf16": FORM_AF_BF16,
-         "af_sym_bf16": FORM_AF_SYM_BF16}
+         "af_sym_bf16": FORM_AF_SYM_BF16, "af_sym_i8": FORM_AF_SYM_I8}
 
 # Every symbol the header declares; the tests check that the library exports all of them.
 EXPORTS = [
@@ -35,7 +35,7 @@ EXPORTS = [
     "cf_q_device", "cf_q_device_ws", "cf_jv_device", "cf_q_device_noalloc", "cf_plan_stream_selftest",
     "cf_ragged_create", "cf_ragged_destroy", "cf_ragged_q", "cf_ragged_graph_launch", "cf_ragged_q_resident",
     "cf_ragged_q_host",
-    "cf_ragged_info", "cf_rk2_workspace_size", "cf_rk2_steps_tiled", "cf_rtensor_sumfac",
+    "cf_ragged_info", "cf_rk2_workspace_size", "cf_rk2_steps_tiled", "cf_rtensor_sumfac", "cf_rtensor_sumfac_packed",
     "cf_gmres_workspace_size", "cf_gmres_solve_tiled",
     "cf_mlp_create", "cf_mlp_destroy", "cf_mlp_num_params", "cf_mlp_copy", "cf_mlp_forward", "cf_mlp_backward",
     "cf_mlp_adam_step", "cf_precond_probe_loss", "cf_precond_assemble",
@@ -58,7 +58,7 @@ class PlanInfo(C.Structure):
     ]
 
 PATH_NAMES = {0: "none", 1: "gather", 2: "tile", 3: "pair", 4: "pair_l1", 5: "pair_split", 6: "tile_mma", 7: "bf16_mma", 8: "tile_quarter",
-              9: "few"}
+              9: "few", 10: "split_i8", 11: "band"}
 
 _DP = C.POINTER(C.c_double)
 
@@ -122,6 +122,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_ragged_q_host.argtypes = [V, V, V]
     lib.cf_rk2_workspace_size.argtypes = [V, _I64, C.POINTER(C.c_size_t)]
     lib.cf_rtensor_sumfac.argtypes = [_D, C.POINTER(SumfacInputs), _I32, C.POINTER(C.c_double)]
+    lib.cf_rtensor_sumfac_packed.argtypes = [_D, C.POINTER(SumfacInputs), _D, _D, _I32, C.POINTER(C.c_double)]
     lib.cf_rk2_steps_tiled.argtypes = [V, V, _I64, C.c_double, _I32, _I32, V, C.c_size_t, V]
     lib.cf_ragged_info.argtypes = [V, C.POINTER(_I32), C.POINTER(_I32), C.POINTER(C.c_int64), C.POINTER(_I32)]
     lib.cf_mlp_create.argtypes = [C.POINTER(V), _I32, _I32, _I32, _I32, C.c_uint64, _I32]

@@ -86,6 +86,37 @@ def block_preconditioner(op, dt: float, rho: float = 1.0) -> np.ndarray:
     return np.ascontiguousarray(np.linalg.inv(A))
 
 
+def exact_block_jacobi(op, f, dt: float, probes_per_launch: int = 131072):
+    """The exact block-Jacobi preconditioner of each cell's (I - dt J(f)): [B, N_Q, K, K] float64 on the
+    device, the inverses of the K x K diagonal blocks of A(f) over the angular modes.
+
+    Column (b, q) of J(f) is J(f) e_(b,q), one J.v with a unit probe: K N_Q probes per state, batched
+    over states and probes through the library's J.v.  This is the best any block-diagonal
+    preconditioner over the angular modes can be for A(f) itself, the ceiling of the learned blocks.
+    """
+    import torch
+
+    B, K, NQ = f.shape[0], op.K, op.N_Q
+    M = K * NQ
+    dev = f.device
+    blocks = torch.empty((B, NQ, K, K), dtype=torch.float64, device=dev)  # [s, q, a, b]: J[(a,q),(b,q)]
+    per = max(1, probes_per_launch // M)  # states per launch
+    eye = torch.eye(M, dtype=torch.float64, device=dev).view(M, K, NQ)  # probe p = b * NQ + q: e_(b,q)
+    qs = torch.arange(NQ, device=dev)
+    for s0 in range(0, B, per):
+        s1 = min(B, s0 + per)
+        n = s1 - s0
+        fs = f[s0:s1].unsqueeze(1).expand(-1, M, -1, -1).reshape(-1, K, NQ).contiguous()
+        vs = eye.unsqueeze(0).expand(n, -1, -1, -1).reshape(-1, K, NQ).contiguous()
+        out = op.jv(fs, vs).view(n, K, NQ, K, NQ)  # [s, b, q (probe), a, q' (output)]
+        # diagonal blocks: q' = q
+        d = out[:, :, qs, :, qs]  # [q, s, b, a]
+        blocks[s0:s1] = d.permute(1, 0, 3, 2)
+        del fs, vs, out
+    A = torch.eye(K, dtype=torch.float64, device=dev).view(1, 1, K, K) - dt * blocks
+    return torch.linalg.inv(A).contiguous()
+
+
 def gmres_solve(op, f, b, dt: float, x0=None, restart: int = 30, tol: float = 1e-10, max_iters: int = 3000,
                 precond=None, stream=None, raise_on_timeout: bool = True):
     """Solve (I - dt J(f)) x = b for every cell with GMRES(restart).

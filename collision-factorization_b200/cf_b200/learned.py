@@ -95,6 +95,8 @@ class LearnedPreconditioner:
         self.sd = np.ones(self.n_in, dtype=np.float32)
         self.nu = abs(implicit.equilibrium_jacobian_blocks(op)[min(6, self.NQ - 1)][0, 0])
         self.gain = {}  # log10(dt nu) (rounded) -> multiplier of the correction, from calibrate()
+        # below this calibrated gain predict() returns the Maxwellian blocks and skips the network
+        self.min_gain = 0.25
 
     def _gain(self, dt) -> float:
         return self.gain.get(round(math.log10(max(dt * self.nu, 1e-12)), 6), 1.0)
@@ -112,12 +114,16 @@ class LearnedPreconditioner:
         return (x - mu) / sd
 
     def predict(self, f, dt, peq=None):
-        """Per-cell blocks [B, N_Q, K, K] float64 on the device."""
+        """Per-cell blocks [B, N_Q, K, K] float64 on the device, or -- when the calibrated gain of this
+        time step is below min_gain, so that the correction cannot pay for its inference -- the shared
+        Maxwellian blocks [N_Q, K, K] themselves (no network call, no per-cell assembly)."""
         import torch
 
         B = f.shape[0]
         peq = torch.as_tensor(implicit.block_preconditioner(self.op, dt) if peq is None else peq,
                               dtype=torch.float64, device=f.device).contiguous()
+        if self._gain(dt) < self.min_gain:
+            return peq
         P = torch.empty((B, self.NQ, self.K, self.K), dtype=torch.float64, device=f.device)
         for b0 in range(0, B, self.net.max_batch):
             b1 = min(B, b0 + self.net.max_batch)

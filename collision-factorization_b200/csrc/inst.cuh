@@ -276,6 +276,15 @@ static LaunchResult launch_rf(const LaunchArgs& a) {
 // The few-cell kernel with f and Q_in (host arrays a.few_host_f, a.few_host_q) copied into its
 // parameter block; Q_out to a.q_cm.  A launch the driver refuses (status -1) leaves the caller to
 // take the copy route; the refusal is not sticky.
+// A parameter-block launch that the device refuses for its size or resources (cudaErrorInvalidValue,
+// cudaErrorLaunchOutOfResources) does not apply, and the caller falls back to the copy route; any
+// other launch error is a failure, reported with its CUDA code.
+static LaunchResult few_param_status(cudaError_t e) {
+    if (e == cudaSuccess) return {0, 1, cudaSuccess, PATH_FEW};
+    if (e == cudaErrorInvalidValue || e == cudaErrorLaunchOutOfResources) return {-1, 0, cudaSuccess, PATH_FEW};
+    return {5, 0, e, PATH_FEW};
+}
+
 template <int K, bool RF, int CAP>
 static LaunchResult launch_few_param(const LaunchArgs& a, dim3 grid, size_t smem, size_t need) {
     static_assert(sizeof(FewPayload<CAP>) + sizeof(DevOp) + 16 <= 32764, "parameter block too large");
@@ -292,9 +301,7 @@ static LaunchResult launch_few_param(const LaunchArgs& a, dim3 grid, size_t smem
     std::memcpy(pay.v + half, a.few_host_q, half * sizeof(double));
     std::memset(pay.v + need, 0, (CAP - need) * sizeof(double));
     kern<<<grid, kFewWarps * 32, smem, a.stream>>>(a.op, pay, (int)a.n_cells, a.q_cm);
-    const cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return {-1, 0, cudaSuccess, PATH_FEW};
-    return {0, 1, cudaSuccess, PATH_FEW};
+    return few_param_status(cudaGetLastError());
 }
 
 // Few-cell kernel on the cell-major arrays: one CTA per (q1 row, cell).  Status -1 where
@@ -349,8 +356,7 @@ static LaunchResult launch_few_exact_param(const LaunchArgs& a, dim3 grid, size_
     std::memcpy(pay.v + half, a.few_host_q, half * sizeof(double));
     std::memset(pay.v + need, 0, (CAP - need) * sizeof(double));
     kern<<<grid, kFewWarps * 32, smem, a.stream>>>(a.op, pay, (int)a.n_cells, a.q_cm);
-    if (cudaGetLastError() != cudaSuccess) return {-1, 0, cudaSuccess, PATH_FEW};
-    return {0, 1, cudaSuccess, PATH_FEW};
+    return few_param_status(cudaGetLastError());
 }
 
 template <int K>

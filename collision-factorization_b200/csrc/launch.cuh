@@ -14,7 +14,9 @@ enum Op { OP_AF = 0, OP_RF = 1, OP_JV = 2 };
 enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3, PATH_PAIR_L1 = 4, PATH_PAIR_SPLIT = 5, PATH_TILE_MMA = 6,
            PATH_BF16_MMA = 7 /* reported only: the BF16-split form's kernel */,
            PATH_TILE4 = 8 /* reported only: the quarter-tile kernel, where the 16-cell tile does not fit */,
-           PATH_FEW = 9 /* reported only: the few-cell kernel (a handful of cells per call) */ };
+           PATH_FEW = 9 /* reported only: the few-cell kernel (a handful of cells per call) */,
+           PATH_SPLIT_I8 = 10 /* reported only: the exact-split form's kernel (split.cu) */,
+           PATH_BAND = 11 /* the FP64 band kernel on the cell-major arrays (split.cu); chosen automatically at K = 12 */ };
 
 struct LaunchArgs {
     DevOp op;

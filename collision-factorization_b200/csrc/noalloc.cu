@@ -40,10 +40,19 @@ int scratch_for_device(int device, void** out) {
     std::lock_guard<std::mutex> lk(g_mu);
     if (g_scratch_ptr[device] == nullptr) {
         int prev = -1;
-        if (cudaGetDevice(&prev) != cudaSuccess) return CF_ECUDA;
-        if (prev != device && cudaSetDevice(device) != cudaSuccess) return CF_ENODEVICE;
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) {
+            cf_set_last_error((std::string("cf_q_device_noalloc: cannot read the current device: ") +
+                               cudaGetErrorString(e)).c_str());
+            return CF_ECUDA;
+        }
+        if (prev != device && (e = cudaSetDevice(device)) != cudaSuccess) {
+            cf_set_last_error((std::string("cf_q_device_noalloc: cannot select device ") + std::to_string(device) +
+                               ": " + cudaGetErrorString(e)).c_str());
+            return CF_ENODEVICE;
+        }
         void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (prev != device) cudaSetDevice(prev);
         if (e != cudaSuccess || p == nullptr) {
             cf_set_last_error((std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e)).c_str());
@@ -63,6 +72,12 @@ extern "C" int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f
     cf_plan_info info;
     int st = cf_plan_get_info(plan, &info);
     if (st != CF_OK) return st;
+    // The split form builds its own device tables on first use (and keeps an error word): refused.
+    if (form == CF_FORM_AF_SYM_I8) {
+        cf_set_last_error("cf_q_device_noalloc: the split form (CF_FORM_AF_SYM_I8) is not available without "
+                          "allocation; use cf_q_device");
+        return CF_EUNSUPPORTED;
+    }
     // The folded forms run on the plan's folded twin, which its first use builds, with allocations.
     const bool folded = form == CF_FORM_AF_SYM || form == CF_FORM_AF_SYM_F32 || form == CF_FORM_AF_SYM_BF16;
     if (folded && !cf_plan_folded_built(plan)) {
@@ -70,6 +85,9 @@ extern "C" int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f
                           "allocates; make one cf_q_device or cf_q_tiled call in a folded form first");
         return CF_EINVAL;
     }
+    // The limit is checked for every batch, also where the route taken (the streamed tile kernel,
+    // the few-cell kernel) would leave the array unused: the size a call may pass does not depend
+    // on the route the library picks for it.
     size_t need = 0;
     st = cf_plan_workspace_size(plan, b, 0, &need);
     if (st != CF_OK) return st;

@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "split.cuh"
 #include "../../include/cf_b200.h"
 #include "common.cuh"
 #include "launch.cuh"
@@ -159,6 +160,10 @@ struct cf_plan {
     cf_plan* sym = nullptr;
     int fold_status = -1;
     std::mutex sym_mu;
+    // exact-split form (CF_FORM_AF_SYM_I8): built on the folded twin on first use
+    cf::SplitPlan* split = nullptr;
+    int split_status = -1;
+    std::mutex split_mu;
     std::vector<double> h_labels, h_vals, h_ic, h_R;  // host copies kept for building the folded operator
 
     DevOp op() const {
@@ -248,6 +253,10 @@ int upload(T** dst, const std::vector<T>& src, int64_t& bytes) {
 
 void free_plan_memory(cf_plan* p);
 void free_plan_memory(cf_plan* p) {
+    if (p->split) {
+        cf::split_destroy(p->split);
+        p->split = nullptr;
+    }
     if (p->sym) {
         free_plan_memory(p->sym);
         delete p->sym;
@@ -561,6 +570,9 @@ int launch_unpack(const cf_plan* p, const double* src, double* dst, int64_t B, c
 // FP64 Q forms on at most kFewCells cells, on the few-cell kernel (one launch).
 int get_sym(cf_plan* p, cf_plan** out);
 bool streamable(const cf_plan* p, const cf_plan* target, int what, bool exact, int f32);
+int run_split(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
+int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
+int check_split(cf_plan* p);
 
 // The fast FP64 angular-first (plain or folded) or radial-first form, or the exact angular-first
 // form, of at most kFewCells cells on the few-cell kernel; kNoFew where that kernel does not apply.  With host_f and host_q (host
@@ -581,6 +593,10 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
     if (B < 0) return fail(CF_ESHAPE, "B = %lld is negative", (long long)B);
     if (B == 0 || p->n_g == 0) return CF_OK;
     if (!q_dev || !f_dev || (what == 2 && !v_dev)) return fail(CF_EINVAL, "null device buffer");
+    if (f32 == 3) {
+        if (what != 0) return fail(CF_EUNSUPPORTED, "the split form computes Q only");
+        return run_split(p, q_dev, f_dev, B, st);
+    }
     {
         const int r = run_few(p, what, exact, q_dev, f_dev, B, st, sym, f32);
         if (r != kNoFew) return r;
@@ -595,6 +611,10 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
     if (what == 0) {
         cf_plan* target = p;
         if (sym) CF_TRY(get_sym(p, &target));
+        if (!exact && f32 == 0) {
+            const int r = run_band64(target, q_dev, f_dev, B, st);
+            if (r != kNoFew) return r;
+        }
         if (streamable(p, target, what, exact, f32)) {
             const StreamSync resident{nullptr, nullptr, nullptr, nullptr, nullptr, 0, 1, 0};
             return dispatch(target, 0, false, nullptr, nullptr, nullptr, B, st, nullptr, false, &resident, f_dev,
@@ -816,6 +836,74 @@ int get_sym(cf_plan* p, cf_plan** out) {
     p->fold_status = 0;
     *out = s;
     return CF_OK;
+}
+
+// The split operator of a folded plan (created on first use).
+int get_split(cf_plan* s, cf::SplitPlan** out) {
+    std::lock_guard<std::mutex> lk(s->split_mu);
+    if (s->split) {
+        *out = s->split;
+        return CF_OK;
+    }
+    if (s->split_status > 0) return fail(s->split_status, "the split form is not available for this operator");
+    const int st = cf::split_build(&s->split, s->op(), s->n_g, s->n_slices, s->device);
+    if (st != CF_OK) {
+        s->split_status = st;
+        return st;  // message set by split_build
+    }
+    s->split_status = 0;
+    s->dev_bytes += cf::split_device_bytes(s->split);
+    *out = s->split;
+    return CF_OK;
+}
+
+// Q += Q(f) in the split form on cell-major device arrays (one launch of af_split_kernel).
+int run_split(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st) {
+    if (!cf::split_supported_k(p->k)) return fail(CF_EUNSUPPORTED, "the split form needs K = 4, 8 or 12 (K = %d)", p->k);
+    cf_plan* target = nullptr;
+    CF_TRY(get_sym(p, &target));
+    cf::SplitPlan* sp = nullptr;
+    CF_TRY(get_split(target, &sp));
+    int64_t launches = 0;
+    CF_TRY(cf::split_run(sp, q_dev, f_dev, B, st, &launches));
+    g_launches += launches;
+    if (launches > 0) {
+        target->last_path = cf::PATH_SPLIT_I8;
+        p->last_path = cf::PATH_SPLIT_I8;
+    }
+    return CF_OK;
+}
+
+// The FP64 band kernel (af_band64_kernel) takes the fast angular-first Q forms at K = 12 with the
+// automatic kernel order, where the 16-cell tile does not fit and the gather kernel was the only
+// family; with kernel path PATH_BAND it takes them at K = 4 and 8 too.  CF_EUNSUPPORTED (not
+// applicable) when the operator has no unique (t, q1) slices, so the caller falls back.
+int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st) {
+    const bool wanted = cf::split_supported_k(target->k) &&
+                        ((target->k == 12 && target->path == 0) || target->path == cf::PATH_BAND);
+    if (!wanted) return kNoFew;
+    cf::SplitPlan* sp = nullptr;
+    const int st_build = get_split(target, &sp);
+    if (st_build != CF_OK) {
+        if (target->path == cf::PATH_BAND) return st_build;
+        g_last_error.clear();
+        return kNoFew;
+    }
+    int64_t launches = 0;
+    CF_TRY(cf::band64_run(sp, q_dev, f_dev, B, st, &launches));
+    g_launches += launches;
+    if (launches > 0) {
+        target->last_path = cf::PATH_BAND;
+        if (target->parent) target->parent->last_path = cf::PATH_BAND;
+    }
+    return CF_OK;
+}
+
+// After a synchronised split-form call: the error word of its launches.
+int check_split(cf_plan* p) {
+    cf_plan* target = p->sym;
+    if (!target || !target->split) return CF_OK;
+    return cf::split_check(target->split);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1211,7 +1299,7 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
         CF_TRY(run_device(p, what, exact, dQ, df, dv, B, p->d_ws, p->ws_bytes, p->stream, sym, f32));
         CF_CUDA(cudaMemcpyAsync(Q, dQ, cell_bytes, cudaMemcpyDeviceToHost, p->stream));
         CF_CUDA(cudaStreamSynchronize(p->stream));
-        return CF_OK;
+        return f32 == 3 ? check_split(p) : CF_OK;
     }
     if (B >= 2 * kHostChunkMin) {
         cf_plan* target = p;
@@ -1252,6 +1340,7 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
         const cudaError_t e = cudaStreamSynchronize(hs);
         if (e != cudaSuccess && st == CF_OK) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
     }
+    if (st == CF_OK && f32 == 3) st = check_split(p);
     return st;
 }
 
@@ -1268,6 +1357,7 @@ int form_what(int form, bool& exact, bool& sym, int& f32) {
         case CF_FORM_AF_EXACT: exact = true; return 0;
         case CF_FORM_RF_EXACT: exact = true; return 1;
         case CF_FORM_AF_SYM: exact = false; sym = true; return 0;
+        case CF_FORM_AF_SYM_I8: exact = false; sym = true; f32 = 3; return 0;
         default: return -1;
     }
 }
@@ -1381,6 +1471,7 @@ int cf_q_device_ws(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b,
     int f32 = 0;
     const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
+    std::lock_guard<std::mutex> lk(plan->mu);
     DeviceGuard guard(plan->device);
     return run_device(plan, what, exact, q_dev, f_dev, nullptr, b, workspace, workspace_bytes, (cudaStream_t)stream,
                       sym, f32);
@@ -1437,7 +1528,7 @@ int cf_q_tiled(cf_plan* plan, double* q_tiled, const double* f_tiled, int64_t b,
     int f32 = 0;
     const int what = form_what(form, exact, sym, f32);
     if (what < 0) return fail(CF_EINVAL, "unknown form %d", form);
-    if (f32) return fail(CF_EUNSUPPORTED, "the FP32 forms read FP64 cells through cf_q_device / cf_contract_host");
+    if (f32) return fail(CF_EUNSUPPORTED, "the FP32, BF16 and split forms read FP64 cells through cf_q_device / cf_contract_host");
     if (b < 0) return fail(CF_ESHAPE, "B is negative");
     if (b == 0 || plan->n_g == 0) return CF_OK;
     if (!q_tiled || !f_tiled) return fail(CF_EINVAL, "null device buffer");
@@ -1499,10 +1590,10 @@ extern "C" {
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    if (path < 0 || path > 6)
+    if (path < 0 || (path > 6 && path != cf::PATH_BAND))
         return fail(CF_EINVAL,
                     "kernel path %d is not 0 (auto), 1 (gather), 2 (tile), 3 (pair), 4 (pair, R via L1), 5 (pair, "
-                    "split rows) or 6 (tile, K^3 step on the FP64 MMA)",
+                    "split rows), 6 (tile, K^3 step on the FP64 MMA) or 11 (band)",
                     path);
     std::lock_guard<std::mutex> lk(plan->mu);
     plan->path = path;

@@ -410,69 +410,81 @@ cudaError_t upload(const S** dst, const S* src, size_t n, std::vector<void*>& ow
     return n ? cudaMemcpy(p, src, n * sizeof(S), cudaMemcpyHostToDevice) : cudaSuccess;
 }
 
-}  // namespace
+// The channels (l-triplets) and the CSR of their valid q_i (the reference stops each list at its
+// first -1), after checking the sizes and indices of the inputs.
+struct Channels {
+    std::vector<int> l1, l2, l3, vq_begin, vq_q;
+};
 
-extern "C" {
-
-int cf_rtensor_sumfac(double* R_out, const cf_sumfac_inputs* in, int32_t device, double* device_seconds) {
+int sumfac_channels(const char* fn, double* R_out, const cf_sumfac_inputs* in, int32_t device, Channels& chn) {
+    char msg[160];
     if (!R_out || !in) {
-        cf_set_last_error("cf_rtensor_sumfac: null argument");
+        snprintf(msg, sizeof(msg), "%s: null argument", fn);
+        cf_set_last_error(msg);
         return CF_EINVAL;
     }
     const int NK = in->k_max + 1, NL = in->n_l, NQ = in->n_q;
     const int L = (int)std::lround(std::sqrt((double)NQ)) - 1;
     if (in->k_max < 0 || NK > 12 || NL < 1 || NQ < 1 || (L + 1) * (L + 1) != NQ || L > kMaxL || in->n_x < 1 ||
         in->n_u1 < 0 || in->n_t1 < 0 || in->n_y2 < 0 || in->n_t2 < 0 || in->n_chi < 0 || in->n_eps < 0) {
-        cf_set_last_error("cf_rtensor_sumfac: sizes out of range (K_max+1 <= 12, N_Q = (L+1)^2 with L <= 31)");
+        snprintf(msg, sizeof(msg), "%s: sizes out of range (K_max+1 <= 12, N_Q = (L+1)^2 with L <= 31)", fn);
+        cf_set_last_error(msg);
         return CF_ESHAPE;
     }
     const double* arrays[] = {in->x_nodes, in->w_x, in->radial_norm, in->sh_norm, in->l_triplets, in->qi_valid};
     for (const double* p : arrays)
         if (!p) {
-            cf_set_last_error("cf_rtensor_sumfac: null input array");
+            snprintf(msg, sizeof(msg), "%s: null input array", fn);
+            cf_set_last_error(msg);
             return CF_EINVAL;
         }
     int n_dev = 0;
     if (cudaGetDeviceCount(&n_dev) != cudaSuccess || n_dev == 0) {
-        cf_set_last_error("cf_rtensor_sumfac: no CUDA device");
+        snprintf(msg, sizeof(msg), "%s: no CUDA device", fn);
+        cf_set_last_error(msg);
         return CF_ENODEVICE;
     }
     if (device < 0 || device >= n_dev) return CF_EINVAL;
 
-    // channels: l-triplets and the CSR of their valid q (the reference stops at the first -1)
-    std::vector<int> l1(NL), l2(NL), l3(NL), vq_begin(NL + 1, 0), vq_q;
+    std::vector<int>&l1 = chn.l1, &l2 = chn.l2, &l3 = chn.l3, &vq_begin = chn.vq_begin, &vq_q = chn.vq_q;
+    l1.assign(NL, 0);
+    l2.assign(NL, 0);
+    l3.assign(NL, 0);
+    vq_begin.assign(NL + 1, 0);
+    vq_q.clear();
     for (int ch = 0; ch < NL; ++ch) {
         l1[ch] = (int)in->l_triplets[ch];
         l2[ch] = (int)in->l_triplets[ch + NL];
         l3[ch] = (int)in->l_triplets[ch + 2 * NL];
         if (l1[ch] < 0 || l1[ch] > L || l2[ch] < 0 || l2[ch] > L || l3[ch] < 0 || l3[ch] > L) {
-            cf_set_last_error("cf_rtensor_sumfac: an l-triplet is outside 0..L");
+            snprintf(msg, sizeof(msg), "%s: an l-triplet is outside 0..L", fn);
+            cf_set_last_error(msg);
             return CF_EBADIDX;
         }
         for (int idx = 0; idx < NQ; ++idx) {
             const int q = (int)in->qi_valid[idx + (size_t)NQ * ch];
             if (q == -1) break;
             if (q < 1 || q > NQ) {
-                cf_set_last_error("cf_rtensor_sumfac: qi_valid holds an index outside 1..N_Q");
+                snprintf(msg, sizeof(msg), "%s: qi_valid holds an index outside 1..N_Q", fn);
+                cf_set_last_error(msg);
                 return CF_EBADIDX;
             }
             vq_q.push_back(q - 1);
         }
         vq_begin[ch + 1] = (int)vq_q.size();
     }
+    return CF_OK;
+}
+
+// The quadrature proper, from the channel lists and the gain tables compressed to the valid
+// (q, channel) pairs: pg1[(u * n_t1 + t) * nnz + j], pg2[y * nnz + j], j running over the pairs in
+// channel order and, within a channel, in qi_valid order.
+int sumfac_run(double* R_out, const cf_sumfac_inputs* in, const Channels& chn, const double* pg1_h,
+               const double* pg2_h, int32_t device, double* device_seconds) {
+    const int NK = in->k_max + 1, NL = in->n_l, NQ = in->n_q;
+    const int L = (int)std::lround(std::sqrt((double)NQ)) - 1;
+    const std::vector<int>&l1 = chn.l1, &l2 = chn.l2, &l3 = chn.l3, &vq_begin = chn.vq_begin, &vq_q = chn.vq_q;
     const int nnz = (int)vq_q.size();
-    // P_gain compressed to the valid (q, channel) pairs, slice-major
-    std::vector<double> pg1((size_t)in->n_u1 * in->n_t1 * nnz), pg2((size_t)in->n_y2 * nnz);
-    for (int ch = 0; ch < NL; ++ch)
-        for (int j = vq_begin[ch]; j < vq_begin[ch + 1]; ++j) {
-            const size_t q = (size_t)vq_q[j];
-            for (int u = 0; u < in->n_u1; ++u)
-                for (int t = 0; t < in->n_t1; ++t)
-                    pg1[((size_t)u * in->n_t1 + t) * nnz + j] =
-                        in->p_gain_p1[t + (size_t)in->n_t1 * (u + (size_t)in->n_u1 * (q + (size_t)NQ * ch))];
-            for (int y = 0; y < in->n_y2; ++y)
-                pg2[(size_t)y * nnz + j] = in->p_gain_p2[y + (size_t)in->n_y2 * (q + (size_t)NQ * ch)];
-        }
     std::vector<double> eps_c(in->n_eps), eps_s(in->n_eps);
     for (int e = 0; e < in->n_eps; ++e) {
         eps_c[e] = std::cos(in->eps[e]);
@@ -548,9 +560,9 @@ int cf_rtensor_sumfac(double* R_out, const cf_sumfac_inputs* in, int32_t device,
     RT_CHECK(upload(&d.vq_begin, vq_begin.data(), vq_begin.size(), owned));
     RT_CHECK(upload(&d.vq_q, vq_q.data(), vq_q.size(), owned));
     RT_CHECK(upload(&d.ploss1, in->p_loss_p1, (size_t)in->n_t1 * in->n_u1 * NL, owned));
-    RT_CHECK(upload(&d.pgain1, pg1.data(), pg1.size(), owned));
+    RT_CHECK(upload(&d.pgain1, pg1_h, (size_t)in->n_u1 * in->n_t1 * nnz, owned));
     RT_CHECK(upload(&d.ploss2, in->p_loss_p2, (size_t)in->n_y2 * NL, owned));
-    RT_CHECK(upload(&d.pgain2, pg2.data(), pg2.size(), owned));
+    RT_CHECK(upload(&d.pgain2, pg2_h, (size_t)in->n_y2 * nnz, owned));
     // chunk of items: the net vectors of a chunk (written by k_items, read once by k_contract) stay
     // within 48 MB, so they live in the 126 MB L2 between the two kernels instead of crossing HBM
     chunk = std::max<int64_t>(1, std::min<int64_t>(n_items, ((int64_t)48 << 20) / ((int64_t)NL * 2 * NK * 8)));
@@ -588,6 +600,50 @@ done:
     for (void* p : owned) cudaFree(p);
     cudaSetDevice(prev);
     return st;
+}
+
+
+}  // namespace
+
+extern "C" {
+
+int cf_rtensor_sumfac(double* R_out, const cf_sumfac_inputs* in, int32_t device, double* device_seconds) {
+    Channels chn;
+    int st = sumfac_channels("cf_rtensor_sumfac", R_out, in, device, chn);
+    if (st != CF_OK) return st;
+    if (!in->p_gain_p1 || !in->p_gain_p2) {
+        cf_set_last_error("cf_rtensor_sumfac: null input array");
+        return CF_EINVAL;
+    }
+    const int NQ = in->n_q;
+    const std::vector<int>&vq_begin = chn.vq_begin, &vq_q = chn.vq_q;
+    const int NL = in->n_l;
+    const int nnz = (int)vq_q.size();
+    // P_gain compressed to the valid (q, channel) pairs, slice-major
+    std::vector<double> pg1((size_t)in->n_u1 * in->n_t1 * nnz), pg2((size_t)in->n_y2 * nnz);
+    for (int ch = 0; ch < NL; ++ch)
+        for (int j = vq_begin[ch]; j < vq_begin[ch + 1]; ++j) {
+            const size_t q = (size_t)vq_q[j];
+            for (int u = 0; u < in->n_u1; ++u)
+                for (int t = 0; t < in->n_t1; ++t)
+                    pg1[((size_t)u * in->n_t1 + t) * nnz + j] =
+                        in->p_gain_p1[t + (size_t)in->n_t1 * (u + (size_t)in->n_u1 * (q + (size_t)NQ * ch))];
+            for (int y = 0; y < in->n_y2; ++y)
+                pg2[(size_t)y * nnz + j] = in->p_gain_p2[y + (size_t)in->n_y2 * (q + (size_t)NQ * ch)];
+        }
+    return sumfac_run(R_out, in, chn, pg1.data(), pg2.data(), device, device_seconds);
+}
+
+int cf_rtensor_sumfac_packed(double* R_out, const cf_sumfac_inputs* in, const double* p_gain_p1_packed,
+                             const double* p_gain_p2_packed, int32_t device, double* device_seconds) {
+    Channels chn;
+    int st = sumfac_channels("cf_rtensor_sumfac_packed", R_out, in, device, chn);
+    if (st != CF_OK) return st;
+    if (!p_gain_p1_packed || !p_gain_p2_packed) {
+        cf_set_last_error("cf_rtensor_sumfac_packed: null packed gain table");
+        return CF_EINVAL;
+    }
+    return sumfac_run(R_out, in, chn, p_gain_p1_packed, p_gain_p2_packed, device, device_seconds);
 }
 
 }  // extern "C"

@@ -1,0 +1,1007 @@
+// split.cu -- the exact-split form CF_FORM_AF_SYM_I8: Q(f) to ~1e-11 with the K^3 step on the
+// int8 tensor cores.
+//
+// What is computed (angular first on the q2 <-> q3 folded operator, as CF_FORM_AF_SYM):
+//
+//   Q[q1,k1] += sum_t sum_kk R_t[k1,kk] Phi_{t,q1}[kk],  Phi_{t,q1} = sum_z G_z f[q2] (x) f[q3]
+//
+// (src/mex/angular_first_collision_kernel_mex.cpp:45-69 is the reference's per-slice loop).  The
+// Phi step runs in FP64 on the CUDA cores.  The K^3 step is a sum of products with exact integer
+// operands on the tensor cores:
+//
+//   * R_t is scaled by a power of two s_t so that |R_t s_t| < 1 (1/s_t goes into G), rounded to
+//     R_int = rint(R_t s_t 2^46) and written as six balanced signed bytes r_0..r_5 at plan time;
+//   * Phi' = sum_z (G_z / s_t) f (x) f of one (row, cell) is scaled by 2^e, e fixed per (row, cell)
+//     from an a-priori bound (below) so that |X| < 2^47, X = rint(Phi' 2^e), and X is split into its
+//     two's-complement bytes a_0..a_4 (unsigned) and a_5 (signed);
+//   * sum_kk X R_int = sum_{i,j} 2^{8(i+j)} sum_kk a_i r_j: every product of bytes is exact, and the
+//     sums over kk accumulate exactly in int32 (tcgen05.mma kind::i8) in tensor memory, one
+//     accumulator block per weight d = i + j over the whole t-list of a row group;
+//   * the blocks are recombined in FP64: Q += sum_d 2^{8d} D_d / 2^{e+46}.  Blocks d < 4 (weights
+//     below 2^-48 of the top) are not formed.
+//
+// The bound: |Phi'_{t,q1}[kk]| <= (sum_z |G_z/s_t|) * max|f(band l2)| * max|f(band l3)|, where the
+// band maxima are taken over the cell's staged coefficients; e = 46 - ceil(log2(bound over the
+// row's slices)).  The error left is the rounding of X and R_int: measured 1.1e-11 of max|Q| on the
+// hard-sphere L = 10, K = 8 operator against 5.6e-10 with one more block dropped.
+//
+// Work decomposition: a CTA (16 warps) owns 4 cells (f resident in shared memory) and a row group
+// of one l1 band: up to 16 "slots" (a row, or a contiguous chunk of a row's entries when a band has
+// few rows), one per warp.  The band's l-triplets t are walked in order; per t every warp computes
+// its slot's Phi (4 cells x 8 lanes, each lane a (k2 half, k3 quarter) part of K^2), quantises it,
+// and the six byte planes are written plane by plane into a 3-deep ring of shared-memory A tiles
+// (M = 64 rows: 16 slots x 4 cells).  One thread issues, per plane, one MMA
+// per 32-byte K step against a window of the six R planes (B, staged per t into a 2-deep ring by
+// one cp.async.bulk each), into the accumulator blocks d = i + j the window reaches.
+// Accumulators are drained when the row group is done (or earlier, before int32 could overflow),
+// and the slots of one row are summed in a fixed order, so results are deterministic.
+//
+// Every wait (mbarriers of the copies and of the MMAs) is bounded by a clock budget; a CTA that
+// gives up records an error word, stops issuing work and leaves through the normal exit path.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cf_b200.h"
+#include "split.cuh"
+#include "tc05.cuh"
+
+void cf_set_last_error(const char* msg);
+
+namespace cf {
+
+namespace {
+
+constexpr int kCells = 4;        // cells per CTA
+constexpr int kSlots = 16;       // row slots per CTA, one per warp
+constexpr int kWarps = 16;
+constexpr int kThreads = kWarps * 32;
+constexpr int kPlanes = 6;       // bytes of X and of R_int
+constexpr int kDMin = 4;         // lowest block weight kept
+constexpr int kNB = 16;          // B rows per R plane (k1, padded)
+constexpr int kDBlocks = 11 - kDMin;
+constexpr int kTmemCols = 128;   // >= kDBlocks * kNB = 112
+// Accumulator row m (M = 64, one CTA) sits in TMEM lane 32 (m / 16) + m % 16: lanes 0-15 of each
+// warp quadrant.
+__device__ __forceinline__ int d_lane(int m) { return 32 * (m >> 4) + (m & 15); }
+constexpr int kARing = 3;
+constexpr int kBRing = 2;
+constexpr int kM = 64;                    // MMA rows: 16 slots x 4 cells
+constexpr int kATile = kM * 32;           // one 32-byte K step of the A tile
+constexpr int kBStep = kPlanes * kNB * 32;  // one K step of the six R planes
+constexpr int kRShift = 46;               // R_int = rint(R_t s_t 2^46)
+constexpr int kXBits = 46;                // |X| <= 2^46 (1 bit of margin below the 47 the bytes hold)
+constexpr long long kWaitCycles = 2000000000LL;  // ~1 s of SM clock per wait
+
+template <int K>
+struct Shape {
+    static_assert(K % 4 == 0 && K <= 12, "the split form splits K^2 over 8 lanes: K in {4, 8, 12}");
+    static constexpr int KH = K / 2;                // k2 per lane (two halves)
+    static constexpr int KQ = K / 4;                // k3 per lane (four quarters)
+    static constexpr int E = KH * KQ;               // Phi elements per lane
+    static constexpr int EP = (E + 3) / 4 * 4;      // bytes per lane in a plane (word aligned)
+    static constexpr int KK = 8 * EP;               // K dimension of the MMA (kk = part * EP + e)
+    static constexpr int NKS = KK / 32;             // 32-byte K steps
+    static_assert(KK % 32 == 0, "whole K steps");
+    static constexpr int PS = E * K + 2;            // FP64 R: doubles per part (16 bytes of padding
+                                                    // keep the 8 parts' 16-byte loads on distinct banks)
+    static constexpr int RT_BYTES = 8 * PS * 8;     // FP64 R_t of one t
+};
+
+struct SplitArgs {
+    const int* slice_e;
+    const uint32_t* e_q23;
+    const double* e_gs;        // G_z / s_t, in slice order (the split kernel)
+    const double* e_g;         // G_z, in slice order (the FP64 band kernel)
+    const double* rfp64;       // FP64 R_t per t as [part][e][k1], parts kPartStride<K> doubles apart
+    const uint8_t* rplanes;    // [t][NKS][K step: 6 planes x 16 rows x 32 bytes, canonical]
+    const double* gs;          // per slice: sum |G_z / s_t|
+    const int* t_l23;          // per t: l2 | l3 << 8
+    const int* units;          // per row group: 8 ints (unit_*)
+    const int* unit_order;     // row groups, heaviest first
+    const int* band_tl;        // t-lists of the bands
+    const int* band_slice;     // per band: [n_t][2 l1 + 1] slice or -1
+    const double* f;           // cell-major [B][K][N_Q]
+    double* q;
+    int* err;
+    long long n_cells;
+    int n_cg;                  // cell groups: ceil(B / 4)
+    int n_q, L;
+    int tseg;                  // t per accumulation segment (int32 bound)
+    // shared-memory offsets (bytes)
+    int off_a, off_b, off_f, off_mb, off_red, off_scale, off_eexp, off_bar, off_misc;
+};
+
+enum { U_L1 = 0, U_R0, U_NR, U_S, U_TLOFF, U_NT, U_TABOFF, U_BROWS, U_INTS };
+
+struct Layout {
+    int off_a, off_b, off_f, off_mb, off_red, off_scale, off_eexp, off_bar, off_misc, total;
+};
+
+template <int K>
+Layout smem_layout(int n_q, int L) {
+    using S = Shape<K>;
+    Layout l{};
+    int o = 0;
+    auto take = [&](int bytes, int align) {
+        o = (o + align - 1) / align * align;
+        const int r = o;
+        o += bytes;
+        return r;
+    };
+    l.off_a = take(kARing * S::NKS * kATile, 1024);
+    l.off_b = take(kBRing * S::NKS * kBStep, 1024);
+    l.off_f = take(kCells * n_q * K * (int)sizeof(double), 16);
+    l.off_mb = take(kCells * (L + 1) * (int)sizeof(double), 16);
+    l.off_red = take(kSlots * kCells * K * (int)sizeof(double), 16);
+    l.off_scale = take(kSlots * kCells * (int)sizeof(double), 16);
+    l.off_eexp = take(kSlots * kCells * (int)sizeof(int), 16);
+    l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
+    l.off_misc = take(16 * (int)sizeof(int), 16);
+    l.total = o;
+    return l;
+}
+
+template <int K>
+Layout band64_layout(int n_q) {
+    using S = Shape<K>;
+    Layout l{};
+    int o = 0;
+    auto take = [&](int bytes, int align) {
+        o = (o + align - 1) / align * align;
+        const int r = o;
+        o += bytes;
+        return r;
+    };
+    l.off_b = take(2 * S::RT_BYTES, 1024);
+    l.off_f = take(kCells * n_q * K * (int)sizeof(double), 16);
+    l.off_red = take(kSlots * kCells * K * (int)sizeof(double), 16);
+    l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
+    l.off_misc = take(16 * (int)sizeof(int), 16);
+    l.total = o;
+    return l;
+}
+
+// Bounded wait on an mbarrier phase; on timeout (or if another thread already gave up) sets the
+// CTA's abort word and the error word, and returns false.
+__device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err) {
+    if (*abort_flag) return false;
+    const long long t0 = clock64();
+    for (;;) {
+        if (tc05::mbar_try_wait(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (clock64() - t0 > kWaitCycles) {
+            *abort_flag = 1;
+            atomicExch(err, 1);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t byte_word(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t x3, int ib) {
+    // byte ib of x0..x3, packed little-endian
+    const uint32_t sel = (uint32_t)ib | ((uint32_t)(ib + 4) << 4);
+    const uint32_t t01 = __byte_perm(x0, x1, sel);
+    const uint32_t t23 = __byte_perm(x2, x3, sel);
+    return __byte_perm(t01, t23, 0x5410);
+}
+
+// Phi of one slot for this lane's (k2 half, k3 quarter) part of one cell: the entries of the slot's
+// chunk of slice sl, grouped by q2 (h = sum G f(q3) over a run of equal q2, then phi += f(q2) (x) h).
+template <int K>
+__device__ __forceinline__ void slot_phi(const SplitArgs& a, const double* __restrict__ gv,
+                                         const double* __restrict__ fs, int NQ, int sl, int ch, int nS, int lane,
+                                         int c, int k2h, int k3q, double (&phi)[Shape<K>::KH][Shape<K>::KQ]) {
+    constexpr int KH = Shape<K>::KH, KQ = Shape<K>::KQ;
+#pragma unroll
+    for (int x = 0; x < KH; ++x)
+#pragma unroll
+        for (int y = 0; y < KQ; ++y) phi[x][y] = 0.0;
+    if (sl < 0) return;
+    const int e0 = a.slice_e[sl], n = a.slice_e[sl + 1] - e0;
+    const int cb = e0 + (int)(((long long)n * ch) / nS), ce = e0 + (int)(((long long)n * (ch + 1)) / nS);
+    double h[KQ];
+#pragma unroll
+    for (int y = 0; y < KQ; ++y) h[y] = 0.0;
+    int cur = -1;
+    auto flush = [&]() {
+#pragma unroll
+        for (int x = 0; x < KH; ++x) {
+            const double f2 = fs[((k2h * KH + x) * NQ + cur) * kCells + c];
+#pragma unroll
+            for (int y = 0; y < KQ; ++y) phi[x][y] = fma(f2, h[y], phi[x][y]);
+        }
+#pragma unroll
+        for (int y = 0; y < KQ; ++y) h[y] = 0.0;
+    };
+    for (int eb = cb; eb < ce; eb += 32) {
+        const int nb = min(32, ce - eb);
+        uint32_t my_q23 = 0;
+        double my_g = 0.0;
+        if (lane < nb) {
+            my_q23 = __ldg(a.e_q23 + eb + lane);
+            my_g = __ldg(gv + eb + lane);
+        }
+        for (int j = 0; j < nb; ++j) {
+            const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, j);
+            const double g = __shfl_sync(0xffffffffu, my_g, j);
+            const int q2 = (int)(q23 & 0xffffu), q3 = (int)(q23 >> 16);
+            if (q2 != cur) {
+                if (cur >= 0) flush();
+                cur = q2;
+            }
+#pragma unroll
+            for (int y = 0; y < KQ; ++y) h[y] = fma(g, fs[((k3q * KQ + y) * NQ + q3) * kCells + c], h[y]);
+        }
+    }
+    if (cur >= 0) flush();
+}
+
+// The cells' f (cell-major in global memory) into shared memory as fs[(k N_Q + q) 4 + cell], zero
+// past the end of the batch.
+__device__ __forceinline__ void stage_f(const SplitArgs& a, double* fs, int M, long long cell0, int tid) {
+    for (int i = tid; i < kCells * M; i += kThreads) {
+        const int cc = i % kCells, r = i / kCells;  // r = k N_Q + q: the cell-major element index
+        const long long cell = cell0 + cc;
+        fs[i] = cell < a.n_cells ? __ldg(a.f + cell * M + r) : 0.0;
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
+    using S = Shape<K>;
+    constexpr int KH = S::KH, KQ = S::KQ, E = S::E, EP = S::EP, NKS = S::NKS;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint8_t* sA = smem + a.off_a;
+    uint8_t* sB = smem + a.off_b;
+    double* fs = reinterpret_cast<double*>(smem + a.off_f);
+    double* mb = reinterpret_cast<double*>(smem + a.off_mb);
+    double* red = reinterpret_cast<double*>(smem + a.off_red);
+    double* scale = reinterpret_cast<double*>(smem + a.off_scale);
+    int* eexp = reinterpret_cast<int*>(smem + a.off_eexp);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + a.off_bar);
+    uint64_t* bfull = bars;        // [2] R planes of a t have landed
+    uint64_t* bfree = bars + 2;    // [2] the MMAs reading a B slot are done
+    uint64_t* afree = bars + 4;    // [3] the MMAs reading an A tile are done
+    uint64_t* dbar = bars + 7;     // all MMAs issued so far are done (drains)
+    int* misc = reinterpret_cast<int*>(smem + a.off_misc);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(misc);
+    volatile int* abort_flag = misc + 1;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int c = lane & 3, part = lane >> 2, k2h = part & 1, k3q = part >> 1;
+    const int NQ = a.n_q, L = a.L, M = NQ * K;
+    const int rg = a.unit_order[blockIdx.x / a.n_cg];
+    const int cg = blockIdx.x % a.n_cg;
+    const int* u = a.units + (size_t)rg * U_INTS;
+    const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], nS = u[U_S], tl_off = u[U_TLOFF], n_t = u[U_NT],
+              tab_off = u[U_TABOFF], brows = u[U_BROWS];
+    const int n_slots = nr * nS;
+    const long long cell0 = (long long)cg * kCells;
+
+    // ---- set-up: barriers, tensor memory, zero A tiles, f staged -----------------------------
+    if (tid == 0) {
+        for (int i = 0; i < 8; ++i) tc05::mbar_init(&bars[i], 1);
+        tc05::fence_mbar_init();
+        *abort_flag = 0;
+    }
+    if (warp == 0) {
+        tc05::tmem_alloc(tslot, kTmemCols);
+        tc05::tmem_relinquish();
+    }
+    {
+        uint4* z = reinterpret_cast<uint4*>(sA);
+        for (int i = tid; i < kARing * NKS * kATile / 16; i += kThreads) z[i] = make_uint4(0, 0, 0, 0);
+    }
+    stage_f(a, fs, M, cell0, tid);
+    tc05::tc_fence_before();
+    __syncthreads();
+    tc05::tc_fence_after();
+    const uint32_t tbase = *tslot;
+    const int bbytes = NKS * kBStep;
+    if (tid == 0) {
+        for (int ti = 0; ti < min(n_t, kBRing); ++ti) {
+            const int t = a.band_tl[tl_off + ti];
+            tc05::mbar_arrive_expect_tx(&bfull[ti], (uint32_t)bbytes);
+            tc05::bulk_g2s(sB + ti * bbytes, a.rplanes + (size_t)t * bbytes, (uint32_t)bbytes, &bfull[ti]);
+        }
+    }
+    // band maxima of |f| per cell: mb[cell][l]
+    for (int pr = warp; pr < kCells * (L + 1); pr += kWarps) {
+        const int cc = pr / (L + 1), l = pr % (L + 1);
+        const int q0 = l * l, nq = 2 * l + 1;
+        double m = 0.0;
+        for (int i = lane; i < nq * K; i += 32) {
+            const int k = i / nq, q = q0 + i % nq;
+            m = fmax(m, fabs(fs[(k * NQ + q) * kCells + cc]));
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0) mb[cc * (L + 1) + l] = m;
+    }
+    __syncthreads();
+    // per (slot, cell): the exponent e from the a-priori bound over the row's slices
+    if (tid < kSlots * kCells) {
+        const int s = tid / kCells, cc = tid % kCells;
+        int e = 0;
+        if (s < n_slots) {
+            const int row = r0 + s / nS;
+            double bound = 0.0;
+            for (int ti = 0; ti < n_t; ++ti) {
+                const int sl = a.band_slice[tab_off + ti * brows + row];
+                if (sl < 0) continue;
+                const int l23 = a.t_l23[a.band_tl[tl_off + ti]];
+                bound = fmax(bound, a.gs[sl] * mb[cc * (L + 1) + (l23 & 0xff)] * mb[cc * (L + 1) + (l23 >> 8)]);
+            }
+            if (bound > 0.0) {
+                int x;
+                frexp(bound, &x);  // bound < 2^x
+                e = min(max(kXBits - x, -1000), 1000);
+            }
+        }
+        eexp[tid] = e;
+        scale[tid] = ldexp(1.0, e);
+    }
+    // zero the accumulators (lanes 0-63: quadrants 0 and 1)
+    auto zero_d = [&]() {
+        const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
+        for (int col = (warp >> 2) * 4; col < kDBlocks * kNB; col += 16)
+            tc05::tmem_st4(tbase + lb + col, 0u, 0u, 0u, 0u);
+        tc05::tmem_wait_st();
+    };
+    zero_d();
+    tc05::tc_fence_before();
+    __syncthreads();
+    tc05::tc_fence_after();
+
+    // ---- drain: accumulators -> FP64 -> Q (rows summed over their slots in a fixed order) ----
+    int n_drains = 0;
+    auto drain = [&]() {
+        if (tid == 0) {
+            if (!*abort_flag) tc05::mma_commit(dbar);
+        }
+        __syncwarp();
+        const bool ok = __all_sync(0xffffffffu, wait_bar(dbar, (uint32_t)(n_drains & 1), abort_flag, a.err));
+        ++n_drains;
+        tc05::tc_fence_after();
+        constexpr int KG = (K + 3) / 4;  // k1 per drain warp
+        // the accumulator row m in TMEM lane 32 (warp % 4) + lane: M = 64 keeps rows 16q..16q+15 in
+        // lanes 0-15 of quadrant q; M = 128 keeps row m in lane m (rows 0-63 in quadrants 0 and 1)
+        const int m = kM == 64 ? 16 * (warp & 3) + (lane & 15) : 32 * (warp & 3) + lane;
+        const bool holds = kM == 64 ? lane < 16 : (warp & 3) < 2;
+        if (ok && (kM == 64 || (warp & 3) < 2)) {
+            const int s = m / kCells, cc = m % kCells;
+            const int kg = warp >> 2;
+            const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
+            double acc[KG];
+#pragma unroll
+            for (int j = 0; j < KG; ++j) acc[j] = 0.0;
+#pragma unroll
+            for (int d = kDMin; d <= 10; ++d) {
+                // the block's 16 columns; this warp keeps k1 = kg * KG .. kg * KG + KG - 1
+                uint32_t r16[16];
+                uint32_t* lo8 = r16;
+                uint32_t* hi8 = r16 + 8;
+                tc05::tmem_ld8(tbase + lb + (uint32_t)((d - kDMin) * kNB), *reinterpret_cast<uint32_t(*)[8]>(lo8));
+                tc05::tmem_ld8(tbase + lb + (uint32_t)((d - kDMin) * kNB + 8), *reinterpret_cast<uint32_t(*)[8]>(hi8));
+                tc05::tmem_wait_ld();
+                const double w = ldexp(1.0, 8 * d - kRShift - eexp[m]);
+#pragma unroll
+                for (int j = 0; j < KG; ++j) {
+                    const int want = kg * KG + j;
+                    uint32_t v = 0;
+#pragma unroll
+                    for (int x = 0; x < 16; ++x) v = (x == want) ? r16[x] : v;
+                    acc[j] += (double)(int)v * w;
+                }
+            }
+            if (holds && s < n_slots)
+#pragma unroll
+                for (int j = 0; j < KG; ++j)
+                    if (kg * KG + j < K) red[(s * kCells + cc) * K + kg * KG + j] = acc[j];
+        }
+        tc05::tc_fence_before();
+        __syncthreads();
+        if (tid < nr * kCells) {
+            const int rl = tid / kCells, cc = tid % kCells;
+            const long long cell = cell0 + cc;
+            if (cell < a.n_cells) {
+                const int q1 = l1 * l1 + r0 + rl;
+                double* qc = a.q + cell * M + q1;
+                for (int k1 = 0; k1 < K; ++k1) {
+                    double sum = 0.0;
+                    for (int ch = 0; ch < nS; ++ch) sum += red[((rl * nS + ch) * kCells + cc) * K + k1];
+                    qc[(size_t)k1 * NQ] += sum;
+                }
+            }
+        }
+        zero_d();
+        tc05::tc_fence_before();
+        __syncthreads();
+        tc05::tc_fence_after();
+    };
+
+    // ---- main loop over the band's l-triplets ------------------------------------------------
+    const bool active = warp < n_slots;
+    const int row = r0 + (active ? warp / nS : 0), ch = active ? warp % nS : 0;
+    const int m_row = warp * kCells + c;  // A row of this lane's (slot, cell)
+    const double sc = scale[m_row < kSlots * kCells ? m_row : 0];
+    constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer
+    for (int ti = 0; ti < n_t; ++ti) {
+        uint32_t lo[E], hi[E];
+        if (active) {
+            double phi[KH][KQ];
+            slot_phi<K>(a, a.e_gs, fs, NQ, a.band_slice[tab_off + ti * brows + row], ch, nS, lane, c, k2h, k3q, phi);
+#pragma unroll
+            for (int x = 0; x < KH; ++x)
+#pragma unroll
+                for (int y = 0; y < KQ; ++y) {
+                    const double yv = fma(phi[x][y], sc, kMagic);
+                    lo[x * KQ + y] = (uint32_t)__double2loint(yv);
+                    hi[x * KQ + y] = (uint32_t)(__double2hiint(yv) - 0x43380000);
+                }
+        }
+        // planes 0..5 through the A ring
+        for (int i = 0; i < kPlanes; ++i) {
+            const int g = ti * kPlanes + i, b = g % kARing, use = g / kARing;
+            if (use >= 1) wait_bar(&afree[b], (uint32_t)((use - 1) & 1), abort_flag, a.err);
+            if (active) {
+                uint8_t* tile = sA + b * NKS * kATile;
+#pragma unroll
+                for (int w = 0; w < EP / 4; ++w) {
+                    uint32_t v[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int e = 4 * w + j;
+                        v[j] = e < E ? (i < 4 ? lo[e < E ? e : 0] : hi[e < E ? e : 0]) : 0u;
+                    }
+                    const uint32_t word = byte_word(v[0], v[1], v[2], v[3], i & 3);
+                    const int kk = part * EP + 4 * w;
+                    const int off = (kk >> 5) * kATile + (m_row >> 3) * 256 + ((kk & 31) >> 4) * 128 + (m_row & 7) * 16 +
+                                    (kk & 15);
+                    *reinterpret_cast<uint32_t*>(tile + off) = word;
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+            tc05::tc_fence_before();
+            __syncthreads();
+            if (tid == 0 && !*abort_flag) {
+                tc05::tc_fence_after();
+                if (i == 0) {
+                    // refill the other B slot with the next t (its previous MMAs finished a plane ago)
+                    const int tn = ti + 1;
+                    if (tn >= kBRing && tn < n_t) {
+                        const int sb = tn % kBRing, useb = tn / kBRing;
+                        if (wait_bar(&bfree[sb], (uint32_t)((useb - 1) & 1), abort_flag, a.err)) {
+                            const int t = a.band_tl[tl_off + tn];
+                            tc05::mbar_arrive_expect_tx(&bfull[sb], (uint32_t)bbytes);
+                            tc05::bulk_g2s(sB + sb * bbytes, a.rplanes + (size_t)t * bbytes, (uint32_t)bbytes,
+                                           &bfull[sb]);
+                        }
+                    }
+                    wait_bar(&bfull[ti % kBRing], (uint32_t)((ti / kBRing) & 1), abort_flag, a.err);
+                }
+                if (!*abort_flag) {
+                    const uint8_t* tile = sA + b * NKS * kATile;
+                    const uint8_t* bslot = sB + (ti % kBRing) * bbytes;
+                    const int j0 = i < kDMin ? kDMin - i : 0;
+                    const int n = (kPlanes - j0) * kNB;
+                    const uint32_t idesc = tc05::idesc_i8(kM, n, i == kPlanes - 1, true);
+                    const uint32_t dcol = (uint32_t)((i + j0 - kDMin) * kNB);
+#pragma unroll
+                    for (int ks = 0; ks < NKS; ++ks) {
+                        const uint64_t ad = tc05::smem_desc_kmajor(tile + ks * kATile, 128, 256);
+                        const uint64_t bd = tc05::smem_desc_kmajor(bslot + ks * kBStep + j0 * (kNB / 8) * 256, 128, 256);
+                        tc05::mma_i8_ss(tbase + dcol, ad, bd, idesc, true);
+                    }
+                    tc05::mma_commit(&afree[b]);
+                    if (i == kPlanes - 1) tc05::mma_commit(&bfree[ti % kBRing]);
+                }
+            }
+            __syncwarp();
+        }
+        if ((ti + 1) % a.tseg == 0 && ti + 1 < n_t) drain();
+    }
+    drain();
+
+    // ---- tear-down --------------------------------------------------------------------------
+    tc05::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc05::tmem_dealloc(tbase, kTmemCols);
+}
+
+// The FP64 band kernel: the same units and Phi step, the K^3 step in FP64 on the CUDA cores from R_t
+// staged per t into a 2-deep shared-memory ring by one cp.async.bulk each ([part][e][k1], so a lane
+// reads its part's K x E block with 16-byte loads shared by the part's 4 cells).  Each lane
+// accumulates its part's share of Q(row, cell) over the band's t-list; the 8 parts and the slots of
+// a row are summed in a fixed order at the end.
+template <int K>
+__global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
+    using S = Shape<K>;
+    constexpr int KH = S::KH, KQ = S::KQ, E = S::E, PS = S::PS, RTB = S::RT_BYTES;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    double* rring = reinterpret_cast<double*>(smem + a.off_b);
+    double* fs = reinterpret_cast<double*>(smem + a.off_f);
+    double* red = reinterpret_cast<double*>(smem + a.off_red);
+    uint64_t* bfull = reinterpret_cast<uint64_t*>(smem + a.off_bar);
+    int* misc = reinterpret_cast<int*>(smem + a.off_misc);
+    volatile int* abort_flag = misc + 1;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int c = lane & 3, part = lane >> 2, k2h = part & 1, k3q = part >> 1;
+    const int NQ = a.n_q, M = NQ * K;
+    const int rg = a.unit_order[blockIdx.x / a.n_cg];
+    const int cg = blockIdx.x % a.n_cg;
+    const int* u = a.units + (size_t)rg * U_INTS;
+    const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], nS = u[U_S], tl_off = u[U_TLOFF], n_t = u[U_NT],
+              tab_off = u[U_TABOFF], brows = u[U_BROWS];
+    const int n_slots = nr * nS;
+    const long long cell0 = (long long)cg * kCells;
+
+    if (tid == 0) {
+        tc05::mbar_init(&bfull[0], 1);
+        tc05::mbar_init(&bfull[1], 1);
+        tc05::fence_mbar_init();
+        *abort_flag = 0;
+    }
+    stage_f(a, fs, M, cell0, tid);
+    __syncthreads();
+    if (tid == 0)
+        for (int ti = 0; ti < min(n_t, 2); ++ti) {
+            const int t = a.band_tl[tl_off + ti];
+            tc05::mbar_arrive_expect_tx(&bfull[ti], (uint32_t)RTB);
+            tc05::bulk_g2s(rring + ti * (RTB / 8), a.rfp64 + (size_t)t * (RTB / 8), (uint32_t)RTB, &bfull[ti]);
+        }
+
+    const bool active = warp < n_slots;
+    const int row = r0 + (active ? warp / nS : 0), ch = active ? warp % nS : 0;
+    double acc[K];
+#pragma unroll
+    for (int k1 = 0; k1 < K; ++k1) acc[k1] = 0.0;
+    for (int ti = 0; ti < n_t; ++ti) {
+        const int sb = ti & 1;
+        const bool ok = wait_bar(&bfull[sb], (uint32_t)((ti >> 1) & 1), abort_flag, a.err);
+        const int sl = active && ok ? a.band_slice[tab_off + ti * brows + row] : -1;
+        if (sl >= 0) {
+            double phi[KH][KQ];
+            slot_phi<K>(a, a.e_g, fs, NQ, sl, ch, nS, lane, c, k2h, k3q, phi);
+            const double* rp = rring + sb * (RTB / 8) + part * PS;
+#pragma unroll
+            for (int x = 0; x < KH; ++x)
+#pragma unroll
+                for (int y = 0; y < KQ; ++y) {
+                    const double2* r2 = reinterpret_cast<const double2*>(rp + (x * KQ + y) * K);
+#pragma unroll
+                    for (int j = 0; j < K / 2; ++j) {
+                        const double2 r = r2[j];
+                        acc[2 * j] = fma(r.x, phi[x][y], acc[2 * j]);
+                        acc[2 * j + 1] = fma(r.y, phi[x][y], acc[2 * j + 1]);
+                    }
+                }
+        }
+        __syncthreads();  // every warp is done with slot sb
+        if (tid == 0 && ti + 2 < n_t && !*abort_flag) {
+            const int t = a.band_tl[tl_off + ti + 2];
+            tc05::mbar_arrive_expect_tx(&bfull[sb], (uint32_t)RTB);
+            tc05::bulk_g2s(rring + sb * (RTB / 8), a.rfp64 + (size_t)t * (RTB / 8), (uint32_t)RTB, &bfull[sb]);
+        }
+    }
+    // the 8 parts of a cell sit in lanes c, c + 4, ..., c + 28
+#pragma unroll
+    for (int k1 = 0; k1 < K; ++k1) {
+        acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], 4);
+        acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], 8);
+        acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], 16);
+    }
+    if (active && lane < kCells)
+#pragma unroll
+        for (int k1 = 0; k1 < K; ++k1) red[(warp * kCells + lane) * K + k1] = acc[k1];
+    __syncthreads();
+    if (tid < nr * kCells) {
+        const int rl = tid / kCells, cc = tid % kCells;
+        const long long cell = cell0 + cc;
+        if (cell < a.n_cells) {
+            double* qc = a.q + cell * M + (l1 * l1 + r0 + rl);
+            for (int k1 = 0; k1 < K; ++k1) {
+                double sum = 0.0;
+                for (int chk = 0; chk < nS; ++chk) sum += red[((rl * nS + chk) * kCells + cc) * K + k1];
+                qc[(size_t)k1 * NQ] += sum;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------------------------------
+// Host side
+// ------------------------------------------------------------------------------------------
+struct SplitPlan {
+    int device = 0, n_q = 0, k = 0, n_l = 0, L = 0;
+    int n_rg = 0, tseg = 1;
+    int64_t bytes = 0;
+    int smem = 0;
+    const int* slice_e = nullptr;     // borrowed from the folded plan
+    const uint32_t* e_q23 = nullptr;  // borrowed
+    uint8_t* d_rplanes = nullptr;
+    double* d_e_gs = nullptr;
+    double* d_gs = nullptr;
+    int* d_t_l23 = nullptr;
+    int* d_units = nullptr;
+    int* d_unit_order = nullptr;
+    int* d_band_tl = nullptr;
+    int* d_band_slice = nullptr;
+    int* d_err = nullptr;             // set to 1 by a CTA whose bounded wait gave up
+    const double* e_g = nullptr;      // borrowed: G in slice order (FP64 band kernel)
+    double* d_rfp64 = nullptr;        // FP64 R_t per t as [part][e][k1] (FP64 band kernel)
+    Layout lay{};
+    Layout lay64{};
+};
+
+namespace {
+
+int fail_split(int st, const std::string& msg) {
+    cf_set_last_error(msg.c_str());
+    return st;
+}
+
+template <typename T>
+cudaError_t upload_vec(T** dst, const std::vector<T>& v, int64_t& bytes) {
+    *dst = nullptr;
+    const size_t n = std::max<size_t>(v.size(), 1);
+    cudaError_t e = cudaMalloc((void**)dst, n * sizeof(T));
+    if (e != cudaSuccess) return e;
+    bytes += (int64_t)(n * sizeof(T));
+    if (!v.empty()) e = cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice);
+    return e;
+}
+
+template <typename T>
+cudaError_t download(std::vector<T>& v, const T* src, size_t n) {
+    v.resize(n);
+    return n ? cudaMemcpy(v.data(), src, n * sizeof(T), cudaMemcpyDeviceToHost) : cudaSuccess;
+}
+
+int isqrt_int(int q) {
+    int l = (int)std::sqrt((double)q);
+    while (l * l > q) --l;
+    while ((l + 1) * (l + 1) <= q) ++l;
+    return l;
+}
+
+template <int K>
+void split_r_planes(const std::vector<double>& R, int n_l, std::vector<uint8_t>& planes, std::vector<double>& st_scale) {
+    using S = Shape<K>;
+    const size_t per_t = (size_t)S::NKS * kBStep;
+    planes.assign(per_t * n_l, 0);
+    st_scale.assign(n_l, 1.0);
+    for (int t = 0; t < n_l; ++t) {
+        const double* Rt = R.data() + (size_t)t * K * K * K;
+        double mx = 0.0;
+        for (int i = 0; i < K * K * K; ++i) mx = std::max(mx, std::fabs(Rt[i]));
+        int x = 0;
+        if (mx > 0.0) std::frexp(mx, &x);  // mx < 2^x
+        const double s = std::ldexp(1.0, -x);
+        st_scale[t] = s;
+        uint8_t* pt = planes.data() + per_t * t;
+        for (int p = 0; p < 8; ++p)
+            for (int e = 0; e < S::E; ++e) {
+                const int k2 = (p & 1) * S::KH + e / S::KQ, k3 = (p >> 1) * S::KQ + e % S::KQ;
+                const int kk = p * S::EP + e;
+                const int ks = kk >> 5, kb = kk & 31;
+                for (int k1 = 0; k1 < K; ++k1) {
+                    long long X = (long long)std::nearbyint(std::ldexp(Rt[k1 + K * k2 + K * K * k3] * s, kRShift));
+                    for (int j = 0; j < kPlanes; ++j) {
+                        long long d = ((X % 256) + 256) % 256;  // 0..255
+                        if (d >= 128) d -= 256;                 // balanced digit in [-128, 127]
+                        X = (X - d) / 256;
+                        const int n = j * kNB + k1;
+                        const size_t off = (size_t)ks * kBStep + (n >> 3) * 256 + (kb >> 4) * 128 + (n & 7) * 16 + (kb & 15);
+                        pt[off] = (uint8_t)(int8_t)d;
+                    }
+                }
+            }
+    }
+}
+
+template <int K>
+int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
+    using S = Shape<K>;
+    const int NQ = op.n_q, NL = op.n_l;
+    const int L = isqrt_int(NQ) - 1;
+    if ((L + 1) * (L + 1) != NQ) return fail_split(CF_EUNSUPPORTED, "split form: N_Q is not (L+1)^2");
+    std::vector<int> q1_begin, slice_t, slice_e;
+    std::vector<uint32_t> e_q23;
+    std::vector<double> e_g, R;
+    cudaError_t ce = download(q1_begin, op.q1_begin, (size_t)NQ + 1);
+    if (ce == cudaSuccess) ce = download(slice_t, op.slice_t, (size_t)n_slices);
+    if (ce == cudaSuccess) ce = download(slice_e, op.slice_e, (size_t)n_slices + 1);
+    if (ce == cudaSuccess) ce = download(e_q23, op.e_q23, (size_t)n_g);
+    if (ce == cudaSuccess) ce = download(e_g, op.e_g, (size_t)n_g);
+    if (ce == cudaSuccess) ce = download(R, op.R, (size_t)K * K * K * NL);
+    if (ce != cudaSuccess) return fail_split(CF_ECUDA, std::string("split form: download: ") + cudaGetErrorString(ce));
+
+    std::vector<uint8_t> planes;
+    std::vector<double> st;
+    split_r_planes<K>(R, NL, planes, st);
+    // FP64 R_t per t as [part][e][k1] with zero padding after each part
+    std::vector<double> rfp64((size_t)NL * 8 * S::PS, 0.0);
+    for (int t = 0; t < NL; ++t)
+        for (int pp = 0; pp < 8; ++pp)
+            for (int e = 0; e < S::E; ++e) {
+                const int k2 = (pp & 1) * S::KH + e / S::KQ, k3 = (pp >> 1) * S::KQ + e % S::KQ;
+                for (int k1 = 0; k1 < K; ++k1)
+                    rfp64[((size_t)t * 8 + pp) * S::PS + (size_t)e * K + k1] =
+                        R[(size_t)t * K * K * K + k1 + (size_t)K * k2 + (size_t)K * K * k3];
+            }
+    // G / s_t per entry, |G / s_t| summed per slice, (l2, l3) per t
+    std::vector<double> e_gs(n_g), gs(n_slices, 0.0);
+    std::vector<int> t_l23(NL, -1);
+    std::vector<int> slice_q1(n_slices, -1);
+    for (int q = 0; q < NQ; ++q)
+        for (int s = q1_begin[q]; s < q1_begin[q + 1]; ++s) slice_q1[s] = q;
+    for (int64_t s = 0; s < n_slices; ++s) {
+        const int t = slice_t[s];
+        for (int z = slice_e[s]; z < slice_e[s + 1]; ++z) {
+            e_gs[z] = e_g[z] / st[t];
+            gs[s] += std::fabs(e_gs[z]);
+            const int l2 = isqrt_int((int)(e_q23[z] & 0xffffu)), l3 = isqrt_int((int)(e_q23[z] >> 16));
+            const int v = l2 | (l3 << 8);
+            if (t_l23[t] < 0) t_l23[t] = v;
+            if (t_l23[t] != v) return fail_split(CF_EUNSUPPORTED, "split form: an l-triplet's entries mix (l2, l3)");
+        }
+    }
+    for (int t = 0; t < NL; ++t)
+        if (t_l23[t] < 0) t_l23[t] = 0;
+    // bands: t-lists and the (t, row) -> slice tables
+    std::vector<int> band_tl, band_slice, units;
+    std::vector<double> work;
+    const int cap = kSlots;
+    for (int l1 = 0; l1 <= L; ++l1) {
+        const int qa = l1 * l1, brows = 2 * l1 + 1;
+        std::vector<int> ts;
+        for (int r = 0; r < brows; ++r)
+            for (int s = q1_begin[qa + r]; s < q1_begin[qa + r + 1]; ++s) ts.push_back(slice_t[s]);
+        std::sort(ts.begin(), ts.end());
+        ts.erase(std::unique(ts.begin(), ts.end()), ts.end());
+        if (ts.empty()) continue;
+        const int tl_off = (int)band_tl.size(), tab_off = (int)band_slice.size();
+        band_tl.insert(band_tl.end(), ts.begin(), ts.end());
+        band_slice.insert(band_slice.end(), ts.size() * brows, -1);
+        std::vector<double> row_work(brows, 0.0);
+        for (int r = 0; r < brows; ++r)
+            for (int s = q1_begin[qa + r]; s < q1_begin[qa + r + 1]; ++s) {
+                const int ti = (int)(std::lower_bound(ts.begin(), ts.end(), slice_t[s]) - ts.begin());
+                int& cell = band_slice[tab_off + (size_t)ti * brows + r];
+                if (cell >= 0) return fail_split(CF_EUNSUPPORTED, "split form: a (t, q1) pair has two slices");
+                cell = s;
+                row_work[r] += (double)(slice_e[s + 1] - slice_e[s]);
+            }
+        // row groups: the split into groups of nr rows x S chunks (nr * S <= 16) that fills most slots
+        int best_g = 1;
+        double best_fill = -1.0;
+        for (int ng = 1; ng <= brows; ++ng) {
+            const int nr = (brows + ng - 1) / ng;
+            if (nr > cap) continue;
+            const double fill = (double)brows * (cap / nr) / (double)(ng * cap);
+            if (fill > best_fill + 1e-9) {
+                best_fill = fill;
+                best_g = ng;
+            }
+        }
+        int r = 0;
+        for (int gi = 0; gi < best_g; ++gi) {
+            const int nr = (brows - r + (best_g - gi) - 1) / (best_g - gi);
+            const int nS = cap / nr;
+            const int uu[U_INTS] = {l1, r, nr, nS, tl_off, (int)ts.size(), tab_off, brows};
+            units.insert(units.end(), uu, uu + U_INTS);
+            double w = 0.0;
+            for (int x = r; x < r + nr; ++x) w += row_work[x];
+            work.push_back(w * K * K + (double)ts.size() * 4096.0);
+            r += nr;
+        }
+    }
+    const int n_rg = (int)work.size();
+    std::vector<int> order(n_rg);
+    for (int i = 0; i < n_rg; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work[x] > work[y]; });
+
+    sp->n_q = NQ;
+    sp->k = K;
+    sp->n_l = NL;
+    sp->L = L;
+    sp->n_rg = n_rg;
+    // int32 accumulators: at most 6 byte products of |255 * 128| per K element and weight
+    sp->tseg = std::max(1, (int)(2147483647LL / (6LL * 255 * 128 * S::KK)));
+    sp->slice_e = op.slice_e;
+    sp->e_q23 = op.e_q23;
+    sp->e_g = op.e_g;
+    sp->lay = smem_layout<K>(NQ, L);
+    sp->lay64 = band64_layout<K>(NQ);
+    sp->smem = sp->lay.total;
+    int64_t bytes = 0;
+    if ((ce = upload_vec(&sp->d_rplanes, planes, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_e_gs, e_gs, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_gs, gs, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_t_l23, t_l23, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_units, units, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_unit_order, order, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_band_tl, band_tl, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_band_slice, band_slice, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_err, std::vector<int>(1, 0), bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_rfp64, rfp64, bytes)) != cudaSuccess)
+        return fail_split(ce == cudaErrorMemoryAllocation ? CF_ENOMEM : CF_ECUDA,
+                          std::string("split form: upload: ") + cudaGetErrorString(ce));
+    sp->bytes = bytes;
+    return CF_OK;
+}
+
+template <int K>
+int run_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        const cudaError_t e = cudaFuncSetAttribute(af_split_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   227 * 1024);
+        if (e != cudaSuccess)
+            return fail_split(CF_ECUDA, std::string("split form: smem attribute: ") + cudaGetErrorString(e));
+        attr_set[dev] = true;
+    }
+    SplitArgs a{};
+    a.slice_e = sp->slice_e;
+    a.e_q23 = sp->e_q23;
+    a.e_gs = sp->d_e_gs;
+    a.rplanes = sp->d_rplanes;
+    a.gs = sp->d_gs;
+    a.t_l23 = sp->d_t_l23;
+    a.units = sp->d_units;
+    a.unit_order = sp->d_unit_order;
+    a.band_tl = sp->d_band_tl;
+    a.band_slice = sp->d_band_slice;
+    a.f = f_cm;
+    a.q = q_cm;
+    a.err = sp->d_err;
+    a.n_cells = B;
+    a.n_cg = (int)((B + kCells - 1) / kCells);
+    a.n_q = sp->n_q;
+    a.L = sp->L;
+    a.tseg = sp->tseg;
+    a.off_a = sp->lay.off_a;
+    a.off_b = sp->lay.off_b;
+    a.off_f = sp->lay.off_f;
+    a.off_mb = sp->lay.off_mb;
+    a.off_red = sp->lay.off_red;
+    a.off_scale = sp->lay.off_scale;
+    a.off_eexp = sp->lay.off_eexp;
+    a.off_bar = sp->lay.off_bar;
+    a.off_misc = sp->lay.off_misc;
+    const long long blocks = (long long)sp->n_rg * a.n_cg;
+    if (blocks > 0x7fffffffLL) return fail_split(CF_ESHAPE, "split form: batch too large for one launch");
+    af_split_kernel<K><<<(unsigned)blocks, kThreads, sp->smem, st>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("split form: launch: ") + cudaGetErrorString(e));
+    if (launches) ++*launches;
+    return CF_OK;
+}
+
+template <int K>
+int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        const cudaError_t e = cudaFuncSetAttribute(af_band64_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   227 * 1024);
+        if (e != cudaSuccess)
+            return fail_split(CF_ECUDA, std::string("band kernel: smem attribute: ") + cudaGetErrorString(e));
+        attr_set[dev] = true;
+    }
+    SplitArgs a{};
+    a.slice_e = sp->slice_e;
+    a.e_q23 = sp->e_q23;
+    a.e_g = sp->e_g;
+    a.rfp64 = sp->d_rfp64;
+    a.units = sp->d_units;
+    a.unit_order = sp->d_unit_order;
+    a.band_tl = sp->d_band_tl;
+    a.band_slice = sp->d_band_slice;
+    a.f = f_cm;
+    a.q = q_cm;
+    a.err = sp->d_err;
+    a.n_cells = B;
+    a.n_cg = (int)((B + kCells - 1) / kCells);
+    a.n_q = sp->n_q;
+    a.L = sp->L;
+    a.off_b = sp->lay64.off_b;
+    a.off_f = sp->lay64.off_f;
+    a.off_red = sp->lay64.off_red;
+    a.off_bar = sp->lay64.off_bar;
+    a.off_misc = sp->lay64.off_misc;
+    const long long blocks = (long long)sp->n_rg * a.n_cg;
+    if (blocks > 0x7fffffffLL) return fail_split(CF_ESHAPE, "band kernel: batch too large for one launch");
+    af_band64_kernel<K><<<(unsigned)blocks, kThreads, sp->lay64.total, st>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("band kernel: launch: ") + cudaGetErrorString(e));
+    if (launches) ++*launches;
+    return CF_OK;
+}
+
+}  // namespace
+
+bool split_supported_k(int k) { return k == 4 || k == 8 || k == 12; }
+
+int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
+    if (B <= 0 || sp->n_rg == 0) return CF_OK;
+    switch (sp->k) {
+        case 4: return run64_impl<4>(sp, q_cm, f_cm, B, st, launches);
+        case 8: return run64_impl<8>(sp, q_cm, f_cm, B, st, launches);
+        default: return run64_impl<12>(sp, q_cm, f_cm, B, st, launches);
+    }
+}
+
+int split_build(SplitPlan** out, const DevOp& folded, int64_t n_g, int64_t n_slices, int device) {
+    *out = nullptr;
+    if (!split_supported_k(folded.k))
+        return fail_split(CF_EUNSUPPORTED, "split form: K must be 4, 8 or 12");
+    SplitPlan* sp = new SplitPlan();
+    sp->device = device;
+    int st = CF_OK;
+    switch (folded.k) {
+        case 4: st = build_impl<4>(sp, folded, n_g, n_slices); break;
+        case 8: st = build_impl<8>(sp, folded, n_g, n_slices); break;
+        default: st = build_impl<12>(sp, folded, n_g, n_slices); break;
+    }
+    if (st == CF_OK) {
+        int optin = 0;
+        cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+        if (sp->smem > optin) {
+            char msg[160];
+            snprintf(msg, sizeof(msg), "split form: %d bytes of shared memory needed, %d available", sp->smem, optin);
+            st = fail_split(CF_EUNSUPPORTED, msg);
+        }
+    }
+    if (st != CF_OK) {
+        split_destroy(sp);
+        return st;
+    }
+    *out = sp;
+    return CF_OK;
+}
+
+void split_destroy(SplitPlan* sp) {
+    if (!sp) return;
+    void* ptrs[] = {sp->d_rplanes, sp->d_e_gs, sp->d_gs, sp->d_t_l23, sp->d_units, sp->d_unit_order, sp->d_band_tl,
+                    sp->d_band_slice, sp->d_err, sp->d_rfp64};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    delete sp;
+}
+
+int64_t split_device_bytes(const SplitPlan* sp) { return sp ? sp->bytes : 0; }
+
+int split_check(const SplitPlan* sp) {
+    int v = 0;
+    if (!sp || cudaMemcpy(&v, sp->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return CF_ECUDA;
+    if (v != 0) {
+        cudaMemset(sp->d_err, 0, sizeof(int));
+        return fail_split(CF_ETIMEOUT, "split form: a bounded wait on the tensor-core pipeline gave up");
+    }
+    return CF_OK;
+}
+
+int split_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
+    if (B <= 0 || sp->n_rg == 0) return CF_OK;
+    switch (sp->k) {
+        case 4: return run_impl<4>(sp, q_cm, f_cm, B, st, launches);
+        case 8: return run_impl<8>(sp, q_cm, f_cm, B, st, launches);
+        default: return run_impl<12>(sp, q_cm, f_cm, B, st, launches);
+    }
+}
+
+}  // namespace cf

@@ -1,0 +1,36 @@
+// split.cuh -- the exact-split form (CF_FORM_AF_SYM_I8): host interface of split.cu.
+//
+// Q(f) on the q2 <-> q3 folded operator with the Phi step in FP64 on the CUDA cores and the
+// K^3 step on the int8 tensor cores (tcgen05.mma kind::i8): Phi and R_t are written as
+// 47-bit fixed-point integers split into six bytes each, the byte products are summed exactly
+// in int32 tensor-memory accumulators, and the accumulators are recombined in FP64.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace cf {
+
+struct SplitPlan;
+
+// Builds the split operator from a folded plan's device operator (downloaded to the host, split,
+// uploaded).  Returns a cf_status; on failure the message is set with cf_set_last_error.
+int split_build(SplitPlan** out, const DevOp& folded, int64_t n_g, int64_t n_slices, int device);
+void split_destroy(SplitPlan* sp);
+int64_t split_device_bytes(const SplitPlan* sp);
+// Q_cm += Q(f_cm) for B cells, cell-major [N_Q x K x B] device arrays; no allocation, no
+// synchronisation.  Returns a cf_status (message set on failure).
+int split_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st,
+              int64_t* launches);
+// The FP64 band kernel on the same units: Q_cm += Q(f_cm) with the K^3 step in FP64 (the plan's own
+// G and R, plain or folded).  No allocation, no synchronisation.
+int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st,
+               int64_t* launches);
+// After the stream has been synchronised: CF_ETIMEOUT (and the flag cleared) if a CTA of an
+// earlier launch gave up a bounded wait, else CF_OK.
+int split_check(const SplitPlan* sp);
+// Whether the split form exists for this K (K divisible by 4, K <= 12).
+bool split_supported_k(int k);
+
+}  // namespace cf

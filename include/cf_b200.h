@@ -63,7 +63,12 @@ typedef enum cf_form {
     CF_FORM_AF_BF16 = 7,   /* angular first with the K^3 step on the BF16 tensor cores as a two-term
                               split: R_t = R_hi + R_lo and Phi = Phi_hi + Phi_lo in BF16, products
                               accumulated in FP32 (the Phi step in FP32); ~1e-5 relative error; K = 8 */
-    CF_FORM_AF_SYM_BF16 = 8 /* the BF16-split form on the folded operator                             */
+    CF_FORM_AF_SYM_BF16 = 8, /* the BF16-split form on the folded operator                            */
+    CF_FORM_AF_SYM_I8 = 9  /* the folded operator with Phi in FP64 and the K^3 step on the int8 tensor
+                              cores (tcgen05): Phi and R_t as 47-bit fixed-point integers split into six
+                              bytes each, byte products summed exactly in int32 tensor memory, recombined
+                              in FP64; ~1e-11 of max|Q|; K = 4, 8 or 12; Q only, cell-major arrays
+                              (cf_q_device, cf_contract_host); no counterpart in the reference */
 } cf_form;
 
 typedef struct cf_plan cf_plan;
@@ -197,7 +202,8 @@ int cf_fp64_fma_peak(int32_t device, double* tflops);
  * tiled copies of f and Q) lives in a fixed array of CF_NOALLOC_SCRATCH_BYTES inside the library,
  * which each device holds from the first call on that device until the process exits; batches
  * whose 2 * ceil(B/32) * 32 * N_Q * K doubles do not fit are rejected with CF_ESHAPE (about 4300
- * cells at N_Q*K = 968).  The first call on a device looks up the array's device address with
+ * cells at N_Q*K = 968), whichever kernel route the batch would take, including the routes that
+ * leave the array unused.  The first call on a device looks up the array's device address with
  * that device current; make that first call before any stream capture.  All calls share the one
  * array, so calls that overlap on the GPU (other streams, other host threads) race on it.  The
  * plan itself is created beforehand with cf_plan_create, which does allocate, and so is its folded
@@ -278,6 +284,16 @@ typedef struct cf_sumfac_inputs {
 } cf_sumfac_inputs;
 /* device_seconds (may be NULL) receives the device time of the quadrature kernels. */
 int cf_rtensor_sumfac(double* R_out, const cf_sumfac_inputs* inputs, int32_t device, double* device_seconds);
+/* The same quadrature with the two gain tables passed already compressed to the valid (q_i, channel)
+ * pairs, so that the dense [n_t1 x n_u1 x N_Q x N_L] table (20 GB at L = 16, K_max = 11, pad 20)
+ * never exists; inputs->p_gain_p1 / p_gain_p2 are ignored.  The pairs j = 0..nnz-1 run over the
+ * channels in order and, within a channel, over its qi_valid list up to the first -1; the tables are
+ * p_gain_p1_packed[(u * n_t1 + t) * nnz + j] = P_gain_p1[t, u, q_j, ch_j] and
+ * p_gain_p2_packed[y * nnz + j] = P_gain_p2[y, q_j, ch_j].  Results equal cf_rtensor_sumfac's bit for
+ * bit on the same tables.  No counterpart in the reference (compute_rtensor_sumfac_mex.cpp:80-397
+ * takes the dense tables). */
+int cf_rtensor_sumfac_packed(double* R_out, const cf_sumfac_inputs* inputs, const double* p_gain_p1_packed,
+                             const double* p_gain_p2_packed, int32_t device, double* device_seconds);
 
 /* ------------------------------------------------------------------------------------------
  * Explicit time stepping df/dt = Q(f) for a batch of cells, Heun's method (RK2):

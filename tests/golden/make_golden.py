@@ -1,6 +1,6 @@
 """Generate the golden fixtures under tests/golden/ (TEST INFRASTRUCTURE).
 
-    python tests/golden/make_golden.py [--big]
+    python tests/golden/make_golden.py [--big | --ragged]
 
 Needs the reference tree (to build oracle/_ref with `make -C oracle`).  Writes:
 
@@ -16,6 +16,8 @@ Needs the reference tree (to build oracle/_ref with `make -C oracle`).  Writes:
     bkw_k5_l1_g0      K_max=5, L=1, gamma=0, pad 16   (tutorial_collisions_bwu_solution.m:23-40)
 * with --big: ``R_hs_k7_l8_pad20.npy`` and ``R_hs_k7_l10_pad20.npy`` -- hard-sphere R for the
   L=8 and L=10, K=8 configurations (minutes to hours of CPU quadrature).
+* with --ragged: ``R_hs_k3_l4_pad20.npy``, ``R_hs_k5_l6_pad20.npy`` and ``R_hs_k5_l8_pad20.npy`` --
+  hard-sphere R of the ragged batch's (L, K) = (4, 4), (6, 6) and (8, 6) buckets.
 """
 from __future__ import annotations
 
@@ -89,6 +91,9 @@ def small_operator(name: str, K_max: int, L: int, gamma: float, pad: int, seed: 
     print(f"wrote op_{name}.npz: N_G={geo.n_g} N_L={geo.n_l} |Q|={np.abs(outs['Q_af']).max():.3e}", flush=True)
 
 
+RAGGED = [(3, 4), (5, 6), (5, 8)]  # (K_max, L) of the ragged batch's (L, K) = (4,4), (6,6), (8,6) buckets
+
+
 def big(K_max: int, L: int):
     geo = geometry.generate_geometry(L)
     R = rtensor.generate_R(geo, K_max, 1.0, 20, 20, flavour="fast")
@@ -98,8 +103,15 @@ def big(K_max: int, L: int):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--big", action="store_true")
+    ap.add_argument("--ragged", action="store_true",
+                    help="only the hard-sphere R of the ragged batch's three smaller buckets")
     ap.add_argument("--only", default=None)
     args = ap.parse_args(argv)
+    if args.ragged:
+        # (L, K) = (4, 4), (6, 6), (8, 6); the fourth bucket, (10, 8), is R_hs_k7_l10_pad20.npy
+        for K_max, L in RAGGED:
+            big(K_max, L)
+        return
     geometry_counts()
     for name, kw in SMALL.items():
         if args.only and args.only != name:

@@ -11,12 +11,14 @@ This script reads them with ``cf_b200.matfile`` and writes ``precalc_k4_pins.npz
 * ``{tag}__R``: the full R for the three smallest operators;
 * ``{tag}__meta``: (K_max, L_max, alpha, n_g, n_l).
 
-Run from the repository root with the reference checked out at /root/reference:
+Run from the repository root with the reference tree at $CF_REFERENCE_DIR (default: a `reference`
+directory beside this repository):
     python tests/golden/make_precalc_pins.py
 """
 from __future__ import annotations
 
 import hashlib
+import os
 import re
 import sys
 from pathlib import Path
@@ -28,7 +30,8 @@ sys.path.insert(0, str(ROOT / "collision-factorization_b200"))
 
 from cf_b200.matfile import load_collision_tensor  # noqa: E402
 
-PRECALC = Path("/root/reference/src/precalc")
+REFERENCE = Path(os.environ.get("CF_REFERENCE_DIR", ROOT.parent / "reference"))
+PRECALC = REFERENCE / "src" / "precalc"
 OUT = Path(__file__).resolve().parent / "precalc_k4_pins.npz"
 FULL = ("l2_g0", "l4_g1", "l6_g0")
 

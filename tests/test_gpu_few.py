@@ -232,3 +232,37 @@ def test_rows_without_slices_pass_through(cuda_available, oracle_lib):
     op.q(torch.from_numpy(np.ascontiguousarray(d["f"].T).reshape(1, K, NQ).copy()).cuda(), out=Qd, form="af")
     assert np.array_equal(Qd.cpu().numpy().reshape(K, NQ).T, Qh)
     op.close()
+
+
+@pytest.mark.parametrize("name", ["cfg1_k3_l4_g0", "hs_k4_l4_g1"])
+def test_single_f_exact_adds_into_nonzero_q_bit_for_bit(name, cuda_available, oracle_lib):
+    """The exact few-cell kernels start from Q_in and add each slice's sum in the reference's order
+    (Q[q1] += q_val, angular_first_collision_kernel_mex.cpp:68): with a nonzero, non-round Q_in the
+    host call (Q_in in the parameter block) and the in-place device call both equal the oracle run
+    on the same Q_in, bit for bit."""
+    import torch
+
+    import cf_b200
+
+    d = load_op(name)
+    NQ, K = d["NQ"], d["K"]
+    args = (d["labels_sorted"], d["vals_sorted"], d["ic_map_sorted"], d["R"], NQ, K)
+    q0 = np.asfortranarray(np.random.default_rng(21).standard_normal((NQ, K)) * (np.pi / 7.0))
+    Qo = q0.copy(order="F")
+    oracle_lib.af(Qo, d["f"], *args)
+    Qh = q0.copy(order="F")
+    cf_b200.contract_batched(Qh, d["f"], *args, form="af_exact")
+    assert cf_b200.few_route_last() == "parameter block"
+    assert np.array_equal(Qh, Qo), np.abs(Qh - Qo).max()
+    op = cf_b200.CollisionOperator(*args)
+    B = 3
+    fb = np.stack([np.ascontiguousarray(d["f"].T)] * B)  # [B, K, NQ]
+    qb = np.stack([np.ascontiguousarray(q0.T) * (1.0 + 0.25 * b) for b in range(B)])
+    Qd = torch.from_numpy(qb.copy()).cuda()
+    op.q(torch.from_numpy(fb.copy()).cuda(), out=Qd, form="af_exact")
+    got = Qd.cpu().numpy()
+    op.close()
+    for b in range(B):
+        ref = np.asfortranarray(qb[b].T)
+        oracle_lib.af(ref, d["f"], *args)
+        assert np.array_equal(got[b].T, ref), (b, np.abs(got[b].T - ref).max())

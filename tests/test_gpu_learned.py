@@ -112,3 +112,90 @@ def test_trained_network_against_maxwellian_blocks(cuda_available):
     assert np.all(rel_eq <= 1e-10) and np.all(rel_ln <= 1e-10)
     assert it_ln.mean() <= it_eq.mean() + 0.5, (it_eq.mean(), it_ln.mean())
     op.close()
+
+
+def test_mlp_gradients_at_the_implicit_configuration_shape(cuda_available):
+    """The network of the implicit configuration (hard spheres L = 8, K = 8: 648 coefficients + log10(dt nu)
+    in, two hidden layers of 512 GELU, 81 blocks of 8 x 8 out): forward and parameter gradients of the
+    library's FP32 kernels against the float64 restatement."""
+    import torch
+
+    from cf_b200.learned import MLP
+    from oracle import mlp as ref
+
+    n_in, hid, n_out, n = 649, 512, 81 * 64, 16
+    net = MLP(n_in, hid, n_out, max_batch=n, seed=5)
+    flat = net.params()
+    params = ref.unpack(flat.astype(np.float64), n_in, hid, n_out)
+    rng = np.random.default_rng(9)
+    x = rng.standard_normal((n, n_in)).astype(np.float32)
+    dy = rng.standard_normal((n, n_out)).astype(np.float32)
+    xt = torch.from_numpy(x).cuda()
+    yt = torch.empty((n, n_out), dtype=torch.float32, device="cuda")
+    net.forward(xt, yt, train=True)
+    y_ref, cache = ref.forward(params, x.astype(np.float64))
+    assert np.abs(yt.cpu().numpy() - y_ref).max() <= 1e-4 * np.abs(y_ref).max()
+    net.backward(xt, torch.from_numpy(dy).cuda())
+    torch.cuda.synchronize()
+    g = net.grads().astype(np.float64)
+    g_ref = ref.pack_like(ref.backward(params, x.astype(np.float64), cache, dy.astype(np.float64)), n_in, hid, n_out)
+    assert np.abs(g - g_ref).max() <= 1e-4 * np.abs(g_ref).max()
+    net.close()
+
+
+def test_learned_solve_not_slower_than_block_at_the_implicit_configuration(cuda_available):
+    """Hard spheres L = 8, K = 8 (R from the reference's quadrature), the implicit configuration's network
+    (2 x 512 GELU): after training and calibration, GMRES(30) to 1e-10 with the learned preconditioner takes
+    no more iterations than with the Maxwellian blocks, and no more time (the network is skipped where its
+    calibrated gain is below the threshold); the exact per-state block-Jacobi inverse, the ceiling of the
+    block-diagonal family, takes no more iterations than either."""
+    import time
+    from pathlib import Path
+
+    import torch
+
+    import cf_b200
+    from cf_b200 import geometry, implicit, workloads
+    from cf_b200.learned import LearnedPreconditioner
+
+    L, K = 8, 8
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = np.asfortranarray(np.load(Path(__file__).resolve().parent / "golden" / "R_hs_k7_l8_pad20.npy"))
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+    lp = LearnedPreconditioner(op, hidden=512, max_batch=1024, scale=0.1, seed=2)
+    train = lp.make_samples(2048, dt_nu_values=(10.0,), n_probes=8, seed=3, amp_range=(0.0, 0.3))
+    lp.fit_normalisation(train)
+    hist = lp.train(train, epochs=3, batch=512, lr=1e-3)
+    assert hist[-1] <= hist[0]
+    del train
+    val = lp.make_samples(512, dt_nu_values=(10.0,), n_probes=8, seed=4, amp_range=(0.0, 0.3))
+    lp.calibrate(val)
+    dt = float(val["dt"][0])
+    del val
+    cells = workloads.stress_cells(K, L, 256, seed=5, amplitude=0.1)
+    cells[:, 0, 4:9] *= np.random.default_rng(6).uniform(0.0, 3.0, size=(256, 1))
+    f = torch.from_numpy(cells).cuda()
+    rhs = op.q(f)
+
+    def timed(make_p):
+        best, out = None, None
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            P = make_p()
+            out = implicit.gmres_solve(op, f, rhs, dt, restart=30, tol=1e-10, precond=P)
+            torch.cuda.synchronize()
+            dt_s = time.perf_counter() - t
+            best = dt_s if best is None else min(best, dt_s)
+        return best, out
+
+    t_block, (_, it_block, rel_block) = timed(lambda: implicit.block_preconditioner(op, dt))
+    t_learn, (_, it_learn, rel_learn) = timed(lambda: lp.predict(f, dt))
+    assert np.all(rel_block <= 1e-10) and np.all(rel_learn <= 1e-10)
+    assert it_learn.mean() <= it_block.mean() + 0.5, (it_block.mean(), it_learn.mean())
+    assert t_learn <= 1.15 * t_block + 2e-3, (t_block, t_learn)
+    P_exact = implicit.exact_block_jacobi(op, f, dt)
+    _, it_exact, rel_exact = implicit.gmres_solve(op, f, rhs, dt, restart=30, tol=1e-10, precond=P_exact)
+    assert np.all(rel_exact <= 1e-10)
+    assert it_exact.mean() <= min(it_block.mean(), it_learn.mean()) + 0.5
+    op.close()

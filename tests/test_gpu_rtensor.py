@@ -61,3 +61,16 @@ def test_sumfac_full_size_hard_spheres(L, cuda_available):
     args = rtensor.sumfac_inputs(geo, 7, 1.0, 20, 20)
     R = rtensor.compute_R(args)
     assert _rel(R, R_fix) < 1e-12
+
+
+@pytest.mark.parametrize("K_max,L,gamma,pad", [(3, 4, 0.0, 20), (4, 4, 1.0, 20), (7, 8, 1.0, 20)])
+def test_sumfac_packed_equals_dense(K_max, L, gamma, pad, cuda_available):
+    """cf_rtensor_sumfac_packed on the compressed gain tables gives cf_rtensor_sumfac's R bit for bit."""
+    from cf_b200 import geometry, rtensor
+
+    geo = geometry.generate_geometry(L)
+    args = rtensor.sumfac_inputs(geo, K_max, gamma, pad, pad)
+    pargs, pg1, pg2 = rtensor.sumfac_inputs(geo, K_max, gamma, pad, pad, packed=True)
+    R_dense = rtensor.compute_R(args, zero_conservation=False)
+    R_packed = rtensor.compute_R(pargs, zero_conservation=False, packed=(pg1, pg2))
+    assert np.array_equal(R_dense, R_packed)

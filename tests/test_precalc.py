@@ -7,13 +7,16 @@ R tensors, and three full R tensors (``make_precalc_pins.py`` reads the files wi
 from __future__ import annotations
 
 import hashlib
+import os
 from pathlib import Path
 
 import numpy as np
 import pytest
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
-PRECALC = Path("/root/reference/src/precalc")
+# the reference tree: $CF_REFERENCE_DIR, else a `reference` directory beside this repository
+REFERENCE = Path(os.environ.get("CF_REFERENCE_DIR", Path(__file__).resolve().parents[2] / "reference"))
+PRECALC = REFERENCE / "src" / "precalc"
 TAGS = ["l2_g0", "l4_g0", "l6_g0", "l2_g1", "l4_g1", "l6_g1", "l8_g1", "l10_g1", "l12_g1"]
 
 
