@@ -874,13 +874,10 @@ int run_split(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStr
     return CF_OK;
 }
 
-// The FP64 band kernel (af_band64_kernel) takes the fast angular-first Q forms at K = 12 with the
-// automatic kernel order, where the 16-cell tile does not fit and the gather kernel was the only
-// family; with kernel path PATH_BAND it takes them at K = 4 and 8 too.  CF_EUNSUPPORTED (not
-// applicable) when the operator has no unique (t, q1) slices, so the caller falls back.
+// The FP64 band kernel (af_band64_kernel) takes the fast angular-first Q forms at K = 4, 8 and 12 on
+// kernel path PATH_BAND.  Where its operator has no unique (t, q1) slices it does not apply.
 int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st) {
-    const bool wanted = cf::split_supported_k(target->k) &&
-                        ((target->k == 12 && target->path == 0) || target->path == cf::PATH_BAND);
+    const bool wanted = cf::split_supported_k(target->k) && target->path == cf::PATH_BAND;
     if (!wanted) return kNoFew;
     cf::SplitPlan* sp = nullptr;
     const int st_build = get_split(target, &sp);

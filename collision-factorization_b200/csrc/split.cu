@@ -25,14 +25,15 @@
 // row's slices)).  The error left is the rounding of X and R_int: measured 1.1e-11 of max|Q| on the
 // hard-sphere L = 10, K = 8 operator against 5.6e-10 with one more block dropped.
 //
-// Work decomposition: a CTA (16 warps) owns 4 cells (f resident in shared memory) and a row group
-// of one l1 band: up to 16 "slots" (a row, or a contiguous chunk of a row's entries when a band has
-// few rows), one per warp.  The band's l-triplets t are walked in order; per t every warp computes
-// its slot's Phi (4 cells x 8 lanes, each lane a (k2 half, k3 quarter) part of K^2), quantises it,
-// and the six byte planes are written plane by plane into a 3-deep ring of shared-memory A tiles
-// (M = 64 rows: 16 slots x 4 cells).  One thread issues, per plane, one MMA
-// per 32-byte K step against a window of the six R planes (B, staged per t into a 2-deep ring by
-// one cp.async.bulk each), into the accumulator blocks d = i + j the window reaches.
+// Work decomposition: a CTA (16 warps) owns C cells (4, or 8 at K = 8 where their f fits; f resident
+// in shared memory) and a row group of one l1 band: up to 16 "slots" (a row, or a contiguous chunk of
+// a row's entries when a band has few rows), one per warp.  The band's l-triplets t are walked in
+// order; per t every warp computes its slot's Phi (C cells x 32/C lanes, each lane a part of K^2: a
+// (k2 half, k3 quarter) for C = 4, a k3 quarter for C = 8), quantises it, and its six byte planes go
+// into a shared-memory A buffer (M = 16 C rows: 16 slots x C cells; two buffers where shared memory
+// allows).  After one barrier, one thread issues, per plane and 32-byte
+// K step, one MMA against a window of the six R planes (B, staged per t into a 2-deep ring by one
+// cp.async.bulk each), into the accumulator blocks d = i + j the window reaches.
 // Accumulators are drained when the row group is done (or earlier, before int32 could overflow),
 // and the slots of one row are summed in a fixed order, so results are deterministic.
 //
@@ -57,7 +58,6 @@ namespace cf {
 
 namespace {
 
-constexpr int kCells = 4;        // cells per CTA
 constexpr int kSlots = 16;       // row slots per CTA, one per warp
 constexpr int kWarps = 16;
 constexpr int kThreads = kWarps * 32;
@@ -66,31 +66,34 @@ constexpr int kDMin = 4;         // lowest block weight kept
 constexpr int kNB = 16;          // B rows per R plane (k1, padded)
 constexpr int kDBlocks = 11 - kDMin;
 constexpr int kTmemCols = 128;   // >= kDBlocks * kNB = 112
-// Accumulator row m (M = 64, one CTA) sits in TMEM lane 32 (m / 16) + m % 16: lanes 0-15 of each
-// warp quadrant.
-__device__ __forceinline__ int d_lane(int m) { return 32 * (m >> 4) + (m & 15); }
-constexpr int kARing = 3;
 constexpr int kBRing = 2;
-constexpr int kM = 64;                    // MMA rows: 16 slots x 4 cells
-constexpr int kATile = kM * 32;           // one 32-byte K step of the A tile
 constexpr int kBStep = kPlanes * kNB * 32;  // one K step of the six R planes
 constexpr int kRShift = 46;               // R_int = rint(R_t s_t 2^46)
 constexpr int kXBits = 46;                // |X| <= 2^46 (1 bit of margin below the 47 the bytes hold)
 constexpr long long kWaitCycles = 2000000000LL;  // ~1 s of SM clock per wait
 
-template <int K>
+// Per (K, C): C cells per CTA (4, or 8 at K = 8), P = 32 / C lanes per cell, each lane holding a part of
+// the K x K Phi: (k2 half, k3 quarter) for P = 8, a k3 quarter for P = 4.
+template <int K, int C>
 struct Shape {
-    static_assert(K % 4 == 0 && K <= 12, "the split form splits K^2 over 8 lanes: K in {4, 8, 12}");
-    static constexpr int KH = K / 2;                // k2 per lane (two halves)
-    static constexpr int KQ = K / 4;                // k3 per lane (four quarters)
+    static_assert((C == 4 && K % 4 == 0 && K <= 12) || (C == 8 && K == 8),
+                  "the band kernels take K in {4, 8, 12} with 4 cells per CTA, or K = 8 with 8");
+    static constexpr int P = 32 / C;                // lanes (parts) per cell
+    static constexpr int KH = P == 8 ? K / 2 : K;   // k2 per lane
+    static constexpr int KQ = K / 4;                // k3 per lane
     static constexpr int E = KH * KQ;               // Phi elements per lane
     static constexpr int EP = (E + 3) / 4 * 4;      // bytes per lane in a plane (word aligned)
-    static constexpr int KK = 8 * EP;               // K dimension of the MMA (kk = part * EP + e)
+    static constexpr int KK = P * EP;               // K dimension of the MMA (kk = part * EP + e)
     static constexpr int NKS = KK / 32;             // 32-byte K steps
     static_assert(KK % 32 == 0, "whole K steps");
+    static constexpr int M = 16 * C;                // MMA rows: 16 slots x C cells
+    static constexpr int ATILE = M * 32;            // one 32-byte K step of an A plane
     static constexpr int PS = E * K + 2;            // FP64 R: doubles per part (16 bytes of padding
-                                                    // keep the 8 parts' 16-byte loads on distinct banks)
-    static constexpr int RT_BYTES = 8 * PS * 8;     // FP64 R_t of one t
+                                                    // keep the parts' 16-byte loads on distinct banks)
+    static constexpr int RT_BYTES = P * PS * 8;     // FP64 R_t of one t
+    // the first k2 and k3 of part p
+    __host__ __device__ static constexpr int k2_of(int p) { return P == 8 ? (p & 1) * KH : 0; }
+    __host__ __device__ static constexpr int k3_of(int p) { return P == 8 ? (p >> 1) * KQ : p * KQ; }
 };
 
 struct SplitArgs {
@@ -100,8 +103,9 @@ struct SplitArgs {
     const double* e_g;         // G_z, in slice order (the FP64 band kernel)
     const double* rfp64;       // FP64 R_t per t as [part][e][k1], parts kPartStride<K> doubles apart
     const uint8_t* rplanes;    // [t][NKS][K step: 6 planes x 16 rows x 32 bytes, canonical]
-    const double* gs;          // per slice: sum |G_z / s_t|
-    const int* t_l23;          // per t: l2 | l3 << 8
+    const int* rb_off;         // per row q1: its slices' bound factors at rb_off[q1] .. rb_off[q1 + 1]
+    const double* rb_gs;       // per slice of a row: sum |G_z / s_t|
+    const int* rb_l23;         // per slice of a row: l2 | l3 << 8 of its l-triplet
     const int* units;          // per row group: 8 ints (unit_*)
     const int* unit_order;     // row groups, heaviest first
     const int* band_tl;        // t-lists of the bands
@@ -113,6 +117,7 @@ struct SplitArgs {
     int n_cg;                  // cell groups: ceil(B / 4)
     int n_q, L;
     int tseg;                  // t per accumulation segment (int32 bound)
+    int n_abuf;                // A buffers of six planes each (2 where shared memory allows, else 1)
     // shared-memory offsets (bytes)
     int off_a, off_b, off_f, off_mb, off_red, off_scale, off_eexp, off_bar, off_misc;
 };
@@ -123,9 +128,9 @@ struct Layout {
     int off_a, off_b, off_f, off_mb, off_red, off_scale, off_eexp, off_bar, off_misc, total;
 };
 
-template <int K>
-Layout smem_layout(int n_q, int L) {
-    using S = Shape<K>;
+template <int K, int C>
+Layout smem_layout(int n_q, int L, int n_abuf) {
+    using S = Shape<K, C>;
     Layout l{};
     int o = 0;
     auto take = [&](int bytes, int align) {
@@ -134,22 +139,22 @@ Layout smem_layout(int n_q, int L) {
         o += bytes;
         return r;
     };
-    l.off_a = take(kARing * S::NKS * kATile, 1024);
+    l.off_a = take(n_abuf * kPlanes * S::NKS * S::ATILE, 1024);
     l.off_b = take(kBRing * S::NKS * kBStep, 1024);
-    l.off_f = take(kCells * n_q * K * (int)sizeof(double), 16);
-    l.off_mb = take(kCells * (L + 1) * (int)sizeof(double), 16);
-    l.off_red = take(kSlots * kCells * K * (int)sizeof(double), 16);
-    l.off_scale = take(kSlots * kCells * (int)sizeof(double), 16);
-    l.off_eexp = take(kSlots * kCells * (int)sizeof(int), 16);
+    l.off_f = take(C * n_q * K * (int)sizeof(double), 16);
+    l.off_mb = take(C * (L + 1) * (int)sizeof(double), 16);
+    l.off_red = take(kSlots * C * K * (int)sizeof(double), 16);
+    l.off_scale = take(kSlots * C * (int)sizeof(double), 16);
+    l.off_eexp = take(kSlots * C * (int)sizeof(int), 16);
     l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
     l.off_misc = take(16 * (int)sizeof(int), 16);
     l.total = o;
     return l;
 }
 
-template <int K>
+template <int K, int C>
 Layout band64_layout(int n_q) {
-    using S = Shape<K>;
+    using S = Shape<K, C>;
     Layout l{};
     int o = 0;
     auto take = [&](int bytes, int align) {
@@ -159,8 +164,8 @@ Layout band64_layout(int n_q) {
         return r;
     };
     l.off_b = take(2 * S::RT_BYTES, 1024);
-    l.off_f = take(kCells * n_q * K * (int)sizeof(double), 16);
-    l.off_red = take(kSlots * kCells * K * (int)sizeof(double), 16);
+    l.off_f = take(C * n_q * K * (int)sizeof(double), 16);
+    l.off_red = take(kSlots * C * K * (int)sizeof(double), 16);
     l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
     l.off_misc = take(16 * (int)sizeof(int), 16);
     l.total = o;
@@ -191,13 +196,15 @@ __device__ __forceinline__ uint32_t byte_word(uint32_t x0, uint32_t x1, uint32_t
     return __byte_perm(t01, t23, 0x5410);
 }
 
-// Phi of one slot for this lane's (k2 half, k3 quarter) part of one cell: the entries of the slot's
-// chunk of slice sl, grouped by q2 (h = sum G f(q3) over a run of equal q2, then phi += f(q2) (x) h).
-template <int K>
+// Phi of one slot for this lane's part (k2 = k2o .. k2o + KH - 1, k3 = k3o .. k3o + KQ - 1) of cell c:
+// the entries of the slot's chunk of slice sl, grouped by q2 (h = sum G f(q3) over a run of equal q2,
+// then phi += f(q2) (x) h).
+template <int K, int C>
 __device__ __forceinline__ void slot_phi(const SplitArgs& a, const double* __restrict__ gv,
                                          const double* __restrict__ fs, int NQ, int sl, int ch, int nS, int lane,
-                                         int c, int k2h, int k3q, double (&phi)[Shape<K>::KH][Shape<K>::KQ]) {
-    constexpr int KH = Shape<K>::KH, KQ = Shape<K>::KQ;
+                                         int c, int k2o, int k3o,
+                                         double (&phi)[Shape<K, C>::KH][Shape<K, C>::KQ]) {
+    constexpr int KH = Shape<K, C>::KH, KQ = Shape<K, C>::KQ;
 #pragma unroll
     for (int x = 0; x < KH; ++x)
 #pragma unroll
@@ -212,7 +219,7 @@ __device__ __forceinline__ void slot_phi(const SplitArgs& a, const double* __res
     auto flush = [&]() {
 #pragma unroll
         for (int x = 0; x < KH; ++x) {
-            const double f2 = fs[((k2h * KH + x) * NQ + cur) * kCells + c];
+            const double f2 = fs[((k2o + x) * NQ + cur) * C + c];
 #pragma unroll
             for (int y = 0; y < KQ; ++y) phi[x][y] = fma(f2, h[y], phi[x][y]);
         }
@@ -236,25 +243,26 @@ __device__ __forceinline__ void slot_phi(const SplitArgs& a, const double* __res
                 cur = q2;
             }
 #pragma unroll
-            for (int y = 0; y < KQ; ++y) h[y] = fma(g, fs[((k3q * KQ + y) * NQ + q3) * kCells + c], h[y]);
+            for (int y = 0; y < KQ; ++y) h[y] = fma(g, fs[((k3o + y) * NQ + q3) * C + c], h[y]);
         }
     }
     if (cur >= 0) flush();
 }
 
-// The cells' f (cell-major in global memory) into shared memory as fs[(k N_Q + q) 4 + cell], zero
+// The C cells' f (cell-major in global memory) into shared memory as fs[(k N_Q + q) C + cell], zero
 // past the end of the batch.
+template <int C>
 __device__ __forceinline__ void stage_f(const SplitArgs& a, double* fs, int M, long long cell0, int tid) {
-    for (int i = tid; i < kCells * M; i += kThreads) {
-        const int cc = i % kCells, r = i / kCells;  // r = k N_Q + q: the cell-major element index
+    for (int i = tid; i < C * M; i += kThreads) {
+        const int cc = i % C, r = i / C;  // r = k N_Q + q: the cell-major element index
         const long long cell = cell0 + cc;
         fs[i] = cell < a.n_cells ? __ldg(a.f + cell * M + r) : 0.0;
     }
 }
 
-template <int K>
+template <int K, int C>
 __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
-    using S = Shape<K>;
+    using S = Shape<K, C>;
     constexpr int KH = S::KH, KQ = S::KQ, E = S::E, EP = S::EP, NKS = S::NKS;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint8_t* sA = smem + a.off_a;
@@ -267,14 +275,14 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + a.off_bar);
     uint64_t* bfull = bars;        // [2] R planes of a t have landed
     uint64_t* bfree = bars + 2;    // [2] the MMAs reading a B slot are done
-    uint64_t* afree = bars + 4;    // [3] the MMAs reading an A tile are done
+    uint64_t* afree = bars + 4;    // [2] the MMAs reading an A buffer are done
     uint64_t* dbar = bars + 7;     // all MMAs issued so far are done (drains)
     int* misc = reinterpret_cast<int*>(smem + a.off_misc);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(misc);
     volatile int* abort_flag = misc + 1;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int c = lane & 3, part = lane >> 2, k2h = part & 1, k3q = part >> 1;
+    const int c = lane % C, part = lane / C, k2o = S::k2_of(part), k3o = S::k3_of(part);
     const int NQ = a.n_q, L = a.L, M = NQ * K;
     const int rg = a.unit_order[blockIdx.x / a.n_cg];
     const int cg = blockIdx.x % a.n_cg;
@@ -282,7 +290,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
     const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], nS = u[U_S], tl_off = u[U_TLOFF], n_t = u[U_NT],
               tab_off = u[U_TABOFF], brows = u[U_BROWS];
     const int n_slots = nr * nS;
-    const long long cell0 = (long long)cg * kCells;
+    const long long cell0 = (long long)cg * C;
 
     // ---- set-up: barriers, tensor memory, zero A tiles, f staged -----------------------------
     if (tid == 0) {
@@ -296,9 +304,9 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
     }
     {
         uint4* z = reinterpret_cast<uint4*>(sA);
-        for (int i = tid; i < kARing * NKS * kATile / 16; i += kThreads) z[i] = make_uint4(0, 0, 0, 0);
+        for (int i = tid; i < a.n_abuf * kPlanes * NKS * S::ATILE / 16; i += kThreads) z[i] = make_uint4(0, 0, 0, 0);
     }
-    stage_f(a, fs, M, cell0, tid);
+    stage_f<C>(a, fs, M, cell0, tid);
     tc05::tc_fence_before();
     __syncthreads();
     tc05::tc_fence_after();
@@ -312,13 +320,13 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
         }
     }
     // band maxima of |f| per cell: mb[cell][l]
-    for (int pr = warp; pr < kCells * (L + 1); pr += kWarps) {
+    for (int pr = warp; pr < C * (L + 1); pr += kWarps) {
         const int cc = pr / (L + 1), l = pr % (L + 1);
         const int q0 = l * l, nq = 2 * l + 1;
         double m = 0.0;
         for (int i = lane; i < nq * K; i += 32) {
             const int k = i / nq, q = q0 + i % nq;
-            m = fmax(m, fabs(fs[(k * NQ + q) * kCells + cc]));
+            m = fmax(m, fabs(fs[(k * NQ + q) * C + cc]));
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -326,17 +334,17 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
     }
     __syncthreads();
     // per (slot, cell): the exponent e from the a-priori bound over the row's slices
-    if (tid < kSlots * kCells) {
-        const int s = tid / kCells, cc = tid % kCells;
+    if (tid < kSlots * C) {
+        const int s = tid / C, cc = tid % C;
         int e = 0;
         if (s < n_slots) {
-            const int row = r0 + s / nS;
+            const int q1 = l1 * l1 + r0 + s / nS;
             double bound = 0.0;
-            for (int ti = 0; ti < n_t; ++ti) {
-                const int sl = a.band_slice[tab_off + ti * brows + row];
-                if (sl < 0) continue;
-                const int l23 = a.t_l23[a.band_tl[tl_off + ti]];
-                bound = fmax(bound, a.gs[sl] * mb[cc * (L + 1) + (l23 & 0xff)] * mb[cc * (L + 1) + (l23 >> 8)]);
+            const int i1 = __ldg(a.rb_off + q1 + 1);
+#pragma unroll 4
+            for (int i = __ldg(a.rb_off + q1); i < i1; ++i) {
+                const int l23 = __ldg(a.rb_l23 + i);
+                bound = fmax(bound, __ldg(a.rb_gs + i) * mb[cc * (L + 1) + (l23 & 0xff)] * mb[cc * (L + 1) + (l23 >> 8)]);
             }
             if (bound > 0.0) {
                 int x;
@@ -371,11 +379,11 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
         tc05::tc_fence_after();
         constexpr int KG = (K + 3) / 4;  // k1 per drain warp
         // the accumulator row m in TMEM lane 32 (warp % 4) + lane: M = 64 keeps rows 16q..16q+15 in
-        // lanes 0-15 of quadrant q; M = 128 keeps row m in lane m (rows 0-63 in quadrants 0 and 1)
-        const int m = kM == 64 ? 16 * (warp & 3) + (lane & 15) : 32 * (warp & 3) + lane;
-        const bool holds = kM == 64 ? lane < 16 : (warp & 3) < 2;
-        if (ok && (kM == 64 || (warp & 3) < 2)) {
-            const int s = m / kCells, cc = m % kCells;
+        // lanes 0-15 of quadrant q; M = 128 keeps row m in lane m
+        const int m = S::M == 64 ? 16 * (warp & 3) + (lane & 15) : 32 * (warp & 3) + lane;
+        const bool holds = S::M == 64 ? lane < 16 : true;
+        if (ok) {
+            const int s = m / C, cc = m % C;
             const int kg = warp >> 2;
             const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
             double acc[KG];
@@ -403,19 +411,19 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
             if (holds && s < n_slots)
 #pragma unroll
                 for (int j = 0; j < KG; ++j)
-                    if (kg * KG + j < K) red[(s * kCells + cc) * K + kg * KG + j] = acc[j];
+                    if (kg * KG + j < K) red[(s * C + cc) * K + kg * KG + j] = acc[j];
         }
         tc05::tc_fence_before();
         __syncthreads();
-        if (tid < nr * kCells) {
-            const int rl = tid / kCells, cc = tid % kCells;
+        if (tid < nr * C) {
+            const int rl = tid / C, cc = tid % C;
             const long long cell = cell0 + cc;
             if (cell < a.n_cells) {
                 const int q1 = l1 * l1 + r0 + rl;
                 double* qc = a.q + cell * M + q1;
                 for (int k1 = 0; k1 < K; ++k1) {
                     double sum = 0.0;
-                    for (int ch = 0; ch < nS; ++ch) sum += red[((rl * nS + ch) * kCells + cc) * K + k1];
+                    for (int ch = 0; ch < nS; ++ch) sum += red[((rl * nS + ch) * C + cc) * K + k1];
                     qc[(size_t)k1 * NQ] += sum;
                 }
             }
@@ -429,14 +437,14 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
     // ---- main loop over the band's l-triplets ------------------------------------------------
     const bool active = warp < n_slots;
     const int row = r0 + (active ? warp / nS : 0), ch = active ? warp % nS : 0;
-    const int m_row = warp * kCells + c;  // A row of this lane's (slot, cell)
-    const double sc = scale[m_row < kSlots * kCells ? m_row : 0];
+    const int m_row = warp * C + c;  // A row of this lane's (slot, cell)
+    const double sc = scale[m_row];
     constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer
     for (int ti = 0; ti < n_t; ++ti) {
         uint32_t lo[E], hi[E];
         if (active) {
             double phi[KH][KQ];
-            slot_phi<K>(a, a.e_gs, fs, NQ, a.band_slice[tab_off + ti * brows + row], ch, nS, lane, c, k2h, k3q, phi);
+            slot_phi<K, C>(a, a.e_gs, fs, NQ, a.band_slice[tab_off + ti * brows + row], ch, nS, lane, c, k2o, k3o, phi);
 #pragma unroll
             for (int x = 0; x < KH; ++x)
 #pragma unroll
@@ -446,12 +454,16 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
                     hi[x * KQ + y] = (uint32_t)(__double2hiint(yv) - 0x43380000);
                 }
         }
-        // planes 0..5 through the A ring
-        for (int i = 0; i < kPlanes; ++i) {
-            const int g = ti * kPlanes + i, b = g % kARing, use = g / kARing;
-            if (use >= 1) wait_bar(&afree[b], (uint32_t)((use - 1) & 1), abort_flag, a.err);
-            if (active) {
-                uint8_t* tile = sA + b * NKS * kATile;
+        // all six planes of this t into A buffer b (the buffer's previous MMAs must be done), one barrier,
+        // then one thread issues the t's MMAs: per plane i and 32-byte K step, A plane i against the
+        // window of R planes j = j0..5 into the accumulator blocks d = i + j
+        const int b = ti % a.n_abuf, use = ti / a.n_abuf;
+        if (use >= 1) wait_bar(&afree[b], (uint32_t)((use - 1) & 1), abort_flag, a.err);
+        uint8_t* abuf = sA + b * kPlanes * NKS * S::ATILE;
+        if (active) {
+#pragma unroll
+            for (int i = 0; i < kPlanes; ++i) {
+                uint8_t* tile = abuf + i * NKS * S::ATILE;
 #pragma unroll
                 for (int w = 0; w < EP / 4; ++w) {
                     uint32_t v[4];
@@ -462,49 +474,49 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
                     }
                     const uint32_t word = byte_word(v[0], v[1], v[2], v[3], i & 3);
                     const int kk = part * EP + 4 * w;
-                    const int off = (kk >> 5) * kATile + (m_row >> 3) * 256 + ((kk & 31) >> 4) * 128 + (m_row & 7) * 16 +
+                    const int off = (kk >> 5) * S::ATILE + (m_row >> 3) * 256 + ((kk & 31) >> 4) * 128 + (m_row & 7) * 16 +
                                     (kk & 15);
                     *reinterpret_cast<uint32_t*>(tile + off) = word;
                 }
             }
-            asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-            tc05::tc_fence_before();
-            __syncthreads();
-            if (tid == 0 && !*abort_flag) {
-                tc05::tc_fence_after();
-                if (i == 0) {
-                    // refill the other B slot with the next t (its previous MMAs finished a plane ago)
-                    const int tn = ti + 1;
-                    if (tn >= kBRing && tn < n_t) {
-                        const int sb = tn % kBRing, useb = tn / kBRing;
-                        if (wait_bar(&bfree[sb], (uint32_t)((useb - 1) & 1), abort_flag, a.err)) {
-                            const int t = a.band_tl[tl_off + tn];
-                            tc05::mbar_arrive_expect_tx(&bfull[sb], (uint32_t)bbytes);
-                            tc05::bulk_g2s(sB + sb * bbytes, a.rplanes + (size_t)t * bbytes, (uint32_t)bbytes,
-                                           &bfull[sb]);
-                        }
-                    }
-                    wait_bar(&bfull[ti % kBRing], (uint32_t)((ti / kBRing) & 1), abort_flag, a.err);
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        tc05::tc_fence_before();
+        __syncthreads();
+        if (tid == 0 && !*abort_flag) {
+            tc05::tc_fence_after();
+            // refill the other B slot with the next t (its MMAs were issued a whole Phi step ago)
+            const int tn = ti + 1;
+            if (tn >= kBRing && tn < n_t) {
+                const int sb = tn % kBRing, useb = tn / kBRing;
+                if (wait_bar(&bfree[sb], (uint32_t)((useb - 1) & 1), abort_flag, a.err)) {
+                    const int t = a.band_tl[tl_off + tn];
+                    tc05::mbar_arrive_expect_tx(&bfull[sb], (uint32_t)bbytes);
+                    tc05::bulk_g2s(sB + sb * bbytes, a.rplanes + (size_t)t * bbytes, (uint32_t)bbytes, &bfull[sb]);
                 }
-                if (!*abort_flag) {
-                    const uint8_t* tile = sA + b * NKS * kATile;
-                    const uint8_t* bslot = sB + (ti % kBRing) * bbytes;
+            }
+            wait_bar(&bfull[ti % kBRing], (uint32_t)((ti / kBRing) & 1), abort_flag, a.err);
+            if (!*abort_flag) {
+                const uint8_t* bslot = sB + (ti % kBRing) * bbytes;
+#pragma unroll
+                for (int i = 0; i < kPlanes; ++i) {
+                    const uint8_t* tile = abuf + i * NKS * S::ATILE;
                     const int j0 = i < kDMin ? kDMin - i : 0;
                     const int n = (kPlanes - j0) * kNB;
-                    const uint32_t idesc = tc05::idesc_i8(kM, n, i == kPlanes - 1, true);
+                    const uint32_t idesc = tc05::idesc_i8(S::M, n, i == kPlanes - 1, true);
                     const uint32_t dcol = (uint32_t)((i + j0 - kDMin) * kNB);
 #pragma unroll
                     for (int ks = 0; ks < NKS; ++ks) {
-                        const uint64_t ad = tc05::smem_desc_kmajor(tile + ks * kATile, 128, 256);
+                        const uint64_t ad = tc05::smem_desc_kmajor(tile + ks * S::ATILE, 128, 256);
                         const uint64_t bd = tc05::smem_desc_kmajor(bslot + ks * kBStep + j0 * (kNB / 8) * 256, 128, 256);
                         tc05::mma_i8_ss(tbase + dcol, ad, bd, idesc, true);
                     }
-                    tc05::mma_commit(&afree[b]);
-                    if (i == kPlanes - 1) tc05::mma_commit(&bfree[ti % kBRing]);
                 }
+                tc05::mma_commit(&afree[b]);
+                tc05::mma_commit(&bfree[ti % kBRing]);
             }
-            __syncwarp();
         }
+        __syncwarp();
         if ((ti + 1) % a.tseg == 0 && ti + 1 < n_t) drain();
     }
     drain();
@@ -520,9 +532,9 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
 // reads its part's K x E block with 16-byte loads shared by the part's 4 cells).  Each lane
 // accumulates its part's share of Q(row, cell) over the band's t-list; the 8 parts and the slots of
 // a row are summed in a fixed order at the end.
-template <int K>
+template <int K, int C>
 __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
-    using S = Shape<K>;
+    using S = Shape<K, C>;
     constexpr int KH = S::KH, KQ = S::KQ, E = S::E, PS = S::PS, RTB = S::RT_BYTES;
     extern __shared__ __align__(1024) unsigned char smem[];
     double* rring = reinterpret_cast<double*>(smem + a.off_b);
@@ -533,7 +545,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
     volatile int* abort_flag = misc + 1;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int c = lane & 3, part = lane >> 2, k2h = part & 1, k3q = part >> 1;
+    const int c = lane % C, part = lane / C, k2o = S::k2_of(part), k3o = S::k3_of(part);
     const int NQ = a.n_q, M = NQ * K;
     const int rg = a.unit_order[blockIdx.x / a.n_cg];
     const int cg = blockIdx.x % a.n_cg;
@@ -541,7 +553,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
     const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], nS = u[U_S], tl_off = u[U_TLOFF], n_t = u[U_NT],
               tab_off = u[U_TABOFF], brows = u[U_BROWS];
     const int n_slots = nr * nS;
-    const long long cell0 = (long long)cg * kCells;
+    const long long cell0 = (long long)cg * C;
 
     if (tid == 0) {
         tc05::mbar_init(&bfull[0], 1);
@@ -549,7 +561,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
         tc05::fence_mbar_init();
         *abort_flag = 0;
     }
-    stage_f(a, fs, M, cell0, tid);
+    stage_f<C>(a, fs, M, cell0, tid);
     __syncthreads();
     if (tid == 0)
         for (int ti = 0; ti < min(n_t, 2); ++ti) {
@@ -569,7 +581,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
         const int sl = active && ok ? a.band_slice[tab_off + ti * brows + row] : -1;
         if (sl >= 0) {
             double phi[KH][KQ];
-            slot_phi<K>(a, a.e_g, fs, NQ, sl, ch, nS, lane, c, k2h, k3q, phi);
+            slot_phi<K, C>(a, a.e_g, fs, NQ, sl, ch, nS, lane, c, k2o, k3o, phi);
             const double* rp = rring + sb * (RTB / 8) + part * PS;
 #pragma unroll
             for (int x = 0; x < KH; ++x)
@@ -591,25 +603,23 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
             tc05::bulk_g2s(rring + sb * (RTB / 8), a.rfp64 + (size_t)t * (RTB / 8), (uint32_t)RTB, &bfull[sb]);
         }
     }
-    // the 8 parts of a cell sit in lanes c, c + 4, ..., c + 28
+    // the parts of a cell sit in lanes c, c + C, c + 2C, ...
 #pragma unroll
-    for (int k1 = 0; k1 < K; ++k1) {
-        acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], 4);
-        acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], 8);
-        acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], 16);
-    }
-    if (active && lane < kCells)
+    for (int k1 = 0; k1 < K; ++k1)
 #pragma unroll
-        for (int k1 = 0; k1 < K; ++k1) red[(warp * kCells + lane) * K + k1] = acc[k1];
+        for (int o = C; o < 32; o <<= 1) acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], o);
+    if (active && lane < C)
+#pragma unroll
+        for (int k1 = 0; k1 < K; ++k1) red[(warp * C + lane) * K + k1] = acc[k1];
     __syncthreads();
-    if (tid < nr * kCells) {
-        const int rl = tid / kCells, cc = tid % kCells;
+    if (tid < nr * C) {
+        const int rl = tid / C, cc = tid % C;
         const long long cell = cell0 + cc;
         if (cell < a.n_cells) {
             double* qc = a.q + cell * M + (l1 * l1 + r0 + rl);
             for (int k1 = 0; k1 < K; ++k1) {
                 double sum = 0.0;
-                for (int chk = 0; chk < nS; ++chk) sum += red[((rl * nS + chk) * kCells + cc) * K + k1];
+                for (int chk = 0; chk < nS; ++chk) sum += red[((rl * nS + chk) * C + cc) * K + k1];
                 qc[(size_t)k1 * NQ] += sum;
             }
         }
@@ -623,15 +633,17 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
 // ------------------------------------------------------------------------------------------
 struct SplitPlan {
     int device = 0, n_q = 0, k = 0, n_l = 0, L = 0;
-    int n_rg = 0, tseg = 1;
+    int n_rg = 0, tseg = 1, n_abuf = 1;
+    int cells = 4;                    // cells per CTA (C)
     int64_t bytes = 0;
     int smem = 0;
     const int* slice_e = nullptr;     // borrowed from the folded plan
     const uint32_t* e_q23 = nullptr;  // borrowed
     uint8_t* d_rplanes = nullptr;
     double* d_e_gs = nullptr;
-    double* d_gs = nullptr;
-    int* d_t_l23 = nullptr;
+    int* d_rb_off = nullptr;
+    double* d_rb_gs = nullptr;
+    int* d_rb_l23 = nullptr;
     int* d_units = nullptr;
     int* d_unit_order = nullptr;
     int* d_band_tl = nullptr;
@@ -674,9 +686,9 @@ int isqrt_int(int q) {
     return l;
 }
 
-template <int K>
+template <int K, int C>
 void split_r_planes(const std::vector<double>& R, int n_l, std::vector<uint8_t>& planes, std::vector<double>& st_scale) {
-    using S = Shape<K>;
+    using S = Shape<K, C>;
     const size_t per_t = (size_t)S::NKS * kBStep;
     planes.assign(per_t * n_l, 0);
     st_scale.assign(n_l, 1.0);
@@ -689,9 +701,9 @@ void split_r_planes(const std::vector<double>& R, int n_l, std::vector<uint8_t>&
         const double s = std::ldexp(1.0, -x);
         st_scale[t] = s;
         uint8_t* pt = planes.data() + per_t * t;
-        for (int p = 0; p < 8; ++p)
+        for (int p = 0; p < S::P; ++p)
             for (int e = 0; e < S::E; ++e) {
-                const int k2 = (p & 1) * S::KH + e / S::KQ, k3 = (p >> 1) * S::KQ + e % S::KQ;
+                const int k2 = S::k2_of(p) + e / S::KQ, k3 = S::k3_of(p) + e % S::KQ;
                 const int kk = p * S::EP + e;
                 const int ks = kk >> 5, kb = kk & 31;
                 for (int k1 = 0; k1 < K; ++k1) {
@@ -709,9 +721,9 @@ void split_r_planes(const std::vector<double>& R, int n_l, std::vector<uint8_t>&
     }
 }
 
-template <int K>
+template <int K, int C>
 int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
-    using S = Shape<K>;
+    using S = Shape<K, C>;
     const int NQ = op.n_q, NL = op.n_l;
     const int L = isqrt_int(NQ) - 1;
     if ((L + 1) * (L + 1) != NQ) return fail_split(CF_EUNSUPPORTED, "split form: N_Q is not (L+1)^2");
@@ -728,15 +740,15 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
 
     std::vector<uint8_t> planes;
     std::vector<double> st;
-    split_r_planes<K>(R, NL, planes, st);
+    split_r_planes<K, C>(R, NL, planes, st);
     // FP64 R_t per t as [part][e][k1] with zero padding after each part
-    std::vector<double> rfp64((size_t)NL * 8 * S::PS, 0.0);
+    std::vector<double> rfp64((size_t)NL * S::P * S::PS, 0.0);
     for (int t = 0; t < NL; ++t)
-        for (int pp = 0; pp < 8; ++pp)
+        for (int pp = 0; pp < S::P; ++pp)
             for (int e = 0; e < S::E; ++e) {
-                const int k2 = (pp & 1) * S::KH + e / S::KQ, k3 = (pp >> 1) * S::KQ + e % S::KQ;
+                const int k2 = S::k2_of(pp) + e / S::KQ, k3 = S::k3_of(pp) + e % S::KQ;
                 for (int k1 = 0; k1 < K; ++k1)
-                    rfp64[((size_t)t * 8 + pp) * S::PS + (size_t)e * K + k1] =
+                    rfp64[((size_t)t * S::P + pp) * S::PS + (size_t)e * K + k1] =
                         R[(size_t)t * K * K * K + k1 + (size_t)K * k2 + (size_t)K * K * k3];
             }
     // G / s_t per entry, |G / s_t| summed per slice, (l2, l3) per t
@@ -758,6 +770,16 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     }
     for (int t = 0; t < NL; ++t)
         if (t_l23[t] < 0) t_l23[t] = 0;
+    // per row, its slices' bound factors, contiguous (the kernel reads them once per (row, cell))
+    std::vector<int> rb_off(NQ + 1, 0), rb_l23;
+    std::vector<double> rb_gs;
+    for (int q = 0; q < NQ; ++q) {
+        for (int s2 = q1_begin[q]; s2 < q1_begin[q + 1]; ++s2) {
+            rb_gs.push_back(gs[s2]);
+            rb_l23.push_back(t_l23[slice_t[s2]]);
+        }
+        rb_off[q + 1] = (int)rb_gs.size();
+    }
     // bands: t-lists and the (t, row) -> slice tables
     std::vector<int> band_tl, band_slice, units;
     std::vector<double> work;
@@ -782,18 +804,10 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
                 cell = s;
                 row_work[r] += (double)(slice_e[s + 1] - slice_e[s]);
             }
-        // row groups: the split into groups of nr rows x S chunks (nr * S <= 16) that fills most slots
-        int best_g = 1;
-        double best_fill = -1.0;
-        for (int ng = 1; ng <= brows; ++ng) {
-            const int nr = (brows + ng - 1) / ng;
-            if (nr > cap) continue;
-            const double fill = (double)brows * (cap / nr) / (double)(ng * cap);
-            if (fill > best_fill + 1e-9) {
-                best_fill = fill;
-                best_g = ng;
-            }
-        }
+        // row groups: as few as the 16 slots allow (every group walks the whole t-list, so the per-t
+        // costs scale with the number of groups); a group of nr < 16 rows splits each row's entries
+        // into S = 16 / nr chunks so that every warp has work
+        const int best_g = (brows + cap - 1) / cap;
         int r = 0;
         for (int gi = 0; gi < best_g; ++gi) {
             const int nr = (brows - r + (best_g - gi) - 1) / (best_g - gi);
@@ -821,14 +835,24 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     sp->slice_e = op.slice_e;
     sp->e_q23 = op.e_q23;
     sp->e_g = op.e_g;
-    sp->lay = smem_layout<K>(NQ, L);
-    sp->lay64 = band64_layout<K>(NQ);
+    int optin = 0;
+    cudaGetDevice(&sp->device);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, sp->device);
+    sp->cells = C;
+    sp->n_abuf = 2;
+    sp->lay = smem_layout<K, C>(NQ, L, 2);
+    if (sp->lay.total > optin) {
+        sp->n_abuf = 1;
+        sp->lay = smem_layout<K, C>(NQ, L, 1);
+    }
+    sp->lay64 = band64_layout<K, C>(NQ);
     sp->smem = sp->lay.total;
     int64_t bytes = 0;
     if ((ce = upload_vec(&sp->d_rplanes, planes, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_e_gs, e_gs, bytes)) != cudaSuccess ||
-        (ce = upload_vec(&sp->d_gs, gs, bytes)) != cudaSuccess ||
-        (ce = upload_vec(&sp->d_t_l23, t_l23, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_rb_off, rb_off, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_rb_gs, rb_gs, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_rb_l23, rb_l23, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_units, units, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_unit_order, order, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_band_tl, band_tl, bytes)) != cudaSuccess ||
@@ -841,13 +865,13 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     return CF_OK;
 }
 
-template <int K>
+template <int K, int C>
 int run_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        const cudaError_t e = cudaFuncSetAttribute(af_split_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        const cudaError_t e = cudaFuncSetAttribute(af_split_kernel<K, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    227 * 1024);
         if (e != cudaSuccess)
             return fail_split(CF_ECUDA, std::string("split form: smem attribute: ") + cudaGetErrorString(e));
@@ -858,8 +882,9 @@ int run_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, c
     a.e_q23 = sp->e_q23;
     a.e_gs = sp->d_e_gs;
     a.rplanes = sp->d_rplanes;
-    a.gs = sp->d_gs;
-    a.t_l23 = sp->d_t_l23;
+    a.rb_off = sp->d_rb_off;
+    a.rb_gs = sp->d_rb_gs;
+    a.rb_l23 = sp->d_rb_l23;
     a.units = sp->d_units;
     a.unit_order = sp->d_unit_order;
     a.band_tl = sp->d_band_tl;
@@ -868,10 +893,11 @@ int run_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, c
     a.q = q_cm;
     a.err = sp->d_err;
     a.n_cells = B;
-    a.n_cg = (int)((B + kCells - 1) / kCells);
+    a.n_cg = (int)((B + C - 1) / C);
     a.n_q = sp->n_q;
     a.L = sp->L;
     a.tseg = sp->tseg;
+    a.n_abuf = sp->n_abuf;
     a.off_a = sp->lay.off_a;
     a.off_b = sp->lay.off_b;
     a.off_f = sp->lay.off_f;
@@ -883,20 +909,20 @@ int run_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, c
     a.off_misc = sp->lay.off_misc;
     const long long blocks = (long long)sp->n_rg * a.n_cg;
     if (blocks > 0x7fffffffLL) return fail_split(CF_ESHAPE, "split form: batch too large for one launch");
-    af_split_kernel<K><<<(unsigned)blocks, kThreads, sp->smem, st>>>(a);
+    af_split_kernel<K, C><<<(unsigned)blocks, kThreads, sp->smem, st>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("split form: launch: ") + cudaGetErrorString(e));
     if (launches) ++*launches;
     return CF_OK;
 }
 
-template <int K>
+template <int K, int C>
 int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        const cudaError_t e = cudaFuncSetAttribute(af_band64_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        const cudaError_t e = cudaFuncSetAttribute(af_band64_kernel<K, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    227 * 1024);
         if (e != cudaSuccess)
             return fail_split(CF_ECUDA, std::string("band kernel: smem attribute: ") + cudaGetErrorString(e));
@@ -915,7 +941,7 @@ int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     a.q = q_cm;
     a.err = sp->d_err;
     a.n_cells = B;
-    a.n_cg = (int)((B + kCells - 1) / kCells);
+    a.n_cg = (int)((B + C - 1) / C);
     a.n_q = sp->n_q;
     a.L = sp->L;
     a.off_b = sp->lay64.off_b;
@@ -925,7 +951,7 @@ int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     a.off_misc = sp->lay64.off_misc;
     const long long blocks = (long long)sp->n_rg * a.n_cg;
     if (blocks > 0x7fffffffLL) return fail_split(CF_ESHAPE, "band kernel: batch too large for one launch");
-    af_band64_kernel<K><<<(unsigned)blocks, kThreads, sp->lay64.total, st>>>(a);
+    af_band64_kernel<K, C><<<(unsigned)blocks, kThreads, sp->lay64.total, st>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("band kernel: launch: ") + cudaGetErrorString(e));
     if (launches) ++*launches;
@@ -939,9 +965,10 @@ bool split_supported_k(int k) { return k == 4 || k == 8 || k == 12; }
 int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
     if (B <= 0 || sp->n_rg == 0) return CF_OK;
     switch (sp->k) {
-        case 4: return run64_impl<4>(sp, q_cm, f_cm, B, st, launches);
-        case 8: return run64_impl<8>(sp, q_cm, f_cm, B, st, launches);
-        default: return run64_impl<12>(sp, q_cm, f_cm, B, st, launches);
+        case 4: return run64_impl<4, 4>(sp, q_cm, f_cm, B, st, launches);
+        case 8: return sp->cells == 8 ? run64_impl<8, 8>(sp, q_cm, f_cm, B, st, launches)
+                                      : run64_impl<8, 4>(sp, q_cm, f_cm, B, st, launches);
+        default: return run64_impl<12, 4>(sp, q_cm, f_cm, B, st, launches);
     }
 }
 
@@ -953,9 +980,17 @@ int split_build(SplitPlan** out, const DevOp& folded, int64_t n_g, int64_t n_sli
     sp->device = device;
     int st = CF_OK;
     switch (folded.k) {
-        case 4: st = build_impl<4>(sp, folded, n_g, n_slices); break;
-        case 8: st = build_impl<8>(sp, folded, n_g, n_slices); break;
-        default: st = build_impl<12>(sp, folded, n_g, n_slices); break;
+        case 4: st = build_impl<4, 4>(sp, folded, n_g, n_slices); break;
+        case 8: {
+            // 8 cells per CTA where their f fits beside one six-plane A buffer and the B ring
+            int optin = 0;
+            cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+            const int L = isqrt_int(folded.n_q) - 1;
+            st = smem_layout<8, 8>(folded.n_q, L, 1).total <= optin ? build_impl<8, 8>(sp, folded, n_g, n_slices)
+                                                                    : build_impl<8, 4>(sp, folded, n_g, n_slices);
+            break;
+        }
+        default: st = build_impl<12, 4>(sp, folded, n_g, n_slices); break;
     }
     if (st == CF_OK) {
         int optin = 0;
@@ -976,7 +1011,7 @@ int split_build(SplitPlan** out, const DevOp& folded, int64_t n_g, int64_t n_sli
 
 void split_destroy(SplitPlan* sp) {
     if (!sp) return;
-    void* ptrs[] = {sp->d_rplanes, sp->d_e_gs, sp->d_gs, sp->d_t_l23, sp->d_units, sp->d_unit_order, sp->d_band_tl,
+    void* ptrs[] = {sp->d_rplanes, sp->d_e_gs, sp->d_rb_off, sp->d_rb_gs, sp->d_rb_l23, sp->d_units, sp->d_unit_order, sp->d_band_tl,
                     sp->d_band_slice, sp->d_err, sp->d_rfp64};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -998,9 +1033,10 @@ int split_check(const SplitPlan* sp) {
 int split_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
     if (B <= 0 || sp->n_rg == 0) return CF_OK;
     switch (sp->k) {
-        case 4: return run_impl<4>(sp, q_cm, f_cm, B, st, launches);
-        case 8: return run_impl<8>(sp, q_cm, f_cm, B, st, launches);
-        default: return run_impl<12>(sp, q_cm, f_cm, B, st, launches);
+        case 4: return run_impl<4, 4>(sp, q_cm, f_cm, B, st, launches);
+        case 8: return sp->cells == 8 ? run_impl<8, 8>(sp, q_cm, f_cm, B, st, launches)
+                                      : run_impl<8, 4>(sp, q_cm, f_cm, B, st, launches);
+        default: return run_impl<12, 4>(sp, q_cm, f_cm, B, st, launches);
     }
 }
 

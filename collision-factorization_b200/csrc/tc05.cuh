@@ -108,6 +108,26 @@ __host__ __device__ constexpr uint32_t idesc_i8(int m, int n, bool a_signed, boo
            | ((uint32_t)(m >> 4) << 24);   // M / 16
 }
 
+// Instruction descriptor of tcgen05.mma kind::f16 with BF16 A and B and an FP32 accumulator, both
+// operands K-major (16 BF16 elements = 32 bytes per K step, the same byte layout as kind::i8).
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n) {
+    return (1u << 4)                      // D format: f32
+           | (1u << 7)                    // A: bf16
+           | (1u << 10)                   // B: bf16
+           | ((uint32_t)(n >> 3) << 17)   // N / 8
+           | ((uint32_t)(m >> 4) << 24);  // M / 16
+}
+
+// D[tmem] (+)= A[smem desc] * B[smem desc] in BF16 with FP32 accumulation.
+__device__ __forceinline__ void mma_bf16_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            bool accumulate) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"((uint32_t)accumulate)
+        : "memory");
+}
+
 // D[tmem] (+)= A[tmem] * B[smem desc], issued by the calling thread (the caller elects one).
 __device__ __forceinline__ void mma_i8_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b_desc, uint32_t idesc,
                                           bool accumulate) {
