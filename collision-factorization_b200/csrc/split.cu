@@ -178,7 +178,7 @@ __device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, volatil
     if (*abort_flag) return false;
     const long long t0 = clock64();
     for (;;) {
-        if (tc05::mbar_try_wait(bar, parity)) return true;
+        if (tc05::mbar_try_wait_sleep(bar, parity, 2000u)) return true;
         if (*abort_flag) return false;
         if (clock64() - t0 > kWaitCycles) {
             *abort_flag = 1;
@@ -276,10 +276,10 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
     uint64_t* bfull = bars;        // [2] R planes of a t have landed
     uint64_t* bfree = bars + 2;    // [2] the MMAs reading a B slot are done
     uint64_t* afree = bars + 4;    // [2] the MMAs reading an A buffer are done
-    uint64_t* dbar = bars + 7;     // all MMAs issued so far are done (drains)
     int* misc = reinterpret_cast<int*>(smem + a.off_misc);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(misc);
     volatile int* abort_flag = misc + 1;
+    int* acount = misc + 2;  // [2] warps that have written an A buffer, summed over its uses
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int c = lane % C, part = lane / C, k2o = S::k2_of(part), k3o = S::k3_of(part);
@@ -297,6 +297,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
         for (int i = 0; i < 8; ++i) tc05::mbar_init(&bars[i], 1);
         tc05::fence_mbar_init();
         *abort_flag = 0;
+        acount[0] = acount[1] = 0;
     }
     if (warp == 0) {
         tc05::tmem_alloc(tslot, kTmemCols);
@@ -368,14 +369,14 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
     tc05::tc_fence_after();
 
     // ---- drain: accumulators -> FP64 -> Q (rows summed over their slots in a fixed order) ----
-    int n_drains = 0;
-    auto drain = [&]() {
-        if (tid == 0) {
-            if (!*abort_flag) tc05::mma_commit(dbar);
-        }
-        __syncwarp();
-        const bool ok = __all_sync(0xffffffffu, wait_bar(dbar, (uint32_t)(n_drains & 1), abort_flag, a.err));
-        ++n_drains;
+    // every MMA issued up to l-triplet ti is done once the commits of the last uses of the A buffers
+    // (those of ti and, with two buffers, ti - 1) have landed: each earlier use was waited for before
+    // its buffer was written again
+    auto drain = [&](int ti) {
+        bool done = true;
+        for (int x = ti; x >= 0 && x > ti - a.n_abuf; --x)
+            done = wait_bar(&afree[x % a.n_abuf], (uint32_t)((x / a.n_abuf) & 1), abort_flag, a.err) && done;
+        const bool ok = __all_sync(0xffffffffu, done);
         tc05::tc_fence_after();
         constexpr int KG = (K + 3) / 4;  // k1 per drain warp
         // the accumulator row m in TMEM lane 32 (warp % 4) + lane: M = 64 keeps rows 16q..16q+15 in
@@ -480,12 +481,20 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
                 }
             }
         }
+        // the warp that writes an A buffer last (per use) issues its MMAs: no CTA-wide barrier, a warp
+        // runs ahead until the ring of A buffers holds it back
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        tc05::tc_fence_before();
-        __syncthreads();
-        if (tid == 0 && !*abort_flag) {
+        __syncwarp();
+        int last = 0;
+        if (lane == 0) {
+            __threadfence_block();
+            last = atomicAdd(&acount[b], 1) == kWarps * (use + 1) - 1;
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last && lane == 0 && !*abort_flag) {
+            __threadfence_block();
             tc05::tc_fence_after();
-            // refill the other B slot with the next t (its MMAs were issued a whole Phi step ago)
+            // refill the other B slot with the next t (its MMAs, of t - 1, were issued a Phi step ago)
             const int tn = ti + 1;
             if (tn >= kBRing && tn < n_t) {
                 const int sb = tn % kBRing, useb = tn / kBRing;
@@ -512,14 +521,15 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
                         tc05::mma_i8_ss(tbase + dcol, ad, bd, idesc, true);
                     }
                 }
-                tc05::mma_commit(&afree[b]);
-                tc05::mma_commit(&bfree[ti % kBRing]);
             }
+            // always arrive, so that waiters are released also on the error path
+            tc05::mma_commit(&afree[b]);
+            tc05::mma_commit(&bfree[ti % kBRing]);
         }
         __syncwarp();
-        if ((ti + 1) % a.tseg == 0 && ti + 1 < n_t) drain();
+        if ((ti + 1) % a.tseg == 0 && ti + 1 < n_t) drain(ti);
     }
-    drain();
+    drain(n_t - 1);
 
     // ---- tear-down --------------------------------------------------------------------------
     tc05::tc_fence_before();
@@ -535,7 +545,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
 template <int K, int C>
 __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
     using S = Shape<K, C>;
-    constexpr int KH = S::KH, KQ = S::KQ, E = S::E, PS = S::PS, RTB = S::RT_BYTES;
+    constexpr int KH = S::KH, KQ = S::KQ, PS = S::PS, RTB = S::RT_BYTES;
     extern __shared__ __align__(1024) unsigned char smem[];
     double* rring = reinterpret_cast<double*>(smem + a.off_b);
     double* fs = reinterpret_cast<double*>(smem + a.off_f);
@@ -543,6 +553,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
     uint64_t* bfull = reinterpret_cast<uint64_t*>(smem + a.off_bar);
     int* misc = reinterpret_cast<int*>(smem + a.off_misc);
     volatile int* abort_flag = misc + 1;
+    int* rcount = misc + 2;  // [2] warps done with an R slot, summed over its uses
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int c = lane % C, part = lane / C, k2o = S::k2_of(part), k3o = S::k3_of(part);
@@ -560,6 +571,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
         tc05::mbar_init(&bfull[1], 1);
         tc05::fence_mbar_init();
         *abort_flag = 0;
+        rcount[0] = rcount[1] = 0;
     }
     stage_f<C>(a, fs, M, cell0, tid);
     __syncthreads();
@@ -596,12 +608,19 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
                     }
                 }
         }
-        __syncthreads();  // every warp is done with slot sb
-        if (tid == 0 && ti + 2 < n_t && !*abort_flag) {
-            const int t = a.band_tl[tl_off + ti + 2];
-            tc05::mbar_arrive_expect_tx(&bfull[sb], (uint32_t)RTB);
-            tc05::bulk_g2s(rring + sb * (RTB / 8), a.rfp64 + (size_t)t * (RTB / 8), (uint32_t)RTB, &bfull[sb]);
+        // the last warp done with slot sb refills it with t + 2 (no CTA-wide barrier)
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            if (atomicAdd(&rcount[sb], 1) == kWarps * ((ti >> 1) + 1) - 1 && ti + 2 < n_t && !*abort_flag) {
+                __threadfence_block();
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                const int t = a.band_tl[tl_off + ti + 2];
+                tc05::mbar_arrive_expect_tx(&bfull[sb], (uint32_t)RTB);
+                tc05::bulk_g2s(rring + sb * (RTB / 8), a.rfp64 + (size_t)t * (RTB / 8), (uint32_t)RTB, &bfull[sb]);
+            }
         }
+        __syncwarp();
     }
     // the parts of a cell sit in lanes c, c + C, c + 2C, ...
 #pragma unroll
