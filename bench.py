@@ -921,13 +921,15 @@ def run_implicit(args):
             implicit.gmres_solve(op, f[:n_exact], rhs[:n_exact], dt, restart=30, tol=1e-10, max_iters=3000,
                                  precond=implicit.block_preconditioner(op, dt), raise_on_timeout=False)[1]))}
         row["speedup_learned_vs_block"] = row["block"]["seconds"] / row["learned"]["seconds"]
-        row["learned_network_used"] = bool(lp._gain(dt) >= lp.min_gain)
+        row["learned_network_used"] = bool(lp.uses_network(dt))
         results[f"dt_nu={dtnu:g}"] = row
     out = {"workload": "implicit_hs_l8_k8_b2048", "cells": B, "M": geo.n_q * K, "R": r_source,
            "gmres": "GMRES(30), right block-Jacobi preconditioning, FP64, tol 1e-10 on |b - A x| / |b| per cell",
            "learned": {"train_states": args.train_states, "epochs": args.epochs, "probes_per_state": 8,
                        "loss_first": hist[0], "loss_last": hist[-1], "sample_s": t_gen, "train_s": t_train,
                        "calibrated_gain_by_dt_nu": {f"{k:.3g}": v for k, v in gains.items()},
+                       "calibrated_benefit_by_dt_nu": {f"{10 ** k:.3g}": v for k, v in lp.benefit.items()},
+                       "min_benefit": lp.min_benefit,
                        "validation_probe_loss": val_loss},
            "results": results}
     print(json.dumps(out), flush=True)

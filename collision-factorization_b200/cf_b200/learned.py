@@ -95,11 +95,21 @@ class LearnedPreconditioner:
         self.sd = np.ones(self.n_in, dtype=np.float32)
         self.nu = abs(implicit.equilibrium_jacobian_blocks(op)[min(6, self.NQ - 1)][0, 0])
         self.gain = {}  # log10(dt nu) (rounded) -> multiplier of the correction, from calibrate()
-        # below this calibrated gain predict() returns the Maxwellian blocks and skips the network
-        self.min_gain = 0.25
+        self.benefit = {}  # log10(dt nu) (rounded) -> fraction of the Maxwellian blocks' probe loss it removes
+        # below this calibrated benefit predict() returns the Maxwellian blocks and skips the network
+        # (a correction that removes less than a tenth of the probe loss cannot pay for its inference)
+        self.min_benefit = 0.1
+
+    def _key(self, dt) -> float:
+        return round(math.log10(max(dt * self.nu, 1e-12)), 6)
 
     def _gain(self, dt) -> float:
-        return self.gain.get(round(math.log10(max(dt * self.nu, 1e-12)), 6), 1.0)
+        return self.gain.get(self._key(dt), 1.0)
+
+    def uses_network(self, dt) -> bool:
+        """Whether predict() runs the network at this time step (calibrated benefit >= min_benefit;
+        uncalibrated time steps use it)."""
+        return self._gain(dt) > 0.0 and self.benefit.get(self._key(dt), 1.0) >= self.min_benefit
 
     def features(self, f, dt):
         """[B, M + 1] float32: the coefficients (standardised) and log10(dt nu)."""
@@ -114,15 +124,16 @@ class LearnedPreconditioner:
         return (x - mu) / sd
 
     def predict(self, f, dt, peq=None):
-        """Per-cell blocks [B, N_Q, K, K] float64 on the device, or -- when the calibrated gain of this
-        time step is below min_gain, so that the correction cannot pay for its inference -- the shared
-        Maxwellian blocks [N_Q, K, K] themselves (no network call, no per-cell assembly)."""
+        """Per-cell blocks [B, N_Q, K, K] float64 on the device, or -- where calibrate() found that the
+        correction removes less than min_benefit of the Maxwellian blocks' probe loss at this time step,
+        so that it cannot pay for its inference -- the shared Maxwellian blocks [N_Q, K, K] themselves
+        (no network call, no per-cell assembly)."""
         import torch
 
         B = f.shape[0]
         peq = torch.as_tensor(implicit.block_preconditioner(self.op, dt) if peq is None else peq,
                               dtype=torch.float64, device=f.device).contiguous()
-        if self._gain(dt) < self.min_gain:
+        if not self.uses_network(dt):
             return peq
         P = torch.empty((B, self.NQ, self.K, self.K), dtype=torch.float64, device=f.device)
         for b0 in range(0, B, self.net.max_batch):
@@ -281,8 +292,11 @@ class LearnedPreconditioner:
             da = torch.einsum("nqij,npqj->npqi", D, a)
             num = float((w * r0 * da).sum())
             den = float((w * da * da).sum())
+            loss0 = float((w * r0 * r0).sum())
             s_opt = min(max(-num / den, 0.0), max_gain) if den > 0 else 0.0
-            key = round(math.log10(max(float(dt_value) * self.nu, 1e-12)), 6)
+            key = self._key(float(dt_value))
             self.gain[key] = s_opt
+            # probe loss at s_opt: loss0 + 2 s num + s^2 den; the fraction of loss0 it removes
+            self.benefit[key] = (-(2.0 * s_opt * num + s_opt * s_opt * den) / loss0) if loss0 > 0 else 0.0
             out[float(dt_value) * self.nu] = s_opt
         return out
