@@ -75,6 +75,17 @@ NCU_TRAFFIC = {
 }
 
 
+PROFILE_FORMS = ("af", "af_sym", "af_exact", "rf", "af_sym_i8", "af_f32", "af_sym_f32", "af_bf16", "af_sym_bf16")
+
+
+def _profile_forms(text):
+    forms = text.split(",")
+    for form in forms:
+        if form not in PROFILE_FORMS:
+            raise argparse.ArgumentTypeError(f"unknown form {form!r}; choose from {', '.join(PROFILE_FORMS)}")
+    return text
+
+
 def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -87,8 +98,9 @@ def parse_args(argv=None):
     ap.add_argument("--seed", type=int, default=20260)
     ap.add_argument("--train-states", type=int, default=100000)
     ap.add_argument("--epochs", type=int, default=12)
-    ap.add_argument("--form", default="af", choices=["af", "af_sym", "af_exact", "rf", "af_sym_i8"],
-                    help="form launched by --profile")
+    ap.add_argument("--form", default="af", type=_profile_forms,
+                    help="form(s) launched by --profile, comma-separated (af, af_sym, af_exact, rf, af_sym_i8, "
+                         "af_f32, af_sym_f32, af_bf16, af_sym_bf16)")
     ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split", "tile_mma",
                                                        "band"],
                     help="kernel family of the angular-first contraction")
@@ -843,11 +855,12 @@ def run_profile(args):
     sh = int(torch.cuda.current_stream().cuda_stream)
     _lib.check(lib.cf_pack_cells(op._h, int(fT.data_ptr()), int(f.data_ptr()), B, sh))
     Q = torch.zeros_like(f)
-    for _ in range(args.steps + 1):
-        if args.entry == "device":
-            op.q(f, out=Q, form=args.form)
-        else:
-            _lib.check(lib.cf_q_tiled(op._h, int(QT.data_ptr()), int(fT.data_ptr()), B, _lib.FORMS[args.form], sh))
+    for form in args.form.split(","):
+        for _ in range(args.steps + 1):
+            if args.entry == "device":
+                op.q(f, out=Q, form=form)
+            else:
+                _lib.check(lib.cf_q_tiled(op._h, int(QT.data_ptr()), int(fT.data_ptr()), B, _lib.FORMS[form], sh))
     torch.cuda.synchronize()
     print(json.dumps({"profile": args.workload, "entry": args.entry, "launches": args.steps + 1, "B": B}))
 

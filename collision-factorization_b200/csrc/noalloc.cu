@@ -21,6 +21,7 @@
 // Sets the message cf_last_error() returns (plan.cu; not part of the C ABI).
 void cf_set_last_error(const char* msg);
 bool cf_plan_folded_built(cf_plan* plan);
+bool cf_plan_band_pending(cf_plan* plan, int form);
 
 namespace {
 
@@ -83,6 +84,12 @@ extern "C" int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f
     if (folded && !cf_plan_folded_built(plan)) {
         cf_set_last_error("cf_q_device_noalloc: this plan's folded operator is not built yet, and building it "
                           "allocates; make one cf_q_device or cf_q_tiled call in a folded form first");
+        return CF_EINVAL;
+    }
+    // The band kernels' tables (BF16-split forms at K = 4 and 12; path 'band') are built on first use.
+    if (cf_plan_band_pending(plan, form)) {
+        cf_set_last_error("cf_q_device_noalloc: this plan's band-kernel tables are not built yet, and building "
+                          "them allocates; make one cf_q_device call in this form first");
         return CF_EINVAL;
     }
     // The limit is checked for every batch, also where the route taken (the streamed tile kernel,

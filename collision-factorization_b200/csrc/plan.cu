@@ -572,6 +572,7 @@ int get_sym(cf_plan* p, cf_plan** out);
 bool streamable(const cf_plan* p, const cf_plan* target, int what, bool exact, int f32);
 int run_split(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
+int run_bf16_band(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int check_split(cf_plan* p);
 
 // The fast FP64 angular-first (plain or folded) or radial-first form, or the exact angular-first
@@ -613,6 +614,10 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
         if (sym) CF_TRY(get_sym(p, &target));
         if (!exact && f32 == 0) {
             const int r = run_band64(target, q_dev, f_dev, B, st);
+            if (r != kNoFew) return r;
+        }
+        if (!exact && f32 == 2) {
+            const int r = run_bf16_band(target, q_dev, f_dev, B, st);
             if (r != kNoFew) return r;
         }
         if (streamable(p, target, what, exact, f32)) {
@@ -896,11 +901,30 @@ int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, c
     return CF_OK;
 }
 
-// After a synchronised split-form call: the error word of its launches.
+// The BF16-split forms at K = 4 and 12 (and at K = 8 on kernel path PATH_BAND) run on the band kernel
+// with the K^3 step on the BF16 tensor cores (af_bf16_band_kernel); K = 8 otherwise keeps the warp-level
+// BF16 kernel.
+int run_bf16_band(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st) {
+    if (!cf::split_supported_k(target->k) || (target->k == 8 && target->path != cf::PATH_BAND)) return kNoFew;
+    cf::SplitPlan* sp = nullptr;
+    CF_TRY(get_split(target, &sp));
+    int64_t launches = 0;
+    CF_TRY(cf::bf16_band_run(sp, q_dev, f_dev, B, st, &launches));
+    g_launches += launches;
+    if (launches > 0) {
+        target->last_path = cf::PATH_BAND_BF16;
+        if (target->parent) target->parent->last_path = cf::PATH_BAND_BF16;
+    }
+    return CF_OK;
+}
+
+// After a synchronised call on a band kernel (split, FP64 or BF16): the error word of its launches,
+// on the plan's own band units and on those of its folded twin.
 int check_split(cf_plan* p) {
-    cf_plan* target = p->sym;
-    if (!target || !target->split) return CF_OK;
-    return cf::split_check(target->split);
+    int st = CF_OK;
+    if (p->split) st = cf::split_check(p->split);
+    if (st == CF_OK && p->sym && p->sym->split) st = cf::split_check(p->sym->split);
+    return st;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1296,7 +1320,7 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
         CF_TRY(run_device(p, what, exact, dQ, df, dv, B, p->d_ws, p->ws_bytes, p->stream, sym, f32));
         CF_CUDA(cudaMemcpyAsync(Q, dQ, cell_bytes, cudaMemcpyDeviceToHost, p->stream));
         CF_CUDA(cudaStreamSynchronize(p->stream));
-        return f32 == 3 ? check_split(p) : CF_OK;
+        return f32 >= 2 || p->path == cf::PATH_BAND ? check_split(p) : CF_OK;
     }
     if (B >= 2 * kHostChunkMin) {
         cf_plan* target = p;
@@ -1337,7 +1361,7 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
         const cudaError_t e = cudaStreamSynchronize(hs);
         if (e != cudaSuccess && st == CF_OK) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
     }
-    if (st == CF_OK && f32 == 3) st = check_split(p);
+    if (st == CF_OK && (f32 >= 2 || p->path == cf::PATH_BAND)) st = check_split(p);
     return st;
 }
 
@@ -1580,6 +1604,26 @@ __attribute__((visibility("hidden"))) void cf_add_launches(int64_t n) { g_launch
 __attribute__((visibility("hidden"))) bool cf_plan_folded_built(cf_plan* plan) {
     std::lock_guard<std::mutex> lk(plan->sym_mu);
     return plan->sym != nullptr;
+}
+
+// Whether a call in this form would first build the plan's band units (the tables of the band
+// kernels, which allocate device memory): the BF16-split forms at K = 4 and 12 (and at K = 8 on path
+// PATH_BAND), the fast FP64 forms on path PATH_BAND.  A folded form whose twin is not built yet
+// answers false (that case is refused on its own).
+__attribute__((visibility("hidden"))) bool cf_plan_band_pending(cf_plan* plan, int form) {
+    bool exact = false, sym = false;
+    int f32 = 0;
+    if (form_what(form, exact, sym, f32) != 0 || exact || !cf::split_supported_k(plan->k)) return false;
+    const bool band = plan->path == cf::PATH_BAND;
+    if (!((f32 == 2 && (plan->k != 8 || band)) || (f32 == 0 && band))) return false;
+    cf_plan* target = plan;
+    if (sym) {
+        std::lock_guard<std::mutex> lk(plan->sym_mu);
+        target = plan->sym;
+    }
+    if (!target) return false;
+    std::lock_guard<std::mutex> lk(target->split_mu);
+    return target->split == nullptr && target->split_status <= 0;
 }
 
 extern "C" {

@@ -39,6 +39,7 @@
 //
 // Every wait (mbarriers of the copies and of the MMAs) is bounded by a clock budget; a CTA that
 // gives up records an error word, stops issuing work and leaves through the normal exit path.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -103,13 +104,14 @@ struct SplitArgs {
     const double* e_g;         // G_z, in slice order (the FP64 band kernel)
     const double* rfp64;       // FP64 R_t per t as [part][e][k1], parts kPartStride<K> doubles apart
     const uint8_t* rplanes;    // [t][NKS][K step: 6 planes x 16 rows x 32 bytes, canonical]
+    const uint8_t* rbf;        // [t][NKS][K step: R hi, R lo, each 16 rows x 16 BF16, canonical]
     const int* rb_off;         // per row q1: its slices' bound factors at rb_off[q1] .. rb_off[q1 + 1]
     const double* rb_gs;       // per slice of a row: sum |G_z / s_t|
     const int* rb_l23;         // per slice of a row: l2 | l3 << 8 of its l-triplet
     const int* units;          // per row group: 8 ints (unit_*)
     const int* unit_order;     // row groups, heaviest first
     const int* band_tl;        // t-lists of the bands
-    const int* band_slice;     // per band: [n_t][2 l1 + 1] slice or -1
+    const int* band_rng;       // per band: [n_t][2 l1 + 1] the slice's entries (begin, end) as int2, (0, 0) if none
     const double* f;           // cell-major [B][K][N_Q]
     double* q;
     int* err;
@@ -122,7 +124,7 @@ struct SplitArgs {
     int off_a, off_b, off_f, off_mb, off_red, off_scale, off_eexp, off_bar, off_misc;
 };
 
-enum { U_L1 = 0, U_R0, U_NR, U_S, U_TLOFF, U_NT, U_TABOFF, U_BROWS, U_INTS };
+enum { U_L1 = 0, U_R0, U_NR, U_S, U_TLOFF, U_NT, U_TABOFF, U_BROWS, U_REM, U_INTS };
 
 struct Layout {
     int off_a, off_b, off_f, off_mb, off_red, off_scale, off_eexp, off_bar, off_misc, total;
@@ -152,8 +154,12 @@ Layout smem_layout(int n_q, int L, int n_abuf) {
     return l;
 }
 
+// Warps per CTA of the FP64 band kernel.  16 at every K: its K^3 step keeps K accumulators and a part
+// of Phi (18 doubles at K = 12) live, so more warps (64 or 80 registers each) spill hundreds of bytes.
+__host__ __device__ constexpr int band64_warps(int) { return 16; }
+
 template <int K, int C>
-Layout band64_layout(int n_q) {
+Layout band64_layout(int n_q, int warps) {
     using S = Shape<K, C>;
     Layout l{};
     int o = 0;
@@ -165,7 +171,7 @@ Layout band64_layout(int n_q) {
     };
     l.off_b = take(2 * S::RT_BYTES, 1024);
     l.off_f = take(C * n_q * K * (int)sizeof(double), 16);
-    l.off_red = take(kSlots * C * K * (int)sizeof(double), 16);
+    l.off_red = take(warps * C * K * (int)sizeof(double), 16);
     l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
     l.off_misc = take(16 * (int)sizeof(int), 16);
     l.total = o;
@@ -196,12 +202,61 @@ __device__ __forceinline__ uint32_t byte_word(uint32_t x0, uint32_t x1, uint32_t
     return __byte_perm(t01, t23, 0x5410);
 }
 
+// A slot's entries of one l-triplet and the first 32 of them, loaded one l-triplet ahead of their use
+// (the band kernels walk a row group's t-list in lockstep, so the next t's metadata and entries are
+// known a whole Phi step before they are needed; without this, three dependent global loads per t
+// sat exposed on every warp).
+struct SlotEntries {
+    int cb, ce;     // the slot's entries cb .. ce - 1
+    uint32_t q23;   // entry cb + lane (if < ce)
+    double g;
+};
+
+// Slots of a row group of nr rows on W warps: q = W / nr chunks per row, and one more for the first
+// rem = W % nr rows, so that every warp has a slot.  Slot w -> (local row, chunk, chunks of the row).
+__device__ __forceinline__ void slot_of(int w, int q, int rem, int& rl, int& ch, int& nch) {
+    const int big = rem * (q + 1);
+    if (w < big) {
+        rl = w / (q + 1);
+        ch = w % (q + 1);
+        nch = q + 1;
+    } else {
+        rl = rem + (w - big) / q;
+        ch = (w - big) % q;
+        nch = q;
+    }
+}
+
+// The first slot of local row rl and its number of chunks.
+__device__ __forceinline__ int row_first_slot(int rl, int q, int rem) {
+    return rl < rem ? rl * (q + 1) : rem * (q + 1) + (rl - rem) * q;
+}
+__device__ __forceinline__ int row_chunks(int rl, int q, int rem) { return rl < rem ? q + 1 : q; }
+
+// The entry range of slot (row, chunk ch of nS) at t-list position ti of the unit's band.
+__device__ __forceinline__ void slot_range(const SplitArgs& a, int tab_off, int brows, int ti, int row, int ch, int nS,
+                                           int& cb, int& ce) {
+    const int2 r = __ldg(reinterpret_cast<const int2*>(a.band_rng) + tab_off + ti * brows + row);
+    const int n = r.y - r.x;
+    cb = r.x + (int)(((long long)n * ch) / nS);
+    ce = r.x + (int)(((long long)n * (ch + 1)) / nS);
+}
+
+__device__ __forceinline__ SlotEntries slot_fetch(const SplitArgs& a, const double* __restrict__ gv, int cb, int ce,
+                                                  int lane) {
+    SlotEntries se{cb, ce, 0u, 0.0};
+    if (cb + lane < ce) {
+        se.q23 = __ldg(a.e_q23 + cb + lane);
+        se.g = __ldg(gv + cb + lane);
+    }
+    return se;
+}
+
 // Phi of one slot for this lane's part (k2 = k2o .. k2o + KH - 1, k3 = k3o .. k3o + KQ - 1) of cell c:
-// the entries of the slot's chunk of slice sl, grouped by q2 (h = sum G f(q3) over a run of equal q2,
-// then phi += f(q2) (x) h).
+// the slot's entries, grouped by q2 (h = sum G f(q3) over a run of equal q2, then phi += f(q2) (x) h).
 template <int K, int C>
 __device__ __forceinline__ void slot_phi(const SplitArgs& a, const double* __restrict__ gv,
-                                         const double* __restrict__ fs, int NQ, int sl, int ch, int nS, int lane,
+                                         const double* __restrict__ fs, int NQ, const SlotEntries& se, int lane,
                                          int c, int k2o, int k3o,
                                          double (&phi)[Shape<K, C>::KH][Shape<K, C>::KQ]) {
     constexpr int KH = Shape<K, C>::KH, KQ = Shape<K, C>::KQ;
@@ -209,9 +264,8 @@ __device__ __forceinline__ void slot_phi(const SplitArgs& a, const double* __res
     for (int x = 0; x < KH; ++x)
 #pragma unroll
         for (int y = 0; y < KQ; ++y) phi[x][y] = 0.0;
-    if (sl < 0) return;
-    const int e0 = a.slice_e[sl], n = a.slice_e[sl + 1] - e0;
-    const int cb = e0 + (int)(((long long)n * ch) / nS), ce = e0 + (int)(((long long)n * (ch + 1)) / nS);
+    const int cb = se.cb, ce = se.ce;
+    if (cb >= ce) return;
     double h[KQ];
 #pragma unroll
     for (int y = 0; y < KQ; ++y) h[y] = 0.0;
@@ -228,11 +282,15 @@ __device__ __forceinline__ void slot_phi(const SplitArgs& a, const double* __res
     };
     for (int eb = cb; eb < ce; eb += 32) {
         const int nb = min(32, ce - eb);
-        uint32_t my_q23 = 0;
-        double my_g = 0.0;
-        if (lane < nb) {
-            my_q23 = __ldg(a.e_q23 + eb + lane);
-            my_g = __ldg(gv + eb + lane);
+        uint32_t my_q23 = se.q23;
+        double my_g = se.g;
+        if (eb != cb) {
+            my_q23 = 0;
+            my_g = 0.0;
+            if (lane < nb) {
+                my_q23 = __ldg(a.e_q23 + eb + lane);
+                my_g = __ldg(gv + eb + lane);
+            }
         }
         for (int j = 0; j < nb; ++j) {
             const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, j);
@@ -251,9 +309,9 @@ __device__ __forceinline__ void slot_phi(const SplitArgs& a, const double* __res
 
 // The C cells' f (cell-major in global memory) into shared memory as fs[(k N_Q + q) C + cell], zero
 // past the end of the batch.
-template <int C>
+template <int C, int NT = kThreads>
 __device__ __forceinline__ void stage_f(const SplitArgs& a, double* fs, int M, long long cell0, int tid) {
-    for (int i = tid; i < C * M; i += kThreads) {
+    for (int i = tid; i < C * M; i += NT) {
         const int cc = i % C, r = i / C;  // r = k N_Q + q: the cell-major element index
         const long long cell = cell0 + cc;
         fs[i] = cell < a.n_cells ? __ldg(a.f + cell * M + r) : 0.0;
@@ -287,9 +345,9 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
     const int rg = a.unit_order[blockIdx.x / a.n_cg];
     const int cg = blockIdx.x % a.n_cg;
     const int* u = a.units + (size_t)rg * U_INTS;
-    const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], nS = u[U_S], tl_off = u[U_TLOFF], n_t = u[U_NT],
-              tab_off = u[U_TABOFF], brows = u[U_BROWS];
-    const int n_slots = nr * nS;
+    const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], cq = u[U_S], crem = u[U_REM], tl_off = u[U_TLOFF],
+              n_t = u[U_NT], tab_off = u[U_TABOFF], brows = u[U_BROWS];
+    const int n_slots = nr * cq + crem;
     const long long cell0 = (long long)cg * C;
 
     // ---- set-up: barriers, tensor memory, zero A tiles, f staged -----------------------------
@@ -339,7 +397,9 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
         const int s = tid / C, cc = tid % C;
         int e = 0;
         if (s < n_slots) {
-            const int q1 = l1 * l1 + r0 + s / nS;
+            int srl, sch, snc;
+            slot_of(s, cq, crem, srl, sch, snc);
+            const int q1 = l1 * l1 + r0 + srl;
             double bound = 0.0;
             const int i1 = __ldg(a.rb_off + q1 + 1);
 #pragma unroll 4
@@ -424,7 +484,8 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
                 double* qc = a.q + cell * M + q1;
                 for (int k1 = 0; k1 < K; ++k1) {
                     double sum = 0.0;
-                    for (int ch = 0; ch < nS; ++ch) sum += red[((rl * nS + ch) * C + cc) * K + k1];
+                    const int s0 = row_first_slot(rl, cq, crem), nc = row_chunks(rl, cq, crem);
+                    for (int ch = 0; ch < nc; ++ch) sum += red[((s0 + ch) * C + cc) * K + k1];
                     qc[(size_t)k1 * NQ] += sum;
                 }
             }
@@ -437,15 +498,29 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
 
     // ---- main loop over the band's l-triplets ------------------------------------------------
     const bool active = warp < n_slots;
-    const int row = r0 + (active ? warp / nS : 0), ch = active ? warp % nS : 0;
+    int srow = 0, ch = 0, nS = 1;
+    if (active) slot_of(warp, cq, crem, srow, ch, nS);
+    const int row = r0 + srow;
     const int m_row = warp * C + c;  // A row of this lane's (slot, cell)
     const double sc = scale[m_row];
     constexpr double kMagic = 6755399441055744.0;  // 1.5 * 2^52: adding it rounds to an integer
+    // the slot's entries of t-list position ti in cur, of ti + 1 fetched during ti, the range of ti + 2
+    SlotEntries cur{0, 0, 0u, 0.0}, nxt{0, 0, 0u, 0.0};
+    int ncb = 0, nce = 0;
+    if (active) {
+        int cb, ce;
+        slot_range(a, tab_off, brows, 0, row, ch, nS, cb, ce);
+        cur = slot_fetch(a, a.e_gs, cb, ce, lane);
+        if (n_t > 1) slot_range(a, tab_off, brows, 1, row, ch, nS, ncb, nce);
+    }
     for (int ti = 0; ti < n_t; ++ti) {
         uint32_t lo[E], hi[E];
         if (active) {
+            if (ti + 1 < n_t) nxt = slot_fetch(a, a.e_gs, ncb, nce, lane);
+            if (ti + 2 < n_t) slot_range(a, tab_off, brows, ti + 2, row, ch, nS, ncb, nce);
             double phi[KH][KQ];
-            slot_phi<K, C>(a, a.e_gs, fs, NQ, a.band_slice[tab_off + ti * brows + row], ch, nS, lane, c, k2o, k3o, phi);
+            slot_phi<K, C>(a, a.e_gs, fs, NQ, cur, lane, c, k2o, k3o, phi);
+            cur = nxt;
 #pragma unroll
             for (int x = 0; x < KH; ++x)
 #pragma unroll
@@ -542,8 +617,8 @@ __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
 // reads its part's K x E block with 16-byte loads shared by the part's 4 cells).  Each lane
 // accumulates its part's share of Q(row, cell) over the band's t-list; the 8 parts and the slots of
 // a row are summed in a fixed order at the end.
-template <int K, int C>
-__global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
+template <int K, int C, int W>
+__global__ void __launch_bounds__(W * 32, 1) af_band64_kernel(SplitArgs a) {
     using S = Shape<K, C>;
     constexpr int KH = S::KH, KQ = S::KQ, PS = S::PS, RTB = S::RT_BYTES;
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -561,9 +636,9 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
     const int rg = a.unit_order[blockIdx.x / a.n_cg];
     const int cg = blockIdx.x % a.n_cg;
     const int* u = a.units + (size_t)rg * U_INTS;
-    const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], nS = u[U_S], tl_off = u[U_TLOFF], n_t = u[U_NT],
-              tab_off = u[U_TABOFF], brows = u[U_BROWS];
-    const int n_slots = nr * nS;
+    const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], cq = u[U_S], crem = u[U_REM], tl_off = u[U_TLOFF],
+              n_t = u[U_NT], tab_off = u[U_TABOFF], brows = u[U_BROWS];
+    const int n_slots = nr * cq + crem;
     const long long cell0 = (long long)cg * C;
 
     if (tid == 0) {
@@ -573,7 +648,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
         *abort_flag = 0;
         rcount[0] = rcount[1] = 0;
     }
-    stage_f<C>(a, fs, M, cell0, tid);
+    stage_f<C, W * 32>(a, fs, M, cell0, tid);
     __syncthreads();
     if (tid == 0)
         for (int ti = 0; ti < min(n_t, 2); ++ti) {
@@ -583,17 +658,35 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
         }
 
     const bool active = warp < n_slots;
-    const int row = r0 + (active ? warp / nS : 0), ch = active ? warp % nS : 0;
+    int srow = 0, ch = 0, nS = 1;
+    if (active) slot_of(warp, cq, crem, srow, ch, nS);
+    const int row = r0 + srow;
     double acc[K];
 #pragma unroll
     for (int k1 = 0; k1 < K; ++k1) acc[k1] = 0.0;
+    // the slot's entries of t-list position ti in cur, of ti + 1 fetched during ti, the range of ti + 2
+    SlotEntries cur{0, 0, 0u, 0.0}, nxt{0, 0, 0u, 0.0};
+    int ncb = 0, nce = 0;
+    if (active) {
+        int cb, ce;
+        slot_range(a, tab_off, brows, 0, row, ch, nS, cb, ce);
+        cur = slot_fetch(a, a.e_g, cb, ce, lane);
+        if (n_t > 1) slot_range(a, tab_off, brows, 1, row, ch, nS, ncb, nce);
+    }
     for (int ti = 0; ti < n_t; ++ti) {
         const int sb = ti & 1;
+        const SlotEntries se = cur;
+        double phi[KH][KQ];
+        if (active) {
+            if (ti + 1 < n_t) nxt = slot_fetch(a, a.e_g, ncb, nce, lane);
+            if (ti + 2 < n_t) slot_range(a, tab_off, brows, ti + 2, row, ch, nS, ncb, nce);
+            slot_phi<K, C>(a, a.e_g, fs, NQ, se, lane, c, k2o, k3o, phi);
+            cur = nxt;
+        }
+        // every warp sees slot sb's copy land before it counts itself done with the slot (the refill of
+        // the slot is armed only after that), also where it reads nothing from it
         const bool ok = wait_bar(&bfull[sb], (uint32_t)((ti >> 1) & 1), abort_flag, a.err);
-        const int sl = active && ok ? a.band_slice[tab_off + ti * brows + row] : -1;
-        if (sl >= 0) {
-            double phi[KH][KQ];
-            slot_phi<K, C>(a, a.e_g, fs, NQ, sl, ch, nS, lane, c, k2o, k3o, phi);
+        if (active && ok && se.cb < se.ce) {
             const double* rp = rring + sb * (RTB / 8) + part * PS;
 #pragma unroll
             for (int x = 0; x < KH; ++x)
@@ -612,7 +705,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
         __syncwarp();
         if (lane == 0) {
             __threadfence_block();
-            if (atomicAdd(&rcount[sb], 1) == kWarps * ((ti >> 1) + 1) - 1 && ti + 2 < n_t && !*abort_flag) {
+            if (atomicAdd(&rcount[sb], 1) == W * ((ti >> 1) + 1) - 1 && ti + 2 < n_t && !*abort_flag) {
                 __threadfence_block();
                 asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
                 const int t = a.band_tl[tl_off + ti + 2];
@@ -638,11 +731,262 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
             double* qc = a.q + cell * M + (l1 * l1 + r0 + rl);
             for (int k1 = 0; k1 < K; ++k1) {
                 double sum = 0.0;
-                for (int chk = 0; chk < nS; ++chk) sum += red[((rl * nS + chk) * C + cc) * K + k1];
+                const int s0 = row_first_slot(rl, cq, crem), nc = row_chunks(rl, cq, crem);
+                for (int chk = 0; chk < nc; ++chk) sum += red[((s0 + chk) * C + cc) * K + k1];
                 qc[(size_t)k1 * NQ] += sum;
             }
         }
     }
+}
+
+// The BF16-split band kernel (CF_FORM_AF_SYM_BF16 / CF_FORM_AF_BF16 where the warp-level BF16 kernel
+// does not exist, K = 12): the same units and FP64 Phi step; Phi = hi + lo and R_t = hi + lo in BF16
+// (round to nearest even), and per 16-element K step the four cross products hi*hi, hi*lo, lo*hi,
+// lo*lo as MMAs (tcgen05.mma kind::f16) into one FP32 accumulator in tensor memory, which runs over
+// the row group's t-list and is added to the FP64 Q at the end.  About 16 significant bits per
+// operand and FP32 accumulation: a reduced-precision form (~1e-5 relative to max|Q|, as the BF16
+// form at K = 8); zero rows of R stay exactly zero.
+template <int K, int C>
+struct ShapeB {
+    using S = Shape<K, C>;
+    static constexpr int KK = S::KK;        // BF16 elements along K (part * EP + e)
+    static constexpr int NKS = KK / 16;     // 16-element (32-byte) K steps
+    static constexpr int ABYTES = 2 * NKS * S::ATILE;  // hi and lo planes of one t
+    static constexpr int BSTEP = 2 * kNB * 32;          // one K step of R hi and lo: 2 x 16 rows x 32 B
+    static constexpr int BBYTES = NKS * BSTEP;
+};
+
+template <int K, int C>
+Layout bf16_layout(int n_q) {
+    using S = Shape<K, C>;
+    using SB = ShapeB<K, C>;
+    Layout l{};
+    int o = 0;
+    auto take = [&](int bytes, int align) {
+        o = (o + align - 1) / align * align;
+        const int r = o;
+        o += bytes;
+        return r;
+    };
+    l.off_a = take(2 * SB::ABYTES, 1024);
+    l.off_b = take(kBRing * SB::BBYTES, 1024);
+    l.off_f = take(C * n_q * K * (int)sizeof(double), 16);
+    l.off_red = take(kSlots * C * K * (int)sizeof(double), 16);
+    l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
+    l.off_misc = take(16 * (int)sizeof(int), 16);
+    l.total = o;
+    return l;
+}
+
+__device__ __forceinline__ uint32_t bf16_bits(float x) { return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x)); }
+
+template <int K, int C>
+__global__ void __launch_bounds__(kThreads, 1) af_bf16_band_kernel(SplitArgs a) {
+    using S = Shape<K, C>;
+    using SB = ShapeB<K, C>;
+    constexpr int KH = S::KH, KQ = S::KQ, E = S::E, EP = S::EP, NKS = SB::NKS;
+    extern __shared__ __align__(1024) unsigned char smem[];
+    uint8_t* sA = smem + a.off_a;
+    uint8_t* sB = smem + a.off_b;
+    double* fs = reinterpret_cast<double*>(smem + a.off_f);
+    double* red = reinterpret_cast<double*>(smem + a.off_red);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + a.off_bar);
+    uint64_t* bfull = bars;      // [2]
+    uint64_t* bfree = bars + 2;  // [2]
+    uint64_t* afree = bars + 4;  // [2]
+    int* misc = reinterpret_cast<int*>(smem + a.off_misc);
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(misc);
+    volatile int* abort_flag = misc + 1;
+    int* acount = misc + 2;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int c = lane % C, part = lane / C, k2o = S::k2_of(part), k3o = S::k3_of(part);
+    const int NQ = a.n_q, M = NQ * K;
+    const int rg = a.unit_order[blockIdx.x / a.n_cg];
+    const int cg = blockIdx.x % a.n_cg;
+    const int* u = a.units + (size_t)rg * U_INTS;
+    const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], cq = u[U_S], crem = u[U_REM], tl_off = u[U_TLOFF],
+              n_t = u[U_NT], tab_off = u[U_TABOFF], brows = u[U_BROWS];
+    const int n_slots = nr * cq + crem;
+    const long long cell0 = (long long)cg * C;
+    const int bbytes = SB::BBYTES;
+
+    if (tid == 0) {
+        for (int i = 0; i < 6; ++i) tc05::mbar_init(&bars[i], 1);
+        tc05::fence_mbar_init();
+        *abort_flag = 0;
+        acount[0] = acount[1] = 0;
+    }
+    if (warp == 0) {
+        tc05::tmem_alloc(tslot, 32);
+        tc05::tmem_relinquish();
+    }
+    {
+        uint4* z = reinterpret_cast<uint4*>(sA);
+        for (int i = tid; i < 2 * SB::ABYTES / 16; i += kThreads) z[i] = make_uint4(0, 0, 0, 0);
+    }
+    stage_f<C>(a, fs, M, cell0, tid);
+    tc05::tc_fence_before();
+    __syncthreads();
+    tc05::tc_fence_after();
+    const uint32_t tbase = *tslot;
+    if (tid == 0)
+        for (int ti = 0; ti < min(n_t, kBRing); ++ti) {
+            const int t = a.band_tl[tl_off + ti];
+            tc05::mbar_arrive_expect_tx(&bfull[ti], (uint32_t)bbytes);
+            tc05::bulk_g2s(sB + ti * bbytes, a.rbf + (size_t)t * bbytes, (uint32_t)bbytes, &bfull[ti]);
+        }
+    {   // zero the accumulator (16 FP32 columns)
+        const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
+        if (warp < 4) {
+            tc05::tmem_st4(tbase + lb + 0, 0u, 0u, 0u, 0u);
+            tc05::tmem_st4(tbase + lb + 4, 0u, 0u, 0u, 0u);
+            tc05::tmem_st4(tbase + lb + 8, 0u, 0u, 0u, 0u);
+            tc05::tmem_st4(tbase + lb + 12, 0u, 0u, 0u, 0u);
+            tc05::tmem_wait_st();
+        }
+    }
+    tc05::tc_fence_before();
+    __syncthreads();
+    tc05::tc_fence_after();
+
+    const bool active = warp < n_slots;
+    int srow = 0, ch = 0, nS = 1;
+    if (active) slot_of(warp, cq, crem, srow, ch, nS);
+    const int row = r0 + srow;
+    const int m_row = warp * C + c;
+    // the slot's entries of t-list position ti in cur, of ti + 1 fetched during ti, the range of ti + 2
+    SlotEntries cur{0, 0, 0u, 0.0}, nxt{0, 0, 0u, 0.0};
+    int ncb = 0, nce = 0;
+    if (active) {
+        int cb, ce;
+        slot_range(a, tab_off, brows, 0, row, ch, nS, cb, ce);
+        cur = slot_fetch(a, a.e_g, cb, ce, lane);
+        if (n_t > 1) slot_range(a, tab_off, brows, 1, row, ch, nS, ncb, nce);
+    }
+    for (int ti = 0; ti < n_t; ++ti) {
+        uint32_t hw[E], lw[E];
+        if (active) {
+            if (ti + 1 < n_t) nxt = slot_fetch(a, a.e_g, ncb, nce, lane);
+            if (ti + 2 < n_t) slot_range(a, tab_off, brows, ti + 2, row, ch, nS, ncb, nce);
+            double phi[KH][KQ];
+            slot_phi<K, C>(a, a.e_g, fs, NQ, cur, lane, c, k2o, k3o, phi);
+            cur = nxt;
+#pragma unroll
+            for (int x = 0; x < KH; ++x)
+#pragma unroll
+                for (int y = 0; y < KQ; ++y) {
+                    const float hf = __bfloat162float(__float2bfloat16_rn((float)phi[x][y]));
+                    hw[x * KQ + y] = bf16_bits(hf);
+                    lw[x * KQ + y] = bf16_bits((float)(phi[x][y] - (double)hf));
+                }
+        }
+        const int b = ti & 1, use = ti >> 1;
+        if (use >= 1) wait_bar(&afree[b], (uint32_t)((use - 1) & 1), abort_flag, a.err);
+        uint8_t* abuf = sA + b * SB::ABYTES;
+        if (active) {
+#pragma unroll
+            for (int pl = 0; pl < 2; ++pl) {
+                uint8_t* tile = abuf + pl * NKS * S::ATILE;
+#pragma unroll
+                for (int w = 0; w < EP / 2; ++w) {
+                    const int e0 = 2 * w, e1 = 2 * w + 1;
+                    const uint32_t v0 = e0 < E ? (pl == 0 ? hw[e0 < E ? e0 : 0] : lw[e0 < E ? e0 : 0]) : 0u;
+                    const uint32_t v1 = e1 < E ? (pl == 0 ? hw[e1 < E ? e1 : 0] : lw[e1 < E ? e1 : 0]) : 0u;
+                    const int byte = 2 * (part * EP + 2 * w);  // element kk = part EP + e at byte 2 kk
+                    const int off = (byte >> 5) * S::ATILE + (m_row >> 3) * 256 + ((byte & 31) >> 4) * 128 +
+                                    (m_row & 7) * 16 + (byte & 15);
+                    *reinterpret_cast<uint32_t*>(tile + off) = v0 | (v1 << 16);
+                }
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        __syncwarp();
+        int last = 0;
+        if (lane == 0) {
+            __threadfence_block();
+            last = atomicAdd(&acount[b], 1) == kWarps * (use + 1) - 1;
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (last && lane == 0 && !*abort_flag) {
+            __threadfence_block();
+            tc05::tc_fence_after();
+            const int tn = ti + 1;
+            if (tn >= kBRing && tn < n_t) {
+                const int sb = tn % kBRing, useb = tn / kBRing;
+                if (wait_bar(&bfree[sb], (uint32_t)((useb - 1) & 1), abort_flag, a.err)) {
+                    const int t = a.band_tl[tl_off + tn];
+                    tc05::mbar_arrive_expect_tx(&bfull[sb], (uint32_t)bbytes);
+                    tc05::bulk_g2s(sB + sb * bbytes, a.rbf + (size_t)t * bbytes, (uint32_t)bbytes, &bfull[sb]);
+                }
+            }
+            wait_bar(&bfull[ti % kBRing], (uint32_t)((ti / kBRing) & 1), abort_flag, a.err);
+            if (!*abort_flag) {
+                const uint8_t* bslot = sB + (ti % kBRing) * bbytes;
+                const uint32_t idesc = tc05::idesc_bf16(S::M, kNB);
+#pragma unroll
+                for (int ks = 0; ks < NKS; ++ks) {
+                    const uint64_t a_hi = tc05::smem_desc_kmajor(abuf + ks * S::ATILE, 128, 256);
+                    const uint64_t a_lo = tc05::smem_desc_kmajor(abuf + NKS * S::ATILE + ks * S::ATILE, 128, 256);
+                    const uint64_t b_hi = tc05::smem_desc_kmajor(bslot + ks * SB::BSTEP, 128, 256);
+                    const uint64_t b_lo = tc05::smem_desc_kmajor(bslot + ks * SB::BSTEP + kNB * 32, 128, 256);
+                    tc05::mma_bf16_ss(tbase, a_hi, b_hi, idesc, true);
+                    tc05::mma_bf16_ss(tbase, a_hi, b_lo, idesc, true);
+                    tc05::mma_bf16_ss(tbase, a_lo, b_hi, idesc, true);
+                    tc05::mma_bf16_ss(tbase, a_lo, b_lo, idesc, true);
+                }
+            }
+            tc05::mma_commit(&afree[b]);
+            tc05::mma_commit(&bfree[ti % kBRing]);
+        }
+        __syncwarp();
+    }
+    // drain: the last uses of both A buffers cover every MMA
+    bool done = true;
+    for (int x = n_t - 1; x >= 0 && x > n_t - 3; --x)
+        done = wait_bar(&afree[x & 1], (uint32_t)((x >> 1) & 1), abort_flag, a.err) && done;
+    const bool ok = __all_sync(0xffffffffu, done);
+    tc05::tc_fence_after();
+    {
+        constexpr int KG = (K + 3) / 4;
+        const int m = S::M == 64 ? 16 * (warp & 3) + (lane & 15) : 32 * (warp & 3) + lane;
+        const bool holds = S::M == 64 ? lane < 16 : true;
+        const int s = m / C, cc = m % C, kg = warp >> 2;
+        if (ok) {
+            uint32_t r16[16];
+            const uint32_t lb = (uint32_t)(32 * (warp & 3)) << 16;
+            tc05::tmem_ld8(tbase + lb, *reinterpret_cast<uint32_t(*)[8]>(r16));
+            tc05::tmem_ld8(tbase + lb + 8, *reinterpret_cast<uint32_t(*)[8]>(r16 + 8));
+            tc05::tmem_wait_ld();
+            if (holds && s < n_slots)
+#pragma unroll
+                for (int j = 0; j < KG; ++j) {
+                    const int want = kg * KG + j;
+                    uint32_t v = 0;
+#pragma unroll
+                    for (int x = 0; x < 16; ++x) v = (x == want) ? r16[x] : v;
+                    if (want < K) red[(s * C + cc) * K + want] = (double)__uint_as_float(v);
+                }
+        }
+    }
+    tc05::tc_fence_before();
+    __syncthreads();
+    if (tid < nr * C) {
+        const int rl = tid / C, cc = tid % C;
+        const long long cell = cell0 + cc;
+        if (cell < a.n_cells) {
+            double* qc = a.q + cell * M + (l1 * l1 + r0 + rl);
+            for (int k1 = 0; k1 < K; ++k1) {
+                double sum = 0.0;
+                const int s0 = row_first_slot(rl, cq, crem), nc = row_chunks(rl, cq, crem);
+                for (int chk = 0; chk < nc; ++chk) sum += red[((s0 + chk) * C + cc) * K + k1];
+                qc[(size_t)k1 * NQ] += sum;
+            }
+        }
+    }
+    tc05::tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tc05::tmem_dealloc(tbase, 32);
 }
 
 }  // namespace
@@ -653,6 +997,7 @@ __global__ void __launch_bounds__(kThreads, 1) af_band64_kernel(SplitArgs a) {
 struct SplitPlan {
     int device = 0, n_q = 0, k = 0, n_l = 0, L = 0;
     int n_rg = 0, tseg = 1, n_abuf = 1;
+    int n_rg64 = 0, w64 = 16;         // the FP64 band kernel's row groups and warps per CTA
     int cells = 4;                    // cells per CTA (C)
     int64_t bytes = 0;
     int smem = 0;
@@ -665,13 +1010,17 @@ struct SplitPlan {
     int* d_rb_l23 = nullptr;
     int* d_units = nullptr;
     int* d_unit_order = nullptr;
+    int* d_units64 = nullptr;         // the FP64 band kernel's row groups (w64 slots each) and their order
+    int* d_unit_order64 = nullptr;
     int* d_band_tl = nullptr;
-    int* d_band_slice = nullptr;
+    int* d_band_rng = nullptr;        // per band: [n_t][rows] (begin, end) of the (t, row) slice's entries
     int* d_err = nullptr;             // set to 1 by a CTA whose bounded wait gave up
     const double* e_g = nullptr;      // borrowed: G in slice order (FP64 band kernel)
     double* d_rfp64 = nullptr;        // FP64 R_t per t as [part][e][k1] (FP64 band kernel)
+    uint8_t* d_rbf = nullptr;         // BF16 hi and lo planes of R_t (BF16-split band kernel)
     Layout lay{};
     Layout lay64{};
+    Layout laybf{};
 };
 
 namespace {
@@ -740,6 +1089,53 @@ void split_r_planes(const std::vector<double>& R, int n_l, std::vector<uint8_t>&
     }
 }
 
+// BF16 bits of a finite float, rounded to nearest even, and back
+uint16_t host_bf16_bits(float x) {
+    uint32_t u;
+    std::memcpy(&u, &x, 4);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+float host_bf16_value(uint16_t b) {
+    const uint32_t u = (uint32_t)b << 16;
+    float x;
+    std::memcpy(&x, &u, 4);
+    return x;
+}
+
+// R_t = hi + lo in BF16 as the B operand of the BF16-split band kernel: per t and 16-element K step,
+// the hi plane then the lo plane, each 16 rows (k1, zero past K) x 32 bytes in the canonical K-major
+// layout; element kk = part EP + e holds (k2, k3) of part's e-th Phi element, zero for e >= E.
+template <int K, int C>
+void split_r_bf16(const std::vector<double>& R, int n_l, std::vector<uint8_t>& planes) {
+    using S = Shape<K, C>;
+    using SB = ShapeB<K, C>;
+    const size_t per_t = (size_t)SB::BBYTES;
+    planes.assign(per_t * n_l, 0);
+    for (int t = 0; t < n_l; ++t) {
+        const double* Rt = R.data() + (size_t)t * K * K * K;
+        uint8_t* pt = planes.data() + per_t * t;
+        for (int p = 0; p < S::P; ++p)
+            for (int e = 0; e < S::E; ++e) {
+                const int k2 = S::k2_of(p) + e / S::KQ, k3 = S::k3_of(p) + e % S::KQ;
+                const int byte = 2 * (p * S::EP + e);
+                const int ks = byte >> 5, kb = byte & 31;
+                for (int k1 = 0; k1 < K; ++k1) {
+                    const double r = Rt[k1 + K * k2 + K * K * k3];
+                    const uint16_t hi = host_bf16_bits((float)r);
+                    const uint16_t lo = host_bf16_bits((float)(r - (double)host_bf16_value(hi)));
+                    for (int pl = 0; pl < 2; ++pl) {
+                        const size_t off = (size_t)ks * SB::BSTEP + pl * kNB * 32 + (k1 >> 3) * 256 + (kb >> 4) * 128 +
+                                           (k1 & 7) * 16 + (kb & 15);
+                        const uint16_t v = pl == 0 ? hi : lo;
+                        std::memcpy(pt + off, &v, 2);
+                    }
+                }
+            }
+    }
+}
+
 template <int K, int C>
 int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     using S = Shape<K, C>;
@@ -757,9 +1153,10 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     if (ce == cudaSuccess) ce = download(R, op.R, (size_t)K * K * K * NL);
     if (ce != cudaSuccess) return fail_split(CF_ECUDA, std::string("split form: download: ") + cudaGetErrorString(ce));
 
-    std::vector<uint8_t> planes;
+    std::vector<uint8_t> planes, rbf;
     std::vector<double> st;
     split_r_planes<K, C>(R, NL, planes, st);
+    split_r_bf16<K, C>(R, NL, rbf);
     // FP64 R_t per t as [part][e][k1] with zero padding after each part
     std::vector<double> rfp64((size_t)NL * S::P * S::PS, 0.0);
     for (int t = 0; t < NL; ++t)
@@ -800,9 +1197,12 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
         rb_off[q + 1] = (int)rb_gs.size();
     }
     // bands: t-lists and the (t, row) -> slice tables
-    std::vector<int> band_tl, band_slice, units;
-    std::vector<double> work;
-    const int cap = kSlots;
+    struct BandInfo {
+        int l1, brows, tl_off, n_t, tab_off;
+        std::vector<double> row_work;
+    };
+    std::vector<BandInfo> bands;
+    std::vector<int> band_tl, band_slice;
     for (int l1 = 0; l1 <= L; ++l1) {
         const int qa = l1 * l1, brows = 2 * l1 + 1;
         std::vector<int> ts;
@@ -823,32 +1223,52 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
                 cell = s;
                 row_work[r] += (double)(slice_e[s + 1] - slice_e[s]);
             }
-        // row groups: as few as the 16 slots allow (every group walks the whole t-list, so the per-t
-        // costs scale with the number of groups); a group of nr < 16 rows splits each row's entries
-        // into S = 16 / nr chunks so that every warp has work
-        const int best_g = (brows + cap - 1) / cap;
-        int r = 0;
-        for (int gi = 0; gi < best_g; ++gi) {
-            const int nr = (brows - r + (best_g - gi) - 1) / (best_g - gi);
-            const int nS = cap / nr;
-            const int uu[U_INTS] = {l1, r, nr, nS, tl_off, (int)ts.size(), tab_off, brows};
-            units.insert(units.end(), uu, uu + U_INTS);
-            double w = 0.0;
-            for (int x = r; x < r + nr; ++x) w += row_work[x];
-            work.push_back(w * K * K + (double)ts.size() * 4096.0);
-            r += nr;
-        }
+        bands.push_back({l1, brows, tl_off, (int)ts.size(), tab_off, row_work});
     }
-    const int n_rg = (int)work.size();
-    std::vector<int> order(n_rg);
-    for (int i = 0; i < n_rg; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work[x] > work[y]; });
-
+    // row groups for a kernel of `cap` slots (one per warp): as few as the slots allow (every group
+    // walks the whole t-list, so the per-t costs scale with the number of groups); a group of
+    // nr < cap rows splits each row's entries into cap / nr chunks, one more for the first cap % nr
+    // rows, so that every warp has work.
+    // Returns the units and their order, heaviest first.
+    auto make_units = [&](int cap, std::vector<int>& units, std::vector<int>& order) {
+        std::vector<double> work;
+        units.clear();
+        for (const BandInfo& bd : bands) {
+            const int best_g = (bd.brows + cap - 1) / cap;
+            int r = 0;
+            for (int gi = 0; gi < best_g; ++gi) {
+                const int nr = (bd.brows - r + (best_g - gi) - 1) / (best_g - gi);
+                const int uu[U_INTS] = {bd.l1, r, nr, cap / nr, bd.tl_off, bd.n_t, bd.tab_off, bd.brows, cap % nr};
+                units.insert(units.end(), uu, uu + U_INTS);
+                double w = 0.0;
+                for (int x = r; x < r + nr; ++x) w += bd.row_work[x];
+                work.push_back(w * K * K + (double)bd.n_t * 4096.0);
+                r += nr;
+            }
+        }
+        order.resize(work.size());
+        for (size_t i = 0; i < work.size(); ++i) order[i] = (int)i;
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return work[x] > work[y]; });
+        return (int)work.size();
+    };
+    std::vector<int> units, order, units64, order64;
+    const int n_rg = make_units(kSlots, units, order);
+    const int w64 = band64_warps(K);
+    const int n_rg64 = make_units(w64, units64, order64);
+    // the (t, row) tables as entry ranges (begin, end), empty where the row has no slice of t
+    std::vector<int> band_rng(2 * band_slice.size(), 0);
+    for (size_t i = 0; i < band_slice.size(); ++i)
+        if (band_slice[i] >= 0) {
+            band_rng[2 * i] = slice_e[band_slice[i]];
+            band_rng[2 * i + 1] = slice_e[band_slice[i] + 1];
+        }
     sp->n_q = NQ;
     sp->k = K;
     sp->n_l = NL;
     sp->L = L;
     sp->n_rg = n_rg;
+    sp->n_rg64 = n_rg64;
+    sp->w64 = w64;
     // int32 accumulators: at most 6 byte products of |255 * 128| per K element and weight
     sp->tseg = std::max(1, (int)(2147483647LL / (6LL * 255 * 128 * S::KK)));
     sp->slice_e = op.slice_e;
@@ -864,7 +1284,8 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
         sp->n_abuf = 1;
         sp->lay = smem_layout<K, C>(NQ, L, 1);
     }
-    sp->lay64 = band64_layout<K, C>(NQ);
+    sp->lay64 = band64_layout<K, C>(NQ, w64);
+    sp->laybf = bf16_layout<K, C>(NQ);
     sp->smem = sp->lay.total;
     int64_t bytes = 0;
     if ((ce = upload_vec(&sp->d_rplanes, planes, bytes)) != cudaSuccess ||
@@ -874,10 +1295,13 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
         (ce = upload_vec(&sp->d_rb_l23, rb_l23, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_units, units, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_unit_order, order, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_units64, units64, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_unit_order64, order64, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_band_tl, band_tl, bytes)) != cudaSuccess ||
-        (ce = upload_vec(&sp->d_band_slice, band_slice, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_band_rng, band_rng, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_err, std::vector<int>(1, 0), bytes)) != cudaSuccess ||
-        (ce = upload_vec(&sp->d_rfp64, rfp64, bytes)) != cudaSuccess)
+        (ce = upload_vec(&sp->d_rfp64, rfp64, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_rbf, rbf, bytes)) != cudaSuccess)
         return fail_split(ce == cudaErrorMemoryAllocation ? CF_ENOMEM : CF_ECUDA,
                           std::string("split form: upload: ") + cudaGetErrorString(ce));
     sp->bytes = bytes;
@@ -907,7 +1331,7 @@ int run_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, c
     a.units = sp->d_units;
     a.unit_order = sp->d_unit_order;
     a.band_tl = sp->d_band_tl;
-    a.band_slice = sp->d_band_slice;
+    a.band_rng = sp->d_band_rng;
     a.f = f_cm;
     a.q = q_cm;
     a.err = sp->d_err;
@@ -937,12 +1361,13 @@ int run_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, c
 
 template <int K, int C>
 int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
+    constexpr int W = band64_warps(K);
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        const cudaError_t e = cudaFuncSetAttribute(af_band64_kernel<K, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   227 * 1024);
+        const cudaError_t e = cudaFuncSetAttribute(af_band64_kernel<K, C, W>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         if (e != cudaSuccess)
             return fail_split(CF_ECUDA, std::string("band kernel: smem attribute: ") + cudaGetErrorString(e));
         attr_set[dev] = true;
@@ -952,10 +1377,10 @@ int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     a.e_q23 = sp->e_q23;
     a.e_g = sp->e_g;
     a.rfp64 = sp->d_rfp64;
-    a.units = sp->d_units;
-    a.unit_order = sp->d_unit_order;
+    a.units = sp->d_units64;
+    a.unit_order = sp->d_unit_order64;
     a.band_tl = sp->d_band_tl;
-    a.band_slice = sp->d_band_slice;
+    a.band_rng = sp->d_band_rng;
     a.f = f_cm;
     a.q = q_cm;
     a.err = sp->d_err;
@@ -968,11 +1393,54 @@ int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     a.off_red = sp->lay64.off_red;
     a.off_bar = sp->lay64.off_bar;
     a.off_misc = sp->lay64.off_misc;
-    const long long blocks = (long long)sp->n_rg * a.n_cg;
+    const long long blocks = (long long)sp->n_rg64 * a.n_cg;
     if (blocks > 0x7fffffffLL) return fail_split(CF_ESHAPE, "band kernel: batch too large for one launch");
-    af_band64_kernel<K, C><<<(unsigned)blocks, kThreads, sp->lay64.total, st>>>(a);
+    af_band64_kernel<K, C, W><<<(unsigned)blocks, W * 32, sp->lay64.total, st>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("band kernel: launch: ") + cudaGetErrorString(e));
+    if (launches) ++*launches;
+    return CF_OK;
+}
+
+template <int K, int C>
+int runbf_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        const cudaError_t e = cudaFuncSetAttribute(af_bf16_band_kernel<K, C>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        if (e != cudaSuccess)
+            return fail_split(CF_ECUDA, std::string("BF16 band kernel: smem attribute: ") + cudaGetErrorString(e));
+        attr_set[dev] = true;
+    }
+    SplitArgs a{};
+    a.slice_e = sp->slice_e;
+    a.e_q23 = sp->e_q23;
+    a.e_g = sp->e_g;
+    a.rbf = sp->d_rbf;
+    a.units = sp->d_units;
+    a.unit_order = sp->d_unit_order;
+    a.band_tl = sp->d_band_tl;
+    a.band_rng = sp->d_band_rng;
+    a.f = f_cm;
+    a.q = q_cm;
+    a.err = sp->d_err;
+    a.n_cells = B;
+    a.n_cg = (int)((B + C - 1) / C);
+    a.n_q = sp->n_q;
+    a.L = sp->L;
+    a.off_a = sp->laybf.off_a;
+    a.off_b = sp->laybf.off_b;
+    a.off_f = sp->laybf.off_f;
+    a.off_red = sp->laybf.off_red;
+    a.off_bar = sp->laybf.off_bar;
+    a.off_misc = sp->laybf.off_misc;
+    const long long blocks = (long long)sp->n_rg * a.n_cg;
+    if (blocks > 0x7fffffffLL) return fail_split(CF_ESHAPE, "BF16 band kernel: batch too large for one launch");
+    af_bf16_band_kernel<K, C><<<(unsigned)blocks, kThreads, sp->laybf.total, st>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("BF16 band kernel: launch: ") + cudaGetErrorString(e));
     if (launches) ++*launches;
     return CF_OK;
 }
@@ -981,8 +1449,26 @@ int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
 
 bool split_supported_k(int k) { return k == 4 || k == 8 || k == 12; }
 
-int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
+int bf16_band_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
     if (B <= 0 || sp->n_rg == 0) return CF_OK;
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, sp->device);
+    if (sp->laybf.total > optin) {
+        char msg[160];
+        snprintf(msg, sizeof(msg), "BF16 band kernel: %d bytes of shared memory needed, %d available", sp->laybf.total,
+                 optin);
+        return fail_split(CF_EUNSUPPORTED, msg);
+    }
+    switch (sp->k) {
+        case 4: return runbf_impl<4, 4>(sp, q_cm, f_cm, B, st, launches);
+        case 8: return sp->cells == 8 ? runbf_impl<8, 8>(sp, q_cm, f_cm, B, st, launches)
+                                      : runbf_impl<8, 4>(sp, q_cm, f_cm, B, st, launches);
+        default: return runbf_impl<12, 4>(sp, q_cm, f_cm, B, st, launches);
+    }
+}
+
+int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
+    if (B <= 0 || sp->n_rg64 == 0) return CF_OK;
     switch (sp->k) {
         case 4: return run64_impl<4, 4>(sp, q_cm, f_cm, B, st, launches);
         case 8: return sp->cells == 8 ? run64_impl<8, 8>(sp, q_cm, f_cm, B, st, launches)
@@ -1031,7 +1517,7 @@ int split_build(SplitPlan** out, const DevOp& folded, int64_t n_g, int64_t n_sli
 void split_destroy(SplitPlan* sp) {
     if (!sp) return;
     void* ptrs[] = {sp->d_rplanes, sp->d_e_gs, sp->d_rb_off, sp->d_rb_gs, sp->d_rb_l23, sp->d_units, sp->d_unit_order, sp->d_band_tl,
-                    sp->d_band_slice, sp->d_err, sp->d_rfp64};
+                    sp->d_band_rng, sp->d_err, sp->d_rfp64, sp->d_rbf, sp->d_units64, sp->d_unit_order64};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete sp;

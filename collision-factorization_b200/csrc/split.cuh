@@ -27,6 +27,11 @@ int split_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, 
 // G and R, plain or folded).  No allocation, no synchronisation.
 int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st,
                int64_t* launches);
+// The BF16-split band kernel on the same units: Q_cm += Q(f_cm) with the K^3 step on the BF16 tensor
+// cores (R_t and Phi as BF16 hi + lo, FP32 accumulation in tensor memory).  CF_EUNSUPPORTED where its
+// shared memory does not fit.  No allocation, no synchronisation.
+int bf16_band_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st,
+                  int64_t* launches);
 // After the stream has been synchronised: CF_ETIMEOUT (and the flag cleared) if a CTA of an
 // earlier launch gave up a bounded wait, else CF_OK.
 int split_check(const SplitPlan* sp);
