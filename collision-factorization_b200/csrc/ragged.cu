@@ -57,12 +57,11 @@ struct Bucket {
     const double* f_cm;
     double* q_cm;
     long long cells;
-    int chunk_base;  // index of the bucket's first upload chunk
-    int hpc;         // half-tiles per chunk
 };
 
 struct Unit {
-    int bucket, ht, bin, pad;
+    int bucket, ht, bin;
+    int chunk;  // the streamed host call's upload chunk holding the half-tile (0 elsewhere)
 };
 
 // TILE = false: the pair routine (8 warps, one mirrored row pair per warp, whole Phi per lane);
@@ -198,7 +197,7 @@ __global__ void __launch_bounds__(kTW * 32, 1)
         const Unit un = units[u];
         const Bucket& bk = s_bk;
         const int M = bk.M, NQ = bk.op.n_q, K = bk.K;
-        const int chunk = bk.chunk_base + un.ht / bk.hpc;
+        const int chunk = un.chunk;
         const long long cell0 = (long long)un.ht * cf::kTileCells;
         const double* fb = rs.ready ? bk.f_cm : ptrs.f[un.bucket];
         double* qb = rs.ready ? bk.q_cm : ptrs.q[un.bucket];
@@ -327,7 +326,30 @@ namespace {
 int64_t ntiles(int64_t B) { return (B + CF_TILE - 1) / CF_TILE; }
 
 constexpr int kHostChunks = 128;            // upload chunks of the streamed host call, at most
-constexpr int kTargetChunks = 24;           // upload chunks aimed at
+// Upload chunks by bytes (f and Q_in of whole half-tiles): the first ones small, so that the kernel
+// starts early, growing to kChunkMaxBytes, and small again over the last 2 kChunkMaxBytes, so that
+// the last contraction and download are short.  Every copy costs a few microseconds of copy-engine
+// time beyond its bytes, so the chunks are as large as the ramp allows.
+constexpr size_t kChunkFirstBytes = size_t(2) << 20;
+constexpr size_t kChunkMaxBytes = size_t(8) << 20;
+
+using StreamWriteValue32 = int (*)(cudaStream_t, unsigned long long, unsigned int, unsigned int);
+
+// cuStreamWriteValue32 through the runtime's driver entry point (no link to the driver library), or
+// null where it is not available: the streamed host call then sets its ready words by 4-byte copies.
+StreamWriteValue32 stream_write_value32() {
+    static StreamWriteValue32 fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuStreamWriteValue32", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (StreamWriteValue32) nullptr;
+        }
+        return reinterpret_cast<StreamWriteValue32>(f);
+    }();
+    return fn;
+}
 constexpr double kHostWaitSeconds = 5.0;     // a CTA gives up on a chunk's ready word after this
 
 void free_ragged(cf_ragged* r) {
@@ -447,42 +469,56 @@ int host_setup(cf_ragged* r) {
                 seen[u.bucket] = 1;
                 order.push_back(u.bucket);
             }
-        // about kTargetChunks chunks in all: every chunk costs three copy calls before the launch
-        int total_ht = 0;
-        for (int b : order) total_ht += (int)((r->cells[b] + 15) / 16);
-        int hpc = std::max(4, (total_ht + kTargetChunks - 1) / kTargetChunks);
+        // chunks of whole half-tiles within one bucket, sized by bytes (f and Q_in): ramped up from
+        // kChunkFirstBytes to kChunkMaxBytes and down again at the end
+        size_t remaining = 0;
+        for (int b : order) remaining += (size_t)r->cells[b] * r->NQ[b] * r->K[b] * 2 * sizeof(double);
+        size_t first = kChunkFirstBytes, maxb = kChunkMaxBytes;
         for (;;) {
-            int n = 0;
-            for (int b : order) n += (int)(((r->cells[b] + 15) / 16 + hpc - 1) / hpc);
-            if (n <= kHostChunks) break;
-            hpc *= 2;
+            // the largest count the ramp can produce: every chunk at least `first`, plus one per bucket
+            if (remaining / first + (size_t)order.size() + 1 <= (size_t)kHostChunks) break;
+            first *= 2;
+            maxb = std::max(maxb, first);
         }
         r->chunk_bucket.clear();
         r->chunk_ht0.clear();
         r->chunk_ht1.clear();
+        std::vector<int> first_chunk(r->n_buckets, 0);
         for (int b : order) {
             const int n_ht = (int)((r->cells[b] + 15) / 16);
-            r->h_buckets[b].chunk_base = (int)r->chunk_bucket.size();
-            r->h_buckets[b].hpc = hpc;
-            for (int h = 0; h < n_ht; h += hpc) {
+            const size_t ht_bytes = (size_t)16 * r->NQ[b] * r->K[b] * 2 * sizeof(double);
+            first_chunk[b] = (int)r->chunk_bucket.size();
+            for (int h = 0; h < n_ht;) {
+                const int i = (int)r->chunk_bucket.size();
+                size_t target = std::min(maxb, first << std::min(i, 16));
+                if (remaining < 2 * maxb) target = std::min(target, std::max(first, remaining / 2));
+                int n = (int)std::max<size_t>(1, target / ht_bytes);
+                n = std::min(n, n_ht - h);
+                // no sliver of a chunk at the end of a bucket
+                if (n_ht - h - n > 0 && (size_t)(n_ht - h - n) * ht_bytes < first / 2) n = n_ht - h;
                 r->chunk_bucket.push_back(b);
                 r->chunk_ht0.push_back(h);
-                r->chunk_ht1.push_back(std::min(n_ht, h + hpc));
+                r->chunk_ht1.push_back(h + n);
+                remaining -= std::min(remaining, (size_t)n * ht_bytes);
+                h += n;
             }
         }
         const int n_chunks = (int)r->chunk_bucket.size();
+        if (n_chunks > kHostChunks) {
+            cf_set_last_error("cf_ragged_q_host: too many upload chunks");
+            return CF_EINVAL;
+        }
         // the streamed work table: the buckets' half-tiles in the upload order, each in 4 q1 bins, so
         // that the first chunk already feeds every SM and results complete (and go back) steadily
         std::vector<Unit> xunits;
-        for (int b : order)
-            for (int h = 0; h < (int)((r->cells[b] + 15) / 16); ++h)
-                for (int k = 0; k < 4; ++k) xunits.push_back({b, h, 1 + k, 0});
+        for (int c = 0; c < n_chunks; ++c)
+            for (int h = r->chunk_ht0[c]; h < r->chunk_ht1[c]; ++h)
+                for (int k = 0; k < 4; ++k) xunits.push_back({r->chunk_bucket[c], h, 1 + k, c});
         r->n_xunits = (int)xunits.size();
         if (!r->d_xunits) RCHECK(cudaMalloc(&r->d_xunits, std::max<size_t>(xunits.size(), 1) * sizeof(Unit)));
         RCHECK(cudaMemcpy(r->d_xunits, xunits.data(), xunits.size() * sizeof(Unit), cudaMemcpyHostToDevice));
         std::vector<int> chunk_units(kHostChunks, 0);
-        for (const Unit& u : xunits)
-            chunk_units[r->h_buckets[u.bucket].chunk_base + u.ht / hpc]++;
+        for (const Unit& u : xunits) chunk_units[u.chunk]++;
         if (!r->d_xsync) RCHECK(cudaMalloc(&r->d_xsync, (3 * kHostChunks + 1) * sizeof(int)));
         RCHECK(cudaMemset(r->d_xsync, 0, (3 * kHostChunks + 1) * sizeof(int)));
         RCHECK(cudaMemcpy(r->d_xsync + 2 * kHostChunks, chunk_units.data(), kHostChunks * sizeof(int),
@@ -495,7 +531,6 @@ int host_setup(cf_ragged* r) {
         r->xwait = (long long)((double)std::max(khz, 1000000) * 1e3 * kHostWaitSeconds);
         RCHECK(cudaFuncSetAttribute(af_ragged_stream_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)r->smem));
-        (void)n_chunks;
     }
     for (int b = 0; b < r->n_buckets; ++b) {
         r->h_buckets[b].f_cm = r->d_io + r->io_off[b];
@@ -527,6 +562,7 @@ int host_streamed(cf_ragged* r, double* const* q_host, const double* const* f_ho
     const int* d_units = r->d_xsync + 2 * kHostChunks;
     int* d_abort = r->d_xsync + 3 * kHostChunks;
     RCHECK(cudaMemsetAsync(d_done, 0, n_chunks * sizeof(int), s_k));
+    const StreamWriteValue32 wv = stream_write_value32();
     auto span = [&](int c, size_t& off, size_t& nb) {
         const int b = r->chunk_bucket[c];
         const int64_t c0 = (int64_t)r->chunk_ht0[c] * 16, c1 = std::min<int64_t>(r->cells[b], (int64_t)r->chunk_ht1[c] * 16);
@@ -541,7 +577,10 @@ int host_streamed(cf_ragged* r, double* const* q_host, const double* const* f_ho
         const Bucket& bk = r->h_buckets[b];
         RCHECK(cudaMemcpyAsync(const_cast<double*>(bk.f_cm) + off, f_host[b] + off, nb, cudaMemcpyHostToDevice, s_in));
         RCHECK(cudaMemcpyAsync(bk.q_cm + off, q_host[b] + off, nb, cudaMemcpyHostToDevice, s_in));
-        RCHECK(cudaMemcpyAsync(d_ready + c, r->h_xepoch + c, sizeof(int), cudaMemcpyHostToDevice, s_in));
+        // the chunk's ready word, ordered after its two copies: a stream memory write (with the fence
+        // that orders the copies' data before it), else a 4-byte copy
+        if (!wv || wv(s_in, (unsigned long long)(uintptr_t)(d_ready + c), (unsigned)epoch, 0u) != 0)
+            RCHECK(cudaMemcpyAsync(d_ready + c, r->h_xepoch + c, sizeof(int), cudaMemcpyHostToDevice, s_in));
     }
     RCHECK(cudaMemsetAsync(r->d_counter, 0, sizeof(int), s_k));
     const RaggedSync rs{d_ready, d_done, d_units, r->h_xsync_dev, r->h_xsync_dev + kHostChunks, d_abort, epoch,
@@ -793,7 +832,6 @@ int cf_ragged_create(cf_ragged** out, cf_plan* const* plans, const int64_t* cell
             hb[b].fT = r->d_tiles + r->tile_off[b];
             hb[b].QT = r->d_tiles + r->tile_off[b] + (size_t)ntiles(r->cells[b]) * CF_TILE * r->NQ[b] * r->K[b];
             hb[b].cells = r->cells[b];
-            hb[b].hpc = 1;
         }
         r->h_buckets = hb;
         e = cudaMemcpy(r->d_buckets, hb.data(), n_buckets * sizeof(Bucket), cudaMemcpyHostToDevice);
