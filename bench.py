@@ -75,7 +75,7 @@ NCU_TRAFFIC = {
 }
 
 
-PROFILE_FORMS = ("af", "af_sym", "af_exact", "rf", "af_sym_i8", "af_f32", "af_sym_f32", "af_bf16", "af_sym_bf16")
+PROFILE_FORMS = ("af", "af_sym", "af_exact", "rf", "af_sym_i8", "af_f32", "af_sym_f32", "af_bf16", "af_sym_bf16", "rf_dense")
 
 
 def _profile_forms(text):
@@ -478,19 +478,22 @@ def run_ours(args):
 
         jv_ms[name] = timed(jstep, max(2, args.steps // 4))
     # reduced-precision forms (FP32 contraction, FP64 accumulation of Q; BF16 split; the exact int8
-    # split on the tensor cores): error and throughput
+    # split on the tensor cores) and the radial-first dense form (FP64): error and throughput
     f32 = {}
     split_ms = None
-    for form in ("af_f32", "af_sym_f32", "af_bf16", "af_sym_bf16", "af_sym_i8"):
+    rfd_ms = None
+    for form in ("af_f32", "af_sym_f32", "af_bf16", "af_sym_bf16", "af_sym_i8", "rf_dense"):
         try:
             step(form)
             err = form_err()
             inv_f = Q.reshape(B, -1)[:, [0, 1, 2, 3, NQ]].abs().max().item()
-            ms = timed(lambda: step(form), max(2, args.steps // 4) if form != "af_sym_i8" else args.steps)
+            ms = timed(lambda: step(form), max(2, args.steps // 4) if form not in ("af_sym_i8", "rf_dense") else args.steps)
             f32[form] = {"cells_per_s": B * len(ms) / (sum(ms) / 1e3), "max_rel_err_vs_fp64": err,
                          "meets_1e-10": bool(err <= 1e-10), "invariants_abs_max": inv_f}
             if form == "af_sym_i8":
                 split_ms, err_split = ms, err
+            if form == "rf_dense":
+                rfd_ms, err_rfd = ms, err
         except Exception as e:
             f32[form] = {"unavailable": str(e)[:160]}
     clk = clocks.stop()
@@ -501,6 +504,8 @@ def run_ours(args):
     cand = {"af": (sum(step_ms) / len(step_ms), err_af, step_ms), "af_sym": (sum(sym_ms) / len(sym_ms), err_sym, sym_ms)}
     if split_ms:
         cand["af_sym_i8"] = (sum(split_ms) / len(split_ms), err_split, split_ms)
+    if rfd_ms:
+        cand["rf_dense"] = (sum(rfd_ms) / len(rfd_ms), err_rfd, rfd_ms)
     chosen = min((k for k, v in cand.items() if v[1] <= 1e-10), key=lambda k: cand[k][0], default="af")
     chosen_ms = cand[chosen][2]
     value, total_s = weak_rate(world, B, args.steps, sum(chosen_ms) / 1e3 * args.steps / len(chosen_ms))
@@ -511,7 +516,7 @@ def run_ours(args):
     step(chosen)
     torch.cuda.synchronize(dev)
     step_path = _lib.PATH_NAMES[op.info()["last_path"]]
-    if step_path in ("split_i8", "band") and _lib.launch_count() - n0 == 1:
+    if (step_path in ("split_i8", "band") and _lib.launch_count() - n0 == 1) or step_path == "rf_dense":
         kern_list = chosen_ms
         last_path = step_path
     else:
@@ -532,7 +537,9 @@ def run_ours(args):
                  "split_i8": "af_split_kernel (Phi in FP64 on the folded operator, K^3 step on the int8 tensor cores "
                              "(tcgen05.mma kind::i8, exact 6x6-byte split); the whole device step)",
                  "band": "af_band64_kernel (l1-band units, 4 cells' f resident, R_t staged per t by cp.async.bulk, "
-                         "FP64; the whole device step)"}.get(last_path, "?")
+                         "FP64; the whole device step)",
+                 "rf_dense": "rf_dense_kernel (radial step as a dense GEMM over cells per (t, q2), FP64; the device step "
+                             "with its f packing and partial-sum reduction)"}.get(last_path, "?")
     kern_s = sum(kern_list) / len(kern_list) / 1e3
     flops_launch = op.flops_q * B
     achieved_tf = flops_launch / kern_s / 1e12

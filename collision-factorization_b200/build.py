@@ -60,7 +60,8 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = True) ->
     units = [(CSRC / "plan.cu", BUILD / "plan.o", []), (CSRC / "noalloc.cu", BUILD / "noalloc.o", []),
              (CSRC / "krylov.cu", BUILD / "krylov.o", []), (CSRC / "mlp.cu", BUILD / "mlp.o", []),
              (CSRC / "ragged.cu", BUILD / "ragged.o", []), (CSRC / "stepping.cu", BUILD / "stepping.o", []),
-             (CSRC / "rtensor.cu", BUILD / "rtensor.o", []), (CSRC / "split.cu", BUILD / "split.o", [])]
+             (CSRC / "rtensor.cu", BUILD / "rtensor.o", []), (CSRC / "split.cu", BUILD / "split.o", []),
+             (CSRC / "rfdense.cu", BUILD / "rfdense.o", [])]
     units += [(CSRC / "inst.cu", BUILD / f"inst_k{k}.o", [f"-DCF_K={k}"]) for k in K_VALUES]
     todo = [u for u in units if force or _stale(u[1])]
     if todo:

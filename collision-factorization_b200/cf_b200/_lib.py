@@ -23,10 +23,10 @@ STATUS_NAMES = {
 }
 
 FORM_AF, FORM_RF, FORM_AF_EXACT, FORM_RF_EXACT, FORM_AF_SYM, FORM_AF_F32, FORM_AF_SYM_F32 = 0, 1, 2, 3, 4, 5, 6
-FORM_AF_BF16, FORM_AF_SYM_BF16, FORM_AF_SYM_I8 = 7, 8, 9
+FORM_AF_BF16, FORM_AF_SYM_BF16, FORM_AF_SYM_I8, FORM_RF_DENSE = 7, 8, 9, 10
 FORMS = {"af": FORM_AF, "rf": FORM_RF, "af_exact": FORM_AF_EXACT, "rf_exact": FORM_RF_EXACT, "af_sym": FORM_AF_SYM,
          "af_f32": FORM_AF_F32, "af_sym_f32": FORM_AF_SYM_F32, "af_bf16": FORM_AF_BF16,
-         "af_sym_bf16": FORM_AF_SYM_BF16, "af_sym_i8": FORM_AF_SYM_I8}
+         "af_sym_bf16": FORM_AF_SYM_BF16, "af_sym_i8": FORM_AF_SYM_I8, "rf_dense": FORM_RF_DENSE}
 
 # Every symbol the header declares; the tests check that the library exports all of them.
 EXPORTS = [
@@ -58,7 +58,7 @@ class PlanInfo(C.Structure):
     ]
 
 PATH_NAMES = {0: "none", 1: "gather", 2: "tile", 3: "pair", 4: "pair_l1", 5: "pair_split", 6: "tile_mma", 7: "bf16_mma", 8: "tile_quarter",
-              9: "few", 10: "split_i8", 11: "band", 12: "band_bf16"}
+              9: "few", 10: "split_i8", 11: "band", 12: "band_bf16", 13: "rf_dense"}
 
 _DP = C.POINTER(C.c_double)
 

@@ -74,6 +74,11 @@ extern "C" int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f
     int st = cf_plan_get_info(plan, &info);
     if (st != CF_OK) return st;
     // The split form builds its own device tables on first use (and keeps an error word): refused.
+    if (form == CF_FORM_RF_DENSE) {
+        cf_set_last_error("cf_q_device_noalloc: the radial-first dense form (CF_FORM_RF_DENSE) allocates its scratch; "
+                          "use cf_q_device");
+        return CF_EUNSUPPORTED;
+    }
     if (form == CF_FORM_AF_SYM_I8) {
         cf_set_last_error("cf_q_device_noalloc: the split form (CF_FORM_AF_SYM_I8) is not available without "
                           "allocation; use cf_q_device");

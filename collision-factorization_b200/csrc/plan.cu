@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "rfdense.cuh"
 #include "split.cuh"
 #include "../../include/cf_b200.h"
 #include "common.cuh"
@@ -164,6 +165,10 @@ struct cf_plan {
     cf::SplitPlan* split = nullptr;
     int split_status = -1;
     std::mutex split_mu;
+    // radial-first dense form (CF_FORM_RF_DENSE): built on first use on the plan it runs on
+    cf::RfDensePlan* rfd = nullptr;
+    int rfd_status = -1;
+    std::mutex rfd_mu;
     std::vector<double> h_labels, h_vals, h_ic, h_R;  // host copies kept for building the folded operator
 
     DevOp op() const {
@@ -253,6 +258,10 @@ int upload(T** dst, const std::vector<T>& src, int64_t& bytes) {
 
 void free_plan_memory(cf_plan* p);
 void free_plan_memory(cf_plan* p) {
+    if (p->rfd) {
+        cf::rfdense_destroy(p->rfd);
+        p->rfd = nullptr;
+    }
     if (p->split) {
         cf::split_destroy(p->split);
         p->split = nullptr;
@@ -573,6 +582,7 @@ bool streamable(const cf_plan* p, const cf_plan* target, int what, bool exact, i
 int run_split(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int run_bf16_band(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
+int run_rfdense(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int check_split(cf_plan* p);
 
 // The fast FP64 angular-first (plain or folded) or radial-first form, or the exact angular-first
@@ -597,6 +607,10 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
     if (f32 == 3) {
         if (what != 0) return fail(CF_EUNSUPPORTED, "the split form computes Q only");
         return run_split(p, q_dev, f_dev, B, st);
+    }
+    if (f32 == 4) {
+        if (what != 0) return fail(CF_EUNSUPPORTED, "the radial-first dense form computes Q only");
+        return run_rfdense(p, q_dev, f_dev, B, st);
     }
     {
         const int r = run_few(p, what, exact, q_dev, f_dev, B, st, sym, f32);
@@ -914,6 +928,39 @@ int run_bf16_band(cf_plan* target, double* q_dev, const double* f_dev, int64_t B
     if (launches > 0) {
         target->last_path = cf::PATH_BAND_BF16;
         if (target->parent) target->parent->last_path = cf::PATH_BAND_BF16;
+    }
+    return CF_OK;
+}
+
+// The radial-first dense form on the plan's folded twin where the operator folds, else on the plan.
+int run_rfdense(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st) {
+    if (!cf::rfdense_supported_k(p->k)) return fail(CF_EUNSUPPORTED, "the radial-first dense form needs K <= 16");
+    cf_plan* target = nullptr;
+    if (get_sym(p, &target) != CF_OK) {
+        g_last_error.clear();
+        target = p;
+    }
+    cf::RfDensePlan* rp = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(target->rfd_mu);
+        if (!target->rfd) {
+            if (target->rfd_status > 0) return fail(target->rfd_status, "the radial-first dense form is not available for this operator");
+            const int st_b = cf::rfdense_build(&target->rfd, target->op(), target->n_g, target->n_slices, target->device);
+            if (st_b != CF_OK) {
+                target->rfd_status = st_b;
+                return st_b;  // message set by rfdense_build
+            }
+            target->rfd_status = 0;
+            target->dev_bytes += cf::rfdense_device_bytes(target->rfd);
+        }
+        rp = target->rfd;
+    }
+    int64_t launches = 0;
+    CF_TRY(cf::rfdense_run(rp, q_dev, f_dev, B, st, &launches));
+    g_launches += launches;
+    if (launches > 0) {
+        target->last_path = cf::PATH_RF_DENSE;
+        p->last_path = cf::PATH_RF_DENSE;
     }
     return CF_OK;
 }
@@ -1379,6 +1426,7 @@ int form_what(int form, bool& exact, bool& sym, int& f32) {
         case CF_FORM_RF_EXACT: exact = true; return 1;
         case CF_FORM_AF_SYM: exact = false; sym = true; return 0;
         case CF_FORM_AF_SYM_I8: exact = false; sym = true; f32 = 3; return 0;
+        case CF_FORM_RF_DENSE: exact = false; sym = true; f32 = 4; return 0;
         default: return -1;
     }
 }

@@ -68,7 +68,14 @@ typedef enum cf_form {
                               cores (tcgen05): Phi and R_t as 47-bit fixed-point integers split into six
                               bytes each, byte products summed exactly in int32 tensor memory, recombined
                               in FP64; ~1e-11 of max|Q|; K = 4, 8 or 12; Q only, cell-major arrays
-                              (cf_q_device, cf_contract_host); no counterpart in the reference */
+                              (cf_q_device, cf_contract_host); no counterpart in the reference */,
+    CF_FORM_RF_DENSE = 10  /* radial first with the radial step factored out of the entries: per
+                              (l-triplet t, q2) a dense [K^2 x K] x [K x cells] product
+                              C = R_t x_2 f(q2) over the batch's cells, then K^2 per entry
+                              (radial_first_collision_kernel_mex.cpp:41-59 computes K^3 per entry);
+                              FP64, on the q2 <-> q3 folded operator where the operator folds; Q only,
+                              cell-major arrays (cf_q_device, cf_contract_host); allocates its scratch
+                              on first use at a batch size */
 } cf_form;
 
 typedef struct cf_plan cf_plan;
