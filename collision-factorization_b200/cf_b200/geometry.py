@@ -262,6 +262,8 @@ def fold_q2q3(geo: Geometry, R: np.ndarray, K: int):
     for z in range(lab.shape[0]):
         q1, q2, q3 = lab[z]
         l2, l3 = l[z, 1], l[z, 2]
+        if (q1, q3, q2) not in where:  # every entry needs its mirror, kept or dropped
+            raise ValueError(f"entry {z + 1} has no (q1, q3, q2) mirror: the list does not fold")
         if not (l2 < l3 or (l2 == l3 and q2 <= q3)):
             continue
         zp = where[(q1, q3, q2)]

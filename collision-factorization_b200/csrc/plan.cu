@@ -777,10 +777,12 @@ int build_folded(const cf_plan* p, std::vector<double>& lab2, std::vector<double
         const int t = (int)ic[z] - 1;
         const int l2 = trip[t][1], l3 = trip[t][2];
         const double q1 = lab[z], q2 = lab[z + NG], q3 = lab[z + 2 * NG];
-        if (!(l2 < l3 || (l2 == l3 && q2 <= q3))) continue;
         const int64_t key = (((int64_t)q1 - 1) * NQ + ((int64_t)q3 - 1)) * NQ + ((int64_t)q2 - 1);
         auto it = where.find(key);
+        // every entry needs its mirror, also the ones the folded list drops (a dropped entry whose
+        // kept mirror is missing would otherwise vanish from Q without a word)
         if (it == where.end()) return fail(CF_EUNSUPPORTED, "fold: entry %lld has no (q1,q3,q2) mirror", (long long)z + 1);
+        if (!(l2 < l3 || (l2 == l3 && q2 <= q3))) continue;
         const double gp = val[it->second];
         if (std::fabs(gp - val[z]) > 1e-10 * gmax)
             return fail(CF_EUNSUPPORTED, "fold: G(q1,q2,q3) and G(q1,q3,q2) differ at entry %lld", (long long)z + 1);

@@ -147,3 +147,26 @@ def test_q2q3_folded_operator_is_the_same_quadratic_form(name, oracle_lib):
     Q = np.zeros((NQ, K), order="F")
     oracle_lib.af(Q, d["f"], lab, vals, ic, Rs, NQ, K)
     assert normwise_err(Q, d["Q_af"]) < 1e-14
+
+
+def test_fold_refuses_a_list_missing_a_kept_entry():
+    """The folded list keeps one entry of each mirror pair (l2 < l3, or l2 = l3 and q2 <= q3).  A list
+    that lacks a kept entry but still holds its mirror does not fold: the restatement refuses it
+    (the library returns CF_EUNSUPPORTED, tests/test_gpu_band_edges.py), instead of dropping the
+    orphaned mirror from Q."""
+    from cf_b200 import geometry
+
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(3))
+    K = 2
+    R = np.zeros((K, K, K, int(geo.ic_map.max())))
+    geometry.fold_q2q3(geo, R, K)  # the full list folds
+    lq = np.floor(np.sqrt(geo.labels - 1.0)).astype(int)
+    z = int(np.nonzero((geo.labels[:, 1] != geo.labels[:, 2]) & (lq[:, 1] < lq[:, 2]))[0][0])
+    keep = np.ones(len(geo.vals), dtype=bool)
+    keep[z] = False
+    import dataclasses
+
+    cut = dataclasses.replace(geo, labels=np.ascontiguousarray(geo.labels[keep]), vals=geo.vals[keep].copy(),
+                              ic_map=geo.ic_map[keep].copy())
+    with pytest.raises(ValueError):
+        geometry.fold_q2q3(cut, R, K)
