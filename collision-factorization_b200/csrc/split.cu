@@ -47,6 +47,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/cf_b200.h"
@@ -77,16 +78,16 @@ constexpr long long kWaitCycles = 2000000000LL;  // ~1 s of SM clock per wait
 // the K x K Phi: (k2 half, k3 quarter) for P = 8, a k3 quarter for P = 4.
 template <int K, int C>
 struct Shape {
-    static_assert((C == 4 && K % 4 == 0 && K <= 12) || (C == 8 && K == 8),
-                  "the band kernels take K in {4, 8, 12} with 4 cells per CTA, or K = 8 with 8");
+    static_assert((C == 4 && K % 4 == 0 && K <= 12) || (C == 8 && (K == 8 || K == 12)),
+                  "the band kernels take K in {4, 8, 12} with 4 cells per CTA, or K = 8 and 12 with 8");
     static constexpr int P = 32 / C;                // lanes (parts) per cell
     static constexpr int KH = P == 8 ? K / 2 : K;   // k2 per lane
     static constexpr int KQ = K / 4;                // k3 per lane
     static constexpr int E = KH * KQ;               // Phi elements per lane
     static constexpr int EP = (E + 3) / 4 * 4;      // bytes per lane in a plane (word aligned)
     static constexpr int KK = P * EP;               // K dimension of the MMA (kk = part * EP + e)
-    static constexpr int NKS = KK / 32;             // 32-byte K steps
-    static_assert(KK % 32 == 0, "whole K steps");
+    static constexpr int NKS = KK / 32;             // 32-byte K steps of the int8 planes (whole
+                                                    // steps checked where they are used)
     static constexpr int M = 16 * C;                // MMA rows: 16 slots x C cells
     static constexpr int ATILE = M * 32;            // one 32-byte K step of an A plane
     static constexpr int PS = E * K + 2;            // FP64 R: doubles per part (16 bytes of padding
@@ -254,31 +255,31 @@ __device__ __forceinline__ SlotEntries slot_fetch(const SplitArgs& a, const doub
 
 // Phi of one slot for this lane's part (k2 = k2o .. k2o + KH - 1, k3 = k3o .. k3o + KQ - 1) of cell c:
 // the slot's entries, grouped by q2 (h = sum G f(q3) over a run of equal q2, then phi += f(q2) (x) h).
-template <int K, int C>
+template <int K, int C, typename T = double>
 __device__ __forceinline__ void slot_phi(const SplitArgs& a, const double* __restrict__ gv,
-                                         const double* __restrict__ fs, int NQ, const SlotEntries& se, int lane,
+                                         const T* __restrict__ fs, int NQ, const SlotEntries& se, int lane,
                                          int c, int k2o, int k3o,
-                                         double (&phi)[Shape<K, C>::KH][Shape<K, C>::KQ]) {
+                                         T (&phi)[Shape<K, C>::KH][Shape<K, C>::KQ]) {
     constexpr int KH = Shape<K, C>::KH, KQ = Shape<K, C>::KQ;
 #pragma unroll
     for (int x = 0; x < KH; ++x)
 #pragma unroll
-        for (int y = 0; y < KQ; ++y) phi[x][y] = 0.0;
+        for (int y = 0; y < KQ; ++y) phi[x][y] = (T)0;
     const int cb = se.cb, ce = se.ce;
     if (cb >= ce) return;
-    double h[KQ];
+    T h[KQ];
 #pragma unroll
-    for (int y = 0; y < KQ; ++y) h[y] = 0.0;
+    for (int y = 0; y < KQ; ++y) h[y] = (T)0;
     int cur = -1;
     auto flush = [&]() {
 #pragma unroll
         for (int x = 0; x < KH; ++x) {
-            const double f2 = fs[((k2o + x) * NQ + cur) * C + c];
+            const T f2 = fs[((k2o + x) * NQ + cur) * C + c];
 #pragma unroll
             for (int y = 0; y < KQ; ++y) phi[x][y] = fma(f2, h[y], phi[x][y]);
         }
 #pragma unroll
-        for (int y = 0; y < KQ; ++y) h[y] = 0.0;
+        for (int y = 0; y < KQ; ++y) h[y] = (T)0;
     };
     for (int eb = cb; eb < ce; eb += 32) {
         const int nb = min(32, ce - eb);
@@ -294,7 +295,7 @@ __device__ __forceinline__ void slot_phi(const SplitArgs& a, const double* __res
         }
         for (int j = 0; j < nb; ++j) {
             const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, j);
-            const double g = __shfl_sync(0xffffffffu, my_g, j);
+            const T g = (T)__shfl_sync(0xffffffffu, my_g, j);
             const int q2 = (int)(q23 & 0xffffu), q3 = (int)(q23 >> 16);
             if (q2 != cur) {
                 if (cur >= 0) flush();
@@ -321,6 +322,7 @@ __device__ __forceinline__ void stage_f(const SplitArgs& a, double* fs, int M, l
 template <int K, int C>
 __global__ void __launch_bounds__(kThreads, 1) af_split_kernel(SplitArgs a) {
     using S = Shape<K, C>;
+    static_assert(S::KK % 32 == 0, "whole 32-byte K steps of the int8 planes");
     constexpr int KH = S::KH, KQ = S::KQ, E = S::E, EP = S::EP, NKS = S::NKS;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint8_t* sA = smem + a.off_a;
@@ -756,8 +758,8 @@ struct ShapeB {
     static constexpr int BBYTES = NKS * BSTEP;
 };
 
-template <int K, int C>
-Layout bf16_layout(int n_q) {
+template <int K, int C, typename T = double>
+Layout bf16_layout(int n_q, int n_abuf = 2) {
     using S = Shape<K, C>;
     using SB = ShapeB<K, C>;
     Layout l{};
@@ -768,27 +770,42 @@ Layout bf16_layout(int n_q) {
         o += bytes;
         return r;
     };
-    l.off_a = take(2 * SB::ABYTES, 1024);
+    l.off_a = take(n_abuf * SB::ABYTES, 1024);
     l.off_b = take(kBRing * SB::BBYTES, 1024);
-    l.off_f = take(C * n_q * K * (int)sizeof(double), 16);
+    l.off_f = take(C * n_q * K * (int)sizeof(T), 16);
     l.off_red = take(kSlots * C * K * (int)sizeof(double), 16);
     l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
     l.off_misc = take(16 * (int)sizeof(int), 16);
     l.total = o;
+    (void)S::M;
     return l;
+}
+
+// The C cells' f as T (FP64, or FP32 for the FP32 Phi step) into shared memory, as stage_f.
+template <int C, typename T>
+__device__ __forceinline__ void stage_f_t(const SplitArgs& a, T* fs, int M, long long cell0, int tid) {
+    for (int i = tid; i < C * M; i += kThreads) {
+        const int cc = i % C, r = i / C;
+        const long long cell = cell0 + cc;
+        fs[i] = cell < a.n_cells ? (T)__ldg(a.f + cell * M + r) : (T)0;
+    }
 }
 
 __device__ __forceinline__ uint32_t bf16_bits(float x) { return (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(x)); }
 
-template <int K, int C>
+// T: the arithmetic of the Phi step (double, or float with f staged in FP32, which halves f's
+// shared memory: 8 cells per CTA at L = 16, K = 12, and an M = 128 MMA).  NAB: A buffers (1 or 2).
+template <int K, int C, typename T = double, int NAB = 2>
 __global__ void __launch_bounds__(kThreads, 1) af_bf16_band_kernel(SplitArgs a) {
     using S = Shape<K, C>;
     using SB = ShapeB<K, C>;
+    static_assert(S::KK % 16 == 0, "whole 16-element K steps");
+    static_assert(NAB == 1 || NAB == 2, "one or two A buffers");
     constexpr int KH = S::KH, KQ = S::KQ, E = S::E, EP = S::EP, NKS = SB::NKS;
     extern __shared__ __align__(1024) unsigned char smem[];
     uint8_t* sA = smem + a.off_a;
     uint8_t* sB = smem + a.off_b;
-    double* fs = reinterpret_cast<double*>(smem + a.off_f);
+    T* fs = reinterpret_cast<T*>(smem + a.off_f);
     double* red = reinterpret_cast<double*>(smem + a.off_red);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + a.off_bar);
     uint64_t* bfull = bars;      // [2]
@@ -823,9 +840,9 @@ __global__ void __launch_bounds__(kThreads, 1) af_bf16_band_kernel(SplitArgs a) 
     }
     {
         uint4* z = reinterpret_cast<uint4*>(sA);
-        for (int i = tid; i < 2 * SB::ABYTES / 16; i += kThreads) z[i] = make_uint4(0, 0, 0, 0);
+        for (int i = tid; i < NAB * SB::ABYTES / 16; i += kThreads) z[i] = make_uint4(0, 0, 0, 0);
     }
-    stage_f<C>(a, fs, M, cell0, tid);
+    stage_f_t<C, T>(a, fs, M, cell0, tid);
     tc05::tc_fence_before();
     __syncthreads();
     tc05::tc_fence_after();
@@ -865,34 +882,30 @@ __global__ void __launch_bounds__(kThreads, 1) af_bf16_band_kernel(SplitArgs a) 
         if (n_t > 1) slot_range(a, tab_off, brows, 1, row, ch, nS, ncb, nce);
     }
     for (int ti = 0; ti < n_t; ++ti) {
-        uint32_t hw[E], lw[E];
+        T phi[KH][KQ];
         if (active) {
             if (ti + 1 < n_t) nxt = slot_fetch(a, a.e_g, ncb, nce, lane);
             if (ti + 2 < n_t) slot_range(a, tab_off, brows, ti + 2, row, ch, nS, ncb, nce);
-            double phi[KH][KQ];
-            slot_phi<K, C>(a, a.e_g, fs, NQ, cur, lane, c, k2o, k3o, phi);
+            slot_phi<K, C, T>(a, a.e_g, fs, NQ, cur, lane, c, k2o, k3o, phi);
             cur = nxt;
-#pragma unroll
-            for (int x = 0; x < KH; ++x)
-#pragma unroll
-                for (int y = 0; y < KQ; ++y) {
-                    const float hf = __bfloat162float(__float2bfloat16_rn((float)phi[x][y]));
-                    hw[x * KQ + y] = bf16_bits(hf);
-                    lw[x * KQ + y] = bf16_bits((float)(phi[x][y] - (double)hf));
-                }
         }
-        const int b = ti & 1, use = ti >> 1;
+        const int b = ti % NAB, use = ti / NAB;
         if (use >= 1) wait_bar(&afree[b], (uint32_t)((use - 1) & 1), abort_flag, a.err);
         uint8_t* abuf = sA + b * SB::ABYTES;
         if (active) {
+            // Phi = hi + lo in BF16 (round to nearest even), two elements per 32-bit word
+            auto part_bits = [&](int e, int pl) -> uint32_t {
+                if (e >= E) return 0u;
+                const T x = phi[(e < E ? e : 0) / KQ][(e < E ? e : 0) % KQ];
+                const float hf = __bfloat162float(__float2bfloat16_rn((float)x));
+                return pl == 0 ? bf16_bits(hf) : bf16_bits((float)(x - (T)hf));
+            };
 #pragma unroll
             for (int pl = 0; pl < 2; ++pl) {
                 uint8_t* tile = abuf + pl * NKS * S::ATILE;
 #pragma unroll
                 for (int w = 0; w < EP / 2; ++w) {
-                    const int e0 = 2 * w, e1 = 2 * w + 1;
-                    const uint32_t v0 = e0 < E ? (pl == 0 ? hw[e0 < E ? e0 : 0] : lw[e0 < E ? e0 : 0]) : 0u;
-                    const uint32_t v1 = e1 < E ? (pl == 0 ? hw[e1 < E ? e1 : 0] : lw[e1 < E ? e1 : 0]) : 0u;
+                    const uint32_t v0 = part_bits(2 * w, pl), v1 = part_bits(2 * w + 1, pl);
                     const int byte = 2 * (part * EP + 2 * w);  // element kk = part EP + e at byte 2 kk
                     const int off = (byte >> 5) * S::ATILE + (m_row >> 3) * 256 + ((byte & 31) >> 4) * 128 +
                                     (m_row & 7) * 16 + (byte & 15);
@@ -943,8 +956,8 @@ __global__ void __launch_bounds__(kThreads, 1) af_bf16_band_kernel(SplitArgs a) 
     }
     // drain: the last uses of both A buffers cover every MMA
     bool done = true;
-    for (int x = n_t - 1; x >= 0 && x > n_t - 3; --x)
-        done = wait_bar(&afree[x & 1], (uint32_t)((x >> 1) & 1), abort_flag, a.err) && done;
+    for (int x = n_t - 1; x >= 0 && x > n_t - 1 - NAB; --x)
+        done = wait_bar(&afree[x % NAB], (uint32_t)((x / NAB) & 1), abort_flag, a.err) && done;
     const bool ok = __all_sync(0xffffffffu, done);
     tc05::tc_fence_after();
     {
@@ -1018,9 +1031,11 @@ struct SplitPlan {
     const double* e_g = nullptr;      // borrowed: G in slice order (FP64 band kernel)
     double* d_rfp64 = nullptr;        // FP64 R_t per t as [part][e][k1] (FP64 band kernel)
     uint8_t* d_rbf = nullptr;         // BF16 hi and lo planes of R_t (BF16-split band kernel)
+    uint8_t* d_rbf8 = nullptr;        // K = 12: the same for 8 cells per CTA (Phi in FP32)
     Layout lay{};
     Layout lay64{};
     Layout laybf{};
+    Layout laybf8{};                  // K = 12: 8 cells per CTA, f and Phi in FP32, one A buffer
 };
 
 namespace {
@@ -1157,6 +1172,8 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     std::vector<double> st;
     split_r_planes<K, C>(R, NL, planes, st);
     split_r_bf16<K, C>(R, NL, rbf);
+    std::vector<uint8_t> rbf8;
+    if constexpr (K == 12) split_r_bf16<12, 8>(R, NL, rbf8);
     // FP64 R_t per t as [part][e][k1] with zero padding after each part
     std::vector<double> rfp64((size_t)NL * S::P * S::PS, 0.0);
     for (int t = 0; t < NL; ++t)
@@ -1286,6 +1303,7 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     }
     sp->lay64 = band64_layout<K, C>(NQ, w64);
     sp->laybf = bf16_layout<K, C>(NQ);
+    if constexpr (K == 12) sp->laybf8 = bf16_layout<12, 8, float>(NQ, 1);
     sp->smem = sp->lay.total;
     int64_t bytes = 0;
     if ((ce = upload_vec(&sp->d_rplanes, planes, bytes)) != cudaSuccess ||
@@ -1301,7 +1319,8 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
         (ce = upload_vec(&sp->d_band_rng, band_rng, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_err, std::vector<int>(1, 0), bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_rfp64, rfp64, bytes)) != cudaSuccess ||
-        (ce = upload_vec(&sp->d_rbf, rbf, bytes)) != cudaSuccess)
+        (ce = upload_vec(&sp->d_rbf, rbf, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_rbf8, rbf8, bytes)) != cudaSuccess)
         return fail_split(ce == cudaErrorMemoryAllocation ? CF_ENOMEM : CF_ECUDA,
                           std::string("split form: upload: ") + cudaGetErrorString(ce));
     sp->bytes = bytes;
@@ -1402,13 +1421,15 @@ int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     return CF_OK;
 }
 
-template <int K, int C>
+template <int K, int C, typename T = double, int NAB = 2>
 int runbf_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
+    const Layout& lay = (std::is_same<T, float>::value && K == 12) ? sp->laybf8 : sp->laybf;
+    const uint8_t* planes = (std::is_same<T, float>::value && K == 12) ? sp->d_rbf8 : sp->d_rbf;
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        const cudaError_t e = cudaFuncSetAttribute(af_bf16_band_kernel<K, C>,
+        const cudaError_t e = cudaFuncSetAttribute(af_bf16_band_kernel<K, C, T, NAB>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         if (e != cudaSuccess)
             return fail_split(CF_ECUDA, std::string("BF16 band kernel: smem attribute: ") + cudaGetErrorString(e));
@@ -1418,7 +1439,7 @@ int runbf_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     a.slice_e = sp->slice_e;
     a.e_q23 = sp->e_q23;
     a.e_g = sp->e_g;
-    a.rbf = sp->d_rbf;
+    a.rbf = planes;
     a.units = sp->d_units;
     a.unit_order = sp->d_unit_order;
     a.band_tl = sp->d_band_tl;
@@ -1430,15 +1451,15 @@ int runbf_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     a.n_cg = (int)((B + C - 1) / C);
     a.n_q = sp->n_q;
     a.L = sp->L;
-    a.off_a = sp->laybf.off_a;
-    a.off_b = sp->laybf.off_b;
-    a.off_f = sp->laybf.off_f;
-    a.off_red = sp->laybf.off_red;
-    a.off_bar = sp->laybf.off_bar;
-    a.off_misc = sp->laybf.off_misc;
+    a.off_a = lay.off_a;
+    a.off_b = lay.off_b;
+    a.off_f = lay.off_f;
+    a.off_red = lay.off_red;
+    a.off_bar = lay.off_bar;
+    a.off_misc = lay.off_misc;
     const long long blocks = (long long)sp->n_rg * a.n_cg;
     if (blocks > 0x7fffffffLL) return fail_split(CF_ESHAPE, "BF16 band kernel: batch too large for one launch");
-    af_bf16_band_kernel<K, C><<<(unsigned)blocks, kThreads, sp->laybf.total, st>>>(a);
+    af_bf16_band_kernel<K, C, T, NAB><<<(unsigned)blocks, kThreads, lay.total, st>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("BF16 band kernel: launch: ") + cudaGetErrorString(e));
     if (launches) ++*launches;
@@ -1453,6 +1474,9 @@ int bf16_band_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t
     if (B <= 0 || sp->n_rg == 0) return CF_OK;
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, sp->device);
+    // K = 12: Phi in FP32 on 8 cells per CTA (M = 128) where its shared memory fits
+    if (sp->k == 12 && sp->laybf8.total > 0 && sp->laybf8.total <= optin)
+        return runbf_impl<12, 8, float, 1>(sp, q_cm, f_cm, B, st, launches);
     if (sp->laybf.total > optin) {
         char msg[160];
         snprintf(msg, sizeof(msg), "BF16 band kernel: %d bytes of shared memory needed, %d available", sp->laybf.total,
@@ -1517,7 +1541,8 @@ int split_build(SplitPlan** out, const DevOp& folded, int64_t n_g, int64_t n_sli
 void split_destroy(SplitPlan* sp) {
     if (!sp) return;
     void* ptrs[] = {sp->d_rplanes, sp->d_e_gs, sp->d_rb_off, sp->d_rb_gs, sp->d_rb_l23, sp->d_units, sp->d_unit_order, sp->d_band_tl,
-                    sp->d_band_rng, sp->d_err, sp->d_rfp64, sp->d_rbf, sp->d_units64, sp->d_unit_order64};
+                    sp->d_band_rng, sp->d_err, sp->d_rfp64, sp->d_rbf, sp->d_units64, sp->d_unit_order64,
+                    sp->d_rbf8};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete sp;
