@@ -164,15 +164,18 @@ class CollisionOperator:
         _lib.check(st)
         return out
 
-    def jv(self, f, v, out=None, exact: bool = False, stream=None, folded: bool = False):
+    def jv(self, f, v, out=None, exact: bool = False, stream=None, folded: bool = False, fp32: bool = False):
         """out += J(f).v = Q(v,f) + Q(f,v) for every cell; returns out.
 
-        exact: the reference-style operation order; folded: the q2 <-> q3 folded operator."""
+        exact: the reference-style operation order; folded: the q2 <-> q3 folded operator; fp32: the
+        contraction in FP32 (added into the FP64 out; with folded, on the folded operator)."""
         import torch
 
         if out is None:
             out = torch.zeros_like(f)
         B = self._check_cells(f, v, out)
-        mode = 2 if folded else int(bool(exact))
+        if fp32 and exact:
+            raise ValueError("the FP32 J.v has no exact-order mode")
+        mode = (4 if folded else 3) if fp32 else (2 if folded else int(bool(exact)))
         _lib.check(_lib.load().cf_jv_device(self._h, _dptr(out), _dptr(f), _dptr(v), B, mode, _stream_handle(stream)))
         return out

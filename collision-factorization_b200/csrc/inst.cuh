@@ -210,7 +210,7 @@ static LaunchResult launch_pair(const LaunchArgs& a) {
         vT = a.vT;
     } else {
         fT = a.fT32;
-        vT = nullptr;
+        vT = a.vT32;
     }
     kern<<<grid, W * 32, smem, a.stream>>>(a.op, sc, fT, vT, a.QT);
     e = cudaGetLastError();
@@ -424,8 +424,16 @@ static LaunchResult launch_for_k(const LaunchArgs& a) {
         // FP32 form: the pair kernel in FP32 (angular first only), R staged in shared memory when the
         // FP32 tile leaves room for it, else read through L1
         if constexpr (K % 2 == 0 && K <= 12) {
-            if (a.what != OP_AF || a.exact) return {8, 0, cudaSuccess, PATH_PAIR};
+            if ((a.what != OP_AF && a.what != OP_JV) || a.exact) return {8, 0, cudaSuccess, PATH_PAIR};
             LaunchResult r{-1, 0, cudaSuccess, PATH_PAIR};
+            if (a.what == OP_JV) {
+                // FP32 J.v: Phi = sum G (f (x) v + v (x) f) in FP32 on the pair kernel
+                if (a.vT32 == nullptr) return {8, 0, cudaSuccess, PATH_PAIR};
+                r = launch_pair<K, 8, false, true, false, float>(a);
+                if (r.status == -1) r = launch_pair<K, 8, false, true, true, float>(a);
+                if (r.status == -1) return {8, 0, cudaSuccess, PATH_PAIR};
+                return r;
+            }
             if constexpr (K <= 8)
                 if (a.path == PATH_PAIR_SPLIT) r = launch_pair<K, 8, false, false, false, float, true>(a);
             if (r.status == -1) r = launch_pair<K, 8, false, false, false, float>(a);

@@ -58,6 +58,8 @@ struct LaunchArgs {
     bool few = false;
     const double* few_host_f = nullptr;
     const double* few_host_q = nullptr;
+    // FP32 J.v: tiled FP32 copy of v
+    const float* vT32 = nullptr;
 };
 
 // Status codes mirror cf_status: 0 ok, 5 CUDA error, 8 unsupported, 2 shape.

@@ -498,7 +498,7 @@ constexpr int kNoFew = -2;
 int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const double* vT, double* QT, int64_t B,
              cudaStream_t st, const float* fT32 = nullptr, bool bf16 = false, const StreamSync* ss = nullptr,
              const double* f_cm = nullptr, double* q_cm = nullptr, bool few = false,
-             const double* few_host_f = nullptr, const double* few_host_q = nullptr) {
+             const double* few_host_f = nullptr, const double* few_host_q = nullptr, const float* vT32 = nullptr) {
     const int64_t nt = n_tiles_for(B);
     // The folded operator has about half the COO entries per slice of the plain one, and its tile
     // routine groups them by q2, so its Phi step is light next to the K^3 step; there the tile kernel
@@ -514,6 +514,7 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
     a.few = few;
     a.few_host_f = few_host_f;
     a.few_host_q = few_host_q;
+    a.vT32 = vT32;
     cf::LaunchResult r{8, 0, cudaSuccess};
     switch (p->k) {
 #define CF_K(KK) \
@@ -640,15 +641,22 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
                             q_dev);
         }
     }
+    float* vT32 = (f32 && what == 2) ? reinterpret_cast<float*>(vT) : nullptr;  // FP32 J.v: v's FP32 tiles
     if (f32)
         CF_TRY(launch_pack32(p, f_dev, fT32, B, st));
     else
         CF_TRY(launch_pack(p, f_dev, fT, B, st));
-    if (what == 2) CF_TRY(launch_pack(p, v_dev, vT, B, st));
+    if (what == 2) {
+        if (vT32)
+            CF_TRY(launch_pack32(p, v_dev, vT32, B, st));
+        else
+            CF_TRY(launch_pack(p, v_dev, vT, B, st));
+    }
     CF_TRY(launch_pack(p, q_dev, QT, B, st));
     cf_plan* target = p;
     if (sym) CF_TRY(get_sym(p, &target));
-    CF_TRY(dispatch(target, what, exact, fT, vT, QT, B, st, fT32, f32 == 2));
+    CF_TRY(dispatch(target, what, exact, fT, vT, QT, B, st, fT32, f32 == 2, nullptr, nullptr, nullptr, false, nullptr,
+                    nullptr, vT32));
     CF_TRY(launch_unpack(p, QT, q_dev, B, st));
     return CF_OK;
 }
@@ -1433,11 +1441,12 @@ int form_what(int form, bool& exact, bool& sym, int& f32) {
     }
 }
 
-// J.v mode argument: 0 fast, 1 exact operation order, 2 folded operator
-bool jv_mode(int mode, bool& exact, bool& sym) {
+// J.v mode argument: 0 fast, 1 exact operation order, 2 folded operator, 3 FP32, 4 FP32 folded
+bool jv_mode(int mode, bool& exact, bool& sym, int& f32) {
     exact = mode == 1;
-    sym = mode == 2;
-    return mode >= 0 && mode <= 2;
+    sym = mode == 2 || mode == 4;
+    f32 = mode >= 3 ? 1 : 0;
+    return mode >= 0 && mode <= 4;
 }
 
 }  // namespace
@@ -1489,8 +1498,10 @@ int cf_jacobian_apply_host(double* out, const double* f, const double* v, int64_
                            int32_t n_q, int32_t k, int32_t exact) {
     g_last_error.clear();
     bool ex = false, sym = false;
-    if (!jv_mode(exact, ex, sym)) return fail(CF_EINVAL, "J.v mode %d is not 0 (fast), 1 (exact) or 2 (folded)", exact);
-    return run_host(2, ex, out, f, v, b, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym);
+    int f32 = 0;
+    if (!jv_mode(exact, ex, sym, f32))
+        return fail(CF_EINVAL, "J.v mode %d is not 0 (fast), 1 (exact), 2 (folded), 3 (FP32) or 4 (FP32 folded)", exact);
+    return run_host(2, ex, out, f, v, b, labels, vals, ic_map, R, n_g, n_l, n_q, k, sym, f32);
 }
 
 int cf_plan_create(cf_plan** plan, const double* labels, const double* vals, const double* ic_map, const double* R,
@@ -1567,11 +1578,14 @@ int cf_jv_device(cf_plan* plan, double* out_dev, const double* f_dev, const doub
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
     bool ex = false, sym = false;
-    if (!jv_mode(exact, ex, sym)) return fail(CF_EINVAL, "J.v mode %d is not 0 (fast), 1 (exact) or 2 (folded)", exact);
+    int f32 = 0;
+    if (!jv_mode(exact, ex, sym, f32))
+        return fail(CF_EINVAL, "J.v mode %d is not 0 (fast), 1 (exact), 2 (folded), 3 (FP32) or 4 (FP32 folded)", exact);
     std::lock_guard<std::mutex> lk(plan->mu);
     DeviceGuard guard(plan->device);
     CF_TRY(ensure_ws(plan, tiled_bytes(plan, b) * 3));
-    return run_device(plan, 2, ex, out_dev, f_dev, v_dev, b, plan->d_ws, plan->ws_bytes, (cudaStream_t)stream, sym);
+    return run_device(plan, 2, ex, out_dev, f_dev, v_dev, b, plan->d_ws, plan->ws_bytes, (cudaStream_t)stream, sym,
+                      f32);
 }
 
 int cf_pack_cells(const cf_plan* plan, double* dst_tiled, const double* src_cells, int64_t b, void* stream) {
@@ -1617,7 +1631,10 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
     if (b == 0 || plan->n_g == 0) return CF_OK;
     if (!out_tiled || !f_tiled || !v_tiled) return fail(CF_EINVAL, "null device buffer");
     bool ex = false, sym = false;
-    if (!jv_mode(exact, ex, sym)) return fail(CF_EINVAL, "J.v mode %d is not 0 (fast), 1 (exact) or 2 (folded)", exact);
+    int f32 = 0;
+    if (!jv_mode(exact, ex, sym, f32))
+        return fail(CF_EINVAL, "J.v mode %d is not 0 (fast), 1 (exact), 2 (folded), 3 (FP32) or 4 (FP32 folded)", exact);
+    if (f32) return fail(CF_EUNSUPPORTED, "the FP32 J.v modes read FP64 cells through cf_jv_device / cf_jacobian_apply_host");
     DeviceGuard guard(plan->device);
     cf_plan* target = plan;
     if (sym) CF_TRY(get_sym(plan, &target));

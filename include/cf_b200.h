@@ -137,7 +137,7 @@ int cf_time_contract_host(int64_t n_calls, double* seconds, double* Q, const dou
 
 /* J(f).v = Q(v,f) + Q(f,v), accumulated into out; no counterpart in the reference (the reference
  * linearises only densely at equilibrium, tutorial_collisions_spectral_properties.m:43).  Host pointers,
- * [N_Q x K x B]. */
+ * [N_Q x K x B].  `exact` is the J.v mode, as for cf_jv_device. */
 int cf_jacobian_apply_host(double* out, const double* f, const double* v, int64_t b,
                            const double* labels, const double* vals, const double* ic_map,
                            const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k,
@@ -170,7 +170,9 @@ int cf_q_device_ws(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b,
                    void* workspace, size_t workspace_bytes, void* stream);
 
 /* out_dev += J(f_dev).v_dev for B cells.  `exact` selects the mode of every J.v call:
- * 0 = fast, 1 = exact operation order, 2 = the q2 <-> q3 folded operator (as CF_FORM_AF_SYM). */
+ * 0 = fast, 1 = exact operation order, 2 = the q2 <-> q3 folded operator (as CF_FORM_AF_SYM),
+ * 3 = FP32 (f, v, R, Phi and the row sums in FP32, added into the FP64 out, as CF_FORM_AF_F32; even
+ * K <= 12), 4 = FP32 on the folded operator.  cf_jv_tiled takes modes 0-2 (its tiles are FP64). */
 int cf_jv_device(cf_plan* plan, double* out_dev, const double* f_dev, const double* v_dev,
                  int64_t b, int32_t exact, void* stream);
 
