@@ -72,6 +72,10 @@ NCU_TRAFFIC = {
     ("hs_l10_k8_b4096", "tile_cell_major", "af_sym"): (64.777728e6 + 2.003456e6,
                                                        "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
                                                        "profiles/af_tile_stream_kernel_folded_hs_l10_k8_b4096.md"),
+    ("hs_l16_k12_b1024", "lblock", "af_sym"): (71.11936e6 + 6.9376e6,
+                                               "ncu dram__bytes_read.sum + dram__bytes_write.sum of the l-block kernel "
+                                               "launch (the pack pass before it not counted), "
+                                               "profiles/af_lblock64_kernel_folded_hs_l16_k12_b1024.md"),
 }
 
 
@@ -102,7 +106,7 @@ def parse_args(argv=None):
                     help="form(s) launched by --profile, comma-separated (af, af_sym, af_exact, rf, af_sym_i8, "
                          "af_f32, af_sym_f32, af_bf16, af_sym_bf16)")
     ap.add_argument("--path", default="auto", choices=["auto", "gather", "tile", "pair", "pair_l1", "pair_split", "tile_mma",
-                                                       "band"],
+                                                       "band", "lblock"],
                     help="kernel family of the angular-first contraction")
     ap.add_argument("--entry", choices=("tiled", "device"), default="tiled",
                     help="--profile: launch the tiled kernel (cf_q_tiled) or the device entry point (cf_q_device)")
@@ -452,7 +456,7 @@ def run_ours(args):
     if sym_single:
         sym_kern_ms = timed(lambda: op.q(f, out=Q, form="af_sym", workspace=ws), max(2, args.steps // 2))
     path_ms, sym_path_ms = {}, {}
-    for path in ("tile_mma", "pair_split", "pair", "pair_l1", "tile", "gather", "band"):
+    for path in ("tile_mma", "pair_split", "pair", "pair_l1", "tile", "gather", "band", "lblock"):
         try:
             op.set_kernel_path(path)
             path_ms[path] = timed(step, max(2, args.steps // 4))
@@ -520,7 +524,9 @@ def run_ours(args):
     step(chosen)
     torch.cuda.synchronize(dev)
     step_path = _lib.PATH_NAMES[op.info()["last_path"]]
-    if (step_path in ("split_i8", "band") and _lib.launch_count() - n0 == 1) or step_path == "rf_dense":
+    step_launches = _lib.launch_count() - n0
+    if ((step_path in ("split_i8", "band") and step_launches == 1) or step_path == "rf_dense"
+            or (step_path == "lblock" and step_launches == 2)):
         kern_list = chosen_ms
         last_path = step_path
     else:
@@ -542,6 +548,9 @@ def run_ours(args):
                              "(tcgen05.mma kind::i8, exact 6x6-byte split); the whole device step)",
                  "band": "af_band64_kernel (l1-band units, 4 cells' f resident, R_t staged per t by cp.async.bulk, "
                          "FP64; the whole device step)",
+                 "lblock": "af_lblock64_kernel (l1-band units, 8 cells per CTA, R_t and the f rows of bands l2 and l3 "
+                           "staged per l-triplet by cp.async.bulk into a ring of stages, FP64; timed with the pack "
+                           "pass before it, the whole device step)",
                  "rf_dense": "rf_dense_kernel (radial step as a dense GEMM over cells per (t, q2), FP64; the device step "
                              "with its f packing and partial-sum reduction)"}.get(last_path, "?")
     kern_s = sum(kern_list) / len(kern_list) / 1e3

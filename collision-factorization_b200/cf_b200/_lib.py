@@ -58,7 +58,8 @@ class PlanInfo(C.Structure):
     ]
 
 PATH_NAMES = {0: "none", 1: "gather", 2: "tile", 3: "pair", 4: "pair_l1", 5: "pair_split", 6: "tile_mma", 7: "bf16_mma", 8: "tile_quarter",
-              9: "few", 10: "split_i8", 11: "band", 12: "band_bf16", 13: "rf_dense"}
+              9: "few", 10: "split_i8", 11: "band", 12: "band_bf16", 13: "rf_dense",
+              14: "lblock"}
 
 _DP = C.POINTER(C.c_double)
 

@@ -18,7 +18,8 @@ enum Path { PATH_AUTO = 0, PATH_GATHER = 1, PATH_TILE = 2, PATH_PAIR = 3, PATH_P
            PATH_SPLIT_I8 = 10 /* reported only: the exact-split form's kernel (split.cu) */,
            PATH_BAND = 11 /* the band kernels on the cell-major arrays (split.cu): the FP64 forms on request */,
            PATH_BAND_BF16 = 12 /* reported only: the BF16-split form on the band kernel (tcgen05, split.cu) */,
-           PATH_RF_DENSE = 13 /* reported only: the radial-first dense form (rfdense.cu) */ };
+           PATH_RF_DENSE = 13 /* reported only: the radial-first dense form (rfdense.cu) */,
+           PATH_LBLOCK = 14 /* the l-block kernel (split.cu): band units, f staged per l-triplet, K = 8 and 12 */ };
 
 struct LaunchArgs {
     DevOp op;

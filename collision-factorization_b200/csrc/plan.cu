@@ -582,6 +582,8 @@ int get_sym(cf_plan* p, cf_plan** out);
 bool streamable(const cf_plan* p, const cf_plan* target, int what, bool exact, int f32);
 int run_split(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
+int run_lblock(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, void* ws, size_t ws_bytes,
+               cudaStream_t st);
 int run_bf16_band(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int run_rfdense(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int check_split(cf_plan* p);
@@ -598,6 +600,9 @@ int run_few(cf_plan* p, int what, bool exact, double* q, const double* f, int64_
     return dispatch(target, what, exact, nullptr, nullptr, nullptr, B, st, nullptr, false, nullptr, f, q, true, host_f,
                     host_q);
 }
+
+// The kernel paths that run on the band units (their bounded waits report through check_split).
+bool band_path(int path) { return path == cf::PATH_BAND || path == cf::PATH_LBLOCK; }
 
 int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_dev, const double* v_dev,
                int64_t B, void* ws, size_t ws_bytes, cudaStream_t st, bool sym = false, int f32 = 0) {
@@ -628,7 +633,9 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
         cf_plan* target = p;
         if (sym) CF_TRY(get_sym(p, &target));
         if (!exact && f32 == 0) {
-            const int r = run_band64(target, q_dev, f_dev, B, st);
+            int r = run_band64(target, q_dev, f_dev, B, st);
+            if (r != kNoFew) return r;
+            r = run_lblock(target, q_dev, f_dev, B, ws, ws_bytes, st);
             if (r != kNoFew) return r;
         }
         if (!exact && f32 == 2) {
@@ -858,6 +865,8 @@ int get_sym(cf_plan* p, cf_plan** out) {
     // for Q at K = 8 with long slices (L = 10: 12.8 entries per slice, 1.654 against 1.699 ms for
     // 4096 cells), not with short ones (L = 8: 9.8 per slice, 0.483 against 0.471 ms) or at K = 4
     // (0.373 against 0.324 ms at L = 8); for J.v from K = 6 on (L = 8, K = 8: 0.619 against 0.655 ms).
+    // (The gather kernel, the automatic family for K > 8, was measured slower grouped: 13.23 against
+    // 12.08 ms at L = 16, K = 12, 1024 cells; its entries' independent gathers hide its L1 latency.)
     const double per_slice = s->n_slices > 0 ? (double)s->n_g / (double)s->n_slices : 0.0;
     s->grouped = ((s->k == 8 && per_slice >= 12.0) ? 1 : 0) | (s->k >= 6 ? 2 : 0);
     s->h_labels.clear();  // the folded plan is never folded again
@@ -921,6 +930,42 @@ int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, c
     if (launches > 0) {
         target->last_path = cf::PATH_BAND;
         if (target->parent) target->parent->last_path = cf::PATH_BAND;
+    }
+    return CF_OK;
+}
+
+// The l-block kernel (af_lblock64_kernel) takes the fast angular-first Q forms at K = 8 and 12 on kernel
+// path PATH_LBLOCK: the band units with R_t and the f rows of bands l2 and l3 staged per l-triplet, from
+// f packed per 8-cell group into the workspace.
+//
+// The automatic order also takes it for the folded fast Q form at K = 12 from L = 8 on, where the
+// gather kernel is the other family (B200, hard-sphere-sized operators, folded, ms per launch, l-block
+// against gather: L = 16, 1024 cells 11.54 / 12.08; L = 12, 1024 cells 3.67 / 4.13; L = 8, 2048
+// cells 1.76 / 1.81; L = 4, 4096 cells 0.52 / 0.42).  The plain operator stays on the gather kernel
+// (L = 16: 27.9 against 23.1 ms): without the fold, its runs of equal q2 are single entries.
+bool lblock_auto(const cf_plan* target) {
+    return target->path == cf::PATH_AUTO && target->parent != nullptr && target->k == 12 && target->n_q >= 81;
+}
+
+int run_lblock(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, void* ws, size_t ws_bytes,
+               cudaStream_t st) {
+    const bool automatic = lblock_auto(target);
+    if (target->path != cf::PATH_LBLOCK && !automatic) return kNoFew;
+    if (target->k != 8 && target->k != 12)
+        return fail(CF_EUNSUPPORTED, "the l-block kernel needs K = 8 or 12 (K = %d)", target->k);
+    cf::SplitPlan* sp = nullptr;
+    const int st_build = get_split(target, &sp);
+    if (st_build != CF_OK || (automatic && !cf::lblock_available(sp))) {
+        if (!automatic) return st_build;
+        g_last_error.clear();  // the automatic order goes on to the gather kernel
+        return kNoFew;
+    }
+    int64_t launches = 0;
+    CF_TRY(cf::lblock64_run(sp, q_dev, f_dev, (double*)ws, ws_bytes, B, st, &launches));
+    g_launches += launches;
+    if (launches > 0) {
+        target->last_path = cf::PATH_LBLOCK;
+        if (target->parent) target->parent->last_path = cf::PATH_LBLOCK;
     }
     return CF_OK;
 }
@@ -1377,7 +1422,7 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
         CF_TRY(run_device(p, what, exact, dQ, df, dv, B, p->d_ws, p->ws_bytes, p->stream, sym, f32));
         CF_CUDA(cudaMemcpyAsync(Q, dQ, cell_bytes, cudaMemcpyDeviceToHost, p->stream));
         CF_CUDA(cudaStreamSynchronize(p->stream));
-        return f32 >= 2 || p->path == cf::PATH_BAND ? check_split(p) : CF_OK;
+        return f32 >= 2 || band_path(p->path) || band_path(p->last_path) ? check_split(p) : CF_OK;
     }
     if (B >= 2 * kHostChunkMin) {
         cf_plan* target = p;
@@ -1418,7 +1463,7 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
         const cudaError_t e = cudaStreamSynchronize(hs);
         if (e != cudaSuccess && st == CF_OK) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
     }
-    if (st == CF_OK && (f32 >= 2 || p->path == cf::PATH_BAND)) st = check_split(p);
+    if (st == CF_OK && (f32 >= 2 || band_path(p->path) || band_path(p->last_path))) st = check_split(p);
     return st;
 }
 
@@ -1682,7 +1727,9 @@ __attribute__((visibility("hidden"))) bool cf_plan_band_pending(cf_plan* plan, i
     int f32 = 0;
     if (form_what(form, exact, sym, f32) != 0 || exact || !cf::split_supported_k(plan->k)) return false;
     const bool band = plan->path == cf::PATH_BAND;
-    if (!((f32 == 2 && (plan->k != 8 || band)) || (f32 == 0 && band))) return false;
+    const bool lblock = (plan->path == cf::PATH_LBLOCK && (plan->k == 8 || plan->k == 12)) ||
+                        (plan->path == cf::PATH_AUTO && sym && plan->k == 12 && plan->n_q >= 81);
+    if (!((f32 == 2 && (plan->k != 8 || band)) || (f32 == 0 && (band || lblock)))) return false;
     cf_plan* target = plan;
     if (sym) {
         std::lock_guard<std::mutex> lk(plan->sym_mu);
@@ -1698,10 +1745,10 @@ extern "C" {
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path) {
     g_last_error.clear();
     if (!plan) return fail(CF_EINVAL, "null plan");
-    if (path < 0 || (path > 6 && path != cf::PATH_BAND))
+    if (path < 0 || (path > 6 && path != cf::PATH_BAND && path != cf::PATH_LBLOCK))
         return fail(CF_EINVAL,
                     "kernel path %d is not 0 (auto), 1 (gather), 2 (tile), 3 (pair), 4 (pair, R via L1), 5 (pair, "
-                    "split rows), 6 (tile, K^3 step on the FP64 MMA) or 11 (band)",
+                    "split rows), 6 (tile, K^3 step on the FP64 MMA), 11 (band) or 14 (l-block)",
                     path);
     std::lock_guard<std::mutex> lk(plan->mu);
     plan->path = path;

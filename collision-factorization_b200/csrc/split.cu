@@ -121,6 +121,10 @@ struct SplitArgs {
     int n_q, L;
     int tseg;                  // t per accumulation segment (int32 bound)
     int n_abuf;                // A buffers of six planes each (2 where shared memory allows, else 1)
+    // the l-block kernel: f packed per cell group as [q][k][cell], one stage per l-triplet
+    const double* pf;          // [n_cg][N_Q][K][C]
+    const int* t_l23;          // per l-triplet: l2 | l3 << 8
+    int n_ring, stage_bytes;   // stages in the ring, bytes per stage (R_t first, then the f rows)
     // shared-memory offsets (bytes)
     int off_a, off_b, off_f, off_mb, off_red, off_scale, off_eexp, off_bar, off_misc;
 };
@@ -173,6 +177,33 @@ Layout band64_layout(int n_q, int warps) {
     l.off_b = take(2 * S::RT_BYTES, 1024);
     l.off_f = take(C * n_q * K * (int)sizeof(double), 16);
     l.off_red = take(warps * C * K * (int)sizeof(double), 16);
+    l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
+    l.off_misc = take(16 * (int)sizeof(int), 16);
+    l.total = o;
+    return l;
+}
+
+// The l-block kernel: 8 cells per CTA (K = 8 and 12), 16 warps, a ring of n_ring stages of
+// stage_bytes each (R_t of Shape<K, 8>, then at most max_rows packed rows of K x 8 doubles).
+// Warps per CTA: 16 at K = 8; 12 at K = 12, whose lanes hold 36 doubles of Phi and 12 of Q (at 16
+// warps, 128 registers, that spilled 288 bytes).
+constexpr int kLbCells = 8;
+constexpr int kLbMaxRing = 8;
+
+__host__ __device__ constexpr bool lblock_supported_k(int k) { return k == 8 || k == 12; }
+__host__ __device__ constexpr int lblock_warps(int k) { return k == 12 ? 12 : 16; }
+
+inline Layout lblock_layout(int n_ring, int stage_bytes, int k) {
+    Layout l{};
+    int o = 0;
+    auto take = [&](int bytes, int align) {
+        o = (o + align - 1) / align * align;
+        const int r = o;
+        o += bytes;
+        return r;
+    };
+    l.off_b = take(n_ring * stage_bytes, 1024);
+    l.off_red = take(lblock_warps(k) * kLbCells * k * (int)sizeof(double), 16);
     l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
     l.off_misc = take(16 * (int)sizeof(int), 16);
     l.total = o;
@@ -741,6 +772,240 @@ __global__ void __launch_bounds__(W * 32, 1) af_band64_kernel(SplitArgs a) {
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// The l-block kernel: the FP64 band kernel's units with f staged per l-triplet instead of whole
+// ------------------------------------------------------------------------------------------
+//
+// A slice of l-triplet t = (l1, l2, l3) reads f only in the rows of band l2 (q2) and band l3 (q3):
+// at most 4L rows of the cell's N_Q = (L+1)^2.  So instead of holding all of f for 4 cells (which is
+// what fits at L = 16, K = 12: 27.7 KB of FP64 f per cell), a CTA holds C = 8 cells and stages, per
+// t of its band's t-list, R_t and those two row blocks into a ring of shared-memory stages: three
+// cp.async.bulk copies per stage on one mbarrier (transaction bytes), from f packed per cell group as
+// [q][k][cell] so that a band's rows are one contiguous run.  Every COO entry's index work and every
+// R_t load then serves 8 cells instead of 4.  The warps walk the t-list as in the band kernel (a slot
+// each); the stage of t is refilled with t + n_ring by the last warp done with it, so warps may drift
+// up to n_ring - 1 l-triplets apart.
+
+// f cell-major [B][K][N_Q] -> packed [cg][q][k][C] (zero past the end of the batch).  One CTA per
+// (cell group, 32 rows q): the 8 cells' K x 32 block is read along q (coalesced) into shared memory
+// and written out as one contiguous run.
+template <int C>
+__global__ void __launch_bounds__(256) pack_cg_kernel(const double* __restrict__ f, double* __restrict__ pf,
+                                                      long long n_cells, int n_q, int K) {
+    extern __shared__ double tile[];  // [32][K][C]
+    const int cg = blockIdx.y, q0 = blockIdx.x * 32;
+    const int nq = min(32, n_q - q0);
+    const long long M = (long long)n_q * K;
+    for (int i = threadIdx.x; i < 32 * K * C; i += blockDim.x) {
+        const int qq = i % 32, k = (i / 32) % K, c = i / (32 * K);
+        const long long cell = (long long)cg * C + c;
+        double v = 0.0;
+        if (qq < nq && cell < n_cells) v = __ldg(f + cell * M + (long long)k * n_q + q0 + qq);
+        tile[(qq * K + k) * C + c] = v;
+    }
+    __syncthreads();
+    double* out = pf + ((long long)cg * n_q + q0) * K * C;
+    for (int i = threadIdx.x; i < nq * K * C; i += blockDim.x) out[i] = tile[i];
+}
+
+// Phi of one slot on a stage: rows of the stage are local (q2 - b2, q3 - b3), f at
+// fsg[(row K + k) C + cell]; grouped by q2 as slot_phi.
+template <int K, int C>
+__device__ __forceinline__ void slot_phi_staged(const double* __restrict__ gv, const uint32_t* __restrict__ eq23,
+                                                const double* __restrict__ fsg, const SlotEntries& se, int lane,
+                                                int c, int k2o, int k3o, int b2, int b3,
+                                                double (&phi)[Shape<K, C>::KH][Shape<K, C>::KQ]) {
+    constexpr int KH = Shape<K, C>::KH, KQ = Shape<K, C>::KQ;
+#pragma unroll
+    for (int x = 0; x < KH; ++x)
+#pragma unroll
+        for (int y = 0; y < KQ; ++y) phi[x][y] = 0.0;
+    const int cb = se.cb, ce = se.ce;
+    if (cb >= ce) return;
+    double h[KQ];
+#pragma unroll
+    for (int y = 0; y < KQ; ++y) h[y] = 0.0;
+    int cur = -1;
+    auto flush = [&]() {
+        const double* __restrict__ f2p = fsg + ((size_t)cur * K + k2o) * C + c;
+#pragma unroll
+        for (int x = 0; x < KH; ++x) {
+            const double f2 = f2p[x * C];
+#pragma unroll
+            for (int y = 0; y < KQ; ++y) phi[x][y] = fma(f2, h[y], phi[x][y]);
+        }
+#pragma unroll
+        for (int y = 0; y < KQ; ++y) h[y] = 0.0;
+    };
+    for (int eb = cb; eb < ce; eb += 32) {
+        const int nb = min(32, ce - eb);
+        uint32_t my_q23 = se.q23;
+        double my_g = se.g;
+        if (eb != cb) {
+            my_q23 = 0;
+            my_g = 0.0;
+            if (lane < nb) {
+                my_q23 = __ldg(eq23 + eb + lane);
+                my_g = __ldg(gv + eb + lane);
+            }
+        }
+        for (int j = 0; j < nb; ++j) {
+            const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, j);
+            const double g = __shfl_sync(0xffffffffu, my_g, j);
+            const int q2 = (int)(q23 & 0xffffu) - b2, q3 = (int)(q23 >> 16) - b3;
+            if (q2 != cur) {
+                if (cur >= 0) flush();
+                cur = q2;
+            }
+            const double* __restrict__ f3p = fsg + ((size_t)q3 * K + k3o) * C + c;
+#pragma unroll
+            for (int y = 0; y < KQ; ++y) h[y] = fma(g, f3p[y * C], h[y]);
+        }
+    }
+    if (cur >= 0) flush();
+}
+
+template <int K, int C, int W>
+__global__ void __launch_bounds__(W * 32, 1) af_lblock64_kernel(SplitArgs a) {
+    using S = Shape<K, C>;
+    constexpr int KH = S::KH, KQ = S::KQ, PS = S::PS, RTB = S::RT_BYTES;
+    constexpr int ROWB = K * C * (int)sizeof(double);  // bytes of one packed row q (K x C doubles)
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* ring = smem + a.off_b;
+    double* red = reinterpret_cast<double*>(smem + a.off_red);
+    uint64_t* bfull = reinterpret_cast<uint64_t*>(smem + a.off_bar);
+    int* misc = reinterpret_cast<int*>(smem + a.off_misc);
+    volatile int* abort_flag = misc + 1;
+    int* rcount = misc + 2;  // [n_ring] warps done with a stage, summed over its uses
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int c = lane % C, part = lane / C, k2o = S::k2_of(part), k3o = S::k3_of(part);
+    const int NQ = a.n_q, M = NQ * K, D = a.n_ring;
+    const int rg = a.unit_order[blockIdx.x / a.n_cg];
+    const int cg = blockIdx.x % a.n_cg;
+    const int* u = a.units + (size_t)rg * U_INTS;
+    const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], cq = u[U_S], crem = u[U_REM], tl_off = u[U_TLOFF],
+              n_t = u[U_NT], tab_off = u[U_TABOFF], brows = u[U_BROWS];
+    const int n_slots = nr * cq + crem;
+    const long long cell0 = (long long)cg * C;
+    const double* __restrict__ pcg = a.pf + (size_t)cg * M * C;
+
+    // stage sb <- R_t and the row blocks of bands l2 and l3 of t-list position ti (thread 0)
+    auto issue = [&](int ti, int sb) {
+        const int t = a.band_tl[tl_off + ti];
+        const int l23 = a.t_l23[t], l2 = l23 & 0xff, l3 = l23 >> 8;
+        const uint32_t fb2 = (uint32_t)((2 * l2 + 1) * ROWB), fb3 = l3 != l2 ? (uint32_t)((2 * l3 + 1) * ROWB) : 0u;
+        unsigned char* st = ring + (size_t)sb * a.stage_bytes;
+        tc05::mbar_arrive_expect_tx(&bfull[sb], (uint32_t)RTB + fb2 + fb3);
+        tc05::bulk_g2s(st, a.rfp64 + (size_t)t * (RTB / 8), (uint32_t)RTB, &bfull[sb]);
+        tc05::bulk_g2s(st + RTB, pcg + (size_t)l2 * l2 * K * C, fb2, &bfull[sb]);
+        if (fb3) tc05::bulk_g2s(st + RTB + fb2, pcg + (size_t)l3 * l3 * K * C, fb3, &bfull[sb]);
+    };
+
+    if (tid == 0) {
+        for (int i = 0; i < D; ++i) {
+            tc05::mbar_init(&bfull[i], 1);
+            rcount[i] = 0;
+        }
+        tc05::fence_mbar_init();
+        *abort_flag = 0;
+    }
+    __syncthreads();
+    if (tid == 0)
+        for (int ti = 0; ti < min(n_t, D); ++ti) issue(ti, ti);
+
+    const bool active = warp < n_slots;
+    int srow = 0, ch = 0, nS = 1;
+    if (active) slot_of(warp, cq, crem, srow, ch, nS);
+    const int row = r0 + srow;
+    double acc[K];
+#pragma unroll
+    for (int k1 = 0; k1 < K; ++k1) acc[k1] = 0.0;
+    // the slot's entries (and l-triplet) of t-list position ti in cur, of ti + 1 fetched during ti
+    SlotEntries cur{0, 0, 0u, 0.0}, nxt{0, 0, 0u, 0.0};
+    int ncb = 0, nce = 0, cur_l23 = 0, nxt_l23 = 0;
+    if (active) {
+        int cb, ce;
+        slot_range(a, tab_off, brows, 0, row, ch, nS, cb, ce);
+        cur = slot_fetch(a, a.e_g, cb, ce, lane);
+        cur_l23 = __ldg(a.t_l23 + __ldg(a.band_tl + tl_off));
+        if (n_t > 1) slot_range(a, tab_off, brows, 1, row, ch, nS, ncb, nce);
+    }
+    for (int ti = 0; ti < n_t; ++ti) {
+        const int sb = ti % D;
+        const SlotEntries se = cur;
+        const int l23 = cur_l23;
+        if (active) {
+            if (ti + 1 < n_t) {
+                nxt = slot_fetch(a, a.e_g, ncb, nce, lane);
+                nxt_l23 = __ldg(a.t_l23 + __ldg(a.band_tl + tl_off + ti + 1));
+            }
+            if (ti + 2 < n_t) slot_range(a, tab_off, brows, ti + 2, row, ch, nS, ncb, nce);
+        }
+        // every warp sees stage sb land before it counts itself done with it (the refill is armed
+        // only after that), also where it reads nothing from it
+        const bool ok = wait_bar(&bfull[sb], (uint32_t)((ti / D) & 1), abort_flag, a.err);
+        if (active && ok && se.cb < se.ce) {
+            const unsigned char* st = ring + (size_t)sb * a.stage_bytes;
+            const int l2 = l23 & 0xff, l3 = l23 >> 8;
+            const int b2 = l2 * l2, b3 = l3 * l3 - (l3 != l2 ? 2 * l2 + 1 : 0);
+            double phi[KH][KQ];
+            slot_phi_staged<K, C>(a.e_g, a.e_q23, reinterpret_cast<const double*>(st + RTB), se, lane, c, k2o, k3o,
+                                  b2, b3, phi);
+            const double* rp = reinterpret_cast<const double*>(st) + part * PS;
+#pragma unroll
+            for (int x = 0; x < KH; ++x)
+#pragma unroll
+                for (int y = 0; y < KQ; ++y) {
+                    const double2* r2 = reinterpret_cast<const double2*>(rp + (x * KQ + y) * K);
+#pragma unroll
+                    for (int j = 0; j < K / 2; ++j) {
+                        const double2 r = r2[j];
+                        acc[2 * j] = fma(r.x, phi[x][y], acc[2 * j]);
+                        acc[2 * j + 1] = fma(r.y, phi[x][y], acc[2 * j + 1]);
+                    }
+                }
+        }
+        if (active) {
+            cur = nxt;
+            cur_l23 = nxt_l23;
+        }
+        // the last warp done with stage sb refills it with t-list position ti + D (no CTA-wide barrier)
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            if (atomicAdd(&rcount[sb], 1) == W * ((ti / D) + 1) - 1 && ti + D < n_t && !*abort_flag) {
+                __threadfence_block();
+                asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                issue(ti + D, sb);
+            }
+        }
+        __syncwarp();
+    }
+    // the parts of a cell sit in lanes c, c + C, c + 2C, ...
+#pragma unroll
+    for (int k1 = 0; k1 < K; ++k1)
+#pragma unroll
+        for (int o = C; o < 32; o <<= 1) acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], o);
+    if (active && lane < C)
+#pragma unroll
+        for (int k1 = 0; k1 < K; ++k1) red[(warp * C + lane) * K + k1] = acc[k1];
+    __syncthreads();
+    if (tid < nr * C) {
+        const int rl = tid / C, cc = tid % C;
+        const long long cell = cell0 + cc;
+        if (cell < a.n_cells) {
+            double* qc = a.q + cell * M + (l1 * l1 + r0 + rl);
+            for (int k1 = 0; k1 < K; ++k1) {
+                double sum = 0.0;
+                const int s0 = row_first_slot(rl, cq, crem), nc = row_chunks(rl, cq, crem);
+                for (int chk = 0; chk < nc; ++chk) sum += red[((s0 + chk) * C + cc) * K + k1];
+                qc[(size_t)k1 * NQ] += sum;
+            }
+        }
+    }
+}
+
 // The BF16-split band kernel (CF_FORM_AF_SYM_BF16 / CF_FORM_AF_BF16 where the warp-level BF16 kernel
 // does not exist, K = 12): the same units and FP64 Phi step; Phi = hi + lo and R_t = hi + lo in BF16
 // (round to nearest even), and per 16-element K step the four cross products hi*hi, hi*lo, lo*hi,
@@ -1032,10 +1297,17 @@ struct SplitPlan {
     double* d_rfp64 = nullptr;        // FP64 R_t per t as [part][e][k1] (FP64 band kernel)
     uint8_t* d_rbf = nullptr;         // BF16 hi and lo planes of R_t (BF16-split band kernel)
     uint8_t* d_rbf8 = nullptr;        // K = 12: the same for 8 cells per CTA (Phi in FP32)
+    double* d_rfl = nullptr;          // the l-block kernel (8 cells per CTA): FP64 R_t as [part][e][k1]
+    int* d_t_l23 = nullptr;           // per l-triplet: l2 | l3 << 8
+    int lb_ring = 0, lb_stage = 0;    // the l-block kernel's stages and bytes per stage (0: unsupported)
+    int n_rg_lb = 0;                  // the l-block kernel's row groups (lblock_warps(K) slots each)
+    int* d_units_lb = nullptr;
+    int* d_unit_order_lb = nullptr;
     Layout lay{};
     Layout lay64{};
     Layout laybf{};
     Layout laybf8{};                  // K = 12: 8 cells per CTA, f and Phi in FP32, one A buffer
+    Layout laylb{};                   // the l-block kernel
 };
 
 namespace {
@@ -1184,6 +1456,20 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
                     rfp64[((size_t)t * S::P + pp) * S::PS + (size_t)e * K + k1] =
                         R[(size_t)t * K * K * K + k1 + (size_t)K * k2 + (size_t)K * K * k3];
             }
+    // the l-block kernel's FP64 R_t (the layout of Shape<K, 8>)
+    std::vector<double> rfl;
+    if constexpr (lblock_supported_k(K)) {
+        using S8 = Shape<K, kLbCells>;
+        rfl.assign((size_t)NL * S8::P * S8::PS, 0.0);
+        for (int t = 0; t < NL; ++t)
+            for (int pp = 0; pp < S8::P; ++pp)
+                for (int e = 0; e < S8::E; ++e) {
+                    const int k2 = S8::k2_of(pp) + e / S8::KQ, k3 = S8::k3_of(pp) + e % S8::KQ;
+                    for (int k1 = 0; k1 < K; ++k1)
+                        rfl[((size_t)t * S8::P + pp) * S8::PS + (size_t)e * K + k1] =
+                            R[(size_t)t * K * K * K + k1 + (size_t)K * k2 + (size_t)K * K * k3];
+                }
+    }
     // G / s_t per entry, |G / s_t| summed per slice, (l2, l3) per t
     std::vector<double> e_gs(n_g), gs(n_slices, 0.0);
     std::vector<int> t_l23(NL, -1);
@@ -1272,6 +1558,8 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     const int n_rg = make_units(kSlots, units, order);
     const int w64 = band64_warps(K);
     const int n_rg64 = make_units(w64, units64, order64);
+    std::vector<int> units_lb, order_lb;
+    const int n_rg_lb = lblock_supported_k(K) ? make_units(lblock_warps(K), units_lb, order_lb) : 0;
     // the (t, row) tables as entry ranges (begin, end), empty where the row has no slice of t
     std::vector<int> band_rng(2 * band_slice.size(), 0);
     for (size_t i = 0; i < band_slice.size(); ++i)
@@ -1285,6 +1573,7 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     sp->L = L;
     sp->n_rg = n_rg;
     sp->n_rg64 = n_rg64;
+    sp->n_rg_lb = n_rg_lb;
     sp->w64 = w64;
     // int32 accumulators: at most 6 byte products of |255 * 128| per K element and weight
     sp->tseg = std::max(1, (int)(2147483647LL / (6LL * 255 * 128 * S::KK)));
@@ -1302,6 +1591,22 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
         sp->lay = smem_layout<K, C>(NQ, L, 1);
     }
     sp->lay64 = band64_layout<K, C>(NQ, w64);
+    // the l-block kernel: a stage holds R_t and the row blocks of bands l2 and l3 of one t
+    if constexpr (lblock_supported_k(K)) {
+        int max_rows = 0;
+        for (int t : band_tl) {
+            const int l2 = t_l23[t] & 0xff, l3 = t_l23[t] >> 8;
+            max_rows = std::max(max_rows, 2 * l2 + 1 + (l3 != l2 ? 2 * l3 + 1 : 0));
+        }
+        const int stage = (Shape<K, kLbCells>::RT_BYTES + max_rows * K * kLbCells * (int)sizeof(double) + 127) / 128 * 128;
+        int ring = kLbMaxRing;
+        while (ring >= 2 && lblock_layout(ring, stage, K).total > optin) --ring;
+        if (ring >= 2) {
+            sp->lb_ring = ring;
+            sp->lb_stage = stage;
+            sp->laylb = lblock_layout(ring, stage, K);
+        }
+    }
     sp->laybf = bf16_layout<K, C>(NQ);
     if constexpr (K == 12) sp->laybf8 = bf16_layout<12, 8, float>(NQ, 1);
     sp->smem = sp->lay.total;
@@ -1320,7 +1625,11 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
         (ce = upload_vec(&sp->d_err, std::vector<int>(1, 0), bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_rfp64, rfp64, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_rbf, rbf, bytes)) != cudaSuccess ||
-        (ce = upload_vec(&sp->d_rbf8, rbf8, bytes)) != cudaSuccess)
+        (ce = upload_vec(&sp->d_rbf8, rbf8, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_rfl, rfl, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_units_lb, units_lb, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_unit_order_lb, order_lb, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_t_l23, t_l23, bytes)) != cudaSuccess)
         return fail_split(ce == cudaErrorMemoryAllocation ? CF_ENOMEM : CF_ECUDA,
                           std::string("split form: upload: ") + cudaGetErrorString(ce));
     sp->bytes = bytes;
@@ -1421,6 +1730,66 @@ int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     return CF_OK;
 }
 
+// Bytes of the packed f that the l-block kernel reads: [ceil(B / 8)][N_Q][K][8] doubles.
+size_t lblock_pack_bytes_of(int n_q, int k, int64_t B) {
+    return (size_t)((B + kLbCells - 1) / kLbCells) * (size_t)n_q * k * kLbCells * sizeof(double);
+}
+
+template <int K>
+int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf, int64_t B, cudaStream_t st,
+               int64_t* launches) {
+    constexpr int C = kLbCells, W = lblock_warps(K);
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+        // (the pack kernel's 32 K C doubles, at most 24 KB, need no attribute)
+        const cudaError_t e = cudaFuncSetAttribute(af_lblock64_kernel<K, C, W>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        if (e != cudaSuccess)
+            return fail_split(CF_ECUDA, std::string("l-block kernel: smem attribute: ") + cudaGetErrorString(e));
+        attr_set[dev] = true;
+    }
+    const long long n_cg = (B + C - 1) / C;
+    if (n_cg > 65535LL || (long long)sp->n_rg_lb * n_cg > 0x7fffffffLL)
+        return fail_split(CF_ESHAPE, "l-block kernel: batch too large for one launch");
+    dim3 pgrid((unsigned)((sp->n_q + 31) / 32), (unsigned)n_cg);
+    static_assert(32 * K * C * 8 <= 48 * 1024, "the pack kernel's tile fits the default shared memory");
+    pack_cg_kernel<C><<<pgrid, 256, 32 * K * C * 8, st>>>(f_cm, pf, B, sp->n_q, K);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("l-block pack: launch: ") + cudaGetErrorString(e));
+    if (launches) ++*launches;
+    SplitArgs a{};
+    a.slice_e = sp->slice_e;
+    a.e_q23 = sp->e_q23;
+    a.e_g = sp->e_g;
+    a.rfp64 = sp->d_rfl;
+    a.units = sp->d_units_lb;
+    a.unit_order = sp->d_unit_order_lb;
+    a.band_tl = sp->d_band_tl;
+    a.band_rng = sp->d_band_rng;
+    a.pf = pf;
+    a.t_l23 = sp->d_t_l23;
+    a.q = q_cm;
+    a.err = sp->d_err;
+    a.n_cells = B;
+    a.n_cg = (int)n_cg;
+    a.n_q = sp->n_q;
+    a.L = sp->L;
+    a.n_ring = sp->lb_ring;
+    a.stage_bytes = sp->lb_stage;
+    a.off_b = sp->laylb.off_b;
+    a.off_red = sp->laylb.off_red;
+    a.off_bar = sp->laylb.off_bar;
+    a.off_misc = sp->laylb.off_misc;
+    const long long blocks = (long long)sp->n_rg_lb * n_cg;
+    af_lblock64_kernel<K, C, W><<<(unsigned)blocks, W * 32, sp->laylb.total, st>>>(a);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("l-block kernel: launch: ") + cudaGetErrorString(e));
+    if (launches) ++*launches;
+    return CF_OK;
+}
+
 template <int K, int C, typename T = double, int NAB = 2>
 int runbf_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st, int64_t* launches) {
     const Layout& lay = (std::is_same<T, float>::value && K == 12) ? sp->laybf8 : sp->laybf;
@@ -1501,6 +1870,20 @@ int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     }
 }
 
+size_t lblock_pack_bytes(const SplitPlan* sp, int64_t B) { return lblock_pack_bytes_of(sp->n_q, sp->k, B); }
+
+bool lblock_available(const SplitPlan* sp) { return sp && lblock_supported_k(sp->k) && sp->lb_ring >= 2; }
+
+int lblock64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf, size_t pf_bytes, int64_t B,
+                 cudaStream_t st, int64_t* launches) {
+    if (B <= 0 || sp->n_rg_lb == 0) return CF_OK;
+    if (!lblock_available(sp))
+        return fail_split(CF_EUNSUPPORTED, "l-block kernel: needs K = 8 or 12 and two stages of shared memory");
+    if (pf_bytes < lblock_pack_bytes(sp, B)) return fail_split(CF_EINVAL, "l-block kernel: packed-f workspace too small");
+    return sp->k == 8 ? runlb_impl<8>(sp, q_cm, f_cm, pf, B, st, launches)
+                      : runlb_impl<12>(sp, q_cm, f_cm, pf, B, st, launches);
+}
+
 int split_build(SplitPlan** out, const DevOp& folded, int64_t n_g, int64_t n_slices, int device) {
     *out = nullptr;
     if (!split_supported_k(folded.k))
@@ -1542,7 +1925,7 @@ void split_destroy(SplitPlan* sp) {
     if (!sp) return;
     void* ptrs[] = {sp->d_rplanes, sp->d_e_gs, sp->d_rb_off, sp->d_rb_gs, sp->d_rb_l23, sp->d_units, sp->d_unit_order, sp->d_band_tl,
                     sp->d_band_rng, sp->d_err, sp->d_rfp64, sp->d_rbf, sp->d_units64, sp->d_unit_order64,
-                    sp->d_rbf8};
+                    sp->d_rbf8, sp->d_rfl, sp->d_t_l23, sp->d_units_lb, sp->d_unit_order_lb};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete sp;

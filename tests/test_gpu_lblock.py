@@ -1,0 +1,146 @@
+"""The l-block kernel (af_lblock64_kernel): the fast angular-first Q forms on the band kernel's l1-band
+work units, 8 cells per CTA, with R_t and the f rows of bands l2 and l3 staged per l-triplet by bulk
+copies from f packed per 8-cell group, on kernel path 'lblock' (K = 8 and 12).
+
+Tolerance: 1e-12 normwise per cell against the oracle's restatement of the reference's angular-first
+kernel (src/mex/angular_first_collision_kernel_mex.cpp:45-69), the FP64 bar of the parity suite.
+"""
+from __future__ import annotations
+
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import per_cell_err
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+TOL_FP64 = 1e-12
+PATH_LBLOCK = 14
+
+
+def _setup(L, K, R=None, seed=3):
+    from cf_b200 import geometry, workloads
+    from oracle import rtensor
+
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    if R is None:
+        R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=seed)
+    return geo, np.asfortranarray(R)
+
+
+def _device_q(op, cells, form, q0=None):
+    import torch
+
+    f = torch.from_numpy(cells).cuda()
+    Q = torch.zeros_like(f) if q0 is None else torch.from_numpy(q0.copy()).cuda()
+    op.q(f, out=Q, form=form)
+    torch.cuda.synchronize()
+    return Q.cpu().numpy()
+
+
+def _oracle(geo, R, K, cells, oracle_lib):
+    f = np.asfortranarray(cells.transpose(2, 1, 0))
+    Qo = np.zeros_like(f, order="F")
+    oracle_lib.af_batch(Qo, f, geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+    return np.ascontiguousarray(Qo.transpose(2, 1, 0))
+
+
+@pytest.mark.parametrize("L,K,B", [(6, 12, 37), (3, 12, 16), (1, 12, 13), (8, 8, 37), (10, 8, 21), (0, 8, 11)])
+def test_lblock_kernel_vs_oracle(L, K, B, cuda_available, oracle_lib):
+    """Plain and folded fast forms on the l-block kernel; batches with a ragged last 8-cell group or
+    whole groups only, and bands whose l-triplets have l2 = l3 (one staged row block) or not."""
+    import cf_b200
+    from cf_b200 import workloads
+
+    R = np.load(GOLDEN / "R_hs_k7_l8_pad20.npy") if (L, K) == (8, 8) else None
+    if (L, K) == (10, 8):
+        R = np.load(GOLDEN / "R_hs_k7_l10_pad20.npy")
+    geo, R = _setup(L, K, R, seed=L + K)
+    cells = workloads.maxwellian_cells(K, L, B, seed=K + B)
+    ref = _oracle(geo, R, K, cells, oracle_lib)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+    op.set_kernel_path("lblock")
+    for form in ("af", "af_sym"):
+        Q = _device_q(op, cells, form)
+        assert op.info()["last_path"] == PATH_LBLOCK, form
+        assert per_cell_err(Q, ref) <= TOL_FP64, (form, per_cell_err(Q, ref))
+    op.close()
+
+
+@pytest.mark.skipif(not (GOLDEN / "R_hs_k11_l16_pad20.npy").exists(), reason="L = 16, K = 12 R fixture absent")
+def test_lblock_kernel_precision_configuration_vs_oracle(cuda_available, oracle_lib):
+    """Hard spheres, L = 16, K = 12 (R from the GPU quadrature), bi-Maxwellian cells: the FP64 forms of
+    the precision configuration on 11 cells (a whole and a ragged 8-cell group) against the oracle;
+    the five invariant entries exactly zero."""
+    import cf_b200
+    from cf_b200 import workloads
+
+    geo, R = _setup(16, 12, np.load(GOLDEN / "R_hs_k11_l16_pad20.npy"))
+    cells = workloads.bimaxwellian_cells(12, 16, 11, seed=20261)
+    ref = _oracle(geo, R, 12, cells, oracle_lib)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, 12)
+    op.set_kernel_path("lblock")
+    for form in ("af", "af_sym"):
+        Q = _device_q(op, cells, form)
+        assert op.info()["last_path"] == PATH_LBLOCK, form
+        assert per_cell_err(Q, ref) <= TOL_FP64, (form, per_cell_err(Q, ref))
+        assert np.abs(Q[:, 0, 0]).max() == 0.0 and np.abs(Q[:, 1, 0]).max() == 0.0
+        assert np.abs(Q[:, 0, 1:4]).max() == 0.0
+    op.close()
+
+
+@pytest.mark.skipif(not (GOLDEN / "R_hs_k11_l16_pad20.npy").exists(), reason="L = 16, K = 12 R fixture absent")
+def test_precision_configuration_automatic_order_vs_oracle(cuda_available, oracle_lib):
+    """The automatic kernel order at L = 16, K = 12 (hard spheres, R from the GPU quadrature): the plain
+    FP64 form on the gather kernel and the folded one on the l-block kernel, both within 1e-12 of the
+    oracle on 13 bi-Maxwellian cells."""
+    import cf_b200
+    from cf_b200 import workloads
+
+    geo, R = _setup(16, 12, np.load(GOLDEN / "R_hs_k11_l16_pad20.npy"))
+    cells = workloads.bimaxwellian_cells(12, 16, 13, seed=20262)
+    ref = _oracle(geo, R, 12, cells, oracle_lib)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, 12)
+    for form, path in (("af", "gather"), ("af_sym", "lblock")):
+        Q = _device_q(op, cells, form)
+        assert cf_b200._lib.PATH_NAMES[op.info()["last_path"]] == path, form
+        assert per_cell_err(Q, ref) <= TOL_FP64, (form, per_cell_err(Q, ref))
+    op.close()
+
+
+def test_lblock_kernel_accumulates_and_is_deterministic(cuda_available, oracle_lib):
+    """out += Q(f) from a nonzero Q, two runs give the same bits, and Q(2f) = 4 Q(f) bit for bit."""
+    import cf_b200
+    from cf_b200 import workloads
+
+    geo, R = _setup(6, 12, seed=5)
+    cells = workloads.maxwellian_cells(12, 6, 19, seed=2)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, 12)
+    op.set_kernel_path("lblock")
+    q0 = np.random.default_rng(1).standard_normal(cells.shape)
+    outs = [_device_q(op, cells, "af_sym", q0) for _ in range(2)]
+    assert np.array_equal(outs[0], outs[1])
+    ref = _oracle(geo, R, 12, cells, oracle_lib)
+    assert per_cell_err(outs[0] - q0, ref) <= 1e-11
+    q1 = _device_q(op, cells, "af_sym")
+    q2 = _device_q(op, 2.0 * cells, "af_sym")
+    assert np.array_equal(q2, 4.0 * q1)
+    op.close()
+
+
+def test_lblock_kernel_refuses_other_k(cuda_available):
+    """K outside {8, 12} on path 'lblock' is refused with CF_EUNSUPPORTED, not run on another kernel."""
+    import cf_b200
+    from cf_b200 import workloads
+
+    geo, R = _setup(4, 4, seed=1)
+    cells = workloads.maxwellian_cells(4, 4, 9, seed=1)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, 4)
+    op.set_kernel_path("lblock")
+    with pytest.raises(cf_b200.CFError) as e:
+        _device_q(op, cells, "af_sym")
+    assert e.value.status == cf_b200._lib.CF_EUNSUPPORTED
+    op.close()
