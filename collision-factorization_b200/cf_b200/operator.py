@@ -119,7 +119,8 @@ class CollisionOperator:
     def set_kernel_path(self, path: str) -> None:
         """'auto' (default), 'gather', 'tile', 'pair', 'pair_l1', 'pair_split', 'tile_mma', 'band' or 'lblock':
         the kernel family of the AF and J.v forms ('band': the FP64 band kernel of the fast Q forms, K = 4, 8,
-        12; 'lblock': the same units with f staged per l-triplet, 8 cells per CTA, K = 8 and 12)."""
+        12; 'lblock': one CTA per band and 8 cells, f staged per l-triplet, the band's slices shared out
+        one at a time, K = 8 and 12)."""
         code = {"auto": 0, "gather": 1, "tile": 2, "pair": 3, "pair_l1": 4, "pair_split": 5, "tile_mma": 6,
                 "band": 11, "lblock": 14}[path]
         _lib.check(_lib.load().cf_plan_set_kernel_path(self._h, code))

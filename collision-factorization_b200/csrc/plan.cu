@@ -935,16 +935,17 @@ int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, c
 }
 
 // The l-block kernel (af_lblock64_kernel) takes the fast angular-first Q forms at K = 8 and 12 on kernel
-// path PATH_LBLOCK: the band units with R_t and the f rows of bands l2 and l3 staged per l-triplet, from
-// f packed per 8-cell group into the workspace.
+// path PATH_LBLOCK: one CTA per (l1 band, 8-cell group) with R_t and the f rows of bands l2 and l3
+// staged per l-triplet, from f packed per 8-cell group into the workspace, and the band's slices
+// handed to the warps one at a time.
 //
-// The automatic order also takes it for the folded fast Q form at K = 12 from L = 8 on, where the
-// gather kernel is the other family (B200, hard-sphere-sized operators, folded, ms per launch, l-block
-// against gather: L = 16, 1024 cells 11.54 / 12.08; L = 12, 1024 cells 3.67 / 4.13; L = 8, 2048
-// cells 1.76 / 1.81; L = 4, 4096 cells 0.52 / 0.42).  The plain operator stays on the gather kernel
-// (L = 16: 27.9 against 23.1 ms): without the fold, its runs of equal q2 are single entries.
+// The automatic order also takes it for the fast Q forms (plain and folded) at K = 12 from L = 8 on,
+// where the gather kernel is the other family (B200, ms per launch, l-block against gather, folded /
+// plain: L = 16, 1024 cells 8.54 / 19.21 against 12.10 / 23.11; L = 12, 1024 cells 2.67 / 5.55 against
+// 3.86 / 7.37; L = 8, 2048 cells 1.25 / 2.30 against 1.69 / 3.07).  Operators whose (t, q1) pairs come
+// in several runs (an unsorted COO list) have no band tables and stay on the gather kernel.
 bool lblock_auto(const cf_plan* target) {
-    return target->path == cf::PATH_AUTO && target->parent != nullptr && target->k == 12 && target->n_q >= 81;
+    return target->path == cf::PATH_AUTO && target->k == 12 && target->n_q >= 81;
 }
 
 int run_lblock(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, void* ws, size_t ws_bytes,
@@ -1728,7 +1729,7 @@ __attribute__((visibility("hidden"))) bool cf_plan_band_pending(cf_plan* plan, i
     if (form_what(form, exact, sym, f32) != 0 || exact || !cf::split_supported_k(plan->k)) return false;
     const bool band = plan->path == cf::PATH_BAND;
     const bool lblock = (plan->path == cf::PATH_LBLOCK && (plan->k == 8 || plan->k == 12)) ||
-                        (plan->path == cf::PATH_AUTO && sym && plan->k == 12 && plan->n_q >= 81);
+                        (plan->path == cf::PATH_AUTO && plan->k == 12 && plan->n_q >= 81);
     if (!((f32 == 2 && (plan->k != 8 || band)) || (f32 == 0 && (band || lblock)))) return false;
     cf_plan* target = plan;
     if (sym) {

@@ -125,6 +125,9 @@ struct SplitArgs {
     const double* pf;          // [n_cg][N_Q][K][C]
     const int* t_l23;          // per l-triplet: l2 | l3 << 8
     int n_ring, stage_bytes;   // stages in the ring, bytes per stage (R_t first, then the f rows)
+    const int4* items;         // per band, its (t, row) slices in t-major order (lbi_*)
+    const int* t_items;        // per t-list position of a band: its number of items
+    int max_rows, max_t;       // sizes of the per-CTA row and t tables
     // shared-memory offsets (bytes)
     int off_a, off_b, off_f, off_mb, off_red, off_scale, off_eexp, off_bar, off_misc;
 };
@@ -185,15 +188,17 @@ Layout band64_layout(int n_q, int warps) {
 
 // The l-block kernel: 8 cells per CTA (K = 8 and 12), 16 warps, a ring of n_ring stages of
 // stage_bytes each (R_t of Shape<K, 8>, then at most max_rows packed rows of K x 8 doubles).
-// Warps per CTA: 16 at K = 8; 12 at K = 12, whose lanes hold 36 doubles of Phi and 12 of Q (at 16
-// warps, 128 registers, that spilled 288 bytes).
+// The l-block kernel: 8 cells per CTA (K = 8 and 12), 16 warps, a ring of up to 8 stages.
 constexpr int kLbCells = 8;
+constexpr int kLbWarps = 16;
 constexpr int kLbMaxRing = 8;
 
 __host__ __device__ constexpr bool lblock_supported_k(int k) { return k == 8 || k == 12; }
-__host__ __device__ constexpr int lblock_warps(int k) { return k == 12 ? 12 : 16; }
 
-inline Layout lblock_layout(int n_ring, int stage_bytes, int k) {
+// The l-block kernel's shared memory: the ring of stages (R_t of Shape<K, 8>, then at most max_rows
+// packed f rows of K x 8 doubles each), the band's Q rows of 8 cells, and the counter, done words, row
+// tickets, per-t item totals and stage assignments.
+inline Layout lblock_layout(int n_ring, int stage_bytes, int k, int max_rows, int max_t) {
     Layout l{};
     int o = 0;
     auto take = [&](int bytes, int align) {
@@ -203,9 +208,9 @@ inline Layout lblock_layout(int n_ring, int stage_bytes, int k) {
         return r;
     };
     l.off_b = take(n_ring * stage_bytes, 1024);
-    l.off_red = take(lblock_warps(k) * kLbCells * k * (int)sizeof(double), 16);
+    l.off_red = take(max_rows * k * kLbCells * (int)sizeof(double), 16);
     l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
-    l.off_misc = take(16 * (int)sizeof(int), 16);
+    l.off_misc = take((2 + 2 * kLbMaxRing + max_rows + max_t) * (int)sizeof(int), 16);
     l.total = o;
     return l;
 }
@@ -773,7 +778,7 @@ __global__ void __launch_bounds__(W * 32, 1) af_band64_kernel(SplitArgs a) {
 }
 
 // ------------------------------------------------------------------------------------------
-// The l-block kernel: the FP64 band kernel's units with f staged per l-triplet instead of whole
+// The l-block kernel: l1-band units with f staged per l-triplet, and a band's slices as work items
 // ------------------------------------------------------------------------------------------
 //
 // A slice of l-triplet t = (l1, l2, l3) reads f only in the rows of band l2 (q2) and band l3 (q3):
@@ -782,9 +787,16 @@ __global__ void __launch_bounds__(W * 32, 1) af_band64_kernel(SplitArgs a) {
 // t of its band's t-list, R_t and those two row blocks into a ring of shared-memory stages: three
 // cp.async.bulk copies per stage on one mbarrier (transaction bytes), from f packed per cell group as
 // [q][k][cell] so that a band's rows are one contiguous run.  Every COO entry's index work and every
-// R_t load then serves 8 cells instead of 4.  The warps walk the t-list as in the band kernel (a slot
-// each); the stage of t is refilled with t + n_ring by the last warp done with it, so warps may drift
-// up to n_ring - 1 l-triplets apart.
+// R_t load then serves 8 cells instead of 4.
+//
+// One CTA takes one (l1 band, 8-cell group).  A band's rows do not divide evenly over the warps of a
+// CTA (33 rows at l1 = 16), and the entries of a (t, row) slice vary widely between rows, so its
+// warps take the band's (t, row) slices one at a time from a shared counter, in t-major order.  A
+// warp computes the slice's Phi and K^3 step, sums the parts of each cell, and adds the result into
+// the band's Q rows, kept in shared memory for the CTA's 8 cells.  Each row takes its slices' results
+// in t order (a ticket per row: the warp holding the row's slice number ord waits until ord - 1 has
+// been added), so the sums, and the bits of Q, do not depend on which warp ran which item.  The stage
+// of t-list position ti is refilled with ti + n_ring by the warp that finishes the last item of ti.
 
 // f cell-major [B][K][N_Q] -> packed [cg][q][k][C] (zero past the end of the batch).  One CTA per
 // (cell group, 32 rows q): the 8 cells' K x 32 block is read along q (coalesced) into shared memory
@@ -865,32 +877,42 @@ __device__ __forceinline__ void slot_phi_staged(const double* __restrict__ gv, c
     if (cur >= 0) flush();
 }
 
+enum { LBI_TR = 0, LBI_ORD, LBI_BEGIN, LBI_END };  // item: t | row << 16, ord | l2 << 16 | l3 << 24, entries
+enum { LBU_L1 = 0, LBU_BROWS, LBU_TLOFF, LBU_NT, LBU_ITOFF, LBU_NIT, LBU_INTS = 8 };
+
 template <int K, int C, int W>
 __global__ void __launch_bounds__(W * 32, 1) af_lblock64_kernel(SplitArgs a) {
     using S = Shape<K, C>;
     constexpr int KH = S::KH, KQ = S::KQ, PS = S::PS, RTB = S::RT_BYTES;
-    constexpr int ROWB = K * C * (int)sizeof(double);  // bytes of one packed row q (K x C doubles)
+    constexpr int ROWB = K * C * (int)sizeof(double);
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* ring = smem + a.off_b;
-    double* red = reinterpret_cast<double*>(smem + a.off_red);
+    double* qacc = reinterpret_cast<double*>(smem + a.off_red);  // [brows][K][C]
     uint64_t* bfull = reinterpret_cast<uint64_t*>(smem + a.off_bar);
     int* misc = reinterpret_cast<int*>(smem + a.off_misc);
+    int* counter = misc;
     volatile int* abort_flag = misc + 1;
-    int* rcount = misc + 2;  // [n_ring] warps done with a stage, summed over its uses
+    int* done = misc + 2;                        // [kLbMaxRing] items finished per stage, summed over uses
+    volatile int* ticket = misc + 2 + kLbMaxRing;  // [max_rows] slices of each row added so far
+    int* cum = misc + 2 + kLbMaxRing + a.max_rows;  // [max_t] items of the stage's uses up to ti
+    // [kLbMaxRing] the t-list position each stage holds or is being filled with.  An item of ti may be
+    // taken while its stage still holds ti - D (items are handed out ahead of the copies), and an
+    // mbarrier cannot tell that phase from the one of ti: a parity wait on a phase two ahead of the
+    // current one returns at once.  So an item first waits for its stage to be assigned ti.
+    volatile int* stage_ti = misc + 2 + kLbMaxRing + a.max_rows + a.max_t;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int c = lane % C, part = lane / C, k2o = S::k2_of(part), k3o = S::k3_of(part);
     const int NQ = a.n_q, M = NQ * K, D = a.n_ring;
-    const int rg = a.unit_order[blockIdx.x / a.n_cg];
+    const int unit = a.unit_order[blockIdx.x / a.n_cg];
     const int cg = blockIdx.x % a.n_cg;
-    const int* u = a.units + (size_t)rg * U_INTS;
-    const int l1 = u[U_L1], r0 = u[U_R0], nr = u[U_NR], cq = u[U_S], crem = u[U_REM], tl_off = u[U_TLOFF],
-              n_t = u[U_NT], tab_off = u[U_TABOFF], brows = u[U_BROWS];
-    const int n_slots = nr * cq + crem;
+    const int* u = a.units + (size_t)unit * LBU_INTS;
+    const int l1 = u[LBU_L1], brows = u[LBU_BROWS], tl_off = u[LBU_TLOFF], n_t = u[LBU_NT], it_off = u[LBU_ITOFF],
+              n_it = u[LBU_NIT];
     const long long cell0 = (long long)cg * C;
     const double* __restrict__ pcg = a.pf + (size_t)cg * M * C;
+    const int4* __restrict__ items = a.items + it_off;
 
-    // stage sb <- R_t and the row blocks of bands l2 and l3 of t-list position ti (thread 0)
     auto issue = [&](int ti, int sb) {
         const int t = a.band_tl[tl_off + ti];
         const int l23 = a.t_l23[t], l2 = l23 & 0xff, l3 = l23 >> 8;
@@ -902,107 +924,141 @@ __global__ void __launch_bounds__(W * 32, 1) af_lblock64_kernel(SplitArgs a) {
         if (fb3) tc05::bulk_g2s(st + RTB + fb2, pcg + (size_t)l3 * l3 * K * C, fb3, &bfull[sb]);
     };
 
+    for (int i = tid; i < brows * K * C; i += W * 32) qacc[i] = 0.0;
+    for (int i = tid; i < brows; i += W * 32) ticket[i] = 0;
     if (tid == 0) {
         for (int i = 0; i < D; ++i) {
             tc05::mbar_init(&bfull[i], 1);
-            rcount[i] = 0;
+            done[i] = 0;
+            stage_ti[i] = i;
         }
         tc05::fence_mbar_init();
         *abort_flag = 0;
+        *counter = 0;
+        // cum[ti]: the items of every use of stage ti % D up to and including ti
+        int run[kLbMaxRing] = {};
+        for (int ti = 0; ti < n_t; ++ti) {
+            run[ti % D] += __ldg(a.t_items + tl_off + ti);
+            cum[ti] = run[ti % D];
+        }
     }
     __syncthreads();
     if (tid == 0)
         for (int ti = 0; ti < min(n_t, D); ++ti) issue(ti, ti);
 
-    const bool active = warp < n_slots;
-    int srow = 0, ch = 0, nS = 1;
-    if (active) slot_of(warp, cq, crem, srow, ch, nS);
-    const int row = r0 + srow;
-    double acc[K];
-#pragma unroll
-    for (int k1 = 0; k1 < K; ++k1) acc[k1] = 0.0;
-    // the slot's entries (and l-triplet) of t-list position ti in cur, of ti + 1 fetched during ti
-    SlotEntries cur{0, 0, 0u, 0.0}, nxt{0, 0, 0u, 0.0};
-    int ncb = 0, nce = 0, cur_l23 = 0, nxt_l23 = 0;
-    if (active) {
-        int cb, ce;
-        slot_range(a, tab_off, brows, 0, row, ch, nS, cb, ce);
-        cur = slot_fetch(a, a.e_g, cb, ce, lane);
-        cur_l23 = __ldg(a.t_l23 + __ldg(a.band_tl + tl_off));
-        if (n_t > 1) slot_range(a, tab_off, brows, 1, row, ch, nS, ncb, nce);
-    }
-    for (int ti = 0; ti < n_t; ++ti) {
+    // the warp's item and, fetched while it works on it, the next one
+    auto grab = [&]() {
+        int v = 0;
+        if (lane == 0) v = atomicAdd(counter, 1);
+        return __shfl_sync(0xffffffffu, v, 0);
+    };
+    int cur_i = grab();
+    int4 it = cur_i < n_it ? __ldg(items + cur_i) : make_int4(0, 0, 0, 0);
+    SlotEntries se = cur_i < n_it ? slot_fetch(a, a.e_g, it.z, it.w, lane) : SlotEntries{0, 0, 0u, 0.0};
+    while (cur_i < n_it) {
+        const int nxt_i = grab();
+        int4 nit = make_int4(0, 0, 0, 0);
+        SlotEntries nse{0, 0, 0u, 0.0};
+        if (nxt_i < n_it) {
+            nit = __ldg(items + nxt_i);
+            nse = slot_fetch(a, a.e_g, nit.z, nit.w, lane);
+        }
+        const int ti = it.x & 0xffff, row = it.x >> 16, ord = it.y & 0xffff;
+        const int l2 = (it.y >> 16) & 0xff, l3 = (it.y >> 24) & 0xff;
         const int sb = ti % D;
-        const SlotEntries se = cur;
-        const int l23 = cur_l23;
-        if (active) {
-            if (ti + 1 < n_t) {
-                nxt = slot_fetch(a, a.e_g, ncb, nce, lane);
-                nxt_l23 = __ldg(a.t_l23 + __ldg(a.band_tl + tl_off + ti + 1));
-            }
-            if (ti + 2 < n_t) slot_range(a, tab_off, brows, ti + 2, row, ch, nS, ncb, nce);
-        }
-        // every warp sees stage sb land before it counts itself done with it (the refill is armed
-        // only after that), also where it reads nothing from it
-        const bool ok = wait_bar(&bfull[sb], (uint32_t)((ti / D) & 1), abort_flag, a.err);
-        if (active && ok && se.cb < se.ce) {
-            const unsigned char* st = ring + (size_t)sb * a.stage_bytes;
-            const int l2 = l23 & 0xff, l3 = l23 >> 8;
-            const int b2 = l2 * l2, b3 = l3 * l3 - (l3 != l2 ? 2 * l2 + 1 : 0);
-            double phi[KH][KQ];
-            slot_phi_staged<K, C>(a.e_g, a.e_q23, reinterpret_cast<const double*>(st + RTB), se, lane, c, k2o, k3o,
-                                  b2, b3, phi);
-            const double* rp = reinterpret_cast<const double*>(st) + part * PS;
-#pragma unroll
-            for (int x = 0; x < KH; ++x)
-#pragma unroll
-                for (int y = 0; y < KQ; ++y) {
-                    const double2* r2 = reinterpret_cast<const double2*>(rp + (x * KQ + y) * K);
-#pragma unroll
-                    for (int j = 0; j < K / 2; ++j) {
-                        const double2 r = r2[j];
-                        acc[2 * j] = fma(r.x, phi[x][y], acc[2 * j]);
-                        acc[2 * j + 1] = fma(r.y, phi[x][y], acc[2 * j + 1]);
-                    }
+        if (lane == 0) {
+            const long long t0 = clock64();
+            while (stage_ti[sb] != ti) {
+                if (*abort_flag || clock64() - t0 > kWaitCycles) {
+                    *abort_flag = 1;
+                    atomicExch(a.err, 1);
+                    break;
                 }
+                __nanosleep(128);
+            }
         }
-        if (active) {
-            cur = nxt;
-            cur_l23 = nxt_l23;
+        __syncwarp();
+        bool ok = wait_bar(&bfull[sb], (uint32_t)((ti / D) & 1), abort_flag, a.err);
+        if (ok) {
+            const unsigned char* st = ring + (size_t)sb * a.stage_bytes;
+            const int b2 = l2 * l2, b3 = l3 * l3 - (l3 != l2 ? 2 * l2 + 1 : 0);
+            double acc[K];
+            {
+                double phi[KH][KQ];
+                slot_phi_staged<K, C>(a.e_g, a.e_q23, reinterpret_cast<const double*>(st + RTB), se, lane, c, k2o,
+                                      k3o, b2, b3, phi);
+                const double* rp = reinterpret_cast<const double*>(st) + part * PS;
+#pragma unroll
+                for (int k1 = 0; k1 < K; ++k1) acc[k1] = 0.0;
+#pragma unroll
+                for (int x = 0; x < KH; ++x)
+#pragma unroll
+                    for (int y = 0; y < KQ; ++y) {
+                        const double2* r2 = reinterpret_cast<const double2*>(rp + (x * KQ + y) * K);
+#pragma unroll
+                        for (int j = 0; j < K / 2; ++j) {
+                            const double2 r = r2[j];
+                            acc[2 * j] = fma(r.x, phi[x][y], acc[2 * j]);
+                            acc[2 * j + 1] = fma(r.y, phi[x][y], acc[2 * j + 1]);
+                        }
+                    }
+            }
+            // the parts of a cell sit in lanes c, c + C, c + 2C, ...: sum them, then part p adds the
+            // k1 of its quarter once this row's earlier slices are in
+#pragma unroll
+            for (int k1 = 0; k1 < K; ++k1)
+#pragma unroll
+                for (int o = C; o < 32; o <<= 1) acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], o);
+            if (lane == 0) {
+                const long long t0 = clock64();
+                while (ticket[row] != ord) {
+                    if (*abort_flag || clock64() - t0 > kWaitCycles) {
+                        *abort_flag = 1;
+                        atomicExch(a.err, 1);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __syncwarp();
+            __threadfence_block();
+            ok = !*abort_flag;
+            if (ok) {
+                double* qr = qacc + (size_t)row * K * C + c;
+                constexpr int KP = K / (32 / C);  // k1 per part
+#pragma unroll
+                for (int k1 = 0; k1 < K; ++k1)
+                    if (k1 / KP == part) qr[k1 * C] += acc[k1];
+            }
+            __syncwarp();
+            if (lane == 0) {
+                __threadfence_block();
+                ticket[row] = ord + 1;
+            }
         }
-        // the last warp done with stage sb refills it with t-list position ti + D (no CTA-wide barrier)
+        // the warp that finishes the last item of ti refills its stage with ti + D
         __syncwarp();
         if (lane == 0) {
             __threadfence_block();
-            if (atomicAdd(&rcount[sb], 1) == W * ((ti / D) + 1) - 1 && ti + D < n_t && !*abort_flag) {
+            if (atomicAdd(&done[sb], 1) == cum[ti] - 1 && ti + D < n_t && !*abort_flag) {
                 __threadfence_block();
                 asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+                stage_ti[sb] = ti + D;
                 issue(ti + D, sb);
             }
         }
         __syncwarp();
+        cur_i = nxt_i;
+        it = nit;
+        se = nse;
     }
-    // the parts of a cell sit in lanes c, c + C, c + 2C, ...
-#pragma unroll
-    for (int k1 = 0; k1 < K; ++k1)
-#pragma unroll
-        for (int o = C; o < 32; o <<= 1) acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], o);
-    if (active && lane < C)
-#pragma unroll
-        for (int k1 = 0; k1 < K; ++k1) red[(warp * C + lane) * K + k1] = acc[k1];
     __syncthreads();
-    if (tid < nr * C) {
-        const int rl = tid / C, cc = tid % C;
+    if (*abort_flag) return;
+    // Q += the band's rows of the 8 cells (cell-major, in place)
+    for (int i = tid; i < brows * K * C; i += W * 32) {
+        const int cc = i % C, k1 = (i / C) % K, r = i / (C * K);
         const long long cell = cell0 + cc;
-        if (cell < a.n_cells) {
-            double* qc = a.q + cell * M + (l1 * l1 + r0 + rl);
-            for (int k1 = 0; k1 < K; ++k1) {
-                double sum = 0.0;
-                const int s0 = row_first_slot(rl, cq, crem), nc = row_chunks(rl, cq, crem);
-                for (int chk = 0; chk < nc; ++chk) sum += red[((s0 + chk) * C + cc) * K + k1];
-                qc[(size_t)k1 * NQ] += sum;
-            }
-        }
+        if (cell < a.n_cells) a.q[cell * M + (size_t)k1 * NQ + l1 * l1 + r] += qacc[i];
     }
 }
 
@@ -1299,10 +1355,13 @@ struct SplitPlan {
     uint8_t* d_rbf8 = nullptr;        // K = 12: the same for 8 cells per CTA (Phi in FP32)
     double* d_rfl = nullptr;          // the l-block kernel (8 cells per CTA): FP64 R_t as [part][e][k1]
     int* d_t_l23 = nullptr;           // per l-triplet: l2 | l3 << 8
-    int lb_ring = 0, lb_stage = 0;    // the l-block kernel's stages and bytes per stage (0: unsupported)
-    int n_rg_lb = 0;                  // the l-block kernel's row groups (lblock_warps(K) slots each)
-    int* d_units_lb = nullptr;
-    int* d_unit_order_lb = nullptr;
+    // the l-block kernel (0 bands: unsupported)
+    int lb_bands = 0, lb_rows = 0, lb_t = 0;  // bands, rows of the largest band, longest t-list
+    int lb_ring = 0, lb_stage = 0;    // stages in the ring, bytes per stage
+    int* d_lb_units = nullptr;        // per band: LBU_INTS ints
+    int* d_lb_order = nullptr;        // bands, heaviest first
+    int4* d_lb_items = nullptr;       // per band: its (t, row) slices in t-major order
+    int* d_lb_titems = nullptr;       // per t-list position: its items
     Layout lay{};
     Layout lay64{};
     Layout laybf{};
@@ -1558,8 +1617,39 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     const int n_rg = make_units(kSlots, units, order);
     const int w64 = band64_warps(K);
     const int n_rg64 = make_units(w64, units64, order64);
-    std::vector<int> units_lb, order_lb;
-    const int n_rg_lb = lblock_supported_k(K) ? make_units(lblock_warps(K), units_lb, order_lb) : 0;
+    // the l-block kernel: per band, its (t, row) slices in t-major order, each with its ordinal among
+    // its row's slices (the row's ticket) and the (l2, l3) of its t
+    std::vector<int> units_lb, order_lb, titems_lb(band_tl.size(), 0);
+    std::vector<int4> items_lb;
+    std::vector<double> work_lb;
+    int lb_rows = 0, lb_t = 0;
+    bool lb_ok = L < 128;
+    for (const BandInfo& bd : bands) {
+        const int it_off = (int)items_lb.size();
+        std::vector<int> ord(bd.brows, 0);
+        for (int ti = 0; ti < bd.n_t; ++ti) {
+            const int t = band_tl[bd.tl_off + ti];
+            const int l23 = t_l23[t];
+            for (int r = 0; r < bd.brows; ++r) {
+                const int sl = band_slice[bd.tab_off + (size_t)ti * bd.brows + r];
+                if (sl < 0) continue;
+                items_lb.push_back(make_int4(ti | (r << 16), ord[r]++ | ((l23 & 0xff) << 16) | ((l23 >> 8) << 24),
+                                              slice_e[sl], slice_e[sl + 1]));
+                ++titems_lb[bd.tl_off + ti];
+            }
+        }
+        const int uu[LBU_INTS] = {bd.l1, bd.brows, bd.tl_off, bd.n_t, it_off, (int)items_lb.size() - it_off, 0, 0};
+        units_lb.insert(units_lb.end(), uu, uu + LBU_INTS);
+        double w = 0.0;
+        for (double x : bd.row_work) w += x;
+        work_lb.push_back(w * K * K + (double)(items_lb.size() - it_off) * K * K * K);
+        lb_rows = std::max(lb_rows, bd.brows);
+        lb_t = std::max(lb_t, bd.n_t);
+        if (bd.n_t > 0xffff || bd.brows > 0x7fff) lb_ok = false;
+    }
+    order_lb.resize(work_lb.size());
+    for (size_t i = 0; i < work_lb.size(); ++i) order_lb[i] = (int)i;
+    std::stable_sort(order_lb.begin(), order_lb.end(), [&](int x, int y) { return work_lb[x] > work_lb[y]; });
     // the (t, row) tables as entry ranges (begin, end), empty where the row has no slice of t
     std::vector<int> band_rng(2 * band_slice.size(), 0);
     for (size_t i = 0; i < band_slice.size(); ++i)
@@ -1573,7 +1663,9 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
     sp->L = L;
     sp->n_rg = n_rg;
     sp->n_rg64 = n_rg64;
-    sp->n_rg_lb = n_rg_lb;
+    sp->lb_bands = lb_ok && lblock_supported_k(K) ? (int)work_lb.size() : 0;
+    sp->lb_rows = lb_rows;
+    sp->lb_t = lb_t;
     sp->w64 = w64;
     // int32 accumulators: at most 6 byte products of |255 * 128| per K element and weight
     sp->tseg = std::max(1, (int)(2147483647LL / (6LL * 255 * 128 * S::KK)));
@@ -1600,11 +1692,13 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
         }
         const int stage = (Shape<K, kLbCells>::RT_BYTES + max_rows * K * kLbCells * (int)sizeof(double) + 127) / 128 * 128;
         int ring = kLbMaxRing;
-        while (ring >= 2 && lblock_layout(ring, stage, K).total > optin) --ring;
+        while (ring >= 2 && lblock_layout(ring, stage, K, lb_rows, lb_t).total > optin) --ring;
         if (ring >= 2) {
             sp->lb_ring = ring;
             sp->lb_stage = stage;
-            sp->laylb = lblock_layout(ring, stage, K);
+            sp->laylb = lblock_layout(ring, stage, K, lb_rows, lb_t);
+        } else {
+            sp->lb_bands = 0;
         }
     }
     sp->laybf = bf16_layout<K, C>(NQ);
@@ -1627,8 +1721,10 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
         (ce = upload_vec(&sp->d_rbf, rbf, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_rbf8, rbf8, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_rfl, rfl, bytes)) != cudaSuccess ||
-        (ce = upload_vec(&sp->d_units_lb, units_lb, bytes)) != cudaSuccess ||
-        (ce = upload_vec(&sp->d_unit_order_lb, order_lb, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_lb_units, units_lb, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_lb_order, order_lb, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_lb_items, items_lb, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_lb_titems, titems_lb, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_t_l23, t_l23, bytes)) != cudaSuccess)
         return fail_split(ce == cudaErrorMemoryAllocation ? CF_ENOMEM : CF_ECUDA,
                           std::string("split form: upload: ") + cudaGetErrorString(ce));
@@ -1737,13 +1833,12 @@ size_t lblock_pack_bytes_of(int n_q, int k, int64_t B) {
 
 template <int K>
 int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf, int64_t B, cudaStream_t st,
-               int64_t* launches) {
-    constexpr int C = kLbCells, W = lblock_warps(K);
+                int64_t* launches) {
+    constexpr int C = kLbCells, W = kLbWarps;
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        // (the pack kernel's 32 K C doubles, at most 24 KB, need no attribute)
         const cudaError_t e = cudaFuncSetAttribute(af_lblock64_kernel<K, C, W>,
                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
         if (e != cudaSuccess)
@@ -1751,7 +1846,7 @@ int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf
         attr_set[dev] = true;
     }
     const long long n_cg = (B + C - 1) / C;
-    if (n_cg > 65535LL || (long long)sp->n_rg_lb * n_cg > 0x7fffffffLL)
+    if (n_cg > 65535LL || (long long)sp->lb_bands * n_cg > 0x7fffffffLL)
         return fail_split(CF_ESHAPE, "l-block kernel: batch too large for one launch");
     dim3 pgrid((unsigned)((sp->n_q + 31) / 32), (unsigned)n_cg);
     static_assert(32 * K * C * 8 <= 48 * 1024, "the pack kernel's tile fits the default shared memory");
@@ -1764,10 +1859,11 @@ int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf
     a.e_q23 = sp->e_q23;
     a.e_g = sp->e_g;
     a.rfp64 = sp->d_rfl;
-    a.units = sp->d_units_lb;
-    a.unit_order = sp->d_unit_order_lb;
+    a.units = sp->d_lb_units;
+    a.unit_order = sp->d_lb_order;
     a.band_tl = sp->d_band_tl;
-    a.band_rng = sp->d_band_rng;
+    a.items = sp->d_lb_items;
+    a.t_items = sp->d_lb_titems;
     a.pf = pf;
     a.t_l23 = sp->d_t_l23;
     a.q = q_cm;
@@ -1778,11 +1874,13 @@ int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf
     a.L = sp->L;
     a.n_ring = sp->lb_ring;
     a.stage_bytes = sp->lb_stage;
+    a.max_rows = sp->lb_rows;
+    a.max_t = sp->lb_t;
     a.off_b = sp->laylb.off_b;
     a.off_red = sp->laylb.off_red;
     a.off_bar = sp->laylb.off_bar;
     a.off_misc = sp->laylb.off_misc;
-    const long long blocks = (long long)sp->n_rg_lb * n_cg;
+    const long long blocks = (long long)sp->lb_bands * n_cg;
     af_lblock64_kernel<K, C, W><<<(unsigned)blocks, W * 32, sp->laylb.total, st>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("l-block kernel: launch: ") + cudaGetErrorString(e));
@@ -1872,11 +1970,11 @@ int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
 
 size_t lblock_pack_bytes(const SplitPlan* sp, int64_t B) { return lblock_pack_bytes_of(sp->n_q, sp->k, B); }
 
-bool lblock_available(const SplitPlan* sp) { return sp && lblock_supported_k(sp->k) && sp->lb_ring >= 2; }
+bool lblock_available(const SplitPlan* sp) { return sp && lblock_supported_k(sp->k) && sp->lb_bands > 0; }
 
 int lblock64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf, size_t pf_bytes, int64_t B,
                  cudaStream_t st, int64_t* launches) {
-    if (B <= 0 || sp->n_rg_lb == 0) return CF_OK;
+    if (B <= 0) return CF_OK;
     if (!lblock_available(sp))
         return fail_split(CF_EUNSUPPORTED, "l-block kernel: needs K = 8 or 12 and two stages of shared memory");
     if (pf_bytes < lblock_pack_bytes(sp, B)) return fail_split(CF_EINVAL, "l-block kernel: packed-f workspace too small");
@@ -1925,7 +2023,8 @@ void split_destroy(SplitPlan* sp) {
     if (!sp) return;
     void* ptrs[] = {sp->d_rplanes, sp->d_e_gs, sp->d_rb_off, sp->d_rb_gs, sp->d_rb_l23, sp->d_units, sp->d_unit_order, sp->d_band_tl,
                     sp->d_band_rng, sp->d_err, sp->d_rfp64, sp->d_rbf, sp->d_units64, sp->d_unit_order64,
-                    sp->d_rbf8, sp->d_rfl, sp->d_t_l23, sp->d_units_lb, sp->d_unit_order_lb};
+                    sp->d_rbf8, sp->d_rfl, sp->d_t_l23, sp->d_lb_units, sp->d_lb_order, sp->d_lb_items,
+                    sp->d_lb_titems};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     delete sp;

@@ -32,9 +32,10 @@ int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
 // shared memory does not fit.  No allocation, no synchronisation.
 int bf16_band_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st,
                   int64_t* launches);
-// The l-block kernel (K = 8 and 12) on the FP64 band kernel's units: 8 cells per CTA, R_t and the f
-// rows of bands l2 and l3 staged per l-triplet by bulk copies.  pf is a device workspace of at least
-// lblock_pack_bytes(sp, B) bytes for the packed f.  No allocation, no synchronisation.
+// The l-block kernel (K = 8 and 12): one CTA per (l1 band, 8-cell group), R_t and the f rows of bands
+// l2 and l3 staged per l-triplet by bulk copies, the band's (t, row) slices taken by the warps one at
+// a time and summed per row in t order.  pf is a device workspace of at least lblock_pack_bytes(sp, B)
+// bytes for the packed f.  No allocation, no synchronisation.
 int lblock64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf, size_t pf_bytes, int64_t B,
                  cudaStream_t st, int64_t* launches);
 size_t lblock_pack_bytes(const SplitPlan* sp, int64_t B);

@@ -189,7 +189,7 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
 /* Kernel family of a plan's angular-first and Jacobian contractions: 0 = automatic (the first of
  * pair, tile, gather that fits; tile before pair for the fast Q form of the folded operator, whose
  * lighter Phi step favours the tile kernel's higher occupancy; the l-block kernel for the fast Q
- * form of the folded operator at K = 12 from L = 8 on), 1 = the gather kernel (warp per row and 32-cell tile,
+ * forms, plain and folded, at K = 12 from L = 8 on), 1 = the gather kernel (warp per row and 32-cell tile,
  * f read through L1/L2), 2 = the tile-resident kernel (16 cells in shared memory, Phi split over
  * two lanes per cell), 3 = the pair kernel (16 cells in shared memory, the mirrored rows (l,+m) and
  * (l,-m) on the two half-warps), 4 = the pair kernel reading R through L1 instead of shared
@@ -197,8 +197,9 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
  * half-warps; fast Q forms with even K <= 8, the pair kernel otherwise), 6 = the tile kernel with
  * its K^3 step on the FP64 tensor cores (warp-level MMA; fast Q form at K = 8, the tile kernel
  * otherwise), 11 = the band kernel (fast FP64 Q forms on l1-band work units, K = 4, 8, 12), 14 = the
- * l-block kernel (the band units with 8 cells per CTA and R_t plus the f rows of bands l2 and l3
- * staged per l-triplet by bulk copies; fast FP64 Q forms, K = 8 and 12).  2-6, 11 and 14 return
+ * l-block kernel (one CTA per l1 band and 8 cells, R_t plus the f rows of bands l2 and l3 staged per
+ * l-triplet by bulk copies, the band's slices taken by the warps one at a time; fast FP64 Q forms,
+ * K = 8 and 12).  2-6, 11 and 14 return
  * CF_EUNSUPPORTED where they do not fit.  All families agree to rounding, and bit for bit in the
  * exact forms. */
 int cf_plan_set_kernel_path(cf_plan* plan, int32_t path);

@@ -1,6 +1,8 @@
-"""The l-block kernel (af_lblock64_kernel): the fast angular-first Q forms on the band kernel's l1-band
-work units, 8 cells per CTA, with R_t and the f rows of bands l2 and l3 staged per l-triplet by bulk
-copies from f packed per 8-cell group, on kernel path 'lblock' (K = 8 and 12).
+"""The l-block kernel (af_lblock64_kernel): the fast angular-first Q forms with one CTA per (l1 band,
+8-cell group), R_t and the f rows of bands l2 and l3 staged per l-triplet by bulk copies from f packed
+per 8-cell group, and the band's (t, row) slices taken by the warps one at a time and summed into each
+row in t order; on kernel path 'lblock' (K = 8 and 12), and in the automatic order at K = 12 from
+L = 8 on.
 
 Tolerance: 1e-12 normwise per cell against the oracle's restatement of the reference's angular-first
 kernel (src/mex/angular_first_collision_kernel_mex.cpp:45-69), the FP64 bar of the parity suite.
@@ -95,8 +97,9 @@ def test_lblock_kernel_precision_configuration_vs_oracle(cuda_available, oracle_
 @pytest.mark.skipif(not (GOLDEN / "R_hs_k11_l16_pad20.npy").exists(), reason="L = 16, K = 12 R fixture absent")
 def test_precision_configuration_automatic_order_vs_oracle(cuda_available, oracle_lib):
     """The automatic kernel order at L = 16, K = 12 (hard spheres, R from the GPU quadrature): the plain
-    FP64 form on the gather kernel and the folded one on the l-block kernel, both within 1e-12 of the
-    oracle on 13 bi-Maxwellian cells."""
+    and folded FP64 forms on the l-block kernel, both within 1e-12 of the oracle on 13 bi-Maxwellian
+    cells; an operator given in an unsorted COO order (several runs per (t, q1)) has no band tables
+    and runs on the gather kernel, to the same tolerance."""
     import cf_b200
     from cf_b200 import workloads
 
@@ -104,15 +107,23 @@ def test_precision_configuration_automatic_order_vs_oracle(cuda_available, oracl
     cells = workloads.bimaxwellian_cells(12, 16, 13, seed=20262)
     ref = _oracle(geo, R, 12, cells, oracle_lib)
     op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, 12)
-    for form, path in (("af", "gather"), ("af_sym", "lblock")):
+    for form in ("af", "af_sym"):
         Q = _device_q(op, cells, form)
-        assert cf_b200._lib.PATH_NAMES[op.info()["last_path"]] == path, form
+        assert cf_b200._lib.PATH_NAMES[op.info()["last_path"]] == "lblock", form
         assert per_cell_err(Q, ref) <= TOL_FP64, (form, per_cell_err(Q, ref))
+    op.close()
+    perm = np.random.default_rng(3).permutation(geo.n_g)
+    op = cf_b200.CollisionOperator(np.asfortranarray(geo.labels[perm]), geo.vals[perm], geo.ic_map[perm], R,
+                                   geo.n_q, 12)
+    Q = _device_q(op, cells, "af")
+    assert cf_b200._lib.PATH_NAMES[op.info()["last_path"]] == "gather"
+    assert per_cell_err(Q, ref) <= TOL_FP64
     op.close()
 
 
 def test_lblock_kernel_accumulates_and_is_deterministic(cuda_available, oracle_lib):
-    """out += Q(f) from a nonzero Q, two runs give the same bits, and Q(2f) = 4 Q(f) bit for bit."""
+    """out += Q(f) from a nonzero Q, two runs give the same bits (whichever warp takes which slice, each
+    row sums its slices in t order), and Q(2f) = 4 Q(f) bit for bit."""
     import cf_b200
     from cf_b200 import workloads
 
