@@ -718,9 +718,11 @@ def run_e2e(op, geo, R, cells, K, args, world, form="af"):
     return {"value": world * B * steps / tot, "unit": "cell-evals/s", "h2d_bytes_per_step": 2 * nbytes,
             "d2h_bytes_per_step": nbytes,
             "form": form,
-            "path": "cf_contract_host (the MEX-compatible host entry point: content-keyed plan cache; the folded "
-                    "fast form streams the batch through one tile-kernel launch while chunks are copied in and out), "
-                    "pinned host buffers, Q_out zeroed by one host thread before each call (outside the timing)"}
+            "path": "cf_contract_host (the MEX-compatible host entry point: content-keyed plan cache, checked while "
+                    "the GPU works from the second call on; the folded fast form at K <= 8 streams the batch through one "
+                    "tile-kernel launch while chunks are copied in and out, other forms run the chunked pipeline on "
+                    "three streams), pinned host buffers, Q_out zeroed by one host thread before each call (outside "
+                    "the timing)"}
 
 
 # --------------------------------------------------------------------------------------------

@@ -141,6 +141,7 @@ struct cf_plan {
     size_t io_bytes = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t host_streams[kHostStreams] = {};  // chunked host path: copies overlap the contraction
+    cudaEvent_t chunk_done[CF_HOST_MAX_CHUNKS] = {};  // chunked host path: a chunk's contraction is done
     // streamed host path: copy-in, kernel and copy-out streams; per chunk a ready flag (device) and
     // a completion word (mapped pinned host memory); the epoch values the flag copies read (pinned)
     cudaStream_t xs[3] = {};
@@ -296,6 +297,8 @@ void free_plan_memory(cf_plan* p) {
     if (p->stream) cudaStreamDestroy(p->stream);
     for (cudaStream_t& hs : p->host_streams)
         if (hs) cudaStreamDestroy(hs);
+    for (cudaEvent_t& ev : p->chunk_done)
+        if (ev) cudaEventDestroy(ev);
     for (cudaStream_t& hs : p->xs)
         if (hs) cudaStreamDestroy(hs);
 }
@@ -1290,6 +1293,72 @@ int run_host_streamed(cf_plan* p, cf_plan* target, double* Q, const double* f, i
 // The streamed contraction with the plan these pointers had last time, while a helper thread checks
 // the operator's content hash; nothing reaches Q before the check passes.  kRetry: no guess, the
 // guess does not stream, or the content changed (Q untouched) -- contract the ordinary way.
+// Chunked host pipeline on plan p (p->mu held): chunk c goes up, is contracted and comes back on stream
+// c mod kHostStreams, so the host<->device copies of one chunk overlap the contraction of the others
+// (pinned host memory makes the copies asynchronous; pageable memory still gives the right answer,
+// serialised).  With a gate (p is a guess from the operator's pointers, its content hash computed on
+// another thread), the downloads wait: once the gate reads 1, every chunk's download is queued on the
+// plan's stream behind an event of its contraction; if it reads 2, nothing is copied back and kRetry
+// is returned.
+int run_host_chunked(cf_plan* p, int what, bool exact, double* Q, const double* f, const double* v, int64_t B,
+                     double* dQ, double* df, double* dv, bool sym, int f32, const std::atomic<int>* gate) {
+    const int64_t M = (int64_t)p->n_q * p->k;
+    const int nbuf = what == 2 ? 3 : 2;
+    for (cudaStream_t& hs : p->host_streams)
+        if (!hs) CF_CUDA(cudaStreamCreateWithFlags(&hs, cudaStreamNonBlocking));
+    int64_t n_chunks = std::min<int64_t>(kHostMaxChunks, B / kHostChunkMin);
+    const int64_t per = (B + n_chunks - 1) / n_chunks;
+    const int64_t chunk = (per + CF_TILE - 1) / CF_TILE * CF_TILE;  // whole 32-cell tiles per chunk
+    n_chunks = (B + chunk - 1) / chunk;
+    const size_t tbc = tiled_bytes(p, chunk) * nbuf;
+    CF_TRY(ensure_ws(p, tbc * kHostStreams));
+    if (gate)
+        for (int64_t c = 0; c < n_chunks; ++c)
+            if (!p->chunk_done[c]) CF_CUDA(cudaEventCreateWithFlags(&p->chunk_done[c], cudaEventDisableTiming));
+    int st = CF_OK;
+    for (int64_t c = 0; c < n_chunks && st == CF_OK; ++c) {
+        cudaStream_t s = p->host_streams[c % kHostStreams];
+        const int64_t b0 = c * chunk, bc = std::min(chunk, B - b0);
+        const size_t off = (size_t)b0 * M, nb = (size_t)bc * M * sizeof(double);
+        void* ws = (char*)p->d_ws + (size_t)(c % kHostStreams) * tbc;
+        cudaError_t e = cudaMemcpyAsync(dQ + off, Q + off, nb, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(df + off, f + off, nb, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && dv) e = cudaMemcpyAsync(dv + off, v + off, nb, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+            break;
+        }
+        st = run_device(p, what, exact, dQ + off, df + off, dv ? dv + off : nullptr, bc, ws, tbc, s, sym, f32);
+        if (st == CF_OK) {
+            e = gate ? cudaEventRecord(p->chunk_done[c], s) : cudaMemcpyAsync(Q + off, dQ + off, nb, cudaMemcpyDeviceToHost, s);
+            if (e != cudaSuccess) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+        }
+    }
+    bool retry = false;
+    if (gate) {
+        while (gate->load(std::memory_order_acquire) == 0) std::this_thread::yield();
+        retry = gate->load(std::memory_order_acquire) == 2;
+        for (int64_t c = 0; c < n_chunks && st == CF_OK && !retry; ++c) {
+            const int64_t b0 = c * chunk, bc = std::min(chunk, B - b0);
+            const size_t off = (size_t)b0 * M, nb = (size_t)bc * M * sizeof(double);
+            cudaError_t e = cudaStreamWaitEvent(p->stream, p->chunk_done[c], 0);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(Q + off, dQ + off, nb, cudaMemcpyDeviceToHost, p->stream);
+            if (e != cudaSuccess) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+        }
+    }
+    for (cudaStream_t hs : p->host_streams) {
+        const cudaError_t e = cudaStreamSynchronize(hs);
+        if (e != cudaSuccess && st == CF_OK) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+    }
+    if (gate) {
+        const cudaError_t e = cudaStreamSynchronize(p->stream);
+        if (e != cudaSuccess && st == CF_OK) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
+    }
+    if (st == CF_OK && (f32 >= 2 || band_path(p->path) || band_path(p->last_path))) st = check_split(p);
+    if (st == CF_OK && retry) return kRetry;
+    return st;
+}
+
 int run_host_speculative(double* Q, const double* f, int64_t B, const double* labels, const double* vals,
                          const double* ic_map, const double* R, int64_t n_g, int32_t n_l, int32_t n_q, int32_t k,
                          bool sym) {
@@ -1302,7 +1371,7 @@ int run_host_speculative(double* Q, const double* f, int64_t B, const double* la
     if (!guard.ok) return kRetry;
     cf_plan* target = p;
     if (sym && get_sym(p, &target) != CF_OK) return kRetry;
-    if (!streamable(p, target, 0, false, 0)) return kRetry;
+    const bool streamed = streamable(p, target, 0, false, 0);
     const size_t cell_bytes = (size_t)B * p->n_q * p->k * sizeof(double);
     if (ensure_io(p, 2 * cell_bytes) != CF_OK) return kRetry;
     std::atomic<int> gate{0};
@@ -1317,7 +1386,10 @@ int run_host_speculative(double* Q, const double* f, int64_t B, const double* la
     }
     double* dQ = p->d_io;
     double* df = (double*)((char*)p->d_io + cell_bytes);
-    const int st = run_host_streamed(p, target, Q, f, B, dQ, df, true, 0, &gate);
+    // the streamed tile kernel where the form runs on it, else the chunked pipeline with its
+    // downloads held back until the hash has matched
+    const int st = streamed ? run_host_streamed(p, target, Q, f, B, dQ, df, true, 0, &gate)
+                            : run_host_chunked(p, 0, false, Q, f, nullptr, B, dQ, df, nullptr, sym, 0, &gate);
     check.join();
     if (gate.load() == 2) return kRetry;  // nothing was copied back: Q is as the caller passed it
     return st;
@@ -1430,42 +1502,7 @@ int run_host(int what, bool exact, double* Q, const double* f, const double* v, 
         if (sym) CF_TRY(get_sym(p, &target));
         if (streamable(p, target, what, exact, f32)) return run_host_streamed(p, target, Q, f, B, dQ, df);
     }
-    // Chunked: chunk c goes up, is contracted and comes back on stream c mod kHostStreams, so the
-    // host<->device copies of one chunk overlap the contraction of the others (pinned host memory
-    // makes the copies asynchronous; pageable memory still gives the right answer, serialised).
-    for (cudaStream_t& hs : p->host_streams)
-        if (!hs) CF_CUDA(cudaStreamCreateWithFlags(&hs, cudaStreamNonBlocking));
-    int64_t n_chunks = std::min<int64_t>(kHostMaxChunks, B / kHostChunkMin);
-    const int64_t per = (B + n_chunks - 1) / n_chunks;
-    const int64_t chunk = (per + CF_TILE - 1) / CF_TILE * CF_TILE;  // whole 32-cell tiles per chunk
-    n_chunks = (B + chunk - 1) / chunk;
-    const size_t tbc = tiled_bytes(p, chunk) * nbuf;
-    CF_TRY(ensure_ws(p, tbc * kHostStreams));
-    int st = CF_OK;
-    for (int64_t c = 0; c < n_chunks && st == CF_OK; ++c) {
-        cudaStream_t s = p->host_streams[c % kHostStreams];
-        const int64_t b0 = c * chunk, bc = std::min(chunk, B - b0);
-        const size_t off = (size_t)b0 * M, nb = (size_t)bc * M * sizeof(double);
-        void* ws = (char*)p->d_ws + (size_t)(c % kHostStreams) * tbc;
-        cudaError_t e = cudaMemcpyAsync(dQ + off, Q + off, nb, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(df + off, f + off, nb, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess && dv) e = cudaMemcpyAsync(dv + off, v + off, nb, cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) {
-            st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
-            break;
-        }
-        st = run_device(p, what, exact, dQ + off, df + off, dv ? dv + off : nullptr, bc, ws, tbc, s, sym, f32);
-        if (st == CF_OK) {
-            e = cudaMemcpyAsync(Q + off, dQ + off, nb, cudaMemcpyDeviceToHost, s);
-            if (e != cudaSuccess) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
-        }
-    }
-    for (cudaStream_t hs : p->host_streams) {
-        const cudaError_t e = cudaStreamSynchronize(hs);
-        if (e != cudaSuccess && st == CF_OK) st = fail(CF_ECUDA, "%s", cudaGetErrorString(e));
-    }
-    if (st == CF_OK && (f32 >= 2 || band_path(p->path) || band_path(p->last_path))) st = check_split(p);
-    return st;
+    return run_host_chunked(p, what, exact, Q, f, v, B, dQ, df, dv, sym, f32, nullptr);
 }
 
 int form_what(int form, bool& exact, bool& sym, int& f32) {

@@ -151,3 +151,43 @@ def test_operator_changed_in_place_between_calls(cuda_available):
     changed = host(Rf)
     assert np.array_equal(changed.transpose(2, 1, 0), device(vals, Rf))
     assert not np.array_equal(changed, first)
+
+
+@pytest.mark.parametrize("L,K,form", [(8, 12, "af_sym"), (8, 12, "af"), (6, 8, "af")])
+def test_chunked_host_call_operator_changed_in_place(L, K, form, cuda_available):
+    """Forms that do not run on the streamed tile kernel take the chunked pipeline; from the second call
+    on it too starts from the plan of the operator arrays' addresses and checks their content while the
+    GPU works, holding every download back until the check passed.  Same arrays: bit for bit the
+    device entry point's result; arrays changed in place: the new operator's result."""
+    import torch
+
+    import cf_b200
+
+    B = 700
+    geo, R, cells, q0 = _setup(L, K, B, seed=7 + K)
+    labels = np.asfortranarray(geo.labels)
+    vals = np.array(geo.vals)
+    ic = np.array(geo.ic_map)
+    Rf = np.asfortranarray(R)
+    f_cm = np.asfortranarray(cells.transpose(2, 1, 0))
+
+    def host():
+        Q = np.array(q0.transpose(2, 1, 0), order="F")
+        cf_b200.contract_batched(Q, f_cm, labels, vals, ic, Rf, geo.n_q, K, form=form)
+        return Q.transpose(2, 1, 0)
+
+    def device():
+        op = cf_b200.CollisionOperator(labels, vals, ic, Rf, geo.n_q, K)
+        Qd = torch.from_numpy(q0.copy()).cuda()
+        op.q(torch.from_numpy(cells).cuda(), out=Qd, form=form)
+        op.close()
+        return Qd.cpu().numpy()
+
+    first = host()
+    assert np.array_equal(host(), first)  # the second call starts from the address guess
+    assert np.array_equal(first, device())
+    Rf *= 1.5  # same addresses, new content (kept symmetric in q2 <-> q3, as the folded form needs)
+    vals *= 0.75
+    changed = host()
+    assert np.array_equal(changed, device())
+    assert not np.array_equal(changed, first)
