@@ -586,7 +586,7 @@ bool streamable(const cf_plan* p, const cf_plan* target, int what, bool exact, i
 int run_split(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int run_lblock(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, void* ws, size_t ws_bytes,
-               cudaStream_t st);
+               cudaStream_t st, bool f32);
 int run_bf16_band(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int run_rfdense(cf_plan* p, double* q_dev, const double* f_dev, int64_t B, cudaStream_t st);
 int check_split(cf_plan* p);
@@ -638,7 +638,11 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
         if (!exact && f32 == 0) {
             int r = run_band64(target, q_dev, f_dev, B, st);
             if (r != kNoFew) return r;
-            r = run_lblock(target, q_dev, f_dev, B, ws, ws_bytes, st);
+            r = run_lblock(target, q_dev, f_dev, B, ws, ws_bytes, st, false);
+            if (r != kNoFew) return r;
+        }
+        if (!exact && f32 == 1) {
+            const int r = run_lblock(target, q_dev, f_dev, B, ws, ws_bytes, st, true);
             if (r != kNoFew) return r;
         }
         if (!exact && f32 == 2) {
@@ -937,10 +941,10 @@ int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, c
     return CF_OK;
 }
 
-// The l-block kernel (af_lblock64_kernel) takes the fast angular-first Q forms at K = 8 and 12 on kernel
-// path PATH_LBLOCK: one CTA per (l1 band, 8-cell group) with R_t and the f rows of bands l2 and l3
-// staged per l-triplet, from f packed per 8-cell group into the workspace, and the band's slices
-// handed to the warps one at a time.
+// The l-block kernels (af_lblock64_kernel, and af_lblock32_kernel for the FP32 forms) take the fast
+// angular-first Q forms at K = 8 and 12 on kernel path PATH_LBLOCK: one CTA per (l1 band, cell group:
+// 8 cells in FP64, 16 in FP32) with R_t and the f rows of bands l2 and l3 staged per l-triplet, from f
+// packed per cell group into the workspace, and the band's slices handed to the warps one at a time.
 //
 // The automatic order also takes it for the fast Q forms (plain and folded) at K = 12 from L = 8 on,
 // where the gather kernel is the other family (B200, ms per launch, l-block against gather, folded /
@@ -952,20 +956,20 @@ bool lblock_auto(const cf_plan* target) {
 }
 
 int run_lblock(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, void* ws, size_t ws_bytes,
-               cudaStream_t st) {
+               cudaStream_t st, bool f32) {
     const bool automatic = lblock_auto(target);
     if (target->path != cf::PATH_LBLOCK && !automatic) return kNoFew;
     if (target->k != 8 && target->k != 12)
         return fail(CF_EUNSUPPORTED, "the l-block kernel needs K = 8 or 12 (K = %d)", target->k);
     cf::SplitPlan* sp = nullptr;
     const int st_build = get_split(target, &sp);
-    if (st_build != CF_OK || (automatic && !cf::lblock_available(sp))) {
+    if (st_build != CF_OK || (automatic && !cf::lblock_available(sp, f32))) {
         if (!automatic) return st_build;
         g_last_error.clear();  // the automatic order goes on to the gather kernel
         return kNoFew;
     }
     int64_t launches = 0;
-    CF_TRY(cf::lblock64_run(sp, q_dev, f_dev, (double*)ws, ws_bytes, B, st, &launches));
+    CF_TRY(cf::lblock_run(sp, q_dev, f_dev, ws, ws_bytes, B, f32, st, &launches));
     g_launches += launches;
     if (launches > 0) {
         target->last_path = cf::PATH_LBLOCK;
@@ -1767,7 +1771,7 @@ __attribute__((visibility("hidden"))) bool cf_plan_band_pending(cf_plan* plan, i
     const bool band = plan->path == cf::PATH_BAND;
     const bool lblock = (plan->path == cf::PATH_LBLOCK && (plan->k == 8 || plan->k == 12)) ||
                         (plan->path == cf::PATH_AUTO && plan->k == 12 && plan->n_q >= 81);
-    if (!((f32 == 2 && (plan->k != 8 || band)) || (f32 == 0 && (band || lblock)))) return false;
+    if (!((f32 == 2 && (plan->k != 8 || band)) || (f32 == 0 && (band || lblock)) || (f32 == 1 && lblock))) return false;
     cf_plan* target = plan;
     if (sym) {
         std::lock_guard<std::mutex> lk(plan->sym_mu);

@@ -198,7 +198,7 @@ __host__ __device__ constexpr bool lblock_supported_k(int k) { return k == 8 || 
 // The l-block kernel's shared memory: the ring of stages (R_t of Shape<K, 8>, then at most max_rows
 // packed f rows of K x 8 doubles each), the band's Q rows of 8 cells, and the counter, done words, row
 // tickets, per-t item totals and stage assignments.
-inline Layout lblock_layout(int n_ring, int stage_bytes, int k, int max_rows, int max_t) {
+inline Layout lblock_layout(int n_ring, int stage_bytes, int k, int max_rows, int max_t, int cells) {
     Layout l{};
     int o = 0;
     auto take = [&](int bytes, int align) {
@@ -208,7 +208,7 @@ inline Layout lblock_layout(int n_ring, int stage_bytes, int k, int max_rows, in
         return r;
     };
     l.off_b = take(n_ring * stage_bytes, 1024);
-    l.off_red = take(max_rows * k * kLbCells * (int)sizeof(double), 16);
+    l.off_red = take(max_rows * k * cells * (int)sizeof(double), 16);
     l.off_bar = take(16 * (int)sizeof(uint64_t), 16);
     l.off_misc = take((2 + 2 * kLbMaxRing + max_rows + max_t) * (int)sizeof(int), 16);
     l.total = o;
@@ -801,10 +801,11 @@ __global__ void __launch_bounds__(W * 32, 1) af_band64_kernel(SplitArgs a) {
 // f cell-major [B][K][N_Q] -> packed [cg][q][k][C] (zero past the end of the batch).  One CTA per
 // (cell group, 32 rows q): the 8 cells' K x 32 block is read along q (coalesced) into shared memory
 // and written out as one contiguous run.
-template <int C>
-__global__ void __launch_bounds__(256) pack_cg_kernel(const double* __restrict__ f, double* __restrict__ pf,
+template <int C, typename T>
+__global__ void __launch_bounds__(256) pack_cg_kernel(const double* __restrict__ f, T* __restrict__ pf,
                                                       long long n_cells, int n_q, int K) {
-    extern __shared__ double tile[];  // [32][K][C]
+    extern __shared__ __align__(16) unsigned char tile_raw[];
+    T* tile = reinterpret_cast<T*>(tile_raw);  // [32][K][C]
     const int cg = blockIdx.y, q0 = blockIdx.x * 32;
     const int nq = min(32, n_q - q0);
     const long long M = (long long)n_q * K;
@@ -813,41 +814,63 @@ __global__ void __launch_bounds__(256) pack_cg_kernel(const double* __restrict__
         const long long cell = (long long)cg * C + c;
         double v = 0.0;
         if (qq < nq && cell < n_cells) v = __ldg(f + cell * M + (long long)k * n_q + q0 + qq);
-        tile[(qq * K + k) * C + c] = v;
+        tile[(qq * K + k) * C + c] = (T)v;
     }
     __syncthreads();
-    double* out = pf + ((long long)cg * n_q + q0) * K * C;
+    T* out = pf + ((long long)cg * n_q + q0) * K * C;
     for (int i = threadIdx.x; i < nq * K * C; i += blockDim.x) out[i] = tile[i];
 }
 
+// The lane layout of the l-block kernels: C cells per CTA, P = 32 / C lanes (parts) per cell, each
+// holding all K values of k2 and KQ = K / P values of k3 of the cell's Phi.  FP64 (C = 8): part p
+// owns k3 = p KQ .. p KQ + KQ - 1 (the packed rows k3 of the four parts fall on distinct banks);
+// FP32 (C = 16): part p owns k3 = p, p + 2, ... (blocked halves would put both half-warps' 32-bit
+// loads on the same 16 banks).  R_t per stage is [part][e = k2 KQ + y][k1] in T, 16 bytes of padding
+// after each part.
+template <int K, int C, typename T>
+struct LbShape {
+    static constexpr int P = 32 / C;
+    static constexpr int KH = K;
+    static constexpr int KQ = K / P;
+    static constexpr int E = KH * KQ;
+    static constexpr int PS = E * K + 16 / (int)sizeof(T);  // T words per part
+    static constexpr int RT_BYTES = P * PS * (int)sizeof(T);
+    static constexpr bool INTERLEAVED = sizeof(T) == 4;
+    __host__ __device__ static constexpr int k3_base(int p) { return INTERLEAVED ? p : p * KQ; }
+    static constexpr int K3_STEP = INTERLEAVED ? P : 1;
+    __host__ __device__ static constexpr int k3(int p, int y) { return k3_base(p) + y * K3_STEP; }
+};
+
 // Phi of one slot on a stage: rows of the stage are local (q2 - b2, q3 - b3), f at
 // fsg[(row K + k) C + cell]; grouped by q2 as slot_phi.
-template <int K, int C>
+template <int K, int C, typename T>
 __device__ __forceinline__ void slot_phi_staged(const double* __restrict__ gv, const uint32_t* __restrict__ eq23,
-                                                const double* __restrict__ fsg, const SlotEntries& se, int lane,
-                                                int c, int k2o, int k3o, int b2, int b3,
-                                                double (&phi)[Shape<K, C>::KH][Shape<K, C>::KQ]) {
-    constexpr int KH = Shape<K, C>::KH, KQ = Shape<K, C>::KQ;
+                                                const T* __restrict__ fsg, const SlotEntries& se, int lane,
+                                                int c, int part, int b2, int b3,
+                                                T (&phi)[LbShape<K, C, T>::KH][LbShape<K, C, T>::KQ]) {
+    using S = LbShape<K, C, T>;
+    constexpr int KH = S::KH, KQ = S::KQ;
+    const int k3o = S::k3_base(part);
 #pragma unroll
     for (int x = 0; x < KH; ++x)
 #pragma unroll
-        for (int y = 0; y < KQ; ++y) phi[x][y] = 0.0;
+        for (int y = 0; y < KQ; ++y) phi[x][y] = (T)0;
     const int cb = se.cb, ce = se.ce;
     if (cb >= ce) return;
-    double h[KQ];
+    T h[KQ];
 #pragma unroll
-    for (int y = 0; y < KQ; ++y) h[y] = 0.0;
+    for (int y = 0; y < KQ; ++y) h[y] = (T)0;
     int cur = -1;
     auto flush = [&]() {
-        const double* __restrict__ f2p = fsg + ((size_t)cur * K + k2o) * C + c;
+        const T* __restrict__ f2p = fsg + (size_t)cur * K * C + c;
 #pragma unroll
         for (int x = 0; x < KH; ++x) {
-            const double f2 = f2p[x * C];
+            const T f2 = f2p[x * C];
 #pragma unroll
             for (int y = 0; y < KQ; ++y) phi[x][y] = fma(f2, h[y], phi[x][y]);
         }
 #pragma unroll
-        for (int y = 0; y < KQ; ++y) h[y] = 0.0;
+        for (int y = 0; y < KQ; ++y) h[y] = (T)0;
     };
     for (int eb = cb; eb < ce; eb += 32) {
         const int nb = min(32, ce - eb);
@@ -863,15 +886,15 @@ __device__ __forceinline__ void slot_phi_staged(const double* __restrict__ gv, c
         }
         for (int j = 0; j < nb; ++j) {
             const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, j);
-            const double g = __shfl_sync(0xffffffffu, my_g, j);
+            const T g = (T)__shfl_sync(0xffffffffu, my_g, j);
             const int q2 = (int)(q23 & 0xffffu) - b2, q3 = (int)(q23 >> 16) - b3;
             if (q2 != cur) {
                 if (cur >= 0) flush();
                 cur = q2;
             }
-            const double* __restrict__ f3p = fsg + ((size_t)q3 * K + k3o) * C + c;
+            const T* __restrict__ f3p = fsg + ((size_t)q3 * K + k3o) * C + c;
 #pragma unroll
-            for (int y = 0; y < KQ; ++y) h[y] = fma(g, f3p[y * C], h[y]);
+            for (int y = 0; y < KQ; ++y) h[y] = fma(g, f3p[y * S::K3_STEP * C], h[y]);
         }
     }
     if (cur >= 0) flush();
@@ -880,11 +903,11 @@ __device__ __forceinline__ void slot_phi_staged(const double* __restrict__ gv, c
 enum { LBI_TR = 0, LBI_ORD, LBI_BEGIN, LBI_END };  // item: t | row << 16, ord | l2 << 16 | l3 << 24, entries
 enum { LBU_L1 = 0, LBU_BROWS, LBU_TLOFF, LBU_NT, LBU_ITOFF, LBU_NIT, LBU_INTS = 8 };
 
-template <int K, int C, int W>
-__global__ void __launch_bounds__(W * 32, 1) af_lblock64_kernel(SplitArgs a) {
-    using S = Shape<K, C>;
+template <int K, int C, typename T, int W>
+__device__ __forceinline__ void lblock_body(const SplitArgs& a) {
+    using S = LbShape<K, C, T>;
     constexpr int KH = S::KH, KQ = S::KQ, PS = S::PS, RTB = S::RT_BYTES;
-    constexpr int ROWB = K * C * (int)sizeof(double);
+    constexpr int ROWB = K * C * (int)sizeof(T);
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* ring = smem + a.off_b;
     double* qacc = reinterpret_cast<double*>(smem + a.off_red);  // [brows][K][C]
@@ -901,8 +924,8 @@ __global__ void __launch_bounds__(W * 32, 1) af_lblock64_kernel(SplitArgs a) {
     // current one returns at once.  So an item first waits for its stage to be assigned ti.
     volatile int* stage_ti = misc + 2 + kLbMaxRing + a.max_rows + a.max_t;
 
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int c = lane % C, part = lane / C, k2o = S::k2_of(part), k3o = S::k3_of(part);
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int c = lane % C, part = lane / C;
     const int NQ = a.n_q, M = NQ * K, D = a.n_ring;
     const int unit = a.unit_order[blockIdx.x / a.n_cg];
     const int cg = blockIdx.x % a.n_cg;
@@ -910,7 +933,8 @@ __global__ void __launch_bounds__(W * 32, 1) af_lblock64_kernel(SplitArgs a) {
     const int l1 = u[LBU_L1], brows = u[LBU_BROWS], tl_off = u[LBU_TLOFF], n_t = u[LBU_NT], it_off = u[LBU_ITOFF],
               n_it = u[LBU_NIT];
     const long long cell0 = (long long)cg * C;
-    const double* __restrict__ pcg = a.pf + (size_t)cg * M * C;
+    const T* __restrict__ pcg = reinterpret_cast<const T*>(a.pf) + (size_t)cg * M * C;
+    const T* __restrict__ rsrc = reinterpret_cast<const T*>(a.rfp64);
     const int4* __restrict__ items = a.items + it_off;
 
     auto issue = [&](int ti, int sb) {
@@ -919,7 +943,7 @@ __global__ void __launch_bounds__(W * 32, 1) af_lblock64_kernel(SplitArgs a) {
         const uint32_t fb2 = (uint32_t)((2 * l2 + 1) * ROWB), fb3 = l3 != l2 ? (uint32_t)((2 * l3 + 1) * ROWB) : 0u;
         unsigned char* st = ring + (size_t)sb * a.stage_bytes;
         tc05::mbar_arrive_expect_tx(&bfull[sb], (uint32_t)RTB + fb2 + fb3);
-        tc05::bulk_g2s(st, a.rfp64 + (size_t)t * (RTB / 8), (uint32_t)RTB, &bfull[sb]);
+        tc05::bulk_g2s(st, rsrc + (size_t)t * (RTB / sizeof(T)), (uint32_t)RTB, &bfull[sb]);
         tc05::bulk_g2s(st + RTB, pcg + (size_t)l2 * l2 * K * C, fb2, &bfull[sb]);
         if (fb3) tc05::bulk_g2s(st + RTB + fb2, pcg + (size_t)l3 * l3 * K * C, fb3, &bfull[sb]);
     };
@@ -982,24 +1006,35 @@ __global__ void __launch_bounds__(W * 32, 1) af_lblock64_kernel(SplitArgs a) {
         if (ok) {
             const unsigned char* st = ring + (size_t)sb * a.stage_bytes;
             const int b2 = l2 * l2, b3 = l3 * l3 - (l3 != l2 ? 2 * l2 + 1 : 0);
-            double acc[K];
+            T acc[K];
             {
-                double phi[KH][KQ];
-                slot_phi_staged<K, C>(a.e_g, a.e_q23, reinterpret_cast<const double*>(st + RTB), se, lane, c, k2o,
-                                      k3o, b2, b3, phi);
-                const double* rp = reinterpret_cast<const double*>(st) + part * PS;
+                T phi[KH][KQ];
+                slot_phi_staged<K, C, T>(a.e_g, a.e_q23, reinterpret_cast<const T*>(st + RTB), se, lane, c, part, b2,
+                                         b3, phi);
+                const T* rp = reinterpret_cast<const T*>(st) + part * PS;
 #pragma unroll
-                for (int k1 = 0; k1 < K; ++k1) acc[k1] = 0.0;
+                for (int k1 = 0; k1 < K; ++k1) acc[k1] = (T)0;
 #pragma unroll
                 for (int x = 0; x < KH; ++x)
 #pragma unroll
                     for (int y = 0; y < KQ; ++y) {
-                        const double2* r2 = reinterpret_cast<const double2*>(rp + (x * KQ + y) * K);
+                        const T* rr = rp + (x * KQ + y) * K;
+                        if constexpr (sizeof(T) == 8) {
 #pragma unroll
-                        for (int j = 0; j < K / 2; ++j) {
-                            const double2 r = r2[j];
-                            acc[2 * j] = fma(r.x, phi[x][y], acc[2 * j]);
-                            acc[2 * j + 1] = fma(r.y, phi[x][y], acc[2 * j + 1]);
+                            for (int j = 0; j < K / 2; ++j) {
+                                const double2 r = reinterpret_cast<const double2*>(rr)[j];
+                                acc[2 * j] = fma((T)r.x, phi[x][y], acc[2 * j]);
+                                acc[2 * j + 1] = fma((T)r.y, phi[x][y], acc[2 * j + 1]);
+                            }
+                        } else {
+#pragma unroll
+                            for (int j = 0; j < K / 4; ++j) {
+                                const float4 r = reinterpret_cast<const float4*>(rr)[j];
+                                acc[4 * j] = fma((T)r.x, phi[x][y], acc[4 * j]);
+                                acc[4 * j + 1] = fma((T)r.y, phi[x][y], acc[4 * j + 1]);
+                                acc[4 * j + 2] = fma((T)r.z, phi[x][y], acc[4 * j + 2]);
+                                acc[4 * j + 3] = fma((T)r.w, phi[x][y], acc[4 * j + 3]);
+                            }
                         }
                     }
             }
@@ -1028,7 +1063,7 @@ __global__ void __launch_bounds__(W * 32, 1) af_lblock64_kernel(SplitArgs a) {
                 constexpr int KP = K / (32 / C);  // k1 per part
 #pragma unroll
                 for (int k1 = 0; k1 < K; ++k1)
-                    if (k1 / KP == part) qr[k1 * C] += acc[k1];
+                    if (k1 / KP == part) qr[k1 * C] += (double)acc[k1];
             }
             __syncwarp();
             if (lane == 0) {
@@ -1060,6 +1095,17 @@ __global__ void __launch_bounds__(W * 32, 1) af_lblock64_kernel(SplitArgs a) {
         const long long cell = cell0 + cc;
         if (cell < a.n_cells) a.q[cell * M + (size_t)k1 * NQ + l1 * l1 + r] += qacc[i];
     }
+}
+
+// FP64: 8 cells per CTA.  FP32 (the FP32 forms: f, Phi and the K^3 step in FP32, each item's result
+// added into the FP64 Q rows): 16 cells per CTA, the same shared memory.
+template <int K>
+__global__ void __launch_bounds__(kLbWarps * 32, 1) af_lblock64_kernel(SplitArgs a) {
+    lblock_body<K, kLbCells, double, kLbWarps>(a);
+}
+template <int K>
+__global__ void __launch_bounds__(kLbWarps * 32, 1) af_lblock32_kernel(SplitArgs a) {
+    lblock_body<K, 2 * kLbCells, float, kLbWarps>(a);
 }
 
 // The BF16-split band kernel (CF_FORM_AF_SYM_BF16 / CF_FORM_AF_BF16 where the warp-level BF16 kernel
@@ -1357,7 +1403,10 @@ struct SplitPlan {
     int* d_t_l23 = nullptr;           // per l-triplet: l2 | l3 << 8
     // the l-block kernel (0 bands: unsupported)
     int lb_bands = 0, lb_rows = 0, lb_t = 0;  // bands, rows of the largest band, longest t-list
-    int lb_ring = 0, lb_stage = 0;    // stages in the ring, bytes per stage
+    int lb_ring = 0, lb_stage = 0;    // stages in the ring, bytes per stage (FP64, 8 cells per CTA)
+    int lb32_ring = 0, lb32_stage = 0;  // the same for the FP32 forms (16 cells per CTA)
+    float* d_rfl32 = nullptr;         // FP32 R_t as [part][e][k1] for 16 cells per CTA
+    Layout laylb32{};
     int* d_lb_units = nullptr;        // per band: LBU_INTS ints
     int* d_lb_order = nullptr;        // bands, heaviest first
     int4* d_lb_items = nullptr;       // per band: its (t, row) slices in t-major order
@@ -1515,19 +1564,25 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
                     rfp64[((size_t)t * S::P + pp) * S::PS + (size_t)e * K + k1] =
                         R[(size_t)t * K * K * K + k1 + (size_t)K * k2 + (size_t)K * K * k3];
             }
-    // the l-block kernel's FP64 R_t (the layout of Shape<K, 8>)
+    // the l-block kernels' R_t: FP64 for 8 cells per CTA, FP32 for 16 (LbShape)
     std::vector<double> rfl;
+    std::vector<float> rfl32;
     if constexpr (lblock_supported_k(K)) {
-        using S8 = Shape<K, kLbCells>;
-        rfl.assign((size_t)NL * S8::P * S8::PS, 0.0);
-        for (int t = 0; t < NL; ++t)
-            for (int pp = 0; pp < S8::P; ++pp)
-                for (int e = 0; e < S8::E; ++e) {
-                    const int k2 = S8::k2_of(pp) + e / S8::KQ, k3 = S8::k3_of(pp) + e % S8::KQ;
-                    for (int k1 = 0; k1 < K; ++k1)
-                        rfl[((size_t)t * S8::P + pp) * S8::PS + (size_t)e * K + k1] =
-                            R[(size_t)t * K * K * K + k1 + (size_t)K * k2 + (size_t)K * K * k3];
-                }
+        auto fill = [&](auto shape, auto& out) {
+            using S8 = decltype(shape);
+            out.assign((size_t)NL * S8::P * S8::PS, 0);
+            for (int t = 0; t < NL; ++t)
+                for (int pp = 0; pp < S8::P; ++pp)
+                    for (int e = 0; e < S8::E; ++e) {
+                        const int k2 = e / S8::KQ, k3 = S8::k3(pp, e % S8::KQ);
+                        for (int k1 = 0; k1 < K; ++k1)
+                            out[((size_t)t * S8::P + pp) * S8::PS + (size_t)e * K + k1] =
+                                (typename std::decay_t<decltype(out)>::value_type)R[(size_t)t * K * K * K + k1 +
+                                                                                   (size_t)K * k2 + (size_t)K * K * k3];
+                    }
+        };
+        fill(LbShape<K, kLbCells, double>{}, rfl);
+        fill(LbShape<K, 2 * kLbCells, float>{}, rfl32);
     }
     // G / s_t per entry, |G / s_t| summed per slice, (l2, l3) per t
     std::vector<double> e_gs(n_g), gs(n_slices, 0.0);
@@ -1690,15 +1745,24 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
             const int l2 = t_l23[t] & 0xff, l3 = t_l23[t] >> 8;
             max_rows = std::max(max_rows, 2 * l2 + 1 + (l3 != l2 ? 2 * l3 + 1 : 0));
         }
-        const int stage = (Shape<K, kLbCells>::RT_BYTES + max_rows * K * kLbCells * (int)sizeof(double) + 127) / 128 * 128;
-        int ring = kLbMaxRing;
-        while (ring >= 2 && lblock_layout(ring, stage, K, lb_rows, lb_t).total > optin) --ring;
+        // FP64, 8 cells; FP32, 16 cells: the same bytes per f row
+        const int stage = (LbShape<K, kLbCells, double>::RT_BYTES + max_rows * K * kLbCells * (int)sizeof(double) + 127) /
+                          128 * 128;
+        const int stage32 =
+            (LbShape<K, 2 * kLbCells, float>::RT_BYTES + max_rows * K * 2 * kLbCells * (int)sizeof(float) + 127) / 128 *
+            128;
+        int ring = kLbMaxRing, ring32 = kLbMaxRing;
+        while (ring >= 2 && lblock_layout(ring, stage, K, lb_rows, lb_t, kLbCells).total > optin) --ring;
+        while (ring32 >= 2 && lblock_layout(ring32, stage32, K, lb_rows, lb_t, 2 * kLbCells).total > optin) --ring32;
         if (ring >= 2) {
             sp->lb_ring = ring;
             sp->lb_stage = stage;
-            sp->laylb = lblock_layout(ring, stage, K, lb_rows, lb_t);
-        } else {
-            sp->lb_bands = 0;
+            sp->laylb = lblock_layout(ring, stage, K, lb_rows, lb_t, kLbCells);
+        }
+        if (ring32 >= 2) {
+            sp->lb32_ring = ring32;
+            sp->lb32_stage = stage32;
+            sp->laylb32 = lblock_layout(ring32, stage32, K, lb_rows, lb_t, 2 * kLbCells);
         }
     }
     sp->laybf = bf16_layout<K, C>(NQ);
@@ -1721,6 +1785,7 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
         (ce = upload_vec(&sp->d_rbf, rbf, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_rbf8, rbf8, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_rfl, rfl, bytes)) != cudaSuccess ||
+        (ce = upload_vec(&sp->d_rfl32, rfl32, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_lb_units, units_lb, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_lb_order, order_lb, bytes)) != cudaSuccess ||
         (ce = upload_vec(&sp->d_lb_items, items_lb, bytes)) != cudaSuccess ||
@@ -1826,21 +1891,25 @@ int run64_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     return CF_OK;
 }
 
-// Bytes of the packed f that the l-block kernel reads: [ceil(B / 8)][N_Q][K][8] doubles.
-size_t lblock_pack_bytes_of(int n_q, int k, int64_t B) {
-    return (size_t)((B + kLbCells - 1) / kLbCells) * (size_t)n_q * k * kLbCells * sizeof(double);
+// Bytes of the packed f that the l-block kernels read: [ceil(B / C)][N_Q][K][C] of T.
+size_t lblock_pack_bytes_of(int n_q, int k, int64_t B, bool f32) {
+    const int C = f32 ? 2 * kLbCells : kLbCells;
+    return (size_t)((B + C - 1) / C) * (size_t)n_q * k * C * (f32 ? sizeof(float) : sizeof(double));
 }
 
-template <int K>
-int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf, int64_t B, cudaStream_t st,
-                int64_t* launches) {
-    constexpr int C = kLbCells, W = kLbWarps;
+template <int K, typename T>
+int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, int64_t B, cudaStream_t st,
+               int64_t* launches) {
+    constexpr bool F32 = sizeof(T) == 4;
+    constexpr int C = F32 ? 2 * kLbCells : kLbCells, W = kLbWarps;
+    auto kern = F32 ? (void (*)(SplitArgs))af_lblock32_kernel<K> : (void (*)(SplitArgs))af_lblock64_kernel<K>;
+    const Layout& lay = F32 ? sp->laylb32 : sp->laylb;
     static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-        const cudaError_t e = cudaFuncSetAttribute(af_lblock64_kernel<K, C, W>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+        const cudaError_t e = cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   227 * 1024);
         if (e != cudaSuccess)
             return fail_split(CF_ECUDA, std::string("l-block kernel: smem attribute: ") + cudaGetErrorString(e));
         attr_set[dev] = true;
@@ -1849,8 +1918,8 @@ int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf
     if (n_cg > 65535LL || (long long)sp->lb_bands * n_cg > 0x7fffffffLL)
         return fail_split(CF_ESHAPE, "l-block kernel: batch too large for one launch");
     dim3 pgrid((unsigned)((sp->n_q + 31) / 32), (unsigned)n_cg);
-    static_assert(32 * K * C * 8 <= 48 * 1024, "the pack kernel's tile fits the default shared memory");
-    pack_cg_kernel<C><<<pgrid, 256, 32 * K * C * 8, st>>>(f_cm, pf, B, sp->n_q, K);
+    static_assert(32 * K * C * sizeof(T) <= 48 * 1024, "the pack kernel's tile fits the default shared memory");
+    pack_cg_kernel<C, T><<<pgrid, 256, 32 * K * C * sizeof(T), st>>>(f_cm, static_cast<T*>(pf), B, sp->n_q, K);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("l-block pack: launch: ") + cudaGetErrorString(e));
     if (launches) ++*launches;
@@ -1858,13 +1927,13 @@ int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf
     a.slice_e = sp->slice_e;
     a.e_q23 = sp->e_q23;
     a.e_g = sp->e_g;
-    a.rfp64 = sp->d_rfl;
+    a.rfp64 = F32 ? reinterpret_cast<const double*>(sp->d_rfl32) : sp->d_rfl;  // read as T by the kernel
     a.units = sp->d_lb_units;
     a.unit_order = sp->d_lb_order;
     a.band_tl = sp->d_band_tl;
     a.items = sp->d_lb_items;
     a.t_items = sp->d_lb_titems;
-    a.pf = pf;
+    a.pf = static_cast<const double*>(pf);  // read as T by the kernel
     a.t_l23 = sp->d_t_l23;
     a.q = q_cm;
     a.err = sp->d_err;
@@ -1872,16 +1941,16 @@ int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf
     a.n_cg = (int)n_cg;
     a.n_q = sp->n_q;
     a.L = sp->L;
-    a.n_ring = sp->lb_ring;
-    a.stage_bytes = sp->lb_stage;
+    a.n_ring = F32 ? sp->lb32_ring : sp->lb_ring;
+    a.stage_bytes = F32 ? sp->lb32_stage : sp->lb_stage;
     a.max_rows = sp->lb_rows;
     a.max_t = sp->lb_t;
-    a.off_b = sp->laylb.off_b;
-    a.off_red = sp->laylb.off_red;
-    a.off_bar = sp->laylb.off_bar;
-    a.off_misc = sp->laylb.off_misc;
+    a.off_b = lay.off_b;
+    a.off_red = lay.off_red;
+    a.off_bar = lay.off_bar;
+    a.off_misc = lay.off_misc;
     const long long blocks = (long long)sp->lb_bands * n_cg;
-    af_lblock64_kernel<K, C, W><<<(unsigned)blocks, W * 32, sp->laylb.total, st>>>(a);
+    kern<<<(unsigned)blocks, W * 32, lay.total, st>>>(a);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("l-block kernel: launch: ") + cudaGetErrorString(e));
     if (launches) ++*launches;
@@ -1968,18 +2037,24 @@ int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
     }
 }
 
-size_t lblock_pack_bytes(const SplitPlan* sp, int64_t B) { return lblock_pack_bytes_of(sp->n_q, sp->k, B); }
+size_t lblock_pack_bytes(const SplitPlan* sp, int64_t B, bool f32) { return lblock_pack_bytes_of(sp->n_q, sp->k, B, f32); }
 
-bool lblock_available(const SplitPlan* sp) { return sp && lblock_supported_k(sp->k) && sp->lb_bands > 0; }
+bool lblock_available(const SplitPlan* sp, bool f32) {
+    return sp && lblock_supported_k(sp->k) && sp->lb_bands > 0 && (f32 ? sp->lb32_ring : sp->lb_ring) >= 2;
+}
 
-int lblock64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf, size_t pf_bytes, int64_t B,
-                 cudaStream_t st, int64_t* launches) {
+int lblock_run(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, size_t pf_bytes, int64_t B, bool f32,
+               cudaStream_t st, int64_t* launches) {
     if (B <= 0) return CF_OK;
-    if (!lblock_available(sp))
+    if (!lblock_available(sp, f32))
         return fail_split(CF_EUNSUPPORTED, "l-block kernel: needs K = 8 or 12 and two stages of shared memory");
-    if (pf_bytes < lblock_pack_bytes(sp, B)) return fail_split(CF_EINVAL, "l-block kernel: packed-f workspace too small");
-    return sp->k == 8 ? runlb_impl<8>(sp, q_cm, f_cm, pf, B, st, launches)
-                      : runlb_impl<12>(sp, q_cm, f_cm, pf, B, st, launches);
+    if (pf_bytes < lblock_pack_bytes(sp, B, f32))
+        return fail_split(CF_EINVAL, "l-block kernel: packed-f workspace too small");
+    if (f32)
+        return sp->k == 8 ? runlb_impl<8, float>(sp, q_cm, f_cm, pf, B, st, launches)
+                          : runlb_impl<12, float>(sp, q_cm, f_cm, pf, B, st, launches);
+    return sp->k == 8 ? runlb_impl<8, double>(sp, q_cm, f_cm, pf, B, st, launches)
+                      : runlb_impl<12, double>(sp, q_cm, f_cm, pf, B, st, launches);
 }
 
 int split_build(SplitPlan** out, const DevOp& folded, int64_t n_g, int64_t n_slices, int device) {
@@ -2023,7 +2098,7 @@ void split_destroy(SplitPlan* sp) {
     if (!sp) return;
     void* ptrs[] = {sp->d_rplanes, sp->d_e_gs, sp->d_rb_off, sp->d_rb_gs, sp->d_rb_l23, sp->d_units, sp->d_unit_order, sp->d_band_tl,
                     sp->d_band_rng, sp->d_err, sp->d_rfp64, sp->d_rbf, sp->d_units64, sp->d_unit_order64,
-                    sp->d_rbf8, sp->d_rfl, sp->d_t_l23, sp->d_lb_units, sp->d_lb_order, sp->d_lb_items,
+                    sp->d_rbf8, sp->d_rfl, sp->d_rfl32, sp->d_t_l23, sp->d_lb_units, sp->d_lb_order, sp->d_lb_items,
                     sp->d_lb_titems};
     for (void* p : ptrs)
         if (p) cudaFree(p);

@@ -32,14 +32,15 @@ int band64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B,
 // shared memory does not fit.  No allocation, no synchronisation.
 int bf16_band_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t B, cudaStream_t st,
                   int64_t* launches);
-// The l-block kernel (K = 8 and 12): one CTA per (l1 band, 8-cell group), R_t and the f rows of bands
-// l2 and l3 staged per l-triplet by bulk copies, the band's (t, row) slices taken by the warps one at
-// a time and summed per row in t order.  pf is a device workspace of at least lblock_pack_bytes(sp, B)
-// bytes for the packed f.  No allocation, no synchronisation.
-int lblock64_run(const SplitPlan* sp, double* q_cm, const double* f_cm, double* pf, size_t pf_bytes, int64_t B,
-                 cudaStream_t st, int64_t* launches);
-size_t lblock_pack_bytes(const SplitPlan* sp, int64_t B);
-bool lblock_available(const SplitPlan* sp);
+// The l-block kernels (K = 8 and 12): one CTA per (l1 band, cell group) -- 8 cells in FP64, 16 in the
+// FP32 forms -- with R_t and the f rows of bands l2 and l3 staged per l-triplet by bulk copies, the
+// band's (t, row) slices taken by the warps one at a time and summed per row in t order into FP64 Q.
+// pf is a device workspace of at least lblock_pack_bytes(sp, B, f32) bytes for the packed f.  No
+// allocation, no synchronisation.
+int lblock_run(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, size_t pf_bytes, int64_t B, bool f32,
+               cudaStream_t st, int64_t* launches);
+size_t lblock_pack_bytes(const SplitPlan* sp, int64_t B, bool f32);
+bool lblock_available(const SplitPlan* sp, bool f32);
 // After the stream has been synchronised: CF_ETIMEOUT (and the flag cleared) if a CTA of an
 // earlier launch gave up a bounded wait, else CF_OK.
 int split_check(const SplitPlan* sp);

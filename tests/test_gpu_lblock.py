@@ -155,3 +155,32 @@ def test_lblock_kernel_refuses_other_k(cuda_available):
         _device_q(op, cells, "af_sym")
     assert e.value.status == cf_b200._lib.CF_EUNSUPPORTED
     op.close()
+
+
+@pytest.mark.parametrize("L,K,B", [(6, 12, 37), (10, 8, 21), (16, 12, 19)])
+def test_lblock_fp32_forms_vs_oracle(L, K, B, cuda_available, oracle_lib):
+    """The FP32 forms on the l-block kernel (16 cells per CTA; f, Phi and the K^3 step in FP32, each
+    slice's result added into FP64 Q): within 1e-5 per cell of the oracle (FP32 arithmetic), the
+    invariant entries exactly zero, two runs bit for bit equal."""
+    import cf_b200
+    from cf_b200 import workloads
+
+    R = None
+    if (L, K) == (10, 8):
+        R = np.load(GOLDEN / "R_hs_k7_l10_pad20.npy")
+    if (L, K) == (16, 12):
+        R = np.load(GOLDEN / "R_hs_k11_l16_pad20.npy")
+    geo, R = _setup(L, K, R, seed=L * K)
+    cells = workloads.bimaxwellian_cells(K, L, B, seed=5) if L == 16 else workloads.maxwellian_cells(K, L, B, seed=5)
+    ref = _oracle(geo, R, K, cells, oracle_lib)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+    op.set_kernel_path("lblock")
+    for form in ("af_f32", "af_sym_f32"):
+        Q = _device_q(op, cells, form)
+        assert op.info()["last_path"] == PATH_LBLOCK, form
+        err = per_cell_err(Q, ref)
+        assert 1e-12 < err <= 1e-5, (form, err)
+        inv = Q.reshape(B, -1)[:, [0, 1, 2, 3, geo.n_q]]
+        assert np.all(inv == 0.0), form
+        assert np.array_equal(_device_q(op, cells, form), Q), form
+    op.close()
