@@ -799,25 +799,27 @@ __global__ void __launch_bounds__(W * 32, 1) af_band64_kernel(SplitArgs a) {
 // of t-list position ti is refilled with ti + n_ring by the warp that finishes the last item of ti.
 
 // f cell-major [B][K][N_Q] -> packed [cg][q][k][C] (zero past the end of the batch).  One CTA per
-// (cell group, 32 rows q): the 8 cells' K x 32 block is read along q (coalesced) into shared memory
-// and written out as one contiguous run.
+// (cell group, 32 rows q), in a one-dimensional grid: the C cells' K x 32 block is read along q
+// (coalesced) into shared memory and written out as one contiguous run.
 template <int C, typename T>
 __global__ void __launch_bounds__(256) pack_cg_kernel(const double* __restrict__ f, T* __restrict__ pf,
                                                       long long n_cells, int n_q, int K) {
     extern __shared__ __align__(16) unsigned char tile_raw[];
     T* tile = reinterpret_cast<T*>(tile_raw);  // [32][K][C]
-    const int cg = blockIdx.y, q0 = blockIdx.x * 32;
+    const int nqb = (n_q + 31) / 32;
+    const long long cg = (long long)blockIdx.x / nqb;
+    const int q0 = (int)(blockIdx.x % nqb) * 32;
     const int nq = min(32, n_q - q0);
     const long long M = (long long)n_q * K;
     for (int i = threadIdx.x; i < 32 * K * C; i += blockDim.x) {
         const int qq = i % 32, k = (i / 32) % K, c = i / (32 * K);
-        const long long cell = (long long)cg * C + c;
+        const long long cell = cg * C + c;
         double v = 0.0;
         if (qq < nq && cell < n_cells) v = __ldg(f + cell * M + (long long)k * n_q + q0 + qq);
         tile[(qq * K + k) * C + c] = (T)v;
     }
     __syncthreads();
-    T* out = pf + ((long long)cg * n_q + q0) * K * C;
+    T* out = pf + (cg * n_q + q0) * K * C;
     for (int i = threadIdx.x; i < nq * K * C; i += blockDim.x) out[i] = tile[i];
 }
 
@@ -1915,9 +1917,10 @@ int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, 
         attr_set[dev] = true;
     }
     const long long n_cg = (B + C - 1) / C;
-    if (n_cg > 65535LL || (long long)sp->lb_bands * n_cg > 0x7fffffffLL)
+    const long long pblocks = n_cg * ((sp->n_q + 31) / 32);
+    if (pblocks > 0x7fffffffLL || (long long)sp->lb_bands * n_cg > 0x7fffffffLL)
         return fail_split(CF_ESHAPE, "l-block kernel: batch too large for one launch");
-    dim3 pgrid((unsigned)((sp->n_q + 31) / 32), (unsigned)n_cg);
+    const unsigned pgrid = (unsigned)pblocks;
     static_assert(32 * K * C * sizeof(T) <= 48 * 1024, "the pack kernel's tile fits the default shared memory");
     pack_cg_kernel<C, T><<<pgrid, 256, 32 * K * C * sizeof(T), st>>>(f_cm, static_cast<T*>(pf), B, sp->n_q, K);
     cudaError_t e = cudaGetLastError();
