@@ -37,6 +37,48 @@ def _stream_handle(stream) -> int | None:
     return int(getattr(stream, "cuda_stream", stream))
 
 
+# Kernel paths the single-operator autotuner times by default ('auto': the library's measured order).
+AUTOTUNE_PATHS = ("auto", "tile", "pair", "gather", "band", "lblock")
+
+
+def choose_fastest(times: dict) -> str:
+    """The candidate with the smallest time; ties go to the earlier candidate (dicts keep order)."""
+    return min(times, key=lambda k: (times[k], list(times).index(k)))
+
+
+def _autotune_cache_path():
+    import os
+    from pathlib import Path
+
+    root = os.environ.get("CF_B200_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "cf_b200")
+    return Path(root) / "kernel_autotune.json"
+
+
+def _autotune_key(op, B: int, form: str, candidates) -> str:
+    import json
+
+    import torch
+
+    dev = torch.cuda.get_device_name(op.device) if torch.cuda.is_available() else "none"
+    sig = [dev, _lib.version(), op.N_Q, op.K, op.n_g, op.n_l, op.content_digest(), int(B), form, list(candidates)]
+    return hashlib.sha256(json.dumps(sig).encode()).hexdigest()[:32]
+
+
+def _time_device(fn, reps: int) -> float:
+    """Best of `reps` CUDA-event timings of fn() on the current stream, in seconds."""
+    import torch
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = float("inf")
+    for _ in range(max(1, int(reps))):
+        e0.record()
+        fn()
+        e1.record()
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1) * 1e-3)
+    return best
+
+
 class CollisionOperator:
     """Q(f) and J(f).v for batches of cells, on the GPU.
 
@@ -124,6 +166,60 @@ class CollisionOperator:
         code = {"auto": 0, "gather": 1, "tile": 2, "pair": 3, "pair_l1": 4, "pair_split": 5, "tile_mma": 6,
                 "band": 11, "lblock": 14}[path]
         _lib.check(_lib.load().cf_plan_set_kernel_path(self._h, code))
+
+    def autotune(self, B: int, form: str = "af_sym", candidates=AUTOTUNE_PATHS, reps: int = 5,
+                 use_cache: bool = True, seed: int = 0):
+        """Pick this operator's kernel family for batches of B cells in `form` by timing every candidate.
+
+        Each candidate path ('auto' is the library's own measured order) runs `form` on B seeded cells
+        on the device; a path that does not fit this operator (CF_EUNSUPPORTED) is skipped; the fastest
+        is set with set_kernel_path and returned with the timings.  The choice applies to every form
+        of the operator (the plan has one kernel path), so tune for the form that dominates.  Choices
+        are cached in a JSON file (CF_B200_CACHE, else ~/.cache/cf_b200) keyed by the device, the
+        library version, the operator's content digest, B, the form and the candidates.
+        """
+        import json
+
+        import torch
+
+        key = _autotune_key(self, int(B), form, candidates)
+        path = _autotune_cache_path()
+        if use_cache and path.exists():
+            try:
+                hit = json.loads(path.read_text()).get(key)
+                if hit:
+                    self.set_kernel_path(hit["path"])
+                    return hit["path"], dict(hit["report"], cached=True)
+            except (OSError, ValueError):
+                pass
+        rng = np.random.default_rng(seed)
+        f = torch.from_numpy(1e-2 * rng.standard_normal((int(B), self.K, self.N_Q))).cuda(self.device)
+        out = torch.zeros_like(f)
+        times = {}
+        for cand in candidates:
+            try:
+                self.set_kernel_path(cand)
+                self.q(f, out=out, form=form)  # builds what the path needs, outside the timing
+                torch.cuda.synchronize(self.device)
+            except _lib.CFError as e:
+                if e.status != _lib.CF_EUNSUPPORTED:
+                    raise
+                continue
+            times[cand] = _time_device(lambda: self.q(f, out=out, form=form), reps)
+        if not times:
+            raise _lib.CFError(_lib.CF_EUNSUPPORTED, f"no kernel path runs form {form!r} for this operator")
+        best = choose_fastest(times)
+        self.set_kernel_path(best)
+        report = {"seconds": times, "B": int(B), "form": form, "cached": False}
+        if use_cache:
+            try:
+                path.parent.mkdir(parents=True, exist_ok=True)
+                data = json.loads(path.read_text()) if path.exists() else {}
+                data[key] = {"path": best, "report": report}
+                path.write_text(json.dumps(data, indent=1))
+            except (OSError, ValueError):
+                pass
+        return best, report
 
     def stream_selftest(self, wait_seconds: float = 1e-3) -> int:
         """Run the streamed host path's bounded-wait self-test; returns the status (CF_ETIMEOUT = 9

@@ -64,3 +64,4 @@ def test_two_gloo_ranks(tmp_path):
         assert r["shape"] == [64, 4, 25]
     assert res[0]["cells_digest"] != res[1]["cells_digest"]  # different shards
     assert res[1]["ref"] is None  # non-zero ranks of the reference arm exit without work
+
