@@ -117,3 +117,32 @@ def test_autotune_chooses_and_caches(cuda_available, tmp_path, monkeypatch):
     assert rep["step_seconds"][f"{family}/{tail}"] == min(rep["step_seconds"].values())
     forms2, tail2, family2, rep2 = ragged.autotune(ops, [64, 48], reps=2)
     assert rep2["cached"] and forms2 == forms and tail2 == tail and family2 == family
+
+
+
+def test_ragged_bucket_beyond_k8_with_graph(cuda_available, oracle_lib):
+    """A K = 12 bucket (L = 8) runs on its own plan's kernel on the tiled buffers beside the fused launch
+    (the gather kernel): eager and two graph replays give the same bits, equal to that plan's gather
+    kernel and within 1e-12 of the oracle."""
+    import torch
+
+    from cf_b200.ragged import RaggedBatch
+
+    buckets, cells = [(4, 4), (8, 12)], [41, 19]
+    ops = _bucket_ops(buckets, seed=11)
+    fs = _cells(buckets, cells)
+    rb = RaggedBatch([o for _, _, o in ops], cells, forms=["af_sym", "af_sym"], tail_split=4, family="tile")
+    qs = [torch.zeros_like(f) for f in fs]
+    rb.q(fs, qs)
+    torch.cuda.synchronize()
+    geo, R, op = ops[1]
+    op.set_kernel_path("gather")
+    assert torch.equal(qs[1], op.q(fs[1], form="af_sym"))
+    for (g, Rb, _), f, q, (L, K) in zip(ops, fs, qs, buckets):
+        assert per_cell_err(q.cpu().numpy(), _oracle_q(oracle_lib, g, Rb, K, f)) <= 1e-12
+    for _ in range(2):
+        qg = [torch.zeros_like(f) for f in fs]
+        rb.q_graph(fs, qg)
+        torch.cuda.synchronize()
+        assert all(torch.equal(a, b) for a, b in zip(qg, qs))
+    rb.close()
