@@ -33,6 +33,7 @@ EXPORTS = [
     "cf_angular_first", "cf_radial_first", "cf_contract_host", "cf_time_contract_host", "cf_jacobian_apply_host",
     "cf_plan_create", "cf_plan_destroy", "cf_plan_get_info", "cf_plan_workspace_size",
     "cf_q_device", "cf_q_device_ws", "cf_jv_device", "cf_q_device_noalloc", "cf_plan_stream_selftest",
+    "cf_plan_lblock_selftest",
     "cf_ragged_create", "cf_ragged_destroy", "cf_ragged_q", "cf_ragged_graph_launch", "cf_ragged_q_resident",
     "cf_ragged_q_host",
     "cf_ragged_info", "cf_rk2_workspace_size", "cf_rk2_steps_tiled", "cf_rtensor_sumfac", "cf_rtensor_sumfac_packed",
@@ -114,6 +115,7 @@ def load(path: str | Path | None = None) -> C.CDLL:
     lib.cf_fp64_fma_peak.argtypes = [_I32, C.POINTER(C.c_double)]
     lib.cf_plan_set_kernel_path.argtypes = [C.c_void_p, _I32]
     lib.cf_plan_stream_selftest.argtypes = [C.c_void_p, C.c_double]
+    lib.cf_plan_lblock_selftest.argtypes = [C.c_void_p, C.c_double]
     V = C.c_void_p
     lib.cf_ragged_create.argtypes = [C.POINTER(V), V, V, V, _I32, _I32, _I32]
     lib.cf_ragged_destroy.argtypes = [V]

@@ -221,6 +221,11 @@ class CollisionOperator:
                 pass
         return best, report
 
+    def lblock_selftest(self, wait_seconds: float = 1e-3) -> int:
+        """Run the l-block kernel's bounded-wait self-test (K = 8 or 12); returns the status (CF_ETIMEOUT
+        = 9 when every wait ran out and the kernel returned, which is the expected outcome)."""
+        return int(_lib.load().cf_plan_lblock_selftest(self._h, float(wait_seconds)))
+
     def stream_selftest(self, wait_seconds: float = 1e-3) -> int:
         """Run the streamed host path's bounded-wait self-test; returns the status (CF_ETIMEOUT = 9
         when the kernel's waits ran out and it returned, which is the expected outcome)."""

@@ -1819,6 +1819,33 @@ int cf_plan_stream_selftest(cf_plan* plan, double wait_seconds) {
     return run_host_streamed(plan, plan, nullptr, nullptr, B, dQ, df, false, cycles);
 }
 
+int cf_plan_lblock_selftest(cf_plan* plan, double wait_seconds) {
+    g_last_error.clear();
+    if (!plan) return fail(CF_EINVAL, "null plan");
+    if (!(wait_seconds > 0.0 && wait_seconds <= 10.0)) return fail(CF_EINVAL, "wait_seconds must be in (0, 10]");
+    std::lock_guard<std::mutex> lk(plan->mu);
+    DeviceGuard guard(plan->device);
+    if (!guard.ok) return fail(CF_ENODEVICE, "cannot select device %d", plan->device);
+    if (plan->n_g == 0 || (plan->k != 8 && plan->k != 12))
+        return fail(CF_EUNSUPPORTED, "the l-block kernel needs K = 8 or 12 and a non-empty operator");
+    cf::SplitPlan* sp = nullptr;
+    CF_TRY(get_split(plan, &sp));
+    const int64_t B = 16;
+    const size_t cell_bytes = (size_t)B * plan->n_q * plan->k * sizeof(double);
+    CF_TRY(ensure_io(plan, 2 * cell_bytes));
+    CF_TRY(ensure_ws(plan, tiled_bytes(plan, B) * 2));
+    int khz = 0;
+    CF_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, plan->device));
+    const long long cycles = std::max(1LL, (long long)((double)std::max(khz, 1000000) * 1e3 * wait_seconds));
+    double* dQ = plan->d_io;
+    double* df = (double*)((char*)plan->d_io + cell_bytes);
+    CF_CUDA(cudaMemsetAsync(plan->d_io, 0, 2 * cell_bytes, plan->stream));
+    int64_t launches = 0;
+    const int st = cf::lblock_selftest(sp, dQ, df, plan->d_ws, plan->ws_bytes, B, cycles, plan->stream, &launches);
+    g_launches += launches;
+    return st;
+}
+
 int cf_fp64_fma_peak(int32_t device, double* tflops) {
     g_last_error.clear();
     if (!tflops) return fail(CF_EINVAL, "null output");

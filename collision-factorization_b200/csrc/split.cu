@@ -128,6 +128,8 @@ struct SplitArgs {
     const int4* items;         // per band, its (t, row) slices in t-major order (lbi_*)
     const int* t_items;        // per t-list position of a band: its number of items
     int max_rows, max_t;       // sizes of the per-CTA row and t tables
+    long long wait_cycles;     // the l-block kernel's budget per bounded wait (SM clocks)
+    int no_copy;               // self-test: no stage is ever filled, so every wait runs out
     // shared-memory offsets (bytes)
     int off_a, off_b, off_f, off_mb, off_red, off_scale, off_eexp, off_bar, off_misc;
 };
@@ -217,13 +219,14 @@ inline Layout lblock_layout(int n_ring, int stage_bytes, int k, int max_rows, in
 
 // Bounded wait on an mbarrier phase; on timeout (or if another thread already gave up) sets the
 // CTA's abort word and the error word, and returns false.
-__device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err) {
+__device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                         long long budget = kWaitCycles) {
     if (*abort_flag) return false;
     const long long t0 = clock64();
     for (;;) {
         if (tc05::mbar_try_wait_sleep(bar, parity, 2000u)) return true;
         if (*abort_flag) return false;
-        if (clock64() - t0 > kWaitCycles) {
+        if (clock64() - t0 > budget) {
             *abort_flag = 1;
             atomicExch(err, 1);
             return false;
@@ -944,6 +947,7 @@ __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
         const int l23 = a.t_l23[t], l2 = l23 & 0xff, l3 = l23 >> 8;
         const uint32_t fb2 = (uint32_t)((2 * l2 + 1) * ROWB), fb3 = l3 != l2 ? (uint32_t)((2 * l3 + 1) * ROWB) : 0u;
         unsigned char* st = ring + (size_t)sb * a.stage_bytes;
+        if (a.no_copy) return;  // self-test: the stage never fills
         tc05::mbar_arrive_expect_tx(&bfull[sb], (uint32_t)RTB + fb2 + fb3);
         tc05::bulk_g2s(st, rsrc + (size_t)t * (RTB / sizeof(T)), (uint32_t)RTB, &bfull[sb]);
         tc05::bulk_g2s(st + RTB, pcg + (size_t)l2 * l2 * K * C, fb2, &bfull[sb]);
@@ -995,7 +999,7 @@ __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
         if (lane == 0) {
             const long long t0 = clock64();
             while (stage_ti[sb] != ti) {
-                if (*abort_flag || clock64() - t0 > kWaitCycles) {
+                if (*abort_flag || clock64() - t0 > a.wait_cycles) {
                     *abort_flag = 1;
                     atomicExch(a.err, 1);
                     break;
@@ -1004,7 +1008,7 @@ __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
             }
         }
         __syncwarp();
-        bool ok = wait_bar(&bfull[sb], (uint32_t)((ti / D) & 1), abort_flag, a.err);
+        bool ok = wait_bar(&bfull[sb], (uint32_t)((ti / D) & 1), abort_flag, a.err, a.wait_cycles);
         if (ok) {
             const unsigned char* st = ring + (size_t)sb * a.stage_bytes;
             const int b2 = l2 * l2, b3 = l3 * l3 - (l3 != l2 ? 2 * l2 + 1 : 0);
@@ -1049,7 +1053,7 @@ __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
             if (lane == 0) {
                 const long long t0 = clock64();
                 while (ticket[row] != ord) {
-                    if (*abort_flag || clock64() - t0 > kWaitCycles) {
+                    if (*abort_flag || clock64() - t0 > a.wait_cycles) {
                         *abort_flag = 1;
                         atomicExch(a.err, 1);
                         break;
@@ -1901,7 +1905,7 @@ size_t lblock_pack_bytes_of(int n_q, int k, int64_t B, bool f32) {
 
 template <int K, typename T>
 int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, int64_t B, cudaStream_t st,
-               int64_t* launches) {
+               int64_t* launches, long long wait_cycles = kWaitCycles, bool no_copy = false) {
     constexpr bool F32 = sizeof(T) == 4;
     constexpr int C = F32 ? 2 * kLbCells : kLbCells, W = kLbWarps;
     auto kern = F32 ? (void (*)(SplitArgs))af_lblock32_kernel<K> : (void (*)(SplitArgs))af_lblock64_kernel<K>;
@@ -1948,6 +1952,8 @@ int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, 
     a.stage_bytes = F32 ? sp->lb32_stage : sp->lb_stage;
     a.max_rows = sp->lb_rows;
     a.max_t = sp->lb_t;
+    a.wait_cycles = wait_cycles;
+    a.no_copy = no_copy ? 1 : 0;
     a.off_b = lay.off_b;
     a.off_red = lay.off_red;
     a.off_bar = lay.off_bar;
@@ -2058,6 +2064,21 @@ int lblock_run(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, 
                           : runlb_impl<12, float>(sp, q_cm, f_cm, pf, B, st, launches);
     return sp->k == 8 ? runlb_impl<8, double>(sp, q_cm, f_cm, pf, B, st, launches)
                       : runlb_impl<12, double>(sp, q_cm, f_cm, pf, B, st, launches);
+}
+
+int lblock_selftest(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, size_t pf_bytes, int64_t B,
+                    long long wait_cycles, cudaStream_t st, int64_t* launches) {
+    if (B <= 0) return fail_split(CF_EINVAL, "l-block self-test: no cells");
+    if (!lblock_available(sp, false))
+        return fail_split(CF_EUNSUPPORTED, "l-block kernel: needs K = 8 or 12 and two stages of shared memory");
+    if (pf_bytes < lblock_pack_bytes(sp, B, false))
+        return fail_split(CF_EINVAL, "l-block kernel: packed-f workspace too small");
+    const int r = sp->k == 8 ? runlb_impl<8, double>(sp, q_cm, f_cm, pf, B, st, launches, wait_cycles, true)
+                             : runlb_impl<12, double>(sp, q_cm, f_cm, pf, B, st, launches, wait_cycles, true);
+    if (r != CF_OK) return r;
+    const cudaError_t e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("l-block self-test: ") + cudaGetErrorString(e));
+    return split_check(sp);
 }
 
 int split_build(SplitPlan** out, const DevOp& folded, int64_t n_g, int64_t n_slices, int device) {

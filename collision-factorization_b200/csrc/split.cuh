@@ -40,6 +40,11 @@ int bf16_band_run(const SplitPlan* sp, double* q_cm, const double* f_cm, int64_t
 int lblock_run(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, size_t pf_bytes, int64_t B, bool f32,
                cudaStream_t st, int64_t* launches);
 size_t lblock_pack_bytes(const SplitPlan* sp, int64_t B, bool f32);
+// Self-test of the l-block kernel's bounded waits: the FP64 kernel on B cells with no stage ever
+// filled and each wait limited to wait_cycles SM clocks; synchronises, and returns CF_ETIMEOUT (the
+// error word cleared) when the waits ran out and the kernel returned, as they must.
+int lblock_selftest(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, size_t pf_bytes, int64_t B,
+                    long long wait_cycles, cudaStream_t st, int64_t* launches);
 bool lblock_available(const SplitPlan* sp, bool f32);
 // After the stream has been synchronised: CF_ETIMEOUT (and the flag cleared) if a CTA of an
 // earlier launch gave up a bounded wait, else CF_OK.

@@ -234,6 +234,14 @@ int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f_dev, int64
  * plan's device scratch then holds garbage, nothing else is touched. */
 int cf_plan_stream_selftest(cf_plan* plan, double wait_seconds);
 
+/* Self-test of the l-block kernel's bounded waits (no counterpart in the reference): launches the
+ * FP64 l-block kernel of `plan` (K = 8 or 12; builds the plan's band tables on first use) over 16
+ * zero cells with no stage of R_t and f ever copied in, so every CTA's wait runs out after
+ * wait_seconds (0 < wait_seconds <= 10) and the kernel returns through its normal exit.  Returns
+ * CF_ETIMEOUT when the waits gave up and reported it, as they should; the plan's device scratch
+ * then holds garbage, nothing else is touched. */
+int cf_plan_lblock_selftest(cf_plan* plan, double wait_seconds);
+
 /* ------------------------------------------------------------------------------------------
  * Ragged batches: cells of several resolutions (one plan per (L, K) bucket) contracted in ONE
  * persistent launch.  cells[b] is bucket b's cell count; q_dev[b], f_dev[b] are its

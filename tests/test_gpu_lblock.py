@@ -184,3 +184,24 @@ def test_lblock_fp32_forms_vs_oracle(L, K, B, cuda_available, oracle_lib):
         assert np.all(inv == 0.0), form
         assert np.array_equal(_device_q(op, cells, form), Q), form
     op.close()
+
+
+def test_lblock_wait_gives_up_and_reports(cuda_available, oracle_lib):
+    """A launch whose stages never fill: every bounded wait (stage assignment, mbarrier, row ticket)
+    runs out after 1 ms, the kernel returns, the call reports CF_ETIMEOUT, and the same plan then
+    contracts correctly (the error word is cleared)."""
+    import cf_b200
+    from cf_b200 import workloads
+
+    geo, R = _setup(6, 12, seed=9)
+    cells = workloads.maxwellian_cells(12, 6, 21, seed=4)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, 12)
+    op.set_kernel_path("lblock")
+    assert op.lblock_selftest(1e-3) == 9
+    assert "gave up" in cf_b200._lib.load().cf_last_error().decode()
+    Q = _device_q(op, cells, "af")
+    assert op.info()["last_path"] == PATH_LBLOCK
+    assert per_cell_err(Q, _oracle(geo, R, 12, cells, oracle_lib)) <= TOL_FP64
+    assert op.lblock_selftest(1e-3) == 9
+    assert np.array_equal(_device_q(op, cells, "af"), Q)
+    op.close()
