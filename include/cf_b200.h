@@ -222,7 +222,10 @@ int cf_fp64_fma_peak(int32_t device, double* tflops);
  * array, so calls that overlap on the GPU (other streams, other host threads) race on it.  The
  * plan itself is created beforehand with cf_plan_create, which does allocate, and so is its folded
  * operator: the folded forms (CF_FORM_AF_SYM and its FP32 / BF16 variants) return CF_EINVAL until
- * one cf_q_device or cf_q_tiled call in a folded form has built it. */
+ * one cf_q_device or cf_q_tiled call in a folded form has built it.  The same holds for the tables
+ * of the band kernels (kernel paths 11 and 14, the BF16-split forms at K = 4 and 12, and the fast
+ * forms at K = 12 from L = 8 on, which run on the l-block kernel): one cf_q_device call in the form
+ * builds them. */
 #define CF_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form,
                         void* stream);

@@ -205,3 +205,32 @@ def test_lblock_wait_gives_up_and_reports(cuda_available, oracle_lib):
     assert op.lblock_selftest(1e-3) == 9
     assert np.array_equal(_device_q(op, cells, "af"), Q)
     op.close()
+
+
+def test_lblock_through_the_allocation_free_entry_point(cuda_available):
+    """At K = 12 from L = 8 on the automatic order runs the fast forms on the l-block kernel, whose band
+    tables are built with allocations on first use: cf_q_device_noalloc refuses the form (CF_EINVAL)
+    until one cf_q_device call has built them, then packs f into its fixed array and gives the bits
+    of cf_q_device, on two calls in a row."""
+    import torch
+
+    import cf_b200
+    from cf_b200 import _lib, workloads
+
+    geo, R = _setup(8, 12, seed=13)
+    B = 50
+    f = torch.from_numpy(workloads.maxwellian_cells(12, 8, B, seed=6)).cuda()
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, 12)
+    lib = _lib.load()
+    s = torch.cuda.current_stream().cuda_stream
+    out = torch.zeros_like(f)
+    assert lib.cf_q_device_noalloc(op._h, out.data_ptr(), f.data_ptr(), B, _lib.FORM_AF, s) == _lib.CF_EINVAL
+    ref = op.q(f, form="af")  # cf_q_device: builds the band tables
+    assert op.info()["last_path"] == PATH_LBLOCK
+    for _ in range(2):
+        out = torch.zeros_like(f)
+        assert lib.cf_q_device_noalloc(op._h, out.data_ptr(), f.data_ptr(), B, _lib.FORM_AF, s) == 0
+        torch.cuda.synchronize()
+        assert op.info()["last_path"] == PATH_LBLOCK
+        assert torch.equal(out, ref)
+    op.close()
