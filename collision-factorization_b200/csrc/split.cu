@@ -801,10 +801,11 @@ __global__ void __launch_bounds__(W * 32, 1) af_band64_kernel(SplitArgs a) {
 // been added), so the sums, and the bits of Q, do not depend on which warp ran which item.  The stage
 // of t-list position ti is refilled with ti + n_ring by the warp that finishes the last item of ti.
 
-// f cell-major [B][K][N_Q] -> packed [cg][q][k][C] (zero past the end of the batch).  One CTA per
+// f cell-major [B][K][N_Q] -> packed [cg][q][k][C], or with CELLROWS [cg][q][C][k] (zero past the
+// end of the batch).  One CTA per
 // (cell group, 32 rows q), in a one-dimensional grid: the C cells' K x 32 block is read along q
 // (coalesced) into shared memory and written out as one contiguous run.
-template <int C, typename T>
+template <int C, typename T, bool CELLROWS = false>
 __global__ void __launch_bounds__(256) pack_cg_kernel(const double* __restrict__ f, T* __restrict__ pf,
                                                       long long n_cells, int n_q, int K) {
     extern __shared__ __align__(16) unsigned char tile_raw[];
@@ -819,7 +820,7 @@ __global__ void __launch_bounds__(256) pack_cg_kernel(const double* __restrict__
         const long long cell = cg * C + c;
         double v = 0.0;
         if (qq < nq && cell < n_cells) v = __ldg(f + cell * M + (long long)k * n_q + q0 + qq);
-        tile[(qq * K + k) * C + c] = (T)v;
+        tile[CELLROWS ? (qq * C + c) * K + k : (qq * K + k) * C + c] = (T)v;
     }
     __syncthreads();
     T* out = pf + (cg * n_q + q0) * K * C;
@@ -905,13 +906,98 @@ __device__ __forceinline__ void slot_phi_staged(const double* __restrict__ gv, c
     if (cur >= 0) flush();
 }
 
+// The FP64 l-block kernel's K^3 step on the FP64 tensor cores (warp-level mma.sync m8n8k4; B200's
+// tcgen05 has no FP64 kind).  Lane l = (g = l >> 2, p = l & 3) holds cell g's Phi for all k2 and
+// k3 = p KQ .. p KQ + KQ - 1: at k-step s = k2 KQ + y that is exactly the B fragment B[k = p][n = g]
+// of the MMA whose K index is kk' = 4 s + p.  Per l-triplet the stage holds R_t as A fragments,
+// [m-tile][s][lane] with A[m = g][k = p] = R_t[k1 = g + 8 m-tile][k2][k3 = p KQ + y] (zero for
+// k1 >= K), so a warp reads each fragment as 32 consecutive doubles.  The product lands in the C
+// fragments D[k1 = g + 8 m-tile][cells 2p, 2p + 1]: the sum over the parts of a cell is the MMA's
+// own, and no lane exchanges anything.  f rows are staged as [q][cell][k], so the four lanes of a
+// cell read their k3 on distinct banks and a run's f(q2) comes in 16-byte pairs.
+template <int K>
+struct LbMma {
+    static constexpr int C = 8;
+    static constexpr int KQ = K / 4;                  // k3 per lane
+    static constexpr int MT = (K + 7) / 8;            // m-tiles of k1
+    static constexpr int S = K * KQ;                  // k-steps of four kk'
+    static constexpr int RT_BYTES = MT * S * 32 * 8;  // A fragments of one R_t
+};
+
+// Phi of one item on an FP64 cell-rows stage (f at fsg[(row C + cell) K + k], rows local as in
+// slot_phi_staged), for lane (cell c, part p): phi[k2][y], k3 = p KQ + y; grouped by q2.
+template <int K>
+__device__ __forceinline__ void slot_phi_cellrows(const double* __restrict__ gv, const uint32_t* __restrict__ eq23,
+                                                  const double* __restrict__ fsg, const SlotEntries& se, int lane,
+                                                  int c, int part, int b2, int b3, double (&phi)[K][K / 4]) {
+    constexpr int C = LbMma<K>::C, KQ = LbMma<K>::KQ;
+    const int k3o = part * KQ;
+#pragma unroll
+    for (int x = 0; x < K; ++x)
+#pragma unroll
+        for (int y = 0; y < KQ; ++y) phi[x][y] = 0.0;
+    const int cb = se.cb, ce = se.ce;
+    if (cb >= ce) return;
+    double h[KQ];
+#pragma unroll
+    for (int y = 0; y < KQ; ++y) h[y] = 0.0;
+    int cur = -1;
+    auto flush = [&]() {
+        const double2* __restrict__ f2p = reinterpret_cast<const double2*>(fsg + ((size_t)cur * C + c) * K);
+#pragma unroll
+        for (int x = 0; x < K / 2; ++x) {
+            const double2 f2 = f2p[x];
+#pragma unroll
+            for (int y = 0; y < KQ; ++y) {
+                phi[2 * x][y] = fma(f2.x, h[y], phi[2 * x][y]);
+                phi[2 * x + 1][y] = fma(f2.y, h[y], phi[2 * x + 1][y]);
+            }
+        }
+#pragma unroll
+        for (int y = 0; y < KQ; ++y) h[y] = 0.0;
+    };
+    for (int eb = cb; eb < ce; eb += 32) {
+        const int nb = min(32, ce - eb);
+        uint32_t my_q23 = se.q23;
+        double my_g = se.g;
+        if (eb != cb) {
+            my_q23 = 0;
+            my_g = 0.0;
+            if (lane < nb) {
+                my_q23 = __ldg(eq23 + eb + lane);
+                my_g = __ldg(gv + eb + lane);
+            }
+        }
+        for (int j = 0; j < nb; ++j) {
+            const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, j);
+            const double g = __shfl_sync(0xffffffffu, my_g, j);
+            const int q2 = (int)(q23 & 0xffffu) - b2, q3 = (int)(q23 >> 16) - b3;
+            if (q2 != cur) {
+                if (cur >= 0) flush();
+                cur = q2;
+            }
+            const double* __restrict__ f3p = fsg + ((size_t)q3 * C + c) * K + k3o;
+#pragma unroll
+            for (int y = 0; y < KQ; ++y) h[y] = fma(g, f3p[y], h[y]);
+        }
+    }
+    if (cur >= 0) flush();
+}
+
+__device__ __forceinline__ void lb_dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 enum { LBI_TR = 0, LBI_ORD, LBI_BEGIN, LBI_END };  // item: t | row << 16, ord | l2 << 16 | l3 << 24, entries
 enum { LBU_L1 = 0, LBU_BROWS, LBU_TLOFF, LBU_NT, LBU_ITOFF, LBU_NIT, LBU_INTS = 8 };
 
-template <int K, int C, typename T, int W>
+template <int K, int C, typename T, int W, bool MMA = false>
 __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
     using S = LbShape<K, C, T>;
-    constexpr int KH = S::KH, KQ = S::KQ, PS = S::PS, RTB = S::RT_BYTES;
+    static_assert(!MMA || (C == LbMma<K>::C && sizeof(T) == 8), "the FP64 tensor-core K^3 step takes 8 FP64 cells");
+    constexpr int KH = S::KH, KQ = S::KQ, PS = S::PS, RTB = MMA ? LbMma<K>::RT_BYTES : S::RT_BYTES;
     constexpr int ROWB = K * C * (int)sizeof(T);
     extern __shared__ __align__(1024) unsigned char smem[];
     unsigned char* ring = smem + a.off_b;
@@ -930,7 +1016,7 @@ __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
     volatile int* stage_ti = misc + 2 + kLbMaxRing + a.max_rows + a.max_t;
 
     const int tid = threadIdx.x, lane = tid & 31;
-    const int c = lane % C, part = lane / C;
+    const int c = MMA ? lane >> 2 : lane % C, part = MMA ? lane & 3 : lane / C;
     const int NQ = a.n_q, M = NQ * K, D = a.n_ring;
     const int unit = a.unit_order[blockIdx.x / a.n_cg];
     const int cg = blockIdx.x % a.n_cg;
@@ -1013,7 +1099,30 @@ __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
             const unsigned char* st = ring + (size_t)sb * a.stage_bytes;
             const int b2 = l2 * l2, b3 = l3 * l3 - (l3 != l2 ? 2 * l2 + 1 : 0);
             T acc[K];
-            {
+            double dq[MMA ? LbMma<K>::MT : 1][2];
+            if constexpr (MMA) {
+                constexpr int MT = LbMma<K>::MT, SS = LbMma<K>::S, QQ = LbMma<K>::KQ;
+                double phi[K][QQ];
+                slot_phi_cellrows<K>(a.e_g, a.e_q23, reinterpret_cast<const double*>(st + RTB), se, lane, c, part,
+                                     b2, b3, phi);
+                const double* __restrict__ ra = reinterpret_cast<const double*>(st) + lane;
+                // two accumulator sets per m-tile (even and odd k-steps): two MMA chains instead of one
+                double d[MT][2][2];
+#pragma unroll
+                for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+                    for (int h2 = 0; h2 < 2; ++h2) d[mt][h2][0] = d[mt][h2][1] = 0.0;
+#pragma unroll
+                for (int ks = 0; ks < SS; ++ks)
+#pragma unroll
+                    for (int mt = 0; mt < MT; ++mt)
+                        lb_dmma(d[mt][ks & 1][0], d[mt][ks & 1][1], ra[(mt * SS + ks) * 32], phi[ks / QQ][ks % QQ]);
+#pragma unroll
+                for (int mt = 0; mt < MT; ++mt) {
+                    dq[mt][0] = d[mt][0][0] + d[mt][1][0];
+                    dq[mt][1] = d[mt][0][1] + d[mt][1][1];
+                }
+            } else {
                 T phi[KH][KQ];
                 slot_phi_staged<K, C, T>(a.e_g, a.e_q23, reinterpret_cast<const T*>(st + RTB), se, lane, c, part, b2,
                                          b3, phi);
@@ -1045,11 +1154,13 @@ __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
                     }
             }
             // the parts of a cell sit in lanes c, c + C, c + 2C, ...: sum them, then part p adds the
-            // k1 of its quarter once this row's earlier slices are in
+            // k1 of its quarter once this row's earlier slices are in (the MMA has summed them already)
+            if constexpr (!MMA) {
 #pragma unroll
-            for (int k1 = 0; k1 < K; ++k1)
+                for (int k1 = 0; k1 < K; ++k1)
 #pragma unroll
-                for (int o = C; o < 32; o <<= 1) acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], o);
+                    for (int o = C; o < 32; o <<= 1) acc[k1] += __shfl_xor_sync(0xffffffffu, acc[k1], o);
+            }
             if (lane == 0) {
                 const long long t0 = clock64();
                 while (ticket[row] != ord) {
@@ -1065,11 +1176,24 @@ __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
             __threadfence_block();
             ok = !*abort_flag;
             if (ok) {
-                double* qr = qacc + (size_t)row * K * C + c;
-                constexpr int KP = K / (32 / C);  // k1 per part
+                if constexpr (MMA) {
+                    // this lane's C fragments: k1 = c + 8 m-tile, cells 2 part and 2 part + 1
 #pragma unroll
-                for (int k1 = 0; k1 < K; ++k1)
-                    if (k1 / KP == part) qr[k1 * C] += (double)acc[k1];
+                    for (int mt = 0; mt < LbMma<K>::MT; ++mt) {
+                        const int k1 = c + 8 * mt;
+                        if (k1 < K) {
+                            double* qr = qacc + ((size_t)row * K + k1) * C + 2 * part;
+                            qr[0] += dq[mt][0];
+                            qr[1] += dq[mt][1];
+                        }
+                    }
+                } else {
+                    double* qr = qacc + (size_t)row * K * C + c;
+                    constexpr int KP = K / (32 / C);  // k1 per part
+#pragma unroll
+                    for (int k1 = 0; k1 < K; ++k1)
+                        if (k1 / KP == part) qr[k1 * C] += (double)acc[k1];
+                }
             }
             __syncwarp();
             if (lane == 0) {
@@ -1107,7 +1231,7 @@ __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
 // added into the FP64 Q rows): 16 cells per CTA, the same shared memory.
 template <int K>
 __global__ void __launch_bounds__(kLbWarps * 32, 1) af_lblock64_kernel(SplitArgs a) {
-    lblock_body<K, kLbCells, double, kLbWarps>(a);
+    lblock_body<K, kLbCells, double, kLbWarps, true>(a);
 }
 template <int K>
 __global__ void __launch_bounds__(kLbWarps * 32, 1) af_lblock32_kernel(SplitArgs a) {
@@ -1570,7 +1694,7 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
                     rfp64[((size_t)t * S::P + pp) * S::PS + (size_t)e * K + k1] =
                         R[(size_t)t * K * K * K + k1 + (size_t)K * k2 + (size_t)K * K * k3];
             }
-    // the l-block kernels' R_t: FP64 for 8 cells per CTA, FP32 for 16 (LbShape)
+    // the l-block kernels' R_t: FP32 for 16 cells per CTA (LbShape), FP64 for 8 as MMA A fragments
     std::vector<double> rfl;
     std::vector<float> rfl32;
     if constexpr (lblock_supported_k(K)) {
@@ -1587,8 +1711,20 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
                                                                                    (size_t)K * k2 + (size_t)K * K * k3];
                     }
         };
-        fill(LbShape<K, kLbCells, double>{}, rfl);
         fill(LbShape<K, 2 * kLbCells, float>{}, rfl32);
+        // FP64: A fragments of the m8n8k4 MMAs, [t][m-tile][k-step][lane] (LbMma)
+        using LM = LbMma<K>;
+        rfl.assign((size_t)NL * LM::MT * LM::S * 32, 0.0);
+        for (int t = 0; t < NL; ++t)
+            for (int mt = 0; mt < LM::MT; ++mt)
+                for (int ks = 0; ks < LM::S; ++ks)
+                    for (int ln = 0; ln < 32; ++ln) {
+                        const int k1 = (ln >> 2) + 8 * mt, p4 = ln & 3;
+                        const int k2 = ks / LM::KQ, k3 = p4 * LM::KQ + ks % LM::KQ;
+                        if (k1 < K)
+                            rfl[(((size_t)t * LM::MT + mt) * LM::S + ks) * 32 + ln] =
+                                R[(size_t)t * K * K * K + k1 + (size_t)K * k2 + (size_t)K * K * k3];
+                    }
     }
     // G / s_t per entry, |G / s_t| summed per slice, (l2, l3) per t
     std::vector<double> e_gs(n_g), gs(n_slices, 0.0);
@@ -1752,8 +1888,7 @@ int build_impl(SplitPlan* sp, const DevOp& op, int64_t n_g, int64_t n_slices) {
             max_rows = std::max(max_rows, 2 * l2 + 1 + (l3 != l2 ? 2 * l3 + 1 : 0));
         }
         // FP64, 8 cells; FP32, 16 cells: the same bytes per f row
-        const int stage = (LbShape<K, kLbCells, double>::RT_BYTES + max_rows * K * kLbCells * (int)sizeof(double) + 127) /
-                          128 * 128;
+        const int stage = (LbMma<K>::RT_BYTES + max_rows * K * kLbCells * (int)sizeof(double) + 127) / 128 * 128;
         const int stage32 =
             (LbShape<K, 2 * kLbCells, float>::RT_BYTES + max_rows * K * 2 * kLbCells * (int)sizeof(float) + 127) / 128 *
             128;
@@ -1926,7 +2061,8 @@ int runlb_impl(const SplitPlan* sp, double* q_cm, const double* f_cm, void* pf, 
         return fail_split(CF_ESHAPE, "l-block kernel: batch too large for one launch");
     const unsigned pgrid = (unsigned)pblocks;
     static_assert(32 * K * C * sizeof(T) <= 48 * 1024, "the pack kernel's tile fits the default shared memory");
-    pack_cg_kernel<C, T><<<pgrid, 256, 32 * K * C * sizeof(T), st>>>(f_cm, static_cast<T*>(pf), B, sp->n_q, K);
+    // FP64: [q][cell][k] rows for the tensor-core kernel; FP32: [q][k][cell]
+    pack_cg_kernel<C, T, !F32><<<pgrid, 256, 32 * K * C * sizeof(T), st>>>(f_cm, static_cast<T*>(pf), B, sp->n_q, K);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail_split(CF_ECUDA, std::string("l-block pack: launch: ") + cudaGetErrorString(e));
     if (launches) ++*launches;
