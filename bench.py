@@ -72,7 +72,7 @@ NCU_TRAFFIC = {
     ("hs_l10_k8_b4096", "tile_cell_major", "af_sym"): (64.777728e6 + 2.003456e6,
                                                        "ncu dram__bytes_read.sum + dram__bytes_write.sum, "
                                                        "profiles/af_tile_stream_kernel_folded_hs_l10_k8_b4096.md"),
-    ("hs_l16_k12_b1024", "lblock", "af_sym"): (71.158272e6 + 5.586944e6,
+    ("hs_l16_k12_b1024", "lblock", "af_sym"): (74.657024e6 + 9.41312e6,
                                                "ncu dram__bytes_read.sum + dram__bytes_write.sum of the l-block kernel "
                                                "launch (the pack pass before it not counted), "
                                                "profiles/af_lblock64_kernel_folded_hs_l16_k12_b1024.md"),
@@ -550,8 +550,8 @@ def run_ours(args):
                          "FP64; the whole device step)",
                  "lblock": "af_lblock64_kernel (one CTA per l1 band and 8 cells, R_t and the f rows of bands l2 and "
                            "l3 staged per l-triplet by cp.async.bulk into a ring of stages, the band's slices taken "
-                           "by the warps one at a time, FP64; timed with the pack pass before it, the whole device "
-                           "step)",
+                           "by the warps one at a time, Phi on the FP64 CUDA cores, K^3 step on the FP64 tensor cores "
+                           "(mma.sync m8n8k4); timed with the pack pass before it, the whole device step)",
                  "rf_dense": "rf_dense_kernel (radial step as a dense GEMM over cells per (t, q2), FP64; the device step "
                              "with its f packing and partial-sum reduction)"}.get(last_path, "?")
     kern_s = sum(kern_list) / len(kern_list) / 1e3
