@@ -946,14 +946,14 @@ int run_band64(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, c
 // 8 cells in FP64, 16 in FP32) with R_t and the f rows of bands l2 and l3 staged per l-triplet, from f
 // packed per cell group into the workspace, and the band's slices handed to the warps one at a time.
 //
-// The automatic order also takes it for the fast Q forms (plain and folded) at K = 12 from L = 8 on,
-// where the gather kernel is the other family (B200, ms per launch, l-block against gather, folded /
-// plain: L = 16, 1024 cells 8.54 / 19.21 against 12.10 / 23.11; L = 12, 1024 cells 2.67 / 5.55 against
-// 3.86 / 7.37; L = 8, 2048 cells 1.25 / 2.30 against 1.69 / 3.07).  Operators whose (t, q1) pairs come
-// in several runs (an unsorted COO list) have no band tables and stay on the gather kernel.
-bool lblock_auto(const cf_plan* target) {
-    return target->path == cf::PATH_AUTO && target->k == 12 && target->n_q >= 81;
-}
+// The automatic order also takes it for the fast Q forms (plain and folded) at K = 12, where the
+// gather kernel is the other family (B200, ms per launch, l-block with its K^3 step on the FP64 tensor
+// cores against gather, folded / plain: L = 16, 1024 cells 6.89 / 15.93 against 12.10 / 23.11;
+// L = 12, 1024 cells 2.29 / 5.07 against 3.86 / 7.37; L = 8, 2048 cells 0.96 / 1.82 against
+// 1.69 / 3.07; L = 6, 2048 cells 0.39 / 0.66 against 0.68 / 1.18; L = 4, 4096 cells 0.27 / 0.38
+// against - / 0.63).  Operators whose (t, q1) pairs come in several runs (an unsorted COO list) have
+// no band tables and stay on the gather kernel.
+bool lblock_auto(const cf_plan* target) { return target->path == cf::PATH_AUTO && target->k == 12; }
 
 int run_lblock(cf_plan* target, double* q_dev, const double* f_dev, int64_t B, void* ws, size_t ws_bytes,
                cudaStream_t st, bool f32) {
@@ -1770,7 +1770,7 @@ __attribute__((visibility("hidden"))) bool cf_plan_band_pending(cf_plan* plan, i
     if (form_what(form, exact, sym, f32) != 0 || exact || !cf::split_supported_k(plan->k)) return false;
     const bool band = plan->path == cf::PATH_BAND;
     const bool lblock = (plan->path == cf::PATH_LBLOCK && (plan->k == 8 || plan->k == 12)) ||
-                        (plan->path == cf::PATH_AUTO && plan->k == 12 && plan->n_q >= 81);
+                        (plan->path == cf::PATH_AUTO && plan->k == 12);
     if (!((f32 == 2 && (plan->k != 8 || band)) || (f32 == 0 && (band || lblock)) || (f32 == 1 && lblock))) return false;
     cf_plan* target = plan;
     if (sym) {

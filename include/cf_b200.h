@@ -189,7 +189,7 @@ int cf_jv_tiled(cf_plan* plan, double* out_tiled, const double* f_tiled, const d
 /* Kernel family of a plan's angular-first and Jacobian contractions: 0 = automatic (the first of
  * pair, tile, gather that fits; tile before pair for the fast Q form of the folded operator, whose
  * lighter Phi step favours the tile kernel's higher occupancy; the l-block kernel for the fast Q
- * forms, plain and folded, at K = 12 from L = 8 on), 1 = the gather kernel (warp per row and 32-cell tile,
+ * forms, plain and folded, at K = 12), 1 = the gather kernel (warp per row and 32-cell tile,
  * f read through L1/L2), 2 = the tile-resident kernel (16 cells in shared memory, Phi split over
  * two lanes per cell), 3 = the pair kernel (16 cells in shared memory, the mirrored rows (l,+m) and
  * (l,-m) on the two half-warps), 4 = the pair kernel reading R through L1 instead of shared
@@ -224,7 +224,7 @@ int cf_fp64_fma_peak(int32_t device, double* tflops);
  * operator: the folded forms (CF_FORM_AF_SYM and its FP32 / BF16 variants) return CF_EINVAL until
  * one cf_q_device or cf_q_tiled call in a folded form has built it.  The same holds for the tables
  * of the band kernels (kernel paths 11 and 14, the BF16-split forms at K = 4 and 12, and the fast
- * forms at K = 12 from L = 8 on, which run on the l-block kernel): one cf_q_device call in the form
+ * forms at K = 12, which run on the l-block kernel): one cf_q_device call in the form
  * builds them. */
 #define CF_NOALLOC_SCRATCH_BYTES ((size_t)64 << 20)
 int cf_q_device_noalloc(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b, int32_t form,

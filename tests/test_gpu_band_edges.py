@@ -138,7 +138,10 @@ def test_noalloc_refusals_and_band_tables(cuda_available):
     s = torch.cuda.current_stream().cuda_stream
     out = torch.zeros_like(f)
     assert lib.cf_q_device_noalloc(op._h, out.data_ptr(), f.data_ptr(), B, _lib.FORM_RF_DENSE, s) == 8
-    op.q(f, out=torch.zeros_like(f), form="af_sym")  # builds the folded twin
+    # builds the folded twin; on the gather kernel, so that no band table exists yet (the automatic
+    # order runs the fast forms at K = 12 on the l-block kernel, whose first use builds them)
+    op.set_kernel_path("gather")
+    op.q(f, out=torch.zeros_like(f), form="af_sym")
     torch.cuda.synchronize()
     assert lib.cf_q_device_noalloc(op._h, out.data_ptr(), f.data_ptr(), B, _lib.FORM_AF_SYM_BF16, s) == 1
     ref = torch.zeros_like(f)

@@ -1,8 +1,8 @@
 """The l-block kernel (af_lblock64_kernel): the fast angular-first Q forms with one CTA per (l1 band,
 8-cell group), R_t and the f rows of bands l2 and l3 staged per l-triplet by bulk copies from f packed
-per 8-cell group, and the band's (t, row) slices taken by the warps one at a time and summed into each
-row in t order; on kernel path 'lblock' (K = 8 and 12), and in the automatic order at K = 12 from
-L = 8 on.
+per 8-cell group, the band's (t, row) slices taken by the warps one at a time and summed into each
+row in t order, and the K^3 step on the FP64 tensor cores; on kernel path 'lblock' (K = 8 and 12), and
+in the automatic order at K = 12.  The FP32 forms run the same schedule on 16 cells per CTA.
 
 Tolerance: 1e-12 normwise per cell against the oracle's restatement of the reference's angular-first
 kernel (src/mex/angular_first_collision_kernel_mex.cpp:45-69), the FP64 bar of the parity suite.
@@ -208,7 +208,7 @@ def test_lblock_wait_gives_up_and_reports(cuda_available, oracle_lib):
 
 
 def test_lblock_through_the_allocation_free_entry_point(cuda_available):
-    """At K = 12 from L = 8 on the automatic order runs the fast forms on the l-block kernel, whose band
+    """At K = 12  the automatic order runs the fast forms on the l-block kernel, whose band
     tables are built with allocations on first use: cf_q_device_noalloc refuses the form (CF_EINVAL)
     until one cf_q_device call has built them, then packs f into its fixed array and gives the bits
     of cf_q_device, on two calls in a row."""
