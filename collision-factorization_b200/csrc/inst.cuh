@@ -361,11 +361,10 @@ static LaunchResult launch_few_exact_param(const LaunchArgs& a, dim3 grid, size_
 
 template <int K>
 static LaunchResult launch_few_exact(const LaunchArgs& a) {
-    if constexpr (K > 8) {
-        return {-1, 0, cudaSuccess, PATH_FEW};
-    } else {
-        if (a.n_cells > kFewCells || a.q_cm == nullptr || (a.f_cm == nullptr && a.few_host_f == nullptr))
+    {
+        if ((a.n_cells > kFewCells && !a.rows) || a.q_cm == nullptr || (a.f_cm == nullptr && a.few_host_f == nullptr))
             return {-1, 0, cudaSuccess, PATH_FEW};
+        if (a.n_cells > 65535) return {2, 0, cudaSuccess, PATH_FEW};
         if (a.op.n_items == 0 || a.n_cells == 0) return {0, 0, cudaSuccess, PATH_FEW};
         const size_t smem = sizeof(double) * ((size_t)a.op.n_q * K + kFewWarps * (K * K + K));
         if (smem + 256 > a.max_smem) return {-1, 0, cudaSuccess, PATH_FEW};

@@ -61,6 +61,9 @@ struct LaunchArgs {
     const double* few_host_q = nullptr;
     // FP32 J.v: tiled FP32 copy of v
     const float* vT32 = nullptr;
+    // with few: the exact form of any number of cells on the row kernel (one CTA per (q1, cell), on the
+    // cell-major arrays), the exact route where the batch kernels' register tiles do not fit (K > 8)
+    bool rows = false;
 };
 
 // Status codes mirror cf_status: 0 ok, 5 CUDA error, 8 unsupported, 2 shape.

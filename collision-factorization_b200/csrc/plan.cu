@@ -501,7 +501,8 @@ constexpr int kNoFew = -2;
 int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const double* vT, double* QT, int64_t B,
              cudaStream_t st, const float* fT32 = nullptr, bool bf16 = false, const StreamSync* ss = nullptr,
              const double* f_cm = nullptr, double* q_cm = nullptr, bool few = false,
-             const double* few_host_f = nullptr, const double* few_host_q = nullptr, const float* vT32 = nullptr) {
+             const double* few_host_f = nullptr, const double* few_host_q = nullptr, const float* vT32 = nullptr,
+             bool rows = false) {
     const int64_t nt = n_tiles_for(B);
     // The folded operator has about half the COO entries per slice of the plain one, and its tile
     // routine groups them by q2, so its Phi step is light next to the K^3 step; there the tile kernel
@@ -518,6 +519,7 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
     a.few_host_f = few_host_f;
     a.few_host_q = few_host_q;
     a.vT32 = vT32;
+    a.rows = rows;
     cf::LaunchResult r{8, 0, cudaSuccess};
     switch (p->k) {
 #define CF_K(KK) \
@@ -623,6 +625,14 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
     }
     {
         const int r = run_few(p, what, exact, q_dev, f_dev, B, st, sym, f32);
+        if (r != kNoFew) return r;
+    }
+    // The exact angular-first form above K = 8, where the batch kernels' per-lane K x K Phi does not
+    // fit in registers: the row kernel of the few-cell route (one CTA per (q1, cell), the reference's
+    // operation order) on the cell-major arrays, for any number of cells.
+    if (exact && what == 0 && f32 == 0 && !sym && p->k > 8) {
+        const int r = dispatch(p, 0, true, nullptr, nullptr, nullptr, B, st, nullptr, false, nullptr, f_dev, q_dev, true,
+                               nullptr, nullptr, nullptr, true);
         if (r != kNoFew) return r;
     }
     const size_t tb = tiled_bytes(p, B);

@@ -234,3 +234,39 @@ def test_lblock_through_the_allocation_free_entry_point(cuda_available):
         assert op.info()["last_path"] == PATH_LBLOCK
         assert torch.equal(out, ref)
     op.close()
+
+
+@pytest.mark.parametrize("L,K,B", [(6, 12, 21), (3, 16, 10), (5, 12, 3)])
+def test_exact_form_above_k8_bitwise(L, K, B, cuda_available, oracle_lib):
+    """The exact angular-first form above K = 8 (one CTA per (q1, cell), the reference's operation
+    order) gives the oracle's bits, which are the compiled reference kernel's: batches of any size and
+    a handful of cells, from Q = 0 and from a nonzero Q."""
+    import cf_b200
+    from cf_b200 import workloads
+
+    geo, R = _setup(L, K, seed=L * K)
+    cells = workloads.maxwellian_cells(K, L, B, seed=B)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+    q0 = np.random.default_rng(2).standard_normal(cells.shape) * 1e-3
+    for start in (None, q0):
+        f = np.asfortranarray(cells.transpose(2, 1, 0))
+        Qo = np.zeros_like(f, order="F") if start is None else np.array(start.transpose(2, 1, 0), order="F")
+        oracle_lib.af_batch(Qo, f, geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+        Q = _device_q(op, cells, "af_exact", start)
+        assert np.array_equal(Q, Qo.transpose(2, 1, 0))
+    op.close()
+
+
+@pytest.mark.skipif(not (GOLDEN / "R_hs_k11_l16_pad20.npy").exists(), reason="L = 16, K = 12 R fixture absent")
+def test_exact_form_precision_configuration_bitwise(cuda_available, oracle_lib):
+    """L = 16, K = 12 (hard spheres, R from the GPU quadrature), 9 bi-Maxwellian cells: the exact form
+    bit for bit the oracle's (the reference kernel's operation order)."""
+    import cf_b200
+    from cf_b200 import workloads
+
+    geo, R = _setup(16, 12, np.load(GOLDEN / "R_hs_k11_l16_pad20.npy"))
+    cells = workloads.bimaxwellian_cells(12, 16, 9, seed=20263)
+    ref = _oracle(geo, R, 12, cells, oracle_lib)
+    op = cf_b200.CollisionOperator(geo.labels, geo.vals, geo.ic_map, R, geo.n_q, 12)
+    assert np.array_equal(_device_q(op, cells, "af_exact"), ref)
+    op.close()
