@@ -631,6 +631,9 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
     // fit in registers: the row kernel of the few-cell route (one CTA per (q1, cell), the reference's
     // operation order) on the cell-major arrays, for any number of cells.
     if (exact && what == 0 && f32 == 0 && !sym && p->k > 8) {
+        if (B > 65535)
+            return fail(CF_ESHAPE, "the exact form above K = 8 takes at most 65535 cells per call (B = %lld)",
+                        (long long)B);
         const int r = dispatch(p, 0, true, nullptr, nullptr, nullptr, B, st, nullptr, false, nullptr, f_dev, q_dev, true,
                                nullptr, nullptr, nullptr, true);
         if (r != kNoFew) return r;
