@@ -188,18 +188,17 @@ Layout band64_layout(int n_q, int warps) {
     return l;
 }
 
-// The l-block kernel: 8 cells per CTA (K = 8 and 12), 16 warps, a ring of n_ring stages of
-// stage_bytes each (R_t of Shape<K, 8>, then at most max_rows packed rows of K x 8 doubles).
-// The l-block kernel: 8 cells per CTA (K = 8 and 12), 16 warps, a ring of up to 8 stages.
+// The l-block kernels (K = 8 and 12): 16 warps, a ring of up to 8 stages; 8 cells per CTA in FP64,
+// 16 in FP32 (the same bytes per packed f row).
 constexpr int kLbCells = 8;
 constexpr int kLbWarps = 16;
 constexpr int kLbMaxRing = 8;
 
 __host__ __device__ constexpr bool lblock_supported_k(int k) { return k == 8 || k == 12; }
 
-// The l-block kernel's shared memory: the ring of stages (R_t of Shape<K, 8>, then at most max_rows
-// packed f rows of K x 8 doubles each), the band's Q rows of 8 cells, and the counter, done words, row
-// tickets, per-t item totals and stage assignments.
+// The l-block kernel's shared memory: the ring of stages (R_t as the kernel reads it, then at most
+// max_rows packed f rows of K x cells values each), the band's FP64 Q rows of the CTA's cells, and the
+// counter, done words, row tickets, per-t item totals and stage assignments.
 inline Layout lblock_layout(int n_ring, int stage_bytes, int k, int max_rows, int max_t, int cells) {
     Layout l{};
     int o = 0;
@@ -1219,7 +1218,7 @@ __device__ __forceinline__ void lblock_body(const SplitArgs& a) {
     }
     __syncthreads();
     if (*abort_flag) return;
-    // Q += the band's rows of the 8 cells (cell-major, in place)
+    // Q += the band's rows of the CTA's cells (cell-major, in place)
     for (int i = tid; i < brows * K * C; i += W * 32) {
         const int cc = i % C, k1 = (i / C) % K, r = i / (C * K);
         const long long cell = cell0 + cc;
@@ -1529,7 +1528,7 @@ struct SplitPlan {
     double* d_rfp64 = nullptr;        // FP64 R_t per t as [part][e][k1] (FP64 band kernel)
     uint8_t* d_rbf = nullptr;         // BF16 hi and lo planes of R_t (BF16-split band kernel)
     uint8_t* d_rbf8 = nullptr;        // K = 12: the same for 8 cells per CTA (Phi in FP32)
-    double* d_rfl = nullptr;          // the l-block kernel (8 cells per CTA): FP64 R_t as [part][e][k1]
+    double* d_rfl = nullptr;          // the FP64 l-block kernel: R_t as MMA A fragments [t][m-tile][k-step][lane]
     int* d_t_l23 = nullptr;           // per l-triplet: l2 | l3 << 8
     // the l-block kernel (0 bands: unsupported)
     int lb_bands = 0, lb_rows = 0, lb_t = 0;  // bands, rows of the largest band, longest t-list
