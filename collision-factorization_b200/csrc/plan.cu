@@ -538,7 +538,7 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
     }
     if (r.status == CF_ECUDA) return fail(CF_ECUDA, "kernel launch: %s", cudaGetErrorString(r.cuda));
     if (r.status == CF_EUNSUPPORTED)
-        return fail(CF_EUNSUPPORTED, "form or kernel path not built for K = %d (exact angular-first needs K <= 8; "
+        return fail(CF_EUNSUPPORTED, "form or kernel path not built for K = %d (the exact J.v needs K <= 8; "
                     "the tile-resident kernels need an even K <= 8 and a tile that fits in shared memory)", p->k);
     if (r.status != CF_OK) return fail(r.status, "launch failed for K = %d", p->k);
     return CF_OK;
