@@ -250,6 +250,102 @@ __global__ void __launch_bounds__(kFewWarps * 32) af_few_exact_kernel(DevOp op, 
     few_row_exact<K>(op, f + off, q + off, q + off, false);
 }
 
+// The exact form of one (q1 row, pair of cells) in place, for the batch route above K = 8: each cell's
+// operations are those of few_row_exact, in the same order, so the bits are the same; the pair shares
+// the entry shuffles and the R_t loads, and lanes c 16 + k1 (k1 < K) run the K^3 sums of cell c, where
+// one cell leaves 20 of 32 lanes idle.  nc (1 or 2) cells from f and q; shared memory: f of both cells
+// (zero for a missing second cell), each warp's two Phi, each warp's two row sums.
+template <int K>
+__device__ __forceinline__ void few_row_exact2(const DevOp& op, const double* __restrict__ f, double* q, int nc) {
+    static_assert(K <= 16, "a cell's K^3 sums take lanes c 16 .. c 16 + K - 1");
+    constexpr int NP = few_pairs_per_lane<K>();
+    extern __shared__ double fs[];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n_q = op.n_q, M = n_q * K;
+    double* phis = fs + 2 * M + warp * 2 * K * K;   // [2][K K]
+    double* sums = fs + 2 * M + kFewWarps * 2 * K * K;  // [kFewWarps][2][K]
+    const int q1 = blockIdx.x;
+    const int s0 = op.q1_begin[q1], s1 = op.q1_begin[q1 + 1];
+    if (s0 == s1) return;  // in place: the row has no slices
+    // thread c 16 + k (c < nc, k < K) carries Q[q1, k] of cell c
+    const int my_c = threadIdx.x >> 4, my_k = threadIdx.x & 15;
+    const bool q_thread = threadIdx.x < 32 && my_k < K && my_c < nc;
+    double acc = 0.0;
+    if (q_thread) acc = q[(size_t)my_c * M + (size_t)my_k * n_q + q1];
+    for (int i = threadIdx.x; i < 2 * M; i += blockDim.x) fs[i] = i < nc * M ? f[i] : 0.0;
+    __syncthreads();
+    for (int base = s0; base < s1; base += kFewWarps) {
+        const int s = base + warp;
+        if (s < s1) {
+            const int t = op.slice_t[s];
+            const int e0 = op.slice_e[s], e1 = op.slice_e[s + 1];
+            double phi[2][NP];
+#pragma unroll
+            for (int j = 0; j < NP; ++j) phi[0][j] = phi[1][j] = 0.0;
+            for (int eb = e0; eb < e1; eb += 32) {
+                const int n = min(32, e1 - eb);
+                uint32_t my_q23 = 0;
+                double my_g = 0.0;
+                if (lane < n) {
+                    my_q23 = __ldg(op.e_q23 + eb + lane);
+                    my_g = __ldg(op.e_g + eb + lane);
+                }
+                for (int z = 0; z < n; ++z) {
+                    const uint32_t q23 = __shfl_sync(0xffffffffu, my_q23, z);
+                    const double g = __shfl_sync(0xffffffffu, my_g, z);
+                    const double* f2 = fs + (q23 & 0xffffu);
+                    const double* f3 = fs + (q23 >> 16);
+#pragma unroll
+                    for (int j = 0; j < NP; ++j) {
+                        const int p = lane + 32 * j;
+                        if (p < K * K) {
+                            const int i2 = (p % K) * n_q, i3 = (p / K) * n_q;
+                            phi[0][j] = __dadd_rn(phi[0][j], __dmul_rn(__dmul_rn(g, f2[i2]), f3[i3]));
+                            phi[1][j] = __dadd_rn(phi[1][j], __dmul_rn(__dmul_rn(g, f2[M + i2]), f3[M + i3]));
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < NP; ++j)
+                if (lane + 32 * j < K * K) {
+                    phis[lane + 32 * j] = phi[0][j];
+                    phis[K * K + lane + 32 * j] = phi[1][j];
+                }
+            __syncwarp();
+            const int c = lane >> 4, k1 = lane & 15;
+            if (k1 < K) {
+                const double* __restrict__ Rt = op.R + (size_t)t * K * K * K;
+                const double* ph = phis + c * K * K;
+                double sacc = 0.0;
+                for (int k3 = 0; k3 < K; ++k3)
+#pragma unroll
+                    for (int k2 = 0; k2 < K; ++k2)
+                        sacc = __dadd_rn(sacc, __dmul_rn(__ldg(Rt + k1 + K * k2 + K * K * k3), ph[k2 + K * k3]));
+                sums[(warp * 2 + c) * K + k1] = sacc;
+            }
+        }
+        __syncthreads();
+        if (q_thread) {
+            const int n = min(kFewWarps, s1 - base);
+            for (int w = 0; w < n; ++w) acc = __dadd_rn(acc, sums[(w * 2 + my_c) * K + my_k]);
+        }
+        __syncthreads();
+    }
+    if (q_thread) q[(size_t)my_c * M + (size_t)my_k * n_q + q1] = acc;
+}
+
+// The exact form in place on the caller's cell-major device arrays, two cells per CTA; grid
+// (N_Q, ceil(cells / 2)).
+template <int K>
+__global__ void __launch_bounds__(kFewWarps * 32) af_few_exact2_kernel(DevOp op, const double* __restrict__ f,
+                                                                        double* q, long long n_cells) {
+    const long long c0 = 2LL * blockIdx.y;
+    const int nc = (int)(n_cells - c0 < 2 ? n_cells - c0 : 2);
+    const size_t off = (size_t)c0 * op.n_q * K;
+    few_row_exact2<K>(op, f + off, q + off, nc);
+}
+
 // The exact form with f and Q_in in the parameter block, Q_out to q_out; grid (N_Q, n_cells).
 template <int K, int CAP>
 __global__ void __launch_bounds__(kFewWarps * 32) af_few_exact_param_kernel(DevOp op, const __grid_constant__ FewPayload<CAP> pay,

@@ -376,6 +376,24 @@ static LaunchResult launch_few_exact(const LaunchArgs& a) {
             if (need <= (size_t)kFewPayloadMax) return launch_few_exact_param<K, kFewPayloadMax>(a, grid, smem, need);
             return {-1, 0, cudaSuccess, PATH_FEW};
         }
+        if constexpr (K > 8) {
+            // the batch route above K = 8: two cells per CTA where their f fits (the same bits)
+            if (a.rows) {
+                const size_t smem2 = sizeof(double) * (2 * (size_t)a.op.n_q * K + 2 * kFewWarps * (K * K + K));
+                if (smem2 + 256 <= a.max_smem) {
+                    auto kern2 = af_few_exact2_kernel<K>;
+                    int per_sm = 0;
+                    const cudaError_t e = resident_ctas((const void*)kern2, kFewWarps * 32, smem2, &per_sm);
+                    if (e != cudaSuccess) return {5, 0, e, PATH_FEW};
+                    if (per_sm >= 1) {
+                        const dim3 grid2((unsigned)a.op.n_q, (unsigned)((a.n_cells + 1) / 2));
+                        kern2<<<grid2, kFewWarps * 32, smem2, a.stream>>>(a.op, a.f_cm, a.q_cm, (long long)a.n_cells);
+                        const cudaError_t e2 = cudaGetLastError();
+                        return {e2 == cudaSuccess ? 0 : 5, 1, e2, PATH_FEW};
+                    }
+                }
+            }
+        }
         auto kern = af_few_exact_kernel<K>;
         if (smem > 48 * 1024) {
             int per_sm = 0;

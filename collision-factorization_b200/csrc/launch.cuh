@@ -61,7 +61,7 @@ struct LaunchArgs {
     const double* few_host_q = nullptr;
     // FP32 J.v: tiled FP32 copy of v
     const float* vT32 = nullptr;
-    // with few: the exact form of any number of cells on the row kernel (one CTA per (q1, cell), on the
+    // with few: the exact form of any number of cells on the row kernel (one CTA per (q1, pair of cells), on the
     // cell-major arrays), the exact route where the batch kernels' register tiles do not fit (K > 8)
     bool rows = false;
 };

@@ -628,7 +628,7 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
         if (r != kNoFew) return r;
     }
     // The exact angular-first form above K = 8, where the batch kernels' per-lane K x K Phi does not
-    // fit in registers: the row kernel of the few-cell route (one CTA per (q1, cell), the reference's
+    // fit in registers: the row kernel of the few-cell route (one CTA per (q1, pair of cells), the reference's
     // operation order) on the cell-major arrays, for any number of cells.
     if (exact && what == 0 && f32 == 0 && !sym && p->k > 8) {
         if (B > 65535)

@@ -238,7 +238,7 @@ def test_lblock_through_the_allocation_free_entry_point(cuda_available):
 
 @pytest.mark.parametrize("L,K,B", [(6, 12, 21), (3, 16, 10), (5, 12, 3)])
 def test_exact_form_above_k8_bitwise(L, K, B, cuda_available, oracle_lib):
-    """The exact angular-first form above K = 8 (one CTA per (q1, cell), the reference's operation
+    """The exact angular-first form above K = 8 (one CTA per (q1, pair of cells), the reference's operation
     order) gives the oracle's bits, which are the compiled reference kernel's: batches of any size and
     a handful of cells, from Q = 0 and from a nonzero Q."""
     import cf_b200
