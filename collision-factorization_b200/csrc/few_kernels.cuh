@@ -253,17 +253,23 @@ __global__ void __launch_bounds__(kFewWarps * 32) af_few_exact_kernel(DevOp op, 
 // The exact form of one (q1 row, pair of cells) in place, for the batch route above K = 8: each cell's
 // operations are those of few_row_exact, in the same order, so the bits are the same; the pair shares
 // the entry shuffles and the R_t loads, and lanes c 16 + k1 (k1 < K) run the K^3 sums of cell c, where
-// one cell leaves 20 of 32 lanes idle.  nc (1 or 2) cells from f and q; shared memory: f of both cells
-// (zero for a missing second cell), each warp's two Phi, each warp's two row sums.
-template <int K>
-__device__ __forceinline__ void few_row_exact2(const DevOp& op, const double* __restrict__ f, double* q, int nc) {
+// one cell leaves 20 of 32 lanes idle.  JV: the exact J(f) v instead, Phi summing
+// G ((v[q2,k2] f[q3,k3]) + (f[q2,k2] v[q3,k3])) with each product and sum rounded separately (the
+// order of the exact J.v of the batch kernels).  nc (1 or 2) cells from f (and v) and q; shared
+// memory: f (and v) of both cells (zero for a missing second cell), each warp's two Phi, each warp's
+// two row sums.
+template <int K, bool JV>
+__device__ __forceinline__ void few_row_exact2(const DevOp& op, const double* __restrict__ f,
+                                               const double* __restrict__ v, double* q, int nc) {
     static_assert(K <= 16, "a cell's K^3 sums take lanes c 16 .. c 16 + K - 1");
     constexpr int NP = few_pairs_per_lane<K>();
+    constexpr int NA = JV ? 2 : 1;  // staged arrays per cell: f (and v)
     extern __shared__ double fs[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n_q = op.n_q, M = n_q * K;
-    double* phis = fs + 2 * M + warp * 2 * K * K;   // [2][K K]
-    double* sums = fs + 2 * M + kFewWarps * 2 * K * K;  // [kFewWarps][2][K]
+    const double* vs = fs + 2 * M;                      // JV: v of both cells
+    double* phis = fs + NA * 2 * M + warp * 2 * K * K;  // [2][K K]
+    double* sums = fs + NA * 2 * M + kFewWarps * 2 * K * K;  // [kFewWarps][2][K]
     const int q1 = blockIdx.x;
     const int s0 = op.q1_begin[q1], s1 = op.q1_begin[q1 + 1];
     if (s0 == s1) return;  // in place: the row has no slices
@@ -273,6 +279,8 @@ __device__ __forceinline__ void few_row_exact2(const DevOp& op, const double* __
     double acc = 0.0;
     if (q_thread) acc = q[(size_t)my_c * M + (size_t)my_k * n_q + q1];
     for (int i = threadIdx.x; i < 2 * M; i += blockDim.x) fs[i] = i < nc * M ? f[i] : 0.0;
+    if constexpr (JV)
+        for (int i = threadIdx.x; i < 2 * M; i += blockDim.x) fs[2 * M + i] = i < nc * M ? v[i] : 0.0;
     __syncthreads();
     for (int base = s0; base < s1; base += kFewWarps) {
         const int s = base + warp;
@@ -295,13 +303,22 @@ __device__ __forceinline__ void few_row_exact2(const DevOp& op, const double* __
                     const double g = __shfl_sync(0xffffffffu, my_g, z);
                     const double* f2 = fs + (q23 & 0xffffu);
                     const double* f3 = fs + (q23 >> 16);
+                    const double* v2 = vs + (q23 & 0xffffu);
+                    const double* v3 = vs + (q23 >> 16);
 #pragma unroll
                     for (int j = 0; j < NP; ++j) {
                         const int p = lane + 32 * j;
                         if (p < K * K) {
                             const int i2 = (p % K) * n_q, i3 = (p / K) * n_q;
-                            phi[0][j] = __dadd_rn(phi[0][j], __dmul_rn(__dmul_rn(g, f2[i2]), f3[i3]));
-                            phi[1][j] = __dadd_rn(phi[1][j], __dmul_rn(__dmul_rn(g, f2[M + i2]), f3[M + i3]));
+#pragma unroll
+                            for (int c = 0; c < 2; ++c) {
+                                const int o2 = c * M + i2, o3 = c * M + i3;
+                                if constexpr (JV)
+                                    phi[c][j] = __dadd_rn(
+                                        phi[c][j], __dmul_rn(g, __dadd_rn(__dmul_rn(v2[o2], f3[o3]), __dmul_rn(f2[o2], v3[o3]))));
+                                else
+                                    phi[c][j] = __dadd_rn(phi[c][j], __dmul_rn(__dmul_rn(g, f2[o2]), f3[o3]));
+                            }
                         }
                     }
                 }
@@ -335,15 +352,16 @@ __device__ __forceinline__ void few_row_exact2(const DevOp& op, const double* __
     if (q_thread) q[(size_t)my_c * M + (size_t)my_k * n_q + q1] = acc;
 }
 
-// The exact form in place on the caller's cell-major device arrays, two cells per CTA; grid
-// (N_Q, ceil(cells / 2)).
-template <int K>
+// The exact form (JV: the exact J(f) v, v non-null) in place on the caller's cell-major device arrays,
+// two cells per CTA; grid (N_Q, ceil(cells / 2)).
+template <int K, bool JV>
 __global__ void __launch_bounds__(kFewWarps * 32) af_few_exact2_kernel(DevOp op, const double* __restrict__ f,
-                                                                        double* q, long long n_cells) {
+                                                                        const double* __restrict__ v, double* q,
+                                                                        long long n_cells) {
     const long long c0 = 2LL * blockIdx.y;
     const int nc = (int)(n_cells - c0 < 2 ? n_cells - c0 : 2);
     const size_t off = (size_t)c0 * op.n_q * K;
-    few_row_exact2<K>(op, f + off, q + off, nc);
+    few_row_exact2<K, JV>(op, f + off, JV ? v + off : nullptr, q + off, nc);
 }
 
 // The exact form with f and Q_in in the parameter block, Q_out to q_out; grid (N_Q, n_cells).

@@ -364,6 +364,10 @@ static LaunchResult launch_few_exact(const LaunchArgs& a) {
     {
         if ((a.n_cells > kFewCells && !a.rows) || a.q_cm == nullptr || (a.f_cm == nullptr && a.few_host_f == nullptr))
             return {-1, 0, cudaSuccess, PATH_FEW};
+        // the exact J.v has this route only above K = 8, on the two-cell kernel (the batch kernels take
+        // it up to K = 8)
+        const bool jv = a.what == OP_JV;
+        if (jv && (K <= 8 || !a.rows || a.v_cm == nullptr || a.f_cm == nullptr)) return {-1, 0, cudaSuccess, PATH_FEW};
         if (a.n_cells > 65535) return {2, 0, cudaSuccess, PATH_FEW};
         if (a.op.n_items == 0 || a.n_cells == 0) return {0, 0, cudaSuccess, PATH_FEW};
         const size_t smem = sizeof(double) * ((size_t)a.op.n_q * K + kFewWarps * (K * K + K));
@@ -377,21 +381,25 @@ static LaunchResult launch_few_exact(const LaunchArgs& a) {
             return {-1, 0, cudaSuccess, PATH_FEW};
         }
         if constexpr (K > 8) {
-            // the batch route above K = 8: two cells per CTA where their f fits (the same bits)
+            // the batch route above K = 8: two cells per CTA where their f (and v) fit (the same bits)
             if (a.rows) {
-                const size_t smem2 = sizeof(double) * (2 * (size_t)a.op.n_q * K + 2 * kFewWarps * (K * K + K));
+                const size_t arrays = jv ? 4 : 2;
+                const size_t smem2 =
+                    sizeof(double) * (arrays * (size_t)a.op.n_q * K + 2 * kFewWarps * (K * K + K));
                 if (smem2 + 256 <= a.max_smem) {
-                    auto kern2 = af_few_exact2_kernel<K>;
+                    auto kern2 = jv ? af_few_exact2_kernel<K, true> : af_few_exact2_kernel<K, false>;
                     int per_sm = 0;
                     const cudaError_t e = resident_ctas((const void*)kern2, kFewWarps * 32, smem2, &per_sm);
                     if (e != cudaSuccess) return {5, 0, e, PATH_FEW};
                     if (per_sm >= 1) {
                         const dim3 grid2((unsigned)a.op.n_q, (unsigned)((a.n_cells + 1) / 2));
-                        kern2<<<grid2, kFewWarps * 32, smem2, a.stream>>>(a.op, a.f_cm, a.q_cm, (long long)a.n_cells);
+                        kern2<<<grid2, kFewWarps * 32, smem2, a.stream>>>(a.op, a.f_cm, jv ? a.v_cm : nullptr, a.q_cm,
+                                                                           (long long)a.n_cells);
                         const cudaError_t e2 = cudaGetLastError();
                         return {e2 == cudaSuccess ? 0 : 5, 1, e2, PATH_FEW};
                     }
                 }
+                if (jv) return {8, 0, cudaSuccess, PATH_FEW};  // f and v of two cells do not fit
             }
         }
         auto kern = af_few_exact_kernel<K>;
@@ -413,8 +421,9 @@ constexpr int tile_W(int K, bool jv) { return jv ? (K >= 8 ? 12 : 16) : 16; }
 template <int K>
 static LaunchResult launch_for_k(const LaunchArgs& a) {
     if (a.few) {
-        if (a.f32 || a.bf16 || a.what == OP_JV) return {-1, 0, cudaSuccess, PATH_FEW};
-        if (a.exact) return a.what == OP_AF ? launch_few_exact<K>(a) : LaunchResult{-1, 0, cudaSuccess, PATH_FEW};
+        if (a.f32 || a.bf16 || (a.what == OP_JV && !(a.exact && a.rows))) return {-1, 0, cudaSuccess, PATH_FEW};
+        if (a.exact)
+            return a.what == OP_AF || a.what == OP_JV ? launch_few_exact<K>(a) : LaunchResult{-1, 0, cudaSuccess, PATH_FEW};
         return a.what == OP_RF ? launch_few<K, true>(a) : launch_few<K, false>(a);
     }
     if (a.ss) {

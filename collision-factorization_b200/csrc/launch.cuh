@@ -53,6 +53,7 @@ struct LaunchArgs {
     const StreamSync* ss = nullptr;
     const double* f_cm = nullptr;
     double* q_cm = nullptr;
+    const double* v_cm = nullptr;  // the exact J.v above K = 8 (rows): v, cell-major like f_cm
     // a handful of cells: the few-cell kernel on cell-major f_cm and q_cm (status -1 where it does not apply);
     // with few_host_f / few_host_q set, f and Q_in are those host arrays, passed in the launch's
     // parameter block, and q_cm receives Q_out

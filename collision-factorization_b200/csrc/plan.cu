@@ -502,7 +502,7 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
              cudaStream_t st, const float* fT32 = nullptr, bool bf16 = false, const StreamSync* ss = nullptr,
              const double* f_cm = nullptr, double* q_cm = nullptr, bool few = false,
              const double* few_host_f = nullptr, const double* few_host_q = nullptr, const float* vT32 = nullptr,
-             bool rows = false) {
+             bool rows = false, const double* v_cm = nullptr) {
     const int64_t nt = n_tiles_for(B);
     // The folded operator has about half the COO entries per slice of the plain one, and its tile
     // routine groups them by q2, so its Phi step is light next to the K^3 step; there the tile kernel
@@ -520,6 +520,7 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
     a.few_host_q = few_host_q;
     a.vT32 = vT32;
     a.rows = rows;
+    a.v_cm = v_cm;
     cf::LaunchResult r{8, 0, cudaSuccess};
     switch (p->k) {
 #define CF_K(KK) \
@@ -538,7 +539,7 @@ int dispatch(const cf_plan* p, int what, bool exact, const double* fT, const dou
     }
     if (r.status == CF_ECUDA) return fail(CF_ECUDA, "kernel launch: %s", cudaGetErrorString(r.cuda));
     if (r.status == CF_EUNSUPPORTED)
-        return fail(CF_EUNSUPPORTED, "form or kernel path not built for K = %d (the exact J.v needs K <= 8; "
+        return fail(CF_EUNSUPPORTED, "form or kernel path not built for K = %d ("
                     "the tile-resident kernels need an even K <= 8 and a tile that fits in shared memory)", p->k);
     if (r.status != CF_OK) return fail(r.status, "launch failed for K = %d", p->k);
     return CF_OK;
@@ -627,15 +628,15 @@ int run_device(cf_plan* p, int what, bool exact, double* q_dev, const double* f_
         const int r = run_few(p, what, exact, q_dev, f_dev, B, st, sym, f32);
         if (r != kNoFew) return r;
     }
-    // The exact angular-first form above K = 8, where the batch kernels' per-lane K x K Phi does not
-    // fit in registers: the row kernel of the few-cell route (one CTA per (q1, pair of cells), the reference's
-    // operation order) on the cell-major arrays, for any number of cells.
-    if (exact && what == 0 && f32 == 0 && !sym && p->k > 8) {
+    // The exact angular-first form and the exact J.v above K = 8, where the batch kernels' per-lane
+    // K x K Phi does not fit in registers: the row kernel of the few-cell route (one CTA per (q1, pair of
+    // cells), the reference's operation order) on the cell-major arrays, for any number of cells.
+    if (exact && (what == 0 || what == 2) && f32 == 0 && !sym && p->k > 8) {
         if (B > 65535)
-            return fail(CF_ESHAPE, "the exact form above K = 8 takes at most 65535 cells per call (B = %lld)",
+            return fail(CF_ESHAPE, "the exact forms above K = 8 take at most 65535 cells per call (B = %lld)",
                         (long long)B);
-        const int r = dispatch(p, 0, true, nullptr, nullptr, nullptr, B, st, nullptr, false, nullptr, f_dev, q_dev, true,
-                               nullptr, nullptr, nullptr, true);
+        const int r = dispatch(p, what, true, nullptr, nullptr, nullptr, B, st, nullptr, false, nullptr, f_dev, q_dev,
+                               true, nullptr, nullptr, nullptr, true, what == 2 ? v_dev : nullptr);
         if (r != kNoFew) return r;
     }
     const size_t tb = tiled_bytes(p, B);
