@@ -170,7 +170,8 @@ int cf_q_device_ws(cf_plan* plan, double* q_dev, const double* f_dev, int64_t b,
                    void* workspace, size_t workspace_bytes, void* stream);
 
 /* out_dev += J(f_dev).v_dev for B cells.  `exact` selects the mode of every J.v call:
- * 0 = fast, 1 = exact operation order, 2 = the q2 <-> q3 folded operator (as CF_FORM_AF_SYM),
+ * 0 = fast, 1 = exact operation order (every K; above K = 8 on the row kernel, at most 65535 cells
+ * per call), 2 = the q2 <-> q3 folded operator (as CF_FORM_AF_SYM),
  * 3 = FP32 (f, v, R, Phi and the row sums in FP32, added into the FP64 out, as CF_FORM_AF_F32; even
  * K <= 12), 4 = FP32 on the folded operator.  cf_jv_tiled takes modes 0-2 (its tiles are FP64). */
 int cf_jv_device(cf_plan* plan, double* out_dev, const double* f_dev, const double* v_dev,
@@ -179,7 +180,9 @@ int cf_jv_device(cf_plan* plan, double* out_dev, const double* f_dev, const doub
 /* Tiled cell layout: [ceil(B/32)][N_Q][K][32] (32 cells per tile, cell index fastest).  Callers
  * that keep their cells resident (time steppers, Krylov solvers) use it directly and skip the
  * two layout passes.  cf_pack_cells / cf_unpack_cells convert from / to [N_Q x K x B]; pack fills
- * the padding cells of the last tile with zeros, unpack overwrites the B cells of dst. */
+ * the padding cells of the last tile with zeros, unpack overwrites the B cells of dst.  The exact
+ * forms above K = 8 (Q and J.v) run on cell-major arrays only: the tiled entries refuse them with
+ * CF_EUNSUPPORTED. */
 int cf_pack_cells(const cf_plan* plan, double* dst_tiled, const double* src_cells, int64_t b, void* stream);
 int cf_unpack_cells(const cf_plan* plan, double* dst_cells, const double* src_tiled, int64_t b, void* stream);
 int cf_q_tiled(cf_plan* plan, double* q_tiled, const double* f_tiled, int64_t b, int32_t form, void* stream);
