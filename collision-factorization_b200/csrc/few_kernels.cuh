@@ -303,21 +303,30 @@ __device__ __forceinline__ void few_row_exact2(const DevOp& op, const double* __
                     const double g = __shfl_sync(0xffffffffu, my_g, z);
                     const double* f2 = fs + (q23 & 0xffffu);
                     const double* f3 = fs + (q23 >> 16);
-                    const double* v2 = vs + (q23 & 0xffffu);
-                    const double* v3 = vs + (q23 >> 16);
+                    if constexpr (JV) {
+                        const double* v2 = vs + (q23 & 0xffffu);
+                        const double* v3 = vs + (q23 >> 16);
 #pragma unroll
-                    for (int j = 0; j < NP; ++j) {
-                        const int p = lane + 32 * j;
-                        if (p < K * K) {
-                            const int i2 = (p % K) * n_q, i3 = (p / K) * n_q;
+                        for (int j = 0; j < NP; ++j) {
+                            const int p = lane + 32 * j;
+                            if (p < K * K) {
+                                const int i2 = (p % K) * n_q, i3 = (p / K) * n_q;
 #pragma unroll
-                            for (int c = 0; c < 2; ++c) {
-                                const int o2 = c * M + i2, o3 = c * M + i3;
-                                if constexpr (JV)
-                                    phi[c][j] = __dadd_rn(
-                                        phi[c][j], __dmul_rn(g, __dadd_rn(__dmul_rn(v2[o2], f3[o3]), __dmul_rn(f2[o2], v3[o3]))));
-                                else
-                                    phi[c][j] = __dadd_rn(phi[c][j], __dmul_rn(__dmul_rn(g, f2[o2]), f3[o3]));
+                                for (int c = 0; c < 2; ++c) {
+                                    const int o2 = c * M + i2, o3 = c * M + i3;
+                                    phi[c][j] = __dadd_rn(phi[c][j], __dmul_rn(g, __dadd_rn(__dmul_rn(v2[o2], f3[o3]),
+                                                                                            __dmul_rn(f2[o2], v3[o3]))));
+                                }
+                            }
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < NP; ++j) {
+                            const int p = lane + 32 * j;
+                            if (p < K * K) {
+                                const int i2 = (p % K) * n_q, i3 = (p / K) * n_q;
+                                phi[0][j] = __dadd_rn(phi[0][j], __dmul_rn(__dmul_rn(g, f2[i2]), f3[i3]));
+                                phi[1][j] = __dadd_rn(phi[1][j], __dmul_rn(__dmul_rn(g, f2[M + i2]), f3[M + i3]));
                             }
                         }
                     }
@@ -353,9 +362,13 @@ __device__ __forceinline__ void few_row_exact2(const DevOp& op, const double* __
 }
 
 // The exact form (JV: the exact J(f) v, v non-null) in place on the caller's cell-major device arrays,
-// two cells per CTA; grid (N_Q, ceil(cells / 2)).
+// two cells per CTA; grid (N_Q, ceil(cells / 2)).  The Q form's shared memory leaves room for two
+// CTAs per SM at L = 16, K = 12 (95 KB each), so up to K = 13 its registers are held to what two CTAs
+// of 16 warps allow (64 a thread; with 76 only one CTA fitted and the launch took 95.7 ms instead of
+// 70.0).  Above K = 13 (Phi and f of two cells take about twice the memory) and for the J.v form
+// (f and v: 151 KB at L = 16, K = 12) one CTA per SM is what shared memory leaves anyway.
 template <int K, bool JV>
-__global__ void __launch_bounds__(kFewWarps * 32) af_few_exact2_kernel(DevOp op, const double* __restrict__ f,
+__global__ void __launch_bounds__(kFewWarps * 32, (JV || K > 13) ? 1 : 2) af_few_exact2_kernel(DevOp op, const double* __restrict__ f,
                                                                         const double* __restrict__ v, double* q,
                                                                         long long n_cells) {
     const long long c0 = 2LL * blockIdx.y;
