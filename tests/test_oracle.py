@@ -170,3 +170,25 @@ def test_fold_refuses_a_list_missing_a_kept_entry():
                               ic_map=geo.ic_map[keep].copy())
     with pytest.raises(ValueError):
         geometry.fold_q2q3(cut, R, K)
+
+
+@pytest.mark.parametrize("K", list(range(1, 17)))
+def test_restatement_bitwise_at_every_k(K, oracle_lib, reference_lib):
+    """The oracle against the reference's compiled angular-first and radial-first kernels at every K
+    the library builds, on the operators the GPU sweep uses (L = 3 + K mod 3, synthetic R), from a
+    nonzero Q: the GPU's exact forms are checked against this oracle at the same K."""
+    from cf_b200 import geometry, workloads
+    from oracle import rtensor
+
+    L = 3 + K % 3
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=100 + K)
+    f = np.asfortranarray(workloads.maxwellian_cells(K, L, 5, seed=K, amplitude=0.05).transpose(2, 1, 0))
+    q0 = np.asfortranarray(np.random.default_rng(K).standard_normal(f.shape))
+    args = (geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+    for kern in ("af", "rf"):
+        Qo = q0.copy(order="F")
+        oracle_lib.af_batch(Qo, f, *args, nthreads=2, form=kern)
+        Qr = q0.copy(order="F")
+        reference_lib.batch(kern, Qr, f, *args, nthreads=2)
+        assert np.array_equal(Qo, Qr), f"{kern} K={K}: max diff {np.abs(Qo - Qr).max():.3e}"
