@@ -192,3 +192,32 @@ def test_restatement_bitwise_at_every_k(K, oracle_lib, reference_lib):
         Qr = q0.copy(order="F")
         reference_lib.batch(kern, Qr, f, *args, nthreads=2)
         assert np.array_equal(Qo, Qr), f"{kern} K={K}: max diff {np.abs(Qo - Qr).max():.3e}"
+
+
+@pytest.mark.parametrize("K", list(range(1, 17)))
+def test_jacobian_oracle_at_every_k(K, oracle_lib):
+    """The oracle's J(f).v at every K on the GPU sweep's operators: J(f).f = 2 Q(f) against the
+    angular-first oracle (itself pinned to the compiled reference), and the central difference of the
+    quadratic Q, (Q(f + h v) - Q(f - h v)) / 2h = J(f).v up to rounding."""
+    from cf_b200 import geometry, workloads
+    from oracle import rtensor
+
+    L = 3 + K % 3
+    geo = geometry.sort_for_contraction(geometry.generate_geometry(L))
+    R = workloads.synthetic_R(rtensor.l_triplets_of(geo), K, seed=100 + K)
+    f = np.asfortranarray(workloads.maxwellian_cells(K, L, 1, seed=K, amplitude=0.05)[0].T)
+    v = np.asfortranarray(np.random.default_rng(K).standard_normal(f.shape))
+    args = (geo.labels, geo.vals, geo.ic_map, R, geo.n_q, K)
+    q = np.zeros_like(f, order="F")
+    oracle_lib.af(q, f, *args)
+    jf = np.zeros_like(f, order="F")
+    oracle_lib.jv(jf, f, f, *args)
+    assert normwise_err(jf, 2.0 * q) < 1e-13
+    jv = np.zeros_like(f, order="F")
+    oracle_lib.jv(jv, f, v, *args)
+    h = 1e-3
+    qp = np.zeros_like(f, order="F")
+    oracle_lib.af(qp, np.asfortranarray(f + h * v), *args)
+    qm = np.zeros_like(f, order="F")
+    oracle_lib.af(qm, np.asfortranarray(f - h * v), *args)
+    assert normwise_err((qp - qm) / (2 * h), jv) < 1e-9
