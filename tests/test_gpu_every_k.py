@@ -45,7 +45,7 @@ def test_q_forms_at_every_k(K, cuda_available, oracle_lib):
     import cf_b200
     from cf_b200 import CFError
 
-    geo, R, f, q0, args = _case(K)
+    _, _, f, q0, args = _case(K)
     ref = {}
     for kind in ("af", "rf"):
         r = q0.copy(order="F")
@@ -80,7 +80,7 @@ def test_q_forms_at_every_k(K, cuda_available, oracle_lib):
 def test_jacobian_apply_at_every_k(K, cuda_available, oracle_lib):
     import cf_b200
 
-    geo, R, f, q0, args = _case(K)
+    _, _, f, q0, args = _case(K)
     v = np.asfortranarray(np.random.default_rng(50 + K).standard_normal(f.shape))
     ref = q0.copy(order="F")
     oracle_lib.jv_batch(ref, f, v, *args)
